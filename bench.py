@@ -1,0 +1,375 @@
+#!/usr/bin/env python
+"""Benchmark of the TDD hot path on B200: DM-trials x samples per second.
+
+Workload (one step = one dedispersion of the whole series): nchan 4096,
+f_top 1500 MHz, channel width -0.078125 MHz, dt 64 us, 2^21 samples of 8-bit
+input, DM list generate_dm_list(0, 2000, 40 us, 1.25) = 3643 DMs, max delay
+35500, float32 output (3643 x 2061652 samples, 30 GB). Seeded synthetic input
+(noise + 8 dispersed pulses) generated on the device; it is larger than L2,
+so no flush is needed between steps.
+
+  value  device-resident input and output (DEDISP_DEVICE_POINTERS), timed
+         with CUDA events on the plan's stream: K1 transpose + K2 kernels.
+  e2e    the C-ABI call dedisp_execute with pinned HOST buffers (H2D of the
+         input and D2H of the 30 GB output inside the timed region).
+
+N > 1 GPUs (torchrun): each rank runs its own replica of the workload (no
+collective on the data path); value = all ranks' units / max-over-ranks time.
+
+--impl reference times the reference's CPU implementation of this path (the
+CPU oracle port: brute-force integer TDD, all host threads) on bounded samples
+of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DM-trials x samples/s (TDD, 1 B200)"
+UNIT = "DM-trials*samples/s"
+
+
+def workload_name(nbits):
+    return f"tdd 4096ch 2^21 samples {nbits}-bit, 3643 DMs (0-2000, 40us, tol 1.25), f32 out"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nbits", type=int, default=8, choices=[2, 4, 8])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (oracle port)
+# ---------------------------------------------------------------------------
+
+def cpu_sample(cfg, dms_all, md, n_dm=16, n_t=65536, seed=99):
+    """A bounded sample of the workload: n_dm DMs spread over the list and
+    n_t output samples (input rows n_t + max_delay, numpy generated)."""
+    from dedisp_tests_b200 import synthetic as sy
+    sub = sy.Config(cfg.name, cfg.nchans, cfg.f_top, cfg.df, cfg.dt, n_t + md, cfg.nbits,
+                    cfg.mean, cfg.sigma, [], seed=seed)
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((sub.nsamps, sub.nchans), dtype=np.float32) * sub.sigma + sub.mean
+    packed = sy.pack(sy.quantise(x, cfg.nbits), cfg.nbits)
+    pick = np.linspace(0, len(dms_all) - 1, n_dm).astype(int)
+    return packed, dms_all[pick], n_t
+
+
+def time_cpu_oracle(cfg, dms_all, md, steps=1, warmup=0, n_dm=16, n_t=65536):
+    from oracle import pyoracle as po
+    packed, dms, n_t = cpu_sample(cfg, dms_all, md, n_dm, n_t)
+    delays = po.delay_table(cfg.nchans, np.float32(cfg.dt), np.float32(cfg.f_top),
+                            np.float32(cfg.df))
+    km = np.ones(cfg.nchans, np.int32)
+    cores = os.cpu_count() or 1
+    times = []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        po.tdd(packed, packed.shape[0], packed.shape[1], cfg.nbits, cfg.nchans, delays, km, dms,
+               32, n_t, nthreads=cores)
+        if i >= warmup:
+            times.append(time.perf_counter() - t0)
+    t = sum(times) / len(times)
+    return {"value": len(dms) * n_t / t, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{len(dms)} DMs spread over the 3643-DM list x {n_t} output samples "
+                      f"x 4096 channels ({cfg.nbits}-bit), oracle brute force, "
+                      f"{len(times)} timed runs of {t:.2f} s"}, t
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            self.p.wait()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        try:
+            for line in open(self.f.name):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        finally:
+            os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# our implementation
+# ---------------------------------------------------------------------------
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import dedisp_tests_b200 as dd
+    from dedisp_tests_b200 import synthetic as sy
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    cfg = sy.config1(nbits=args.nbits)
+    stream = torch.cuda.current_stream()
+
+    def make_plan(kernel=0):
+        p = dd.TDDPlan(cfg.nchans, cfg.dt, cfg.f_top, cfg.df, local)
+        p.generate_dm_list(*cfg.dm_gen)
+        p.set_stream(stream.cuda_stream)
+        if kernel:
+            p.set_kernel(kernel)
+        return p
+
+    plan = make_plan()
+    ndm, md = plan.get_dm_count(), plan.get_max_delay()
+    nout = cfg.nsamps - md
+    units = ndm * nout
+    d_in = sy.make_input_torch(cfg, device=f"cuda:{local}")
+    d_out = torch.empty((ndm, nout), dtype=torch.float32, device=f"cuda:{local}")
+    flags = dd.DEDISP_DEVICE_POINTERS
+
+    def step(p, nbits=args.nbits, inp=d_in):
+        p.execute(cfg.nsamps, inp, nbits, d_out, 32, flags)
+
+    # --- value: device-resident ---------------------------------------------
+    plan.set_timing(True)
+    for _ in range(args.warmup):
+        step(plan)
+    torch.cuda.synchronize()
+    barrier()
+    kms, pms, launches = [], [], 0
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step(plan)
+            t = plan.get_timing()
+            kms.append(t["kernel_ms"])
+            pms.append(t["prep_ms"])
+            launches += t["launches"] + 1  # + one K1 transpose launch
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    clocks = clk.summary()
+    ms = max_over_ranks(e0.elapsed_time(e1)) / args.steps
+    value = units * world / (ms * 1e-3)
+
+    # --- roofline of the dominant kernel (K2) --------------------------------
+    import ctypes as C
+    peak = C.c_double()
+    dd.lib().dedisp_b200_alu_probe(local, C.byref(peak))
+    k2_ms = sum(kms) / len(kms)
+    adds = float(units) * cfg.nchans
+    achieved = adds / (k2_ms * 1e-3) / 1e12
+    roofline = {"bound": "int-alu", "achieved": round(achieved, 3), "peak": round(peak.value / 1e12, 3),
+                "unit": "Tadd/s", "frac": round(achieved * 1e12 / peak.value, 4),
+                "traffic": None,
+                "peak_source": "measured in this run: dedisp_b200_alu_probe (32-bit add "
+                               "lane-ops/s, all SMs)",
+                "k2_ms": round(k2_ms, 3), "k1_ms": round(sum(pms) / len(pms), 3),
+                "algorithmic": "nchan=4096 integer adds per DM-trial x sample; "
+                               f"{adds:.3e} adds per step",
+                "hbm_view": {"algorithmic_bytes": int(cfg.nsamps * 4096 * args.nbits // 8 +
+                                                      units * 4),
+                             "achieved_GBs": round((cfg.nsamps * 4096 * args.nbits // 8 +
+                                                    units * 4) / (k2_ms * 1e-3) / 1e9, 1)}}
+
+    # --- variants: plain form, other input widths -----------------------------
+    variants = {}
+    if not args.no_variants:
+        plain = make_plan(kernel=1)
+        plain.set_timing(True)
+        step(plain)
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        step(plain)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        pm = max_over_ranks(ev0.elapsed_time(ev1))
+        variants["plain_8bit"] = {"value": units * world / (pm * 1e-3), "ms_per_step": pm,
+                                  "kernel_ms": plain.get_timing()["kernel_ms"]}
+        del plain
+        for nb in (2, 4, 8):
+            if nb == args.nbits:
+                continue
+            c2 = sy.config1(nbits=nb)
+            inp = sy.make_input_torch(c2, device=f"cuda:{local}")
+            p2 = make_plan()
+            p2.set_timing(True)
+            step(p2, nb, inp)
+            torch.cuda.synchronize()
+            ev0.record(stream)
+            for _ in range(2):
+                step(p2, nb, inp)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            vm = max_over_ranks(ev0.elapsed_time(ev1)) / 2
+            t = p2.get_timing()
+            variants[f"tiled_{nb}bit"] = {"value": units * world / (vm * 1e-3),
+                                          "ms_per_step": vm, "kernel_ms": t["kernel_ms"],
+                                          "frac_int_alu": round(adds / (t["kernel_ms"] * 1e-3)
+                                                                / peak.value, 4)}
+            del inp, p2
+        variants[f"tiled_{args.nbits}bit"] = {"value": value, "ms_per_step": ms,
+                                              "kernel_ms": k2_ms}
+        torch.cuda.empty_cache()
+
+    # --- e2e: host buffers through the C ABI ----------------------------------
+    e2e = None
+    if not args.no_e2e:
+        try:
+            import psutil
+            need = d_in.numel() + ndm * nout * 4
+            avail = psutil.virtual_memory().available
+            if avail < need * 1.25:
+                e2e = {"value": None, "unit": UNIT, "skipped": f"host RAM {avail/1e9:.0f} GB < "
+                                                               f"{need*1.25/1e9:.0f} GB needed"}
+            else:
+                h_in = torch.empty(d_in.shape, dtype=torch.uint8, pin_memory=True)
+                h_in.copy_(d_in)
+                h_out = torch.empty((ndm, nout), dtype=torch.float32, pin_memory=True)
+                del d_out
+                torch.cuda.empty_cache()
+                hp = dd.TDDPlan(cfg.nchans, cfg.dt, cfg.f_top, cfg.df, local)
+                hp.generate_dm_list(*cfg.dm_gen)
+                hp.execute(cfg.nsamps, h_in, args.nbits, h_out, 32)  # warm-up
+                torch.cuda.synchronize()
+                barrier()
+                ksteps = max(1, min(args.steps, 2))
+                t0 = time.perf_counter()
+                for _ in range(ksteps):
+                    hp.execute(cfg.nsamps, h_in, args.nbits, h_out, 32)
+                torch.cuda.synchronize()
+                dt_e2e = max_over_ranks(time.perf_counter() - t0) / ksteps
+                e2e = {"value": units * world / dt_e2e, "unit": UNIT,
+                       "h2d_bytes_per_step": int(h_in.numel()),
+                       "d2h_bytes_per_step": int(ndm * nout * 4), "ms_per_step": dt_e2e * 1e3,
+                       "steps": ksteps}
+                del h_in, h_out, hp
+        except Exception as ex:  # report, do not hide
+            e2e = {"value": None, "unit": UNIT, "error": repr(ex)}
+
+    # --- CPU baseline (rank 0 at N=1) -------------------------------------------
+    cpu = None
+    if not args.no_cpu and world == 1:
+        cpu, _ = time_cpu_oracle(cfg, plan.get_dm_list(), md)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": f"u{args.nbits}->u32 sums->f32", "data": "synthetic (seeded, on device)",
+            "config": {"workload": workload_name(args.nbits), "nchans": 4096,
+                       "nsamps": cfg.nsamps, "ndm": ndm, "max_delay": md,
+                       "in_nbits": args.nbits, "out_nbits": 32,
+                       "l2": "inputs (8.6 GB) larger than L2; no flush",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches * world, "clocks": clocks, "variants": variants,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    """The reference's CPU implementation of the path: the oracle port (the
+    reference's own CPU code for this path needs FFTW, absent here)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from dedisp_tests_b200 import synthetic as sy
+    from oracle import pyoracle as po
+    cfg = sy.config1(nbits=args.nbits)
+    dms = po.generate_dm_list(cfg.nchans, cfg.dt, cfg.f_top, cfg.df, *cfg.dm_gen)
+    delays = po.delay_table(cfg.nchans, np.float32(cfg.dt), np.float32(cfg.f_top),
+                            np.float32(cfg.df))
+    md = po.max_delay(dms, delays)
+    cpu, t = time_cpu_oracle(cfg, dms, md, steps=args.steps, warmup=min(args.warmup, 1))
+    line = {"metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": f"u{args.nbits}->u32 sums->f32", "data": "synthetic (seeded)",
+            "config": {"workload": workload_name(args.nbits), "sample": cpu["sample"]},
+            "impl": "reference", "cpu_baseline": cpu,
+            "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)

@@ -1,0 +1,284 @@
+"""B200-native dedispersion engine: Python mirror of the dedisp C interface.
+
+The product is the C-ABI shared library ``lib/libdedisp.so`` (CUDA kernels for
+sm_100a plus C++ plan classes; declarations in ``include/dedisp.h`` and
+``include/dedisp_b200.h``). This module binds it with ctypes and mirrors the
+reference's C++ plan classes (``DedispPlan``, ``TDDPlan``, ``FDDGPUPlan``;
+reference src/Plan.hpp, src/tdd/TDDPlan.hpp, src/fdd/FDDGPUPlan.hpp) so that
+tests and benchmarks read like the reference's own ``run<PlanType>()`` tests.
+
+There is no CPU fallback: importing works without a GPU (plans can be built
+and queried), but ``execute`` needs the library and a CUDA device and raises
+otherwise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+__all__ = [
+    "DedispError", "lib", "build", "Plan", "DedispPlan", "TDDPlan", "FDDGPUPlan",
+    "DEDISP_USE_DEFAULT", "DEDISP_HOST_POINTERS", "DEDISP_DEVICE_POINTERS",
+    "DEDISP_WAIT", "DEDISP_ASYNC", "DEDISP_DEDISP", "DEDISP_TDD", "DEDISP_FDD",
+    "ERROR_NAMES",
+]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libdedisp.so")
+
+DEDISP_USE_DEFAULT = 0
+DEDISP_HOST_POINTERS = 1 << 1
+DEDISP_DEVICE_POINTERS = 1 << 2
+DEDISP_WAIT = 1 << 3
+DEDISP_ASYNC = 1 << 4
+
+DEDISP_DEDISP, DEDISP_TDD, DEDISP_FDD = 0, 1, 2
+
+ERROR_NAMES = [
+    "DEDISP_NO_ERROR", "DEDISP_MEM_ALLOC_FAILED", "DEDISP_MEM_COPY_FAILED",
+    "DEDISP_NCHANS_EXCEEDS_LIMIT", "DEDISP_INVALID_PLAN", "DEDISP_INVALID_POINTER",
+    "DEDISP_INVALID_STRIDE", "DEDISP_NO_DM_LIST_SET", "DEDISP_TOO_FEW_NSAMPS",
+    "DEDISP_INVALID_FLAG_COMBINATION", "DEDISP_UNSUPPORTED_IN_NBITS",
+    "DEDISP_UNSUPPORTED_OUT_NBITS", "DEDISP_INVALID_DEVICE_INDEX",
+    "DEDISP_DEVICE_ALREADY_SET", "DEDISP_PRIOR_GPU_ERROR", "DEDISP_INTERNAL_GPU_ERROR",
+    "DEDISP_UNKNOWN_ERROR",
+]
+
+
+class DedispError(RuntimeError):
+    """A dedisp_error code returned by the library. ``code`` is what the C
+    call returned (DEDISP_UNKNOWN_ERROR for plan-level failures, as in the
+    reference); ``detail`` is the specific code from dedisp_b200_last_error."""
+
+    def __init__(self, code: int, detail: int = 0, message: str = ""):
+        self.code = code
+        self.detail = detail
+        self.message = message
+        super().__init__(f"{ERROR_NAMES[code] if 0 <= code < len(ERROR_NAMES) else code}"
+                         f" ({ERROR_NAMES[detail] if 0 <= detail < len(ERROR_NAMES) else detail})"
+                         f": {message}")
+
+
+def build(jobs: int = 8) -> None:
+    """Compile lib/libdedisp.so in-tree (nvcc, sm_100a)."""
+    import subprocess
+    subprocess.run(["make", "-s", f"-j{jobs}", "-C", os.path.join(HERE, "csrc")], check=True)
+
+
+_lib: Optional[C.CDLL] = None
+_vp = C.c_void_p
+_sz = C.c_ulong
+
+
+def lib() -> C.CDLL:
+    """Load libdedisp.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run dedisp_tests_b200.build() first")
+    L = C.CDLL(LIB_PATH)
+    err = C.c_int
+    sig = {
+        "dedisp_select_implementation": (err, [C.c_int]),
+        "dedisp_create_plan": (err, [C.POINTER(_vp), _sz, C.c_float, C.c_float, C.c_float]),
+        "dedisp_destroy_plan": (None, [_vp]),
+        "dedisp_set_device": (err, [C.c_int]),
+        "dedisp_set_gulp_size": (err, [_vp, _sz]),
+        "dedisp_get_gulp_size": (_sz, [_vp]),
+        "dedisp_set_killmask": (err, [_vp, _vp]),
+        "dedisp_set_dm_list": (err, [_vp, _vp, _sz]),
+        "dedisp_generate_dm_list": (err, [_vp, C.c_float, C.c_float, C.c_float, C.c_float]),
+        "dedisp_get_max_delay": (_sz, [_vp]),
+        "dedisp_get_dm_delay": (_sz, [_vp, C.c_int]),
+        "dedisp_get_channel_count": (_sz, [_vp]),
+        "dedisp_get_dm_count": (_sz, [_vp]),
+        "dedisp_get_dm_list": (C.POINTER(C.c_float), [_vp]),
+        "dedisp_get_killmask": (C.POINTER(C.c_int), [_vp]),
+        "dedisp_get_dt": (C.c_float, [_vp]),
+        "dedisp_get_f0": (C.c_float, [_vp]),
+        "dedisp_get_df": (C.c_float, [_vp]),
+        "dedisp_get_error_string": (C.c_char_p, [C.c_int]),
+        "dedisp_execute": (err, [_vp, _sz, _vp, _sz, _vp, _sz, C.c_uint]),
+        "dedisp_execute_adv": (err, [_vp, _sz, _vp, _sz, _sz, _vp, _sz, _sz, C.c_uint]),
+        "dedisp_execute_guru": (err, [_vp, _sz, _vp, _sz, _sz, _vp, _sz, _sz, _sz, _sz,
+                                      C.c_uint]),
+        "dedisp_sync": (err, []),
+        "dedisp_b200_set_tdd_kernel": (err, [_vp, C.c_int]),
+        "dedisp_b200_set_stream": (err, [_vp, _vp]),
+        "dedisp_b200_set_timing": (err, [_vp, C.c_int]),
+        "dedisp_b200_get_timing": (err, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                         C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "dedisp_b200_last_error": (err, [C.c_char_p, _sz]),
+        "dedisp_b200_set_fdd_options": (err, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _sz]),
+        "dedisp_b200_output_row_length": (_sz, [_vp, _sz]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(code: int) -> None:
+    if code != 0:
+        buf = C.create_string_buffer(512)
+        detail = lib().dedisp_b200_last_error(buf, 512)
+        raise DedispError(code, detail, buf.value.decode(errors="replace"))
+
+
+def _addr(x) -> int:
+    """Address of a numpy array, a torch tensor (host or CUDA) or an int."""
+    if x is None:
+        return 0
+    if isinstance(x, int):
+        return x
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    raise TypeError(f"cannot take the address of {type(x)!r}")
+
+
+class Plan:
+    """Handle on a dedisp_plan (mirrors dedisp::Plan, src/Plan.hpp)."""
+
+    IMPLEMENTATION = DEDISP_DEDISP
+
+    def __init__(self, nchans: int, dt: float, f0: float, df: float, device_idx: int = 0):
+        L = lib()
+        _check(L.dedisp_set_device(device_idx))
+        _check(L.dedisp_select_implementation(self.IMPLEMENTATION))
+        h = _vp()
+        _check(L.dedisp_create_plan(C.byref(h), nchans, dt, f0, df))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().dedisp_destroy_plan(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # setup -------------------------------------------------------------
+    def generate_dm_list(self, dm_start: float, dm_end: float, ti: float, tol: float) -> None:
+        _check(lib().dedisp_generate_dm_list(self._h, dm_start, dm_end, ti, tol))
+
+    def set_dm_list(self, dms) -> None:
+        arr = np.ascontiguousarray(dms, np.float32)
+        _check(lib().dedisp_set_dm_list(self._h, arr.ctypes.data, len(arr)))
+
+    def set_killmask(self, killmask=None) -> None:
+        if killmask is None:
+            _check(lib().dedisp_set_killmask(self._h, None))
+        else:
+            km = np.ascontiguousarray(killmask, np.int32)
+            _check(lib().dedisp_set_killmask(self._h, km.ctypes.data))
+
+    def set_gulp_size(self, n: int) -> None:
+        _check(lib().dedisp_set_gulp_size(self._h, n))
+
+    def get_gulp_size(self) -> int:
+        return int(lib().dedisp_get_gulp_size(self._h))
+
+    # getters -----------------------------------------------------------
+    def get_max_delay(self) -> int:
+        return int(lib().dedisp_get_max_delay(self._h))
+
+    def get_dm_delay(self, i: int) -> int:
+        return int(lib().dedisp_get_dm_delay(self._h, i))
+
+    def get_channel_count(self) -> int:
+        return int(lib().dedisp_get_channel_count(self._h))
+
+    def get_dm_count(self) -> int:
+        return int(lib().dedisp_get_dm_count(self._h))
+
+    def get_dm_list(self) -> np.ndarray:
+        n = self.get_dm_count()
+        p = lib().dedisp_get_dm_list(self._h)
+        return np.ctypeslib.as_array(p, (n,)).copy() if n else np.zeros(0, np.float32)
+
+    def get_killmask(self) -> np.ndarray:
+        n = self.get_channel_count()
+        p = lib().dedisp_get_killmask(self._h)
+        return np.ctypeslib.as_array(p, (n,)).copy()
+
+    def get_dt(self) -> float:
+        return float(lib().dedisp_get_dt(self._h))
+
+    def get_f0(self) -> float:
+        return float(lib().dedisp_get_f0(self._h))
+
+    def get_df(self) -> float:
+        return float(lib().dedisp_get_df(self._h))
+
+    def output_row_length(self, nsamps: int) -> int:
+        return int(lib().dedisp_b200_output_row_length(self._h, nsamps))
+
+    # execution ---------------------------------------------------------
+    def execute(self, nsamps: int, inp, in_nbits: int, out, out_nbits: int,
+                flags: int = 0) -> None:
+        _check(lib().dedisp_execute(self._h, nsamps, _addr(inp), in_nbits, _addr(out),
+                                    out_nbits, flags))
+
+    def execute_adv(self, nsamps, inp, in_nbits, in_stride, out, out_nbits, out_stride,
+                    flags: int = 0) -> None:
+        _check(lib().dedisp_execute_adv(self._h, nsamps, _addr(inp), in_nbits, in_stride,
+                                        _addr(out), out_nbits, out_stride, flags))
+
+    def execute_guru(self, nsamps, inp, in_nbits, in_stride, out, out_nbits, out_stride,
+                     first_dm_idx, dm_count, flags: int = 0) -> None:
+        _check(lib().dedisp_execute_guru(self._h, nsamps, _addr(inp), in_nbits, in_stride,
+                                         _addr(out), out_nbits, out_stride, first_dm_idx,
+                                         dm_count, flags))
+
+    def sync(self) -> None:
+        _check(lib().dedisp_sync())
+
+    # extensions ----------------------------------------------------------
+    def set_stream(self, stream_ptr: int) -> None:
+        _check(lib().dedisp_b200_set_stream(self._h, stream_ptr or None))
+
+    def set_timing(self, enable: bool = True) -> None:
+        _check(lib().dedisp_b200_set_timing(self._h, int(enable)))
+
+    def get_timing(self) -> dict:
+        k, p = C.c_float(), C.c_float()
+        n, v = C.c_int(), C.c_int()
+        _check(lib().dedisp_b200_get_timing(self._h, C.byref(k), C.byref(p), C.byref(n),
+                                            C.byref(v)))
+        return {"kernel_ms": k.value, "prep_ms": p.value, "launches": n.value,
+                "variant": v.value}
+
+
+class DedispPlan(Plan):
+    """Original dedisp interface (reference src/dedisp/DedispPlan.hpp)."""
+    IMPLEMENTATION = DEDISP_DEDISP
+
+    def set_kernel(self, kernel: int) -> None:
+        """0 auto, 1 plain (one thread per sample pair), 2 tiled."""
+        _check(lib().dedisp_b200_set_tdd_kernel(self._h, kernel))
+
+
+class TDDPlan(DedispPlan):
+    """Time-domain dedispersion (reference src/tdd/TDDPlan.hpp)."""
+    IMPLEMENTATION = DEDISP_TDD
+
+
+class FDDGPUPlan(Plan):
+    """Fourier-domain dedispersion (reference src/fdd/FDDGPUPlan.hpp)."""
+    IMPLEMENTATION = DEDISP_FDD
+
+    def set_options(self, segmented: int = -1, timeseries: bool = False, precision: int = 0,
+                    round_delays: bool = False, segment_nfft: int = 0) -> None:
+        _check(lib().dedisp_b200_set_fdd_options(self._h, segmented, int(timeseries),
+                                                 precision, int(round_delays), segment_nfft))

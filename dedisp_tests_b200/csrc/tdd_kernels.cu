@@ -1,0 +1,511 @@
+// Time-domain dedispersion kernels for sm_100a.
+//
+//   K1  transpose_kernel       time-major packed -> channel-major packed
+//   K2p dedisperse_plain       one thread per (DM, sample pair), global loads
+//                              (the reference algorithm, kept as baseline)
+//   K2  dedisperse_tiled       shared-memory staged channel windows, packed
+//                              SIMD-within-a-register accumulation
+//
+// Exactness: the sums are the reference's integer sums
+// (src/tdd/dedisperse/dedisperse_kernel.cuh:145-181): every integer delay is
+// __float2uint_rn(__fmul_rn(dm, delay[c])) and every partial sum is exact
+// (narrow lanes are flushed into 32-bit sums before they can overflow). The
+// FP32 epilogue repeats the reference operation order with IEEE rounding
+// intrinsics (dedisperse_kernel.cuh:45-64).
+#include "tdd_kernels.hpp"
+
+#include "runtime.hpp"
+
+namespace dedisp {
+namespace kern {
+namespace {
+
+// ---------------------------------------------------------------------------
+// Epilogue: src/tdd/dedisperse/dedisperse_kernel.cuh:45-87
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float sum_to_float(uint32_t s) { return __uint2float_rn(s); }
+__device__ __forceinline__ float sum_to_float(unsigned long long s) { return __ull2float_rn(s); }
+
+template <typename S>
+__device__ __forceinline__ void store_out(void* out, size_t idx, int out_nbits, S sum,
+                                          float den, float factor)
+{
+    const float fs = sum_to_float(sum);
+    if (out_nbits == 32) {
+        // out_range == 1.f: (fs * 1.f) == fs exactly
+        static_cast<float*>(out)[idx] = __fmul_rn(__fdiv_rn(fs, den), factor);
+    } else {
+        const float out_range = (out_nbits == 8) ? 255.f : 65535.f;
+        float v = __fmul_rn(__fdiv_rn(__fmul_rn(fs, out_range), den), factor);
+        // min(max(v, 0.), out_range) in double equals the float clip here:
+        // both bounds are exact floats and v is never NaN.
+        v = fminf(fmaxf(v, 0.f), out_range);
+        if (out_nbits == 8) static_cast<uint8_t*>(out)[idx] = (uint8_t)__float2uint_rz(v);
+        else static_cast<uint16_t*>(out)[idx] = (uint16_t)__float2uint_rz(v);
+    }
+}
+
+__device__ __forceinline__ uint32_t delay_rn(float dm, float delay)
+{
+    // src/tdd/dedisperse/dedisperse_kernel.cuh:163-165
+    return __float2uint_rn(__fmul_rn(dm, delay));
+}
+
+template <int NBITS>
+__device__ __forceinline__ constexpr uint32_t sample_mask()
+{
+    return NBITS == 32 ? 0xFFFFFFFFu : ((1u << NBITS) - 1u);
+}
+
+// ---------------------------------------------------------------------------
+// K1: transpose
+// ---------------------------------------------------------------------------
+template <int NBITS>
+struct TrGeom {
+    static constexpr int SPW = 32 / NBITS;                      // samples per word
+    static constexpr int TC = (NBITS <= 8) ? 512 / NBITS : 64;  // channels per tile
+    static constexpr int SEGW = TC * NBITS / 32;                // input words per row
+    static constexpr int TR = 128;                              // samples per tile
+    static constexpr int OW = TR / SPW;                         // output words per row
+};
+
+template <int NBITS>
+__global__ void __launch_bounds__(256) transpose_kernel(TransposeArgs a, int aligned)
+{
+    using G = TrGeom<NBITS>;
+    __shared__ uint32_t tile[G::TR][G::SEGW + 1];
+    const size_t r0 = (size_t)blockIdx.x * G::TR;
+    const size_t c0 = (size_t)blockIdx.y * G::TC;
+    const size_t row_words = a.nchans * NBITS / 32;
+    const size_t w0 = c0 * NBITS / 32;
+
+    for (int i = threadIdx.x; i < G::TR * G::SEGW; i += 256) {
+        const int r = i / G::SEGW, k = i % G::SEGW;
+        const size_t row = r0 + r, wi = w0 + k;
+        uint32_t v = 0;
+        if (row < a.rows_valid && wi < row_words) {
+            const uint8_t* p = a.in + row * a.in_pitch + wi * 4;
+            if (aligned) {
+                v = __ldg(reinterpret_cast<const uint32_t*>(p));
+            } else {
+                v = (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) |
+                    ((uint32_t)p[3] << 24);
+            }
+        }
+        tile[r][k] = v;
+    }
+    __syncthreads();
+
+    constexpr uint32_t MASK = sample_mask<NBITS>();
+    for (int i = threadIdx.x; i < G::TC * G::OW; i += 256) {
+        const int cl = i / G::OW, w = i % G::OW;
+        const size_t c = c0 + cl;
+        const size_t gw = r0 / G::SPW + w;
+        if (c >= a.nchans || gw >= a.tr_words) continue;
+        const size_t ow = a.tr_word_offset + gw;
+        const int bit = cl * NBITS, kw = bit >> 5, sh = bit & 31;
+        uint32_t out = 0;
+#pragma unroll
+        for (int s = 0; s < G::SPW; ++s) {
+            const uint32_t v = (tile[w * G::SPW + s][kw] >> sh) & MASK;
+            out |= v << ((s * NBITS) & 31);
+        }
+        a.tr[c * a.tr_pitch_words + ow] = out;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K2p: plain form -- the reference thread decomposition on our layout
+// (block 8 sample pairs x 32 DMs, src/tdd/dedisperse/TDDKernel.cu:133-151)
+// ---------------------------------------------------------------------------
+template <int NBITS>
+__global__ void __launch_bounds__(256) dedisperse_plain_kernel(DedisperseArgs a)
+{
+    using Sum = typename std::conditional<NBITS == 32, unsigned long long, uint32_t>::type;
+    constexpr int SPW = 32 / NBITS;
+    constexpr uint32_t MASK = sample_mask<NBITS>();
+    const size_t tp = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int slot = blockIdx.y * blockDim.y + threadIdx.y;
+    if (slot >= a.ndm) return;
+    const size_t t = tp * 2;
+    if (t >= a.nsamp_out) return;
+    const float dm = a.dms[slot];
+    Sum s0 = 0, s1 = 0;
+    for (int j = 0; j < a.nact; ++j) {
+        const int c = a.chan_list[j];
+        const uint32_t km = a.km_vals[j];
+        const uint32_t d = delay_rn(dm, a.delay_table[c]);
+        const uint32_t* row = a.tr + (size_t)c * a.tr_pitch_words;
+        const size_t p0 = t + d, p1 = p0 + 1;
+        const uint32_t v0 = (__ldg(row + p0 / SPW) >> ((p0 % SPW) * NBITS % 32)) & MASK;
+        const uint32_t v1 = (__ldg(row + p1 / SPW) >> ((p1 % SPW) * NBITS % 32)) & MASK;
+        s0 += (Sum)(uint32_t)(km * v0);
+        s1 += (Sum)(uint32_t)(km * v1);
+    }
+    const int row = a.perm ? a.perm[slot] : slot;
+    const size_t base = (size_t)row * a.out_stride;
+    store_out(a.out, base + t, a.out_nbits, s0, a.den, a.factor);
+    if (t + 1 < a.nsamp_out) store_out(a.out, base + t + 1, a.out_nbits, s1, a.den, a.factor);
+}
+
+// ---------------------------------------------------------------------------
+// K2: tiled form
+//
+// Block = BD DMs (NW warps x DPW DMs each) x BT output samples (32 lanes x R
+// consecutive samples each, R = J words). Channels are staged CS at a time:
+// for every staged channel, the window of input words that any DM of the
+// block can touch is copied into shared memory (cp.async, double buffered).
+// A lane reads J+1 consecutive words of a channel window at word offset
+// (q + lane*J); with J odd the 32 lanes hit 32 different banks. A funnel
+// shift aligns each word to the lane's sample boundary, then masks split it
+// into narrow lanes (8 or 16 bit) that are summed as plain 32-bit adds
+// (SIMD within a register). Narrow lanes are flushed into exact 32-bit sums
+// before they can overflow.
+// ---------------------------------------------------------------------------
+template <int NBITS>
+struct Tiled;
+// J: words per lane (odd); DPW: DMs per warp; FLP: channel pairs per narrow
+// flush (narrow lane capacity / (2 * max sample)).
+template <> struct Tiled<8>  { static constexpr int J = 5, DPW = 2, NN = 2, FLP = 128; };
+template <> struct Tiled<4>  { static constexpr int J = 3, DPW = 2, NN = 2, FLP = 8; };
+template <> struct Tiled<2>  { static constexpr int J = 1, DPW = 2, NN = 4, FLP = 42; };
+template <> struct Tiled<1>  { static constexpr int J = 1, DPW = 1, NN = 8, FLP = 127; };
+template <> struct Tiled<16> { static constexpr int J = 7, DPW = 2, NN = 1, FLP = 0; };
+template <> struct Tiled<32> { static constexpr int J = 7, DPW = 2, NN = 1, FLP = 0; };
+constexpr int TILED_NW = 16;
+
+template <int NBITS>
+struct TiledGeom {
+    static constexpr int SPW = 32 / NBITS;
+    static constexpr int J = Tiled<NBITS>::J;
+    static constexpr int R = J * SPW;       // samples per lane
+    static constexpr int BT = 32 * R;       // samples per block
+    static constexpr int DPW = Tiled<NBITS>::DPW;
+    static constexpr int BD = TILED_NW * DPW;
+    static constexpr int NT = TILED_NW * 32;
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
+// Narrow-lane accumulation of two channels' aligned words v1, v2 for word k.
+template <int NBITS, int J, int NN>
+__device__ __forceinline__ void narrow_add(uint32_t (&n)[J][NN], int k, uint32_t v1, uint32_t v2)
+{
+    if constexpr (NBITS == 8) {
+        constexpr uint32_t M = 0x00FF00FFu;
+        n[k][0] += (v1 & M) + (v2 & M);
+        n[k][1] += ((v1 >> 8) & M) + ((v2 >> 8) & M);
+    } else if constexpr (NBITS == 4) {
+        constexpr uint32_t M = 0x0F0F0F0Fu;
+        n[k][0] += (v1 & M) + (v2 & M);
+        n[k][1] += ((v1 >> 4) & M) + ((v2 >> 4) & M);
+    } else if constexpr (NBITS == 2) {
+        constexpr uint32_t M = 0x03030303u;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) n[k][m] += ((v1 >> (2 * m)) & M) + ((v2 >> (2 * m)) & M);
+    } else if constexpr (NBITS == 1) {
+        constexpr uint32_t M = 0x01010101u;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) n[k][m] += ((v1 >> m) & M) + ((v2 >> m) & M);
+    }
+}
+
+// Narrow lanes -> exact 32-bit sums; acc index = sample offset in the lane run.
+template <int NBITS, int J, int NN, int R>
+__device__ __forceinline__ void narrow_flush(uint32_t (&n)[J][NN], uint32_t (&acc)[R])
+{
+#pragma unroll
+    for (int k = 0; k < J; ++k) {
+        if constexpr (NBITS == 8) {
+            acc[4 * k + 0] += n[k][0] & 0xFFFFu;
+            acc[4 * k + 2] += n[k][0] >> 16;
+            acc[4 * k + 1] += n[k][1] & 0xFFFFu;
+            acc[4 * k + 3] += n[k][1] >> 16;
+        } else if constexpr (NBITS == 4) {
+#pragma unroll
+            for (int L = 0; L < 4; ++L) {
+                acc[8 * k + 2 * L] += (n[k][0] >> (8 * L)) & 0xFFu;
+                acc[8 * k + 2 * L + 1] += (n[k][1] >> (8 * L)) & 0xFFu;
+            }
+        } else if constexpr (NBITS == 2) {
+#pragma unroll
+            for (int m = 0; m < 4; ++m)
+#pragma unroll
+                for (int L = 0; L < 4; ++L) acc[16 * k + 4 * L + m] += (n[k][m] >> (8 * L)) & 0xFFu;
+        } else if constexpr (NBITS == 1) {
+#pragma unroll
+            for (int m = 0; m < 8; ++m)
+#pragma unroll
+                for (int L = 0; L < 4; ++L) acc[32 * k + 8 * L + m] += (n[k][m] >> (8 * L)) & 0xFFu;
+        }
+#pragma unroll
+        for (int m = 0; m < NN; ++m) n[k][m] = 0;
+    }
+}
+
+template <int NBITS>
+__global__ void __launch_bounds__(TiledGeom<NBITS>::NT, 1) dedisperse_tiled_kernel(DedisperseArgs a)
+{
+    using G = TiledGeom<NBITS>;
+    constexpr int SPW = G::SPW, J = G::J, R = G::R, BT = G::BT, DPW = G::DPW, BD = G::BD,
+                  NT = G::NT, NN = Tiled<NBITS>::NN, FLP = Tiled<NBITS>::FLP;
+    using Acc = typename std::conditional<NBITS == 32, unsigned long long, uint32_t>::type;
+
+    extern __shared__ __align__(16) uint32_t smem[];
+    const int W = a.win_words, CS = a.chan_per_stage;
+    uint32_t* s_win = smem;                       // [2][CS][W]
+    uint32_t* s_info = s_win + 2 * CS * W;        // [2][BD][CS]
+    float* s_dm = reinterpret_cast<float*>(s_info + 2 * BD * CS);  // [BD]
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int i0 = blockIdx.x * BD;
+    const size_t t0 = (size_t)blockIdx.y * BT;
+    const int nvalid = min(BD, a.ndm - i0);
+    const float dm_first = a.dms[i0];
+    const float dm_last = a.dms[i0 + nvalid - 1];
+    if (tid < BD) s_dm[tid] = a.dms[i0 + min(tid, nvalid - 1)];
+    __syncthreads();
+
+    // Stage `stage` of the channel list into buffer `buf`.
+    auto prep = [&](int stage, int buf) {
+        const int32_t* cl = a.chan_list + (size_t)stage * CS;
+        for (int j = warp; j < CS; j += TILED_NW) {
+            const int c = cl[j];
+            const float dl = a.delay_table[c];
+            const uint32_t lo = min(delay_rn(dm_first, dl), delay_rn(dm_last, dl));
+            const size_t A = ((t0 + lo) / (4 * SPW)) * (4 * SPW);
+            const uint32_t* src = a.tr + (size_t)c * a.tr_pitch_words + A / SPW;
+            uint32_t* dst = s_win + (size_t)(buf * CS + j) * W;
+            for (int k = lane * 4; k < W; k += 128) cp_async16(dst + k, src + k);
+        }
+        for (int idx = tid; idx < BD * CS; idx += NT) {
+            const int slot = idx / CS, j = idx - slot * CS;
+            const int c = cl[j];
+            const float dl = a.delay_table[c];
+            const uint32_t lo = min(delay_rn(dm_first, dl), delay_rn(dm_last, dl));
+            const size_t A = ((t0 + lo) / (4 * SPW)) * (4 * SPW);
+            const uint32_t d = delay_rn(s_dm[slot], dl);
+            const uint32_t rel = (uint32_t)(t0 + d - A);
+            s_info[(buf * BD + slot) * CS + j] = ((rel / SPW) << 5) | ((rel % SPW) * NBITS);
+        }
+    };
+
+    Acc acc[DPW][R];
+    uint32_t nar[DPW][J][NN];
+#pragma unroll
+    for (int di = 0; di < DPW; ++di) {
+#pragma unroll
+        for (int k = 0; k < R; ++k) acc[di][k] = 0;
+#pragma unroll
+        for (int k = 0; k < J; ++k)
+#pragma unroll
+            for (int m = 0; m < NN; ++m) nar[di][k][m] = 0;
+    }
+
+    prep(0, 0);
+    cp_async_commit();
+    int pairs = 0;
+    for (int s = 0; s < a.nstages; ++s) {
+        const int buf = s & 1;
+        if (s + 1 < a.nstages) prep(s + 1, buf ^ 1);
+        cp_async_commit();
+        cp_async_wait_1();
+        __syncthreads();
+
+        const uint32_t* win = s_win + (size_t)buf * CS * W;
+        const uint32_t* info = s_info + buf * BD * CS;
+        for (int j = 0; j < CS; j += 2) {
+#pragma unroll
+            for (int di = 0; di < DPW; ++di) {
+                const int slot = warp * DPW + di;
+                const uint32_t f1 = info[slot * CS + j];
+                const uint32_t f2 = info[slot * CS + j + 1];
+                const uint32_t* p1 = win + j * W + (f1 >> 5) + lane * J;
+                const uint32_t* p2 = win + (j + 1) * W + (f2 >> 5) + lane * J;
+                if constexpr (NBITS == 32) {
+#pragma unroll
+                    for (int k = 0; k < J; ++k)
+                        acc[di][k] += (unsigned long long)p1[k] + (unsigned long long)p2[k];
+                } else {
+                    const uint32_t b1 = f1 & 31, b2 = f2 & 31;
+                    uint32_t w1[J + 1], w2[J + 1];
+#pragma unroll
+                    for (int k = 0; k <= J; ++k) {
+                        w1[k] = p1[k];
+                        w2[k] = p2[k];
+                    }
+#pragma unroll
+                    for (int k = 0; k < J; ++k) {
+                        const uint32_t v1 = __funnelshift_r(w1[k], w1[k + 1], b1);
+                        const uint32_t v2 = __funnelshift_r(w2[k], w2[k + 1], b2);
+                        if constexpr (NBITS == 16) {
+                            acc[di][2 * k] += (v1 & 0xFFFFu) + (v2 & 0xFFFFu);
+                            acc[di][2 * k + 1] += (v1 >> 16) + (v2 >> 16);
+                        } else {
+                            narrow_add<NBITS, J, NN>(nar[di], k, v1, v2);
+                        }
+                    }
+                }
+            }
+            if constexpr (FLP > 0) {
+                if (++pairs == FLP) {
+#pragma unroll
+                    for (int di = 0; di < DPW; ++di) narrow_flush<NBITS, J, NN, R>(nar[di], acc[di]);
+                    pairs = 0;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if constexpr (FLP > 0) {
+#pragma unroll
+        for (int di = 0; di < DPW; ++di) narrow_flush<NBITS, J, NN, R>(nar[di], acc[di]);
+    }
+
+#pragma unroll
+    for (int di = 0; di < DPW; ++di) {
+        const int slot = warp * DPW + di;
+        if (slot >= nvalid) continue;
+        const int row = a.perm ? a.perm[i0 + slot] : i0 + slot;
+        const size_t base = (size_t)row * a.out_stride;
+        const size_t tl = t0 + (size_t)lane * R;
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const size_t t = tl + k;
+            if (t < a.nsamp_out) store_out(a.out, base + t, a.out_nbits, acc[di][k], a.den, a.factor);
+        }
+    }
+}
+
+template <int NBITS>
+void launch_tiled_n(const DedisperseArgs& a, cudaStream_t s)
+{
+    using G = TiledGeom<NBITS>;
+    const size_t smem = tiled_smem_bytes(NBITS, a.win_words, a.chan_per_stage);
+    // The attribute is per device context; remember what each device has.
+    static size_t configured[64] = {};
+    int dev = 0;
+    RT_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64 || smem > configured[dev]) {
+        RT_CHECK(cudaFuncSetAttribute(dedisperse_tiled_kernel<NBITS>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if (dev >= 0 && dev < 64) configured[dev] = smem;
+    }
+    dim3 grid((a.ndm + G::BD - 1) / G::BD, (unsigned)((a.nsamp_out + G::BT - 1) / G::BT));
+    dedisperse_tiled_kernel<NBITS><<<grid, G::NT, smem, s>>>(a);
+    RT_CHECK(cudaGetLastError());
+}
+
+template <int NBITS>
+void launch_plain_n(const DedisperseArgs& a, cudaStream_t s)
+{
+    dim3 block(8, 32);
+    dim3 grid((unsigned)((a.nsamp_out + 15) / 16), (a.ndm + 31) / 32);
+    dedisperse_plain_kernel<NBITS><<<grid, block, 0, s>>>(a);
+    RT_CHECK(cudaGetLastError());
+}
+
+template <int NBITS>
+void launch_transpose_n(const TransposeArgs& a, cudaStream_t s)
+{
+    using G = TrGeom<NBITS>;
+    const size_t samples = a.tr_words * G::SPW;
+    dim3 grid((unsigned)((samples + G::TR - 1) / G::TR), (unsigned)((a.nchans + G::TC - 1) / G::TC));
+    const int aligned = ((uintptr_t)a.in % 4 == 0) && (a.in_pitch % 4 == 0);
+    transpose_kernel<NBITS><<<grid, 256, 0, s>>>(a, aligned);
+    RT_CHECK(cudaGetLastError());
+}
+
+}  // namespace
+
+int tiled_block_samples(int nbits)
+{
+    switch (nbits) {
+    case 1: return TiledGeom<1>::BT;
+    case 2: return TiledGeom<2>::BT;
+    case 4: return TiledGeom<4>::BT;
+    case 8: return TiledGeom<8>::BT;
+    case 16: return TiledGeom<16>::BT;
+    default: return TiledGeom<32>::BT;
+    }
+}
+
+int tiled_block_dms(int nbits)
+{
+    switch (nbits) {
+    case 1: return TiledGeom<1>::BD;
+    case 2: return TiledGeom<2>::BD;
+    case 4: return TiledGeom<4>::BD;
+    case 8: return TiledGeom<8>::BD;
+    case 16: return TiledGeom<16>::BD;
+    default: return TiledGeom<32>::BD;
+    }
+}
+
+int tiled_lane_words(int nbits)
+{
+    switch (nbits) {
+    case 1: return TiledGeom<1>::J;
+    case 2: return TiledGeom<2>::J;
+    case 4: return TiledGeom<4>::J;
+    case 8: return TiledGeom<8>::J;
+    case 16: return TiledGeom<16>::J;
+    default: return TiledGeom<32>::J;
+    }
+}
+
+size_t tiled_smem_bytes(int nbits, int win_words, int chan_per_stage)
+{
+    const size_t bd = (size_t)tiled_block_dms(nbits);
+    return (2ull * chan_per_stage * win_words + 2ull * bd * chan_per_stage + bd) * 4ull;
+}
+
+size_t tiled_max_smem_bytes() { return 200 * 1024; }
+
+void launch_transpose(const TransposeArgs& a, cudaStream_t s)
+{
+    switch (a.nbits) {
+    case 1: launch_transpose_n<1>(a, s); break;
+    case 2: launch_transpose_n<2>(a, s); break;
+    case 4: launch_transpose_n<4>(a, s); break;
+    case 8: launch_transpose_n<8>(a, s); break;
+    case 16: launch_transpose_n<16>(a, s); break;
+    case 32: launch_transpose_n<32>(a, s); break;
+    default: DD_THROW(DEDISP_UNSUPPORTED_IN_NBITS);
+    }
+}
+
+void launch_dedisperse_plain(const DedisperseArgs& a, cudaStream_t s)
+{
+    switch (a.nbits) {
+    case 1: launch_plain_n<1>(a, s); break;
+    case 2: launch_plain_n<2>(a, s); break;
+    case 4: launch_plain_n<4>(a, s); break;
+    case 8: launch_plain_n<8>(a, s); break;
+    case 16: launch_plain_n<16>(a, s); break;
+    case 32: launch_plain_n<32>(a, s); break;
+    default: DD_THROW(DEDISP_UNSUPPORTED_IN_NBITS);
+    }
+}
+
+void launch_dedisperse_tiled(const DedisperseArgs& a, cudaStream_t s)
+{
+    switch (a.nbits) {
+    case 1: launch_tiled_n<1>(a, s); break;
+    case 2: launch_tiled_n<2>(a, s); break;
+    case 4: launch_tiled_n<4>(a, s); break;
+    case 8: launch_tiled_n<8>(a, s); break;
+    case 16: launch_tiled_n<16>(a, s); break;
+    case 32: launch_tiled_n<32>(a, s); break;
+    default: DD_THROW(DEDISP_UNSUPPORTED_IN_NBITS);
+    }
+}
+
+}  // namespace kern
+}  // namespace dedisp

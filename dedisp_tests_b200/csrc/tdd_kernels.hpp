@@ -1,0 +1,68 @@
+// Launch interface of the time-domain (TDD) kernels.
+//
+// Device layout ("channel-major packed"): channel c of a gulp is a row of
+// 32-bit words at tr + c * tr_pitch_words; word w holds samples
+// w*spw .. w*spw+spw-1 (spw = 32/nbits), sample i of the word at bits
+// i*nbits, LSB first. Row `nchans` is an all-zero row used to pad channel
+// lists. The same little-endian packing as the input format, with time and
+// channel swapped.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace dedisp {
+namespace kern {
+
+// K1: time-major packed rows -> channel-major packed rows.
+struct TransposeArgs {
+    const uint8_t* in;      // row r at in + r * in_pitch
+    size_t in_pitch;        // bytes
+    size_t rows_valid;      // rows present in `in`; later samples are zero
+    size_t nchans;
+    int nbits;
+    uint32_t* tr;           // channel-major output
+    size_t tr_pitch_words;  // words between channel rows
+    size_t tr_word_offset;  // first word written in each row (= first row / spw)
+    size_t tr_words;        // words written per row from there (zeros past rows_valid)
+};
+void launch_transpose(const TransposeArgs& a, cudaStream_t s);
+
+// K2: dedispersion of one gulp.
+struct DedisperseArgs {
+    const uint32_t* tr;
+    size_t tr_pitch_words;
+    int nbits;
+    size_t nchans;              // total channels (epilogue normalisation)
+    const int32_t* chan_list;   // active channels, padded with `nchans`
+    int nact;                   // active channels (plain kernel loop bound)
+    int nstages;                // tiled: padded list length / chan_per_stage
+    const uint32_t* km_vals;    // plain: multiplier per active channel
+    const float* delay_table;   // nchans + 1 entries, last one 0
+    const float* dms;           // DM per slot (sorted ascending for tiled)
+    const int32_t* perm;        // output row of slot i (nullptr: identity)
+    int ndm;
+    size_t nsamp_out;           // output samples in this gulp
+    void* out;                  // row r at out + r * out_stride elements
+    size_t out_stride;          // elements
+    int out_nbits;              // 8, 16 or 32 (float)
+    float den;                  // (float)(2^nbits-1) * (float)nchans
+    float factor;               // (3.f*1024.f)/255.f/16.f
+    int win_words;              // tiled: staged window per channel (words)
+    int chan_per_stage;         // tiled: channels per pipeline stage (even)
+};
+
+// Tile geometry of the tiled kernel for a given input width.
+int tiled_block_samples(int nbits);  // output samples per block
+int tiled_block_dms(int nbits);      // DMs per block
+int tiled_lane_words(int nbits);     // J: words per lane
+size_t tiled_smem_bytes(int nbits, int win_words, int chan_per_stage);
+size_t tiled_max_smem_bytes();
+
+void launch_dedisperse_plain(const DedisperseArgs& a, cudaStream_t s);
+void launch_dedisperse_tiled(const DedisperseArgs& a, cudaStream_t s);
+
+}  // namespace kern
+}  // namespace dedisp
