@@ -91,10 +91,14 @@ GPU_CASES = [
     ("dedisp", 128, 1581.8, -1.5625, 250e-6, 8192, 8, 32, 32, 200.0, 7, 17),
     ("dedisp", 256, 1500.0, -0.5, 64e-6, 6000, 2, 16, 20, 150.0, 0, 18),
 ]
+# The reference FDD kernel is only launched for channel batches of
+# 1/16/32/64/128/256 (FDDKernel.cu:79-87, batch = min(nchans/4, 64)) and
+# touches a popped DM job when ndm is a multiple of its DM batch
+# (FDDGPUPlan.cpp:352-368), so the cases use nchans 64/128 and ndm 18/14.
 FDD_CASES = [
     # (nchans, f0, df, dt, nsamps, ndm, dm_max, segmented, seed)
-    ("fdd", 32, 1581.8, -3.125, 250e-6, 12000, 16, 60.0, 0, 21),
-    ("fdd", 64, 1581.8, -1.5625, 250e-6, 40000, 12, 80.0, 1, 22),
+    ("fdd", 64, 1581.8, -3.125, 250e-6, 12000, 18, 60.0, 0, 21),
+    ("fdd", 128, 1581.8, -1.5625, 250e-6, 40000, 14, 80.0, 1, 22),
 ]
 
 
