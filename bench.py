@@ -54,7 +54,36 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile-case", default="",
+                    help="run one small case for ncu and exit: tdd (the TDD workload with "
+                         "2^17 samples) or fdd (config-2 geometry with 2^18 samples)")
     return ap.parse_args()
+
+
+def profile_case(args):
+    """One execution of a reduced workload, sized for ncu captures: the same
+    kernels and DM list as the benchmark, fewer samples."""
+    import torch
+    import dedisp_tests_b200 as dd
+    from dedisp_tests_b200 import synthetic as sy
+    if args.profile_case == "tdd":
+        cfg = sy.config1(nbits=args.nbits, nsamps=1 << 17)
+        p = dd.TDDPlan(cfg.nchans, cfg.dt, cfg.f_top, cfg.df)
+        p.generate_dm_list(*cfg.dm_gen)
+        nbits = args.nbits
+    else:
+        cfg = sy.config2(nsamps=1 << 18)
+        p = dd.FDDGPUPlan(cfg.nchans, cfg.dt, cfg.f_top, cfg.df)
+        p.set_dm_list(cfg.dm_list)
+        p.set_options(segmented=1, precision=1 if args.profile_case == "fdd-tc" else 0)
+        nbits = 32
+    d_in = sy.make_input_torch(cfg)
+    rows = p.output_row_length(cfg.nsamps)
+    d_out = torch.empty((p.get_dm_count(), rows), dtype=torch.float32, device="cuda")
+    for _ in range(2):
+        p.execute(cfg.nsamps, d_in, nbits, d_out, 32, dd.DEDISP_DEVICE_POINTERS)
+    torch.cuda.synchronize()
+    print("profile case done:", args.profile_case, cfg.nsamps, p.get_dm_count())
 
 
 # ---------------------------------------------------------------------------
@@ -369,7 +398,9 @@ def run_reference(args):
 
 if __name__ == "__main__":
     a = parse()
-    if a.impl == "reference":
+    if a.profile_case:
+        profile_case(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_ours(a)

@@ -1,18 +1,190 @@
-// FDD execution engine (placeholder until the Fourier-domain kernels land).
+// FDD execution engine: unpack -> real FFT per (channel, segment) ->
+// bin-major -> phasor MAC -> spectrum output, or DM-major -> inverse real
+// FFT with stitching (src/fdd/FDDGPUPlan.cpp:58-706 whole series,
+// :725-1271 segmented).
 #include "fdd_engine.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "fdd_kernels.hpp"
+#include "host_math.hpp"
 
 namespace dedisp {
 namespace detail {
 
-struct FddEngine::Impl {};
+namespace {
+size_t round_up(size_t a, size_t b) { return (a + b - 1) / b * b; }
+}  // namespace
+
+struct FddEngine::Impl {
+    rt::DeviceBuffer in, x, X, Xt, Yt, Y, out, tw_lo, tw_hi, dms, chan, km, delay_act;
+    unsigned tw_n = 0;
+    unsigned long version = ~0ul;
+    int nact = 0;
+};
 
 FddEngine::FddEngine(GpuState& gpu) : m_gpu(gpu), m_impl(new Impl()) {}
-FddEngine::~FddEngine() {}
+FddEngine::~FddEngine()
+{
+    if (m_gpu.has_device) {
+        rt::DeviceGuard g(m_gpu.device);
+        cudaStreamSynchronize(m_gpu.stream());
+    }
+}
 
-void FddEngine::execute(const FddOptions&, const FddView&, const FddCall&)
+void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& c)
 {
     m_gpu.require_device();
-    DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "FDD execution not available in this build");
+    rt::DeviceGuard guard(m_gpu.device);
+    Impl& m = *m_impl;
+    stats = ExecTiming();
+
+    const FddGeometry g = fdd_geometry(opt, c.nsamps, v.max_delay);
+    if (g.nfft > (size_t)kern::kMaxSmemFft || g.nfft < 512)
+        DD_THROW_MSG(DEDISP_UNKNOWN_ERROR,
+                     "FDD transform length outside the supported range (512..32768)");
+    const bool dev = (c.flags & DEDISP_DEVICE_POINTERS) != 0;
+    cudaStream_t st = m_gpu.stream();
+    const size_t nchans = v.nchans, ndm = v.ndm, nseg = g.nchunk;
+    const size_t nbins = g.nbins;
+    const size_t bin_pitch = round_up(nbins, 32);
+    const size_t seg_stride = g.segmented ? g.nsamp_good : 0;
+    const size_t x_len = round_up((nseg - 1) * seg_stride + g.nfft, 32);
+    const size_t in_stride = nchans * (size_t)c.in_nbits / 8;
+
+    // Per-plan state: active channels, killmask multipliers, DM list.
+    if (m.version != v.version) {
+        std::vector<int32_t> chan;
+        std::vector<float> km, dl;
+        for (size_t i = 0; i < nchans; ++i) {
+            if (v.killmask[i] == 0) continue;
+            chan.push_back((int32_t)i);
+            km.push_back((float)v.killmask[i]);
+            dl.push_back(v.delays[i]);
+        }
+        m.nact = (int)chan.size();
+        const size_t n = std::max<size_t>(1, chan.size());
+        chan.resize(n, 0);
+        km.resize(n, 0.f);
+        dl.resize(n, 0.f);
+        m.chan.reserve(n * 4);
+        m.km.reserve(n * 4);
+        m.delay_act.reserve(n * 4);
+        m.dms.reserve(ndm * 4);
+        RT_CHECK(cudaMemcpy(m.chan.get(), chan.data(), n * 4, cudaMemcpyHostToDevice));
+        RT_CHECK(cudaMemcpy(m.km.get(), km.data(), n * 4, cudaMemcpyHostToDevice));
+        RT_CHECK(cudaMemcpy(m.delay_act.get(), dl.data(), n * 4, cudaMemcpyHostToDevice));
+        RT_CHECK(cudaMemcpy(m.dms.get(), v.dms, ndm * 4, cudaMemcpyHostToDevice));
+        m.version = v.version;
+    }
+    // Twiddles W_N^t = exp(-2 pi i t / N) as hi[t >> 8] * lo[t & 255].
+    if (m.tw_n != g.nfft) {
+        const unsigned n = (unsigned)g.nfft;
+        std::vector<float2> lo(256), hi(n / 256);
+        for (unsigned l = 0; l < 256; ++l) {
+            const double a = -2.0 * 3.14159265358979323846 * (double)l / (double)n;
+            lo[l] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
+        for (unsigned h = 0; h < n / 256; ++h) {
+            const double a = -2.0 * 3.14159265358979323846 * (double)h * 256.0 / (double)n;
+            hi[h] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
+        m.tw_lo.reserve(256 * sizeof(float2));
+        m.tw_hi.reserve(hi.size() * sizeof(float2));
+        RT_CHECK(cudaMemcpy(m.tw_lo.get(), lo.data(), 256 * sizeof(float2), cudaMemcpyHostToDevice));
+        RT_CHECK(cudaMemcpy(m.tw_hi.get(), hi.data(), hi.size() * sizeof(float2),
+                            cudaMemcpyHostToDevice));
+        m.tw_n = n;
+    }
+    kern::TwiddleTable tw{m.tw_lo.get<float2>(), m.tw_hi.get<float2>(), (unsigned)g.nfft};
+
+    // Buffers.
+    const uint8_t* d_in = c.in;
+    if (!dev) {
+        m.in.reserve(c.nsamps * in_stride);
+        d_in = m.in.get<uint8_t>();
+    }
+    m.x.reserve(nchans * x_len * sizeof(float));
+    m.X.reserve(nchans * nseg * bin_pitch * sizeof(float2));
+    m.Xt.reserve(nbins * nseg * std::max(1, m.nact) * sizeof(float2));
+    m.Yt.reserve(nbins * nseg * ndm * sizeof(float2));
+    const bool inverse = g.timeseries;
+    if (inverse) m.Y.reserve(ndm * nseg * bin_pitch * sizeof(float2));
+    float* d_out = reinterpret_cast<float*>(c.out);
+    if (!dev) {
+        m.out.reserve(ndm * g.row_len * sizeof(float));
+        d_out = m.out.get<float>();
+    }
+
+    std::unique_ptr<rt::Event> e0, e1, e2, e3;
+    if (record_timing) {
+        e0.reset(new rt::Event(true));
+        e1.reset(new rt::Event(true));
+        e2.reset(new rt::Event(true));
+        e3.reset(new rt::Event(true));
+    }
+    if (!dev)
+        RT_CHECK(cudaMemcpyAsync(m.in.get(), c.in, c.nsamps * in_stride, cudaMemcpyHostToDevice, st));
+    if (e0) e0->record(st);
+
+    const float scale = (float)(1.0 / (double)nchans);
+    kern::launch_fdd_unpack(d_in, in_stride, c.in_nbits, c.nsamps, nchans, scale, m.x.get<float>(),
+                            x_len, x_len, st);
+    kern::launch_fft_r2c(m.x.get<float>(), x_len, nchans, nseg, seg_stride, (int)g.nfft,
+                         m.X.get<float2>(), bin_pitch, tw, st);
+    if (m.nact > 0)
+        kern::launch_fdd_to_binmajor(m.X.get<float2>(), bin_pitch, nseg, nbins, m.chan.get<int32_t>(),
+                                     m.km.get<float>(), m.nact, m.Xt.get<float2>(), st);
+    if (e1) e1->record(st);
+
+    if (m.nact > 0) {
+        kern::MacArgs a;
+        a.Xt = m.Xt.get<float2>();
+        a.Yt = m.Yt.get<float2>();
+        a.dms = m.dms.get<float>();
+        a.delay_act = m.delay_act.get<float>();
+        a.nact = m.nact;
+        a.ndm = (int)ndm;
+        a.nseg = (int)nseg;
+        a.nbins = nbins;
+        a.nfft = (unsigned)g.nfft;
+        a.round_delays = opt.round_delays ? 1 : 0;
+        a.tw = tw;
+        kern::launch_fdd_mac_plain(a, st);
+        stats.launches = 1;
+    } else {
+        RT_CHECK(cudaMemsetAsync(m.Yt.get(), 0, nbins * nseg * ndm * sizeof(float2), st));
+    }
+    if (e2) e2->record(st);
+
+    if (!inverse) {
+        // spectrum: first nfft/2 bins of each DM row, interleaved re/im
+        kern::launch_fdd_spectrum_out(m.Yt.get<float2>(), ndm, g.nfft / 2, d_out, g.row_len, st);
+    } else {
+        kern::launch_fdd_to_dmmajor(m.Yt.get<float2>(), nseg, ndm, nbins, m.Y.get<float2>(),
+                                    bin_pitch, st);
+        const size_t keep = g.segmented ? g.nsamp_good : g.nfft;
+        kern::launch_fft_c2r(m.Y.get<float2>(), bin_pitch, ndm, nseg, (int)g.nfft, d_out, g.row_len,
+                             keep, g.row_len, tw, st);
+    }
+    if (e3) e3->record(st);
+    if (!dev)
+        RT_CHECK(cudaMemcpyAsync(c.out, d_out, ndm * g.row_len * sizeof(float),
+                                 cudaMemcpyDeviceToHost, st));
+    const bool async = dev && (c.flags & DEDISP_ASYNC);
+    if (!async) RT_CHECK(cudaStreamSynchronize(st));
+    if (record_timing) {
+        RT_CHECK(cudaEventSynchronize(*e3));
+        float pre = 0.f, mac = 0.f, post = 0.f;
+        RT_CHECK(cudaEventElapsedTime(&pre, *e0, *e1));
+        RT_CHECK(cudaEventElapsedTime(&mac, *e1, *e2));
+        RT_CHECK(cudaEventElapsedTime(&post, *e2, *e3));
+        stats.prep_ms = pre + post;
+        stats.kernel_ms = mac;
+        stats.variant = (int)opt.precision;
+    }
 }
 
 }  // namespace detail

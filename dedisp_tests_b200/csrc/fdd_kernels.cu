@@ -1,0 +1,558 @@
+// Fourier-domain dedispersion kernels for sm_100a (FP32 forms).
+//
+//   fdd_unpack          time-major input -> channel-major float rows
+//   fft_r2c / fft_c2r   batched real FFTs, one CTA per transform, the whole
+//                       transform resident in shared memory; radix-16 DIF
+//                       passes in registers; real<->complex via the
+//                       half-length complex transform
+//   to_binmajor         X[c][seg][k] -> Xt[k][seg][j] (active channels,
+//                       killmask multiplier folded in)
+//   mac_plain           per-bin complex GEMM on CUDA cores: phasors
+//                       W(k*d mod N) generated on chip from exact integer
+//                       phase indices and a two-level twiddle table
+//   to_dmmajor / spectrum_out
+//
+// Conventions follow the reference: forward transform e^{-2 pi i k n/N}
+// (cuFFT R2C, FDDGPUPlan.cpp:160-175), phasor e^{+2 pi i k d/N} with
+// d = (int)(dm * delay[c]) (fdd_kernel.cuh:226-235), inverse scaled by 1/N
+// (fdd_kernel.cuh:262-273).
+#include "fdd_kernels.hpp"
+
+#include "runtime.hpp"
+
+namespace dedisp {
+namespace kern {
+namespace {
+
+__device__ __forceinline__ float2 operator+(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 operator-(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b)
+{
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
+
+// exp(-2 pi i t / 16), t = 0..7 (forward); conjugated for the inverse.
+__device__ __forceinline__ float2 w16(int t, bool inv)
+{
+    const float c[8] = {1.0f, 0.92387953251128674f, 0.70710678118654752f, 0.38268343236508977f,
+                        0.0f, -0.38268343236508977f, -0.70710678118654752f, -0.92387953251128674f};
+    const float s[8] = {0.0f, 0.38268343236508977f, 0.70710678118654752f, 0.92387953251128674f,
+                        1.0f, 0.92387953251128674f, 0.70710678118654752f, 0.38268343236508977f};
+    return make_float2(c[t], inv ? s[t] : -s[t]);
+}
+
+// In-register DFT of R = 2,4,8,16 points (radix-2 DIF network), output in
+// natural order.
+template <int R, bool INV>
+__device__ __forceinline__ void dft_reg(float2 (&v)[R])
+{
+#pragma unroll
+    for (int span = R / 2; span >= 1; span >>= 1) {
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            if ((i & span) == 0) {
+                const int j = i + span;
+                const float2 a = v[i], b = v[j];
+                v[i] = a + b;
+                const float2 d = a - b;
+                const int t = (i & (span - 1)) * (8 / span);  // W_{2 span}^t' in units of W_16
+                v[j] = (t == 0) ? d : cmul(d, w16(t, INV));
+            }
+        }
+    }
+    float2 o[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+        int r = 0;
+#pragma unroll
+        for (int b = 1, rb = R / 2; b < R; b <<= 1, rb >>= 1)
+            if (q & b) r |= rb;
+        o[q] = v[r];
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = o[q];
+}
+
+// Radix of pass p for M = 2^LOGM: radix 16 while possible, the remainder last.
+template <int LOGM>
+struct FftPlan {
+    static constexpr int NP = (LOGM + 3) / 4;
+    __host__ __device__ static constexpr int last_bits() { return LOGM - 4 * (NP - 1); }
+    __host__ __device__ static constexpr int bits(int p) { return p < NP - 1 ? 4 : last_bits(); }
+};
+
+// Smem position of frequency k after all DIF passes (mixed-radix digit
+// reversal; each pass's output digit is the next frequency digit).
+template <int LOGM>
+__device__ __forceinline__ unsigned fft_pos(unsigned k)
+{
+    using P = FftPlan<LOGM>;
+    unsigned pos = 0, rem = LOGM;
+#pragma unroll
+    for (int p = 0; p < P::NP; ++p) {
+        const int b = P::bits(p);
+        const unsigned q = k & ((1u << b) - 1u);
+        k >>= b;
+        rem -= b;
+        pos |= q << rem;
+    }
+    return pos;
+}
+
+__device__ __forceinline__ float2 twiddle(const float2* lo, const float2* hi, unsigned t, bool inv)
+{
+    const float2 w = cmul(hi[t >> 8], lo[t & 255]);
+    return inv ? conjf2(w) : w;
+}
+
+// One DIF pass of radix R on sub-transforms of length L (in place).
+template <int R, bool INV>
+__device__ __forceinline__ void fft_pass(float2* s, unsigned M, unsigned L, int log_nl,
+                                         const float2* lo, const float2* hi)
+{
+    const unsigned sub = L / R;
+    const unsigned groups = M / R;
+    for (unsigned g = threadIdx.x; g < groups; g += blockDim.x) {
+        const unsigned blk = g / sub, j = g - blk * sub;
+        const unsigned base = blk * L + j;
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = s[base + r * sub];
+        dft_reg<R, INV>(v);
+#pragma unroll
+        for (int q = 1; q < R; ++q) {
+            // W_L^{j q} = W_N^{j q N / L}, N = 2M
+            const unsigned t = (j * q) << log_nl;
+            if (j) v[q] = cmul(v[q], twiddle(lo, hi, t, INV));
+        }
+#pragma unroll
+        for (int q = 0; q < R; ++q) s[base + q * sub] = v[q];
+    }
+}
+
+template <int LOGM, bool INV>
+__device__ __forceinline__ void fft_smem(float2* s, const float2* lo, const float2* hi)
+{
+    using P = FftPlan<LOGM>;
+    constexpr unsigned M = 1u << LOGM;
+    unsigned L = M;
+    int log_nl = 1;  // log2(N / L), N = 2M
+#pragma unroll
+    for (int p = 0; p < P::NP; ++p) {
+        const int b = P::bits(p);
+        __syncthreads();
+        if (b == 4) fft_pass<16, INV>(s, M, L, log_nl, lo, hi);
+        else if (b == 3) fft_pass<8, INV>(s, M, L, log_nl, lo, hi);
+        else if (b == 2) fft_pass<4, INV>(s, M, L, log_nl, lo, hi);
+        else if (b == 1) fft_pass<2, INV>(s, M, L, log_nl, lo, hi);
+        L >>= b;
+        log_nl += b;
+    }
+    __syncthreads();
+}
+
+template <int LOGM>
+__global__ void __launch_bounds__(512) fft_r2c_kernel(const float* x, size_t x_pitch, size_t nseg,
+                                                      size_t seg_stride, float2* X, size_t bin_pitch,
+                                                      TwiddleTable tw)
+{
+    constexpr unsigned M = 1u << LOGM;
+    extern __shared__ __align__(16) float2 s_fft[];
+    float2* s = s_fft;
+    float2* lo = s + M;
+    float2* hi = lo + 256;
+    const unsigned nhi = (2 * M) / 256;
+    for (unsigned i = threadIdx.x; i < 256; i += blockDim.x) lo[i] = tw.lo[i];
+    for (unsigned i = threadIdx.x; i < nhi; i += blockDim.x) hi[i] = tw.hi[i];
+
+    const size_t row = blockIdx.x;
+    const size_t c = row / nseg, seg = row - c * nseg;
+    const float* src = x + c * x_pitch + seg * seg_stride;
+    for (unsigned n = threadIdx.x; n < M; n += blockDim.x)
+        s[n] = make_float2(src[2 * n], src[2 * n + 1]);
+    fft_smem<LOGM, false>(s, lo, hi);
+
+    float2* dst = X + row * bin_pitch;
+    for (unsigned k = threadIdx.x; k <= M; k += blockDim.x) {
+        const float2 zk = s[fft_pos<LOGM>(k & (M - 1))];
+        const float2 zm = s[fft_pos<LOGM>((M - k) & (M - 1))];
+        const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+        const float2 d = make_float2(zk.x - zm.x, zk.y + zm.y);  // zk - conj(zm)
+        const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);   // d / (2i)
+        const float2 w = (k == M) ? make_float2(-1.f, 0.f) : twiddle(lo, hi, k, false);
+        dst[k] = e + cmul(w, o);
+    }
+}
+
+template <int LOGM>
+__global__ void __launch_bounds__(512) fft_c2r_kernel(const float2* Y, size_t bin_pitch, size_t nseg,
+                                                      float* out, size_t out_stride, size_t keep,
+                                                      size_t out_len, TwiddleTable tw)
+{
+    constexpr unsigned M = 1u << LOGM;
+    extern __shared__ __align__(16) float2 s_fft[];
+    float2* s = s_fft;
+    float2* lo = s + M;
+    float2* hi = lo + 256;
+    const unsigned nhi = (2 * M) / 256;
+    for (unsigned i = threadIdx.x; i < 256; i += blockDim.x) lo[i] = tw.lo[i];
+    for (unsigned i = threadIdx.x; i < nhi; i += blockDim.x) hi[i] = tw.hi[i];
+    __syncthreads();
+
+    const size_t row = blockIdx.x;
+    const size_t dm = row / nseg, seg = row - dm * nseg;
+    const float2* src = Y + row * bin_pitch;
+    for (unsigned k = threadIdx.x; k < M; k += blockDim.x) {
+        float2 xk = src[k], xm = src[M - k];
+        if (k == 0) {  // the DC and Nyquist imaginary parts are ignored (C2R)
+            xk.y = 0.f;
+            xm.y = 0.f;
+        }
+        const float2 e = make_float2(0.5f * (xk.x + xm.x), 0.5f * (xk.y - xm.y));
+        const float2 d = make_float2(0.5f * (xk.x - xm.x), 0.5f * (xk.y + xm.y));
+        const float2 o = cmul(d, conjf2(twiddle(lo, hi, k, false)));
+        s[k] = make_float2(e.x - o.y, e.y + o.x);  // E + i O
+    }
+    fft_smem<LOGM, true>(s, lo, hi);
+
+    const float scale = 1.0f / (float)M;
+    float* dst = out + dm * out_stride;
+    const size_t o0 = seg * keep;
+    for (unsigned n = threadIdx.x; n < M; n += blockDim.x) {
+        const float2 z = s[fft_pos<LOGM>(n)];
+        const size_t i0 = 2 * (size_t)n, i1 = i0 + 1;
+        if (i0 < keep && o0 + i0 < out_len) dst[o0 + i0] = z.x * scale;
+        if (i1 < keep && o0 + i1 < out_len) dst[o0 + i1] = z.y * scale;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// unpack / transposes
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) fdd_unpack_kernel(const uint8_t* in, size_t in_stride,
+                                                         int in_nbits, size_t nsamps, size_t nchans,
+                                                         float scale, float* x, size_t x_pitch,
+                                                         size_t x_len)
+{
+    __shared__ float tile[32][33];
+    const size_t t0 = (size_t)blockIdx.x * 32, c0 = (size_t)blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+    for (int r = ty; r < 32; r += 8) {
+        const size_t t = t0 + r, c = c0 + tx;
+        float v = 0.f;
+        if (t < nsamps && c < nchans) {
+            if (in_nbits == 8) {
+                v = ((float)in[t * in_stride + c] - 127.5f) * scale;
+            } else {
+                const uint8_t* p = in + t * in_stride + 4 * c;
+                uint32_t u = (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) |
+                             ((uint32_t)p[3] << 24);
+                v = __uint_as_float(u) * scale;
+            }
+        }
+        tile[r][tx] = v;
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const size_t c = c0 + r, t = t0 + tx;
+        if (c < nchans && t < x_len) x[c * x_pitch + t] = tile[tx][r];
+    }
+}
+
+// X[c*nseg + seg][k] -> Xt[k][seg][j] for active channel j (km[j] applied).
+__global__ void __launch_bounds__(256) to_binmajor_kernel(const float2* X, size_t bin_pitch,
+                                                          size_t nseg, size_t nbins,
+                                                          const int32_t* chan, const float* km,
+                                                          int nact, float2* Xt)
+{
+    __shared__ float2 tile[32][33];
+    const size_t k0 = (size_t)blockIdx.x * 32;
+    const int j0 = blockIdx.y * 32;
+    const size_t seg = blockIdx.z;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int r = ty; r < 32; r += 8) {
+        const int j = j0 + r;
+        const size_t k = k0 + tx;
+        float2 v = make_float2(0.f, 0.f);
+        if (j < nact && k < nbins) {
+            v = X[((size_t)chan[j] * nseg + seg) * bin_pitch + k];
+            const float m = km[j];
+            v.x *= m;
+            v.y *= m;
+        }
+        tile[r][tx] = v;
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const size_t k = k0 + r;
+        const int j = j0 + tx;
+        if (k < nbins && j < nact) Xt[(k * nseg + seg) * nact + j] = tile[tx][r];
+    }
+}
+
+// Yt[k][seg][dm] -> Y[dm*nseg + seg][k]
+__global__ void __launch_bounds__(256) to_dmmajor_kernel(const float2* Yt, size_t nseg, size_t ndm,
+                                                         size_t nbins, float2* Y, size_t bin_pitch)
+{
+    __shared__ float2 tile[32][33];
+    const size_t k0 = (size_t)blockIdx.x * 32, d0 = (size_t)blockIdx.y * 32;
+    const size_t seg = blockIdx.z;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int r = ty; r < 32; r += 8) {
+        const size_t k = k0 + r, d = d0 + tx;
+        tile[r][tx] = (k < nbins && d < ndm) ? Yt[(k * nseg + seg) * ndm + d] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const size_t d = d0 + r, k = k0 + tx;
+        if (d < ndm && k < nbins) Y[(d * nseg + seg) * bin_pitch + k] = tile[tx][r];
+    }
+}
+
+// Yt[k][0][dm] -> out[dm][2k], out[dm][2k+1] for k < nspec
+__global__ void __launch_bounds__(256) spectrum_out_kernel(const float2* Yt, size_t ndm, size_t nspec,
+                                                           float* out, size_t out_stride)
+{
+    __shared__ float2 tile[32][33];
+    const size_t k0 = (size_t)blockIdx.x * 32, d0 = (size_t)blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int r = ty; r < 32; r += 8) {
+        const size_t k = k0 + r, d = d0 + tx;
+        tile[r][tx] = (k < nspec && d < ndm) ? Yt[k * ndm + d] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const size_t d = d0 + r, k = k0 + tx;
+        if (d < ndm && k < nspec) {
+            const float2 v = tile[tx][r];
+            out[d * out_stride + 2 * k] = v.x;
+            out[d * out_stride + 2 * k + 1] = v.y;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Plain FP32 phasor MAC: a complex GEMM per bin on CUDA cores.
+// Block tile: 64 DMs x 40 segments (thread tile 4 x 5), channel chunk 32.
+// ---------------------------------------------------------------------------
+constexpr int MAC_BM = 64, MAC_BN = 40, MAC_BK = 32, MAC_TM = 4, MAC_TN = 5;
+constexpr int MAC_THREADS = (MAC_BM / MAC_TM) * (MAC_BN / MAC_TN);  // 128
+
+__device__ __forceinline__ int fdd_delay(float dm, float delay, int round_delays)
+{
+    const float x = __fmul_rn(dm, delay);
+    return round_delays ? (int)__float2uint_rn(x) : __float2int_rz(x);
+}
+
+// exp(+2 pi i m / N) for 0 <= m < N
+__device__ __forceinline__ float2 phasor(const float2* lo, const float2* hi, unsigned m)
+{
+    return conjf2(cmul(hi[m >> 8], lo[m & 255]));
+}
+
+__device__ __forceinline__ unsigned phase_index(size_t k, int d, unsigned nfft, bool pow2)
+{
+    if (pow2) return (unsigned)((unsigned)k * (unsigned)d) & (nfft - 1u);
+    long long p = (long long)k * (long long)d % (long long)nfft;
+    if (p < 0) p += nfft;
+    return (unsigned)p;
+}
+
+__global__ void __launch_bounds__(MAC_THREADS) mac_plain_kernel(MacArgs a, int bins_per_block)
+{
+    extern __shared__ __align__(16) float2 s_mac[];
+    float2* As = s_mac;                        // [BK][BM]
+    float2* Bs = As + MAC_BK * MAC_BM;         // [BK][BN]
+    float2* lo = Bs + MAC_BK * MAC_BN;         // 256
+    float2* hi = lo + 256;                     // nfft / 256
+    const unsigned nhi = a.nfft / 256;
+    for (unsigned i = threadIdx.x; i < 256; i += blockDim.x) lo[i] = a.tw.lo[i];
+    for (unsigned i = threadIdx.x; i < nhi; i += blockDim.x) hi[i] = a.tw.hi[i];
+
+    const int tid = threadIdx.x;
+    const int tm = tid % (MAC_BM / MAC_TM), tn = tid / (MAC_BM / MAC_TM);
+    const int dm0 = blockIdx.x * MAC_BM;
+    const bool pow2 = (a.nfft & (a.nfft - 1u)) == 0;
+    // phasor generation: this thread owns DM (dm0 + tid % 64), channels
+    // tid/64 + 2i of each chunk
+    const int gdm = tid % MAC_BM, gk0 = tid / MAC_BM;
+    const float my_dm = a.dms[min(dm0 + gdm, a.ndm - 1)];
+
+    const size_t kb0 = (size_t)blockIdx.y * bins_per_block;
+    const size_t kb1 = min(a.nbins, kb0 + bins_per_block);
+    for (size_t k = kb0; k < kb1; ++k) {
+        for (int s0 = 0; s0 < a.nseg; s0 += MAC_BN) {
+            float2 acc[MAC_TM][MAC_TN];
+#pragma unroll
+            for (int i = 0; i < MAC_TM; ++i)
+#pragma unroll
+                for (int j = 0; j < MAC_TN; ++j) acc[i][j] = make_float2(0.f, 0.f);
+
+            for (int c0 = 0; c0 < a.nact; c0 += MAC_BK) {
+                __syncthreads();
+                for (int kc = gk0; kc < MAC_BK; kc += MAC_THREADS / MAC_BM) {
+                    const int j = c0 + kc;
+                    float2 w = make_float2(0.f, 0.f);
+                    if (j < a.nact) {
+                        const int d = fdd_delay(my_dm, a.delay_act[j], a.round_delays);
+                        w = phasor(lo, hi, phase_index(k, d, a.nfft, pow2));
+                    }
+                    As[kc * MAC_BM + gdm] = w;
+                }
+                for (int i = tid; i < MAC_BK * MAC_BN; i += MAC_THREADS) {
+                    const int kc = i / MAC_BN, sn = i - kc * MAC_BN;
+                    const int j = c0 + kc, seg = s0 + sn;
+                    Bs[kc * MAC_BN + sn] = (j < a.nact && seg < a.nseg)
+                                               ? a.Xt[(k * a.nseg + seg) * a.nact + j]
+                                               : make_float2(0.f, 0.f);
+                }
+                __syncthreads();
+#pragma unroll 4
+                for (int kc = 0; kc < MAC_BK; ++kc) {
+                    float2 av[MAC_TM], bv[MAC_TN];
+#pragma unroll
+                    for (int i = 0; i < MAC_TM; ++i) av[i] = As[kc * MAC_BM + tm + i * (MAC_BM / MAC_TM)];
+#pragma unroll
+                    for (int j = 0; j < MAC_TN; ++j) bv[j] = Bs[kc * MAC_BN + tn + j * (MAC_BN / MAC_TN)];
+#pragma unroll
+                    for (int i = 0; i < MAC_TM; ++i)
+#pragma unroll
+                        for (int j = 0; j < MAC_TN; ++j) {
+                            acc[i][j].x = fmaf(av[i].x, bv[j].x, acc[i][j].x);
+                            acc[i][j].x = fmaf(-av[i].y, bv[j].y, acc[i][j].x);
+                            acc[i][j].y = fmaf(av[i].x, bv[j].y, acc[i][j].y);
+                            acc[i][j].y = fmaf(av[i].y, bv[j].x, acc[i][j].y);
+                        }
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < MAC_TM; ++i) {
+                const int dm = dm0 + tm + i * (MAC_BM / MAC_TM);
+                if (dm >= a.ndm) continue;
+#pragma unroll
+                for (int j = 0; j < MAC_TN; ++j) {
+                    const int seg = s0 + tn + j * (MAC_BN / MAC_TN);
+                    if (seg < a.nseg) a.Yt[(k * a.nseg + seg) * a.ndm + dm] = acc[i][j];
+                }
+            }
+        }
+    }
+}
+
+template <int LOGM>
+void launch_r2c_n(const float* x, size_t x_pitch, size_t nchans, size_t nseg, size_t seg_stride,
+                  float2* X, size_t bin_pitch, const TwiddleTable& tw, cudaStream_t s)
+{
+    constexpr unsigned M = 1u << LOGM;
+    const size_t smem = (M + 256 + 2 * M / 256) * sizeof(float2);
+    RT_CHECK(cudaFuncSetAttribute(fft_r2c_kernel<LOGM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    const unsigned threads = M >= 8192 ? 512 : (M >= 1024 ? 256 : 128);
+    fft_r2c_kernel<LOGM><<<(unsigned)(nchans * nseg), threads, smem, s>>>(x, x_pitch, nseg,
+                                                                        seg_stride, X, bin_pitch, tw);
+    RT_CHECK(cudaGetLastError());
+}
+
+template <int LOGM>
+void launch_c2r_n(const float2* Y, size_t bin_pitch, size_t ndm, size_t nseg, float* out,
+                  size_t out_stride, size_t keep, size_t out_len, const TwiddleTable& tw,
+                  cudaStream_t s)
+{
+    constexpr unsigned M = 1u << LOGM;
+    const size_t smem = (M + 256 + 2 * M / 256) * sizeof(float2);
+    RT_CHECK(cudaFuncSetAttribute(fft_c2r_kernel<LOGM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    const unsigned threads = M >= 8192 ? 512 : (M >= 1024 ? 256 : 128);
+    fft_c2r_kernel<LOGM><<<(unsigned)(ndm * nseg), threads, smem, s>>>(Y, bin_pitch, nseg, out,
+                                                                      out_stride, keep, out_len, tw);
+    RT_CHECK(cudaGetLastError());
+}
+
+int log2_exact(int n)
+{
+    int l = 0;
+    while ((1 << l) < n) ++l;
+    return (1 << l) == n ? l : -1;
+}
+
+}  // namespace
+
+void launch_fdd_unpack(const uint8_t* in, size_t in_stride, int in_nbits, size_t nsamps,
+                       size_t nchans, float scale, float* x, size_t x_pitch, size_t x_len,
+                       cudaStream_t s)
+{
+    dim3 grid((unsigned)((x_len + 31) / 32), (unsigned)((nchans + 31) / 32));
+    fdd_unpack_kernel<<<grid, 256, 0, s>>>(in, in_stride, in_nbits, nsamps, nchans, scale, x,
+                                           x_pitch, x_len);
+    RT_CHECK(cudaGetLastError());
+}
+
+void launch_fft_r2c(const float* x, size_t x_pitch, size_t nchans, size_t nseg, size_t seg_stride,
+                    int nfft, float2* X, size_t bin_pitch, const TwiddleTable& tw, cudaStream_t s)
+{
+    switch (log2_exact(nfft)) {
+#define R2C(L) case L + 1: launch_r2c_n<L>(x, x_pitch, nchans, nseg, seg_stride, X, bin_pitch, tw, s); break;
+        R2C(4) R2C(5) R2C(6) R2C(7) R2C(8) R2C(9) R2C(10) R2C(11) R2C(12) R2C(13) R2C(14)
+#undef R2C
+    default: DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unsupported FFT length");
+    }
+}
+
+void launch_fft_c2r(const float2* Y, size_t bin_pitch, size_t ndm, size_t nseg, int nfft,
+                    float* out, size_t out_stride, size_t keep, size_t out_len,
+                    const TwiddleTable& tw, cudaStream_t s)
+{
+    switch (log2_exact(nfft)) {
+#define C2R(L) case L + 1: launch_c2r_n<L>(Y, bin_pitch, ndm, nseg, out, out_stride, keep, out_len, tw, s); break;
+        C2R(4) C2R(5) C2R(6) C2R(7) C2R(8) C2R(9) C2R(10) C2R(11) C2R(12) C2R(13) C2R(14)
+#undef C2R
+    default: DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unsupported FFT length");
+    }
+}
+
+void launch_fdd_to_binmajor(const float2* X, size_t bin_pitch, size_t nseg, size_t nbins,
+                            const int32_t* chan, const float* km, int nact, float2* Xt,
+                            cudaStream_t s)
+{
+    dim3 grid((unsigned)((nbins + 31) / 32), (unsigned)((nact + 31) / 32), (unsigned)nseg);
+    to_binmajor_kernel<<<grid, 256, 0, s>>>(X, bin_pitch, nseg, nbins, chan, km, nact, Xt);
+    RT_CHECK(cudaGetLastError());
+}
+
+void launch_fdd_to_dmmajor(const float2* Yt, size_t nseg, size_t ndm, size_t nbins, float2* Y,
+                           size_t bin_pitch, cudaStream_t s)
+{
+    dim3 grid((unsigned)((nbins + 31) / 32), (unsigned)((ndm + 31) / 32), (unsigned)nseg);
+    to_dmmajor_kernel<<<grid, 256, 0, s>>>(Yt, nseg, ndm, nbins, Y, bin_pitch);
+    RT_CHECK(cudaGetLastError());
+}
+
+void launch_fdd_spectrum_out(const float2* Yt, size_t ndm, size_t nspec, float* out,
+                             size_t out_stride, cudaStream_t s)
+{
+    dim3 grid((unsigned)((nspec + 31) / 32), (unsigned)((ndm + 31) / 32));
+    spectrum_out_kernel<<<grid, 256, 0, s>>>(Yt, ndm, nspec, out, out_stride);
+    RT_CHECK(cudaGetLastError());
+}
+
+void launch_fdd_mac_plain(const MacArgs& a, cudaStream_t s)
+{
+    const size_t smem = (MAC_BK * MAC_BM + MAC_BK * MAC_BN + 256 + a.nfft / 256) * sizeof(float2);
+    if (smem > 200 * 1024) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "FFT length too large for the MAC table");
+    RT_CHECK(cudaFuncSetAttribute(mac_plain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    const unsigned dm_tiles = (unsigned)((a.ndm + MAC_BM - 1) / MAC_BM);
+    // enough blocks to fill the GPU several times over
+    const size_t want_blocks = 148 * 8;
+    size_t bin_blocks = std::max<size_t>(1, want_blocks / dm_tiles);
+    bin_blocks = std::min(bin_blocks, a.nbins);
+    const int per = (int)((a.nbins + bin_blocks - 1) / bin_blocks);
+    bin_blocks = (a.nbins + per - 1) / per;
+    dim3 grid(dm_tiles, (unsigned)bin_blocks);
+    mac_plain_kernel<<<grid, MAC_THREADS, smem, s>>>(a, per);
+    RT_CHECK(cudaGetLastError());
+}
+
+}  // namespace kern
+}  // namespace dedisp

@@ -57,6 +57,8 @@ FDDGPUPlan::FDDGPUPlan(size_type nchans, float_type dt, float_type f0, float_typ
 FDDGPUPlan::~FDDGPUPlan() {}
 
 void FDDGPUPlan::set_options(const FddOptions& opt) { m_opt = opt; }
+void FDDGPUPlan::set_timing(bool enable) { m_engine->record_timing = enable; }
+ExecTiming FDDGPUPlan::last_timing() const { return m_engine->stats; }
 const FddOptions& FDDGPUPlan::get_options() const { return m_opt; }
 
 FDDGPUPlan::size_type FDDGPUPlan::output_row_length(size_type nsamps) const

@@ -198,9 +198,11 @@ template <int NBITS, int J, int NN>
 __device__ __forceinline__ void narrow_add(uint32_t (&n)[J][NN], int k, uint32_t v1, uint32_t v2)
 {
     if constexpr (NBITS == 8) {
+        // even bytes in place; odd bytes moved down into 16-bit lanes with
+        // one byte permute each (selector 0x4341: b1, 0, b3, 0)
         constexpr uint32_t M = 0x00FF00FFu;
         n[k][0] += (v1 & M) + (v2 & M);
-        n[k][1] += ((v1 >> 8) & M) + ((v2 >> 8) & M);
+        n[k][1] += __byte_perm(v1, 0u, 0x4341) + __byte_perm(v2, 0u, 0x4341);
     } else if constexpr (NBITS == 4) {
         constexpr uint32_t M = 0x0F0F0F0Fu;
         n[k][0] += (v1 & M) + (v2 & M);

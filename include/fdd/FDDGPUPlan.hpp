@@ -56,6 +56,9 @@ public:
      * under the current options. */
     size_type output_row_length(size_type nsamps) const;
 
+    void set_timing(bool enable) override;
+    ExecTiming last_timing() const override;
+
 private:
     FddOptions m_opt;
     std::unique_ptr<detail::FddEngine> m_engine;

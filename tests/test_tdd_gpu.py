@@ -181,8 +181,14 @@ def test_reference_gpu_plan_bit_exact(plan, nbits, nchans, out_nbits):
                             gulp_size=1 << 30)
     refout = raw.view(OUT_DTYPE[out_nbits]).reshape(len(dms), nout)
     orc = _oracle(packed, nsamps, nbits, params, dms, km, out_nbits, nout)
+    assert np.array_equal(ours.view(np.uint8), orc.view(np.uint8))
+    if plan == "tdd" and nbits == 32:
+        # Reference defect: TDDPlan's transpose_unpack has no 32-bit
+        # instantiation (src/tdd/unpack/unpack.cu:187-196), so no unpack
+        # kernel runs and the sums come out as zero.
+        assert np.all(refout == 0)
+        return
     assert np.array_equal(refout.view(np.uint8), orc.view(np.uint8))
-    assert np.array_equal(ours.view(np.uint8), refout.view(np.uint8))
 
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "ref_gpu_outputs.npz")
@@ -202,6 +208,9 @@ def test_golden_reference_outputs():
             km[::kme] = 0
         cls = dd.TDDPlan if plan == "tdd" else dd.DedispPlan
         ours, nout = _run(cls, inp, ns, nb, (nch, dt, f0, df), dms, onb, km=km)
+        if plan == "tdd" and nb == 32:  # reference defect, see above
+            assert not g[f"out_{k}"].any()
+            continue
         assert np.array_equal(ours.view(np.uint8).ravel(), g[f"out_{k}"]), k
 
 
