@@ -385,6 +385,156 @@ __global__ void __launch_bounds__(TiledGeom<NBITS>::NT, 1) dedisperse_tiled_kern
     }
 }
 
+// ---------------------------------------------------------------------------
+// K2 for 8-bit input: integer work balanced across the ALU and FMA pipes.
+//
+// The 32-bit integer ALU pipe issues at half the rate of the FMA pipe, and
+// the generic kernel keeps it ~80% busy (funnel shift, mask, byte permute,
+// 3-input add per word). Here:
+//   * each staged channel window is also stored shifted by 1, 2 and 3
+//     bytes (built once per stage, reused by all BD DMs), so a lane reads
+//     already-aligned words and no per-word funnel shift is needed;
+//   * the 16-bit-lane sums are accumulated with IMAD (multiplier `one` = 1,
+//     a kernel argument, so the multiply-add stays on the FMA pipe).
+// Per word and channel: 1 LOP (even bytes) + 1 PRMT (odd bytes) on the ALU
+// pipe, 2 IMAD on the FMA pipe.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t imad(uint32_t a, uint32_t b, uint32_t c)
+{
+    uint32_t d;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+
+__global__ void __launch_bounds__(TiledGeom<8>::NT, 1) dedisperse_tiled8_kernel(DedisperseArgs a,
+                                                                                uint32_t one)
+{
+    using G = TiledGeom<8>;
+    constexpr int J = G::J, R = G::R, BT = G::BT, DPW = G::DPW, BD = G::BD, NT = G::NT;
+    constexpr int FLP = Tiled<8>::FLP;
+
+    extern __shared__ __align__(16) uint32_t smem[];
+    const int W = a.win_words, CS = a.chan_per_stage;
+    const int CSW = CS * W;
+    uint32_t* s_win = smem;                        // [2][CS][W]   raw windows
+    uint32_t* s_shift = s_win + 2 * CSW;           // [3][CS][W]   shifted by 1..3 bytes
+    uint32_t* s_info = s_shift + 3 * CSW;          // [2][BD][CS]  word offset into smem
+    float* s_dm = reinterpret_cast<float*>(s_info + 2 * BD * CS);  // [BD]
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int i0 = blockIdx.x * BD;
+    const size_t t0 = (size_t)blockIdx.y * BT;
+    const int nvalid = min(BD, a.ndm - i0);
+    const float dm_first = a.dms[i0];
+    const float dm_last = a.dms[i0 + nvalid - 1];
+    if (tid < BD) s_dm[tid] = a.dms[i0 + min(tid, nvalid - 1)];
+    __syncthreads();
+
+    auto prep = [&](int stage, int buf) {
+        const int32_t* cl = a.chan_list + (size_t)stage * CS;
+        for (int j = warp; j < CS; j += TILED_NW) {
+            const int c = cl[j];
+            const float dl = a.delay_table[c];
+            const uint32_t lo = min(delay_rn(dm_first, dl), delay_rn(dm_last, dl));
+            const size_t A = ((t0 + lo) / 16) * 16;
+            const uint32_t* src = a.tr + (size_t)c * a.tr_pitch_words + A / 4;
+            uint32_t* dst = s_win + buf * CSW + j * W;
+            for (int k = lane * 4; k < W; k += 128) cp_async16(dst + k, src + k);
+        }
+        for (int idx = tid; idx < BD * CS; idx += NT) {
+            const int slot = idx / CS, j = idx - slot * CS;
+            const int c = cl[j];
+            const float dl = a.delay_table[c];
+            const uint32_t lo = min(delay_rn(dm_first, dl), delay_rn(dm_last, dl));
+            const size_t A = ((t0 + lo) / 16) * 16;
+            const uint32_t rel = (uint32_t)(t0 + delay_rn(s_dm[slot], dl) - A);
+            const uint32_t r = rel & 3u, q = rel >> 2;
+            const uint32_t base = r == 0 ? (uint32_t)(buf * CSW) : (uint32_t)(2 * CSW + (r - 1) * CSW);
+            s_info[(buf * BD + slot) * CS + j] = base + (uint32_t)(j * W) + q;
+        }
+    };
+
+    uint32_t acc[DPW][R];
+    uint32_t nar[DPW][J][2];
+#pragma unroll
+    for (int di = 0; di < DPW; ++di) {
+#pragma unroll
+        for (int k = 0; k < R; ++k) acc[di][k] = 0;
+#pragma unroll
+        for (int k = 0; k < J; ++k) nar[di][k][0] = nar[di][k][1] = 0;
+    }
+
+    prep(0, 0);
+    cp_async_commit();
+    int pairs = 0;
+    for (int s = 0; s < a.nstages; ++s) {
+        const int buf = s & 1;
+        asm volatile("cp.async.wait_group 0;\n" ::);
+        __syncthreads();
+        // shifted copies of this stage's windows (the last word of each
+        // shifted row is never read)
+        {
+            const uint32_t* src = s_win + buf * CSW;
+            for (int i = tid; i < CSW; i += NT) {
+                const int w = i % W;
+                if (w + 1 < W) {
+                    const uint32_t lo = src[i], hi = src[i + 1];
+                    s_shift[i] = __funnelshift_r(lo, hi, 8);
+                    s_shift[CSW + i] = __funnelshift_r(lo, hi, 16);
+                    s_shift[2 * CSW + i] = __funnelshift_r(lo, hi, 24);
+                }
+            }
+        }
+        __syncthreads();
+        if (s + 1 < a.nstages) prep(s + 1, buf ^ 1);
+        cp_async_commit();
+
+        const uint32_t* info = s_info + buf * BD * CS;
+        for (int j = 0; j < CS; j += 2) {
+#pragma unroll
+            for (int di = 0; di < DPW; ++di) {
+                const int slot = warp * DPW + di;
+                const uint32_t* p1 = smem + info[slot * CS + j] + lane * J;
+                const uint32_t* p2 = smem + info[slot * CS + j + 1] + lane * J;
+                uint32_t w1[J], w2[J];
+#pragma unroll
+                for (int k = 0; k < J; ++k) {
+                    w1[k] = p1[k];
+                    w2[k] = p2[k];
+                }
+#pragma unroll
+                for (int k = 0; k < J; ++k) {
+                    nar[di][k][0] = imad(w1[k] & 0x00FF00FFu, one, nar[di][k][0]);
+                    nar[di][k][0] = imad(w2[k] & 0x00FF00FFu, one, nar[di][k][0]);
+                    nar[di][k][1] = imad(__byte_perm(w1[k], 0u, 0x4341), one, nar[di][k][1]);
+                    nar[di][k][1] = imad(__byte_perm(w2[k], 0u, 0x4341), one, nar[di][k][1]);
+                }
+            }
+            if (++pairs == FLP) {
+#pragma unroll
+                for (int di = 0; di < DPW; ++di) narrow_flush<8, J, 2, R>(nar[di], acc[di]);
+                pairs = 0;
+            }
+        }
+    }
+#pragma unroll
+    for (int di = 0; di < DPW; ++di) narrow_flush<8, J, 2, R>(nar[di], acc[di]);
+
+#pragma unroll
+    for (int di = 0; di < DPW; ++di) {
+        const int slot = warp * DPW + di;
+        if (slot >= nvalid) continue;
+        const int row = a.perm ? a.perm[i0 + slot] : i0 + slot;
+        const size_t base = (size_t)row * a.out_stride;
+        const size_t tl = t0 + (size_t)lane * R;
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const size_t t = tl + k;
+            if (t < a.nsamp_out) store_out(a.out, base + t, a.out_nbits, acc[di][k], a.den, a.factor);
+        }
+    }
+}
+
 template <int NBITS>
 void launch_tiled_n(const DedisperseArgs& a, cudaStream_t s)
 {
@@ -394,13 +544,14 @@ void launch_tiled_n(const DedisperseArgs& a, cudaStream_t s)
     static size_t configured[64] = {};
     int dev = 0;
     RT_CHECK(cudaGetDevice(&dev));
+    auto kfn = (NBITS == 8) ? (void*)dedisperse_tiled8_kernel : (void*)dedisperse_tiled_kernel<NBITS>;
     if (dev < 0 || dev >= 64 || smem > configured[dev]) {
-        RT_CHECK(cudaFuncSetAttribute(dedisperse_tiled_kernel<NBITS>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        RT_CHECK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         if (dev >= 0 && dev < 64) configured[dev] = smem;
     }
     dim3 grid((a.ndm + G::BD - 1) / G::BD, (unsigned)((a.nsamp_out + G::BT - 1) / G::BT));
-    dedisperse_tiled_kernel<NBITS><<<grid, G::NT, smem, s>>>(a);
+    if constexpr (NBITS == 8) dedisperse_tiled8_kernel<<<grid, G::NT, smem, s>>>(a, 1u);
+    else dedisperse_tiled_kernel<NBITS><<<grid, G::NT, smem, s>>>(a);
     RT_CHECK(cudaGetLastError());
 }
 
@@ -465,7 +616,9 @@ int tiled_lane_words(int nbits)
 size_t tiled_smem_bytes(int nbits, int win_words, int chan_per_stage)
 {
     const size_t bd = (size_t)tiled_block_dms(nbits);
-    return (2ull * chan_per_stage * win_words + 2ull * bd * chan_per_stage + bd) * 4ull;
+    // 8-bit: two raw buffers plus three byte-shifted copies per stage
+    const size_t windows = nbits == 8 ? 5ull : 2ull;
+    return (windows * chan_per_stage * win_words + 2ull * bd * chan_per_stage + bd) * 4ull;
 }
 
 size_t tiled_max_smem_bytes() { return 200 * 1024; }

@@ -91,13 +91,16 @@ GPU_CASES = [
     ("dedisp", 128, 1581.8, -1.5625, 250e-6, 8192, 8, 32, 32, 200.0, 7, 17),
     ("dedisp", 256, 1500.0, -0.5, 64e-6, 6000, 2, 16, 20, 150.0, 0, 18),
 ]
-# The reference FDD kernel is only launched for channel batches of
-# 1/16/32/64/128/256 (FDDKernel.cu:79-87, batch = min(nchans/4, 64)) and
-# touches a popped DM job when ndm is a multiple of its DM batch
-# (FDDGPUPlan.cpp:352-368), so the cases use nchans 64/128 and ndm 18/14.
+# The reference whole-series FDD runs its forward FFT nchan_batch/64 times
+# (FDDGPUPlan.cpp:114-115,486-494, batch = min(nchans/4, 64)), i.e. never for
+# fewer than 256 channels; its phasor kernel is only launched for channel
+# batches of 1/16/32/64/128/256 (FDDKernel.cu:79-87); and it touches a popped
+# DM job when ndm is a multiple of its DM batch (FDDGPUPlan.cpp:352-368). The
+# cases therefore use 256 channels (whole series), 128 (segmented, fixed batch
+# of 32) and ndm 18 / 14.
 FDD_CASES = [
     # (nchans, f0, df, dt, nsamps, ndm, dm_max, segmented, seed)
-    ("fdd", 64, 1581.8, -3.125, 250e-6, 12000, 18, 60.0, 0, 21),
+    ("fdd", 256, 1581.8, -0.78125, 250e-6, 12000, 18, 60.0, 0, 21),
     ("fdd", 128, 1581.8, -1.5625, 250e-6, 40000, 14, 80.0, 1, 22),
 ]
 
