@@ -56,6 +56,34 @@ dedisp_error dedisp_b200_set_fdd_options(dedisp_plan plan, int segmented, int ti
  * state the roofline of the integer-bound TDD kernel. */
 dedisp_error dedisp_b200_alu_probe(int device, double* lane_adds_per_s);
 
+/* Allocation-free time-domain dedispersion. No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc -- real-time pipelines that forbid
+ * allocation once started (an allocation can block on the driver for an
+ * unbounded time), or processes whose device memory belongs to another
+ * allocator.
+ * Computes what a DEDISP_TDD plan with DEDISP_DEVICE_POINTERS computes (same
+ * bit-exact output) for a plan described by (nchans, dt, f0, df), the host
+ * DM list and killmask (NULL: all channels; values must be 0 or 1), reading
+ * d_in (device, time-major, in_stride bytes per sample) and writing d_out
+ * (device, dm_count rows of out_stride bytes), then waits for `stream`.
+ *
+ * It allocates no device memory: its scratch is a fixed 64 MiB array in the
+ * library (plus small tables for up to 16384 DMs and 8192 channels), held by
+ * every GPU that loads the library until the process exits. Requests whose
+ * channel-major copy, (nchans + 1) x (nsamps rounded up + padding) samples,
+ * does not fit are rejected with DEDISP_MEM_ALLOC_FAILED. The first call on
+ * a device looks up the arrays' device addresses (cudaGetSymbolAddress) and
+ * should therefore come before any stream capture on that device. All calls
+ * share the scratch: calls that overlap on the GPU race. On failure,
+ * dedisp_b200_noalloc_last_message() describes the reason. */
+dedisp_error dedisp_b200_tdd_execute_noalloc(
+    dedisp_size nchans, dedisp_float dt, dedisp_float f0, dedisp_float df,
+    const dedisp_float* dm_list, dedisp_size dm_count, const dedisp_bool* killmask,
+    dedisp_size nsamps, const dedisp_byte* d_in, dedisp_size in_nbits, dedisp_size in_stride,
+    dedisp_byte* d_out, dedisp_size out_nbits, dedisp_size out_stride, void* stream);
+const char* dedisp_b200_noalloc_last_message(void);
+
 /* Floats per DM row that execute() writes for nsamps input samples. */
 dedisp_size dedisp_b200_output_row_length(dedisp_plan plan, dedisp_size nsamps);
 
