@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fdd", action="store_true")
+    ap.add_argument("--fdd-only", action="store_true",
+                    help="run only the FDD forms (config 2) and print their JSON object")
     ap.add_argument("--profile-case", default="",
                     help="run one small case for ncu and exit: tdd (the TDD workload with "
                          "2^17 samples) or fdd (config-2 geometry with 2^18 samples)")
@@ -174,6 +177,119 @@ class Clocks:
 
 
 # ---------------------------------------------------------------------------
+# FDD forms (plain FP32 CUDA-core MAC vs 3xBF16 tensor-core MAC)
+# ---------------------------------------------------------------------------
+
+def delay_table_f32(nchans, dt, f0, df):
+    """The plan's per-channel delay table, in the same float32 operation order
+    (df forced negative; a = 1/(f0 + c df); (float)(4.15e3/dt * (a^2 - b^2)))."""
+    f0 = np.float32(f0)
+    df = -np.abs(np.float32(df))
+    c = np.arange(nchans, dtype=np.float32)
+    a = np.float32(1.0) / (f0 + c * df)
+    b = np.float32(1.0) / f0
+    diff = a * a - b * b
+    return (4.15e3 / np.float64(np.float32(dt)) * diff.astype(np.float64)).astype(np.float32)
+
+
+def fdd_fp64_rows(x_tc, delays, dms, nout):
+    """Dedispersed time series in float64 for a few DMs: sum_c x[c][t + d],
+    d = trunc(float32(dm * delay[c])) (the FDD plan's delay rule); x_tc is
+    the unpacked input [nsamps][nchans] (float32, already scaled)."""
+    out = np.zeros((len(dms), nout), np.float64)
+    for i, dm in enumerate(dms):
+        d = np.trunc(np.float32(dm) * delays).astype(np.int64)
+        for c in range(x_tc.shape[1]):
+            out[i] += x_tc[d[c]:d[c] + nout, c]
+    return out
+
+
+def run_fdd(args, local, world, stream, max_over_ranks):
+    """Config 2: 1024 ch, 2^20 float32 samples, 2048 DMs over 0-1000,
+    segmented with 2^15-sample FFTs. Both MAC forms, device-resident, with
+    their error against float64 on a DM subset."""
+    import torch
+    import dedisp_tests_b200 as dd
+    from dedisp_tests_b200 import synthetic as sy
+    cfg = sy.config2()
+    d_in = sy.make_input_torch(cfg, device=f"cuda:{local}")
+    # float64 check on 4 DMs over the first 2^17 output samples
+    h_in = d_in.cpu().numpy().view(np.float32).reshape(cfg.nsamps, cfg.nchans)
+    scale = np.float32(1.0 / cfg.nchans)
+    delays = delay_table_f32(cfg.nchans, cfg.dt, cfg.f_top, cfg.df)
+    dm_list = np.asarray(cfg.dm_list, np.float32)
+    rows = np.array([1, 700, 1400, 2047])
+    n_chk = 1 << 17
+    x_tc = None
+    out = {}
+    for name, prec in (("fdd_fp32_plain", 0), ("fdd_bf16x3_tc", 1)):
+        p = dd.FDDGPUPlan(cfg.nchans, cfg.dt, cfg.f_top, cfg.df, local)
+        p.set_dm_list(dm_list)
+        p.set_options(segmented=1, precision=prec, segment_nfft=1 << 15)
+        p.set_stream(stream.cuda_stream)
+        p.set_timing(True)
+        ndm, md = p.get_dm_count(), p.get_max_delay()
+        nout = p.output_row_length(cfg.nsamps)
+        d_out = torch.empty((ndm, nout), dtype=torch.float32, device=f"cuda:{local}")
+        for _ in range(max(1, min(args.warmup, 2))):
+            p.execute(cfg.nsamps, d_in, 32, d_out, 32, dd.DEDISP_DEVICE_POINTERS)
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        kms, launches = [], 0
+        steps = max(1, min(args.steps, 3))
+        ev0.record(stream)
+        for _ in range(steps):
+            p.execute(cfg.nsamps, d_in, 32, d_out, 32, dd.DEDISP_DEVICE_POINTERS)
+            t = p.get_timing()
+            kms.append(t["kernel_ms"])
+            launches += t["launches"]
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(ev0.elapsed_time(ev1)) / steps
+        mac_ms = sum(kms) / len(kms)
+        units = ndm * nout
+        nseg = -(-cfg.nsamps // ((1 << 15) - md))
+        nbins = (1 << 15) // 2 + 1
+        cmac = float(ndm) * cfg.nchans * nseg * nbins
+        if x_tc is None:
+            x_tc = h_in[: n_chk + md] * scale
+            ref = fdd_fp64_rows(x_tc, delays, dm_list[rows], n_chk)
+        got = d_out[torch.as_tensor(rows, device=d_out.device), :n_chk].double().cpu().numpy()
+        rel = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+        mx = float(np.abs(got - ref).max() / np.abs(ref).max())
+        if prec == 0:
+            roof = {"bound": "fp32-fma", "flop": 8 * cmac,
+                    "achieved_TFLOPs": round(8 * cmac / (mac_ms * 1e-3) / 1e12, 2),
+                    "note": "8 real flops per complex MAC on CUDA cores"}
+        else:
+            peak = measured_peaks().get("bf16_tflops")
+            ach = 24 * cmac / (mac_ms * 1e-3) / 1e12
+            roof = {"bound": "tensor", "flop": 24 * cmac, "achieved_TFLOPs": round(ach, 2),
+                    "peak_TFLOPs": peak, "frac": round(ach / peak, 4) if peak else None,
+                    "note": "3 bf16 real GEMMs [ndm x 2nact] x [2nact x 2nseg] per bin"}
+        out[name] = {"value": units * world / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+                     "mac_ms": mac_ms, "launches_per_step": launches / steps,
+                     "rel_l2_vs_fp64": rel, "max_abs_vs_fp64": mx,
+                     "error_sample": f"DMs {rows.tolist()} x first {n_chk} samples",
+                     "roofline": roof, "ndm": ndm, "nseg": nseg, "nfft": 1 << 15,
+                     "max_delay": md}
+        del d_out, p
+        torch.cuda.empty_cache()
+    del d_in
+    torch.cuda.empty_cache()
+    return out
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+# ---------------------------------------------------------------------------
 # our implementation
 # ---------------------------------------------------------------------------
 
@@ -203,8 +319,16 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    cfg = sy.config1(nbits=args.nbits)
     stream = torch.cuda.current_stream()
+    if args.fdd_only:
+        fdd = run_fdd(args, local, world, stream, max_over_ranks)
+        if rank == 0:
+            print(json.dumps({"fdd": fdd}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    cfg = sy.config1(nbits=args.nbits)
 
     def make_plan(kernel=0):
         p = dd.TDDPlan(cfg.nchans, cfg.dt, cfg.f_top, cfg.df, local)
@@ -352,6 +476,14 @@ def run_ours(args):
     if not args.no_cpu and world == 1:
         cpu, _ = time_cpu_oracle(cfg, plan.get_dm_list(), md)
 
+    # --- FDD forms (config 2) -------------------------------------------------------
+    fdd = None
+    if not args.no_fdd:
+        del plan, d_in
+        d_out = None
+        torch.cuda.empty_cache()
+        fdd = run_fdd(args, local, world, stream, max_over_ranks)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -365,6 +497,7 @@ def run_ours(args):
                        "parallelism": f"replicas x{world}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches * world, "clocks": clocks, "variants": variants,
+            "fdd": fdd,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "fdd_kernels.hpp"
+#include "fdd_tc.hpp"
 #include "host_math.hpp"
 
 namespace dedisp {
@@ -20,9 +21,15 @@ size_t round_up(size_t a, size_t b) { return (a + b - 1) / b * b; }
 
 struct FddEngine::Impl {
     rt::DeviceBuffer in, x, X, Xt, Yt, Y, out, tw_lo, tw_hi, dms, chan, km, delay_act;
+    // tensor-core form
+    rt::DeviceBuffer B, delay_pad, qtable, err;
+    unsigned qtable_n = 0;
+    int delay_pad_n = -1;
     unsigned tw_n = 0;
     unsigned long version = ~0ul;
+    unsigned long pad_version = ~0ul;
     int nact = 0;
+    std::vector<float> delays_active;
 };
 
 FddEngine::FddEngine(GpuState& gpu) : m_gpu(gpu), m_impl(new Impl()) {}
@@ -77,8 +84,11 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
         RT_CHECK(cudaMemcpy(m.km.get(), km.data(), n * 4, cudaMemcpyHostToDevice));
         RT_CHECK(cudaMemcpy(m.delay_act.get(), dl.data(), n * 4, cudaMemcpyHostToDevice));
         RT_CHECK(cudaMemcpy(m.dms.get(), v.dms, ndm * 4, cudaMemcpyHostToDevice));
+        m.delays_active.assign(dl.begin(), dl.begin() + m.nact);
         m.version = v.version;
     }
+    const bool use_tc = opt.precision == FddPrecision::BF16x3 &&
+                        kern::tc_supported((int)nseg, (unsigned)g.nfft, m.nact);
     // Twiddles W_N^t = exp(-2 pi i t / N) as hi[t >> 8] * lo[t & 255].
     if (m.tw_n != g.nfft) {
         const unsigned n = (unsigned)g.nfft;
@@ -108,7 +118,30 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
     }
     m.x.reserve(nchans * x_len * sizeof(float));
     m.X.reserve(nchans * nseg * bin_pitch * sizeof(float2));
-    m.Xt.reserve(nbins * nseg * std::max(1, m.nact) * sizeof(float2));
+    int nact_pad = 0, npad = 0;
+    if (use_tc) {
+        nact_pad = kern::tc_pad_channels(m.nact);
+        npad = kern::tc_pad_n((int)nseg);
+        m.B.reserve(kern::tc_b_bytes(nbins, nact_pad, npad));
+        if (m.pad_version != v.version || m.delay_pad_n != nact_pad) {
+            std::vector<float> dp(m.delays_active);
+            dp.resize(nact_pad, 0.f);
+            m.delay_pad.reserve(dp.size() * 4);
+            RT_CHECK(cudaMemcpy(m.delay_pad.get(), dp.data(), dp.size() * 4, cudaMemcpyHostToDevice));
+            m.pad_version = v.version;
+            m.delay_pad_n = nact_pad;
+        }
+        if (m.qtable_n != g.nfft) {
+            const std::vector<uint2> t = kern::tc_quarter_table((unsigned)g.nfft);
+            m.qtable.reserve(t.size() * sizeof(uint2));
+            RT_CHECK(cudaMemcpy(m.qtable.get(), t.data(), t.size() * sizeof(uint2),
+                                cudaMemcpyHostToDevice));
+            m.qtable_n = (unsigned)g.nfft;
+        }
+        m.err.reserve(sizeof(unsigned));
+    } else {
+        m.Xt.reserve(nbins * nseg * std::max(1, m.nact) * sizeof(float2));
+    }
     m.Yt.reserve(nbins * nseg * ndm * sizeof(float2));
     const bool inverse = g.timeseries;
     if (inverse) m.Y.reserve(ndm * nseg * bin_pitch * sizeof(float2));
@@ -134,12 +167,32 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
                             x_len, x_len, st);
     kern::launch_fft_r2c(m.x.get<float>(), x_len, nchans, nseg, seg_stride, (int)g.nfft,
                          m.X.get<float2>(), bin_pitch, tw, st);
-    if (m.nact > 0)
+    if (use_tc)
+        kern::launch_fdd_prep_b(m.X.get<float2>(), bin_pitch, (int)nseg, nbins, m.chan.get<int32_t>(),
+                                m.km.get<float>(), m.nact, nact_pad, npad, m.B.get(), st);
+    else if (m.nact > 0)
         kern::launch_fdd_to_binmajor(m.X.get<float2>(), bin_pitch, nseg, nbins, m.chan.get<int32_t>(),
                                      m.km.get<float>(), m.nact, m.Xt.get<float2>(), st);
     if (e1) e1->record(st);
 
-    if (m.nact > 0) {
+    if (use_tc) {
+        RT_CHECK(cudaMemsetAsync(m.err.get(), 0, sizeof(unsigned), st));
+        kern::TcMacArgs ta;
+        ta.Yt = m.Yt.get<float2>();
+        ta.dms = m.dms.get<float>();
+        ta.delay_act = m.delay_pad.get<float>();
+        ta.table = m.qtable.get<uint2>();
+        ta.err = m.err.get<unsigned>();
+        ta.nact_pad = nact_pad;
+        ta.ndm = (int)ndm;
+        ta.nseg = (int)nseg;
+        ta.npad = npad;
+        ta.nbins = nbins;
+        ta.nfft = (unsigned)g.nfft;
+        ta.round_delays = opt.round_delays ? 1 : 0;
+        kern::launch_fdd_mac_tc(ta, m.B.get(), st);
+        stats.launches = 1;
+    } else if (m.nact > 0) {
         kern::MacArgs a;
         a.Xt = m.Xt.get<float2>();
         a.Yt = m.Yt.get<float2>();
@@ -173,8 +226,13 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
     if (!dev)
         RT_CHECK(cudaMemcpyAsync(c.out, d_out, ndm * g.row_len * sizeof(float),
                                  cudaMemcpyDeviceToHost, st));
-    const bool async = dev && (c.flags & DEDISP_ASYNC);
+    const bool async = dev && (c.flags & DEDISP_ASYNC) && !use_tc;
     if (!async) RT_CHECK(cudaStreamSynchronize(st));
+    if (use_tc) {
+        unsigned err = 0;
+        RT_CHECK(cudaMemcpy(&err, m.err.get(), sizeof(err), cudaMemcpyDeviceToHost));
+        if (err) DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "tensor-core MAC pipeline wait expired");
+    }
     if (record_timing) {
         RT_CHECK(cudaEventSynchronize(*e3));
         float pre = 0.f, mac = 0.f, post = 0.f;
@@ -183,7 +241,7 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
         RT_CHECK(cudaEventElapsedTime(&post, *e2, *e3));
         stats.prep_ms = pre + post;
         stats.kernel_ms = mac;
-        stats.variant = (int)opt.precision;
+        stats.variant = use_tc ? 1 : 0;
     }
 }
 

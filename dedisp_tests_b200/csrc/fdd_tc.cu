@@ -1,0 +1,555 @@
+// FDD phasor multiply-accumulate on the 5th-generation tensor cores
+// (tcgen05, sm_100a) as a 3xBF16 complex GEMM per frequency bin.
+//
+// For bin k, with C real and the complex product written out,
+//   Yr[dm][s] = sum_c  Pr(dm,c) Xr(c,s) - Pi(dm,c) Xi(c,s)
+//   Yi[dm][s] = sum_c  Pr(dm,c) Xi(c,s) + Pi(dm,c) Xr(c,s)
+// is the real GEMM  D[m][n] = sum_kk A[m][kk] B[kk][n]  with
+//   A[m][2c] = Pr, A[m][2c+1] = Pi                        (M = DMs, K = 2*nact)
+//   B[2c][n] = Xr(c,n), B[2c+1][n] = -Xi(c,n)             (n <  nseg)
+//   B[2c][n] = Xi(c,s), B[2c+1][n] =  Xr(c,s), s = n-nseg (n >= nseg)
+// and each operand is split into BF16 hi + lo parts:
+//   D = Ah Bh + Ah Bl + Al Bh   (FP32 accumulation in tensor memory).
+//
+// Roles (one CTA per SM, 128 DMs per CTA, a range of bins per CTA):
+//   warps 0-7   phasor producers: each thread owns one DM row (its TMEM
+//               lane) and half of every 64-channel chunk; phasors come from
+//               the exact integer phase index (k*d) mod nfft and a quarter-
+//               wave table of pre-split BF16 (cos, sin) pairs, and are stored
+//               into tensor memory as the A operand; the same warps read the
+//               accumulator of each finished bin and write Yt[k][s][dm].
+//   warp 8      TMA producer for the B chunks (pre-split BF16, 128B swizzle).
+//   warp 9      TMEM allocation and the single-thread MMA issuer.
+// Every wait on an mbarrier is bounded; on expiry the kernel records an
+// error code and winds down without waiting further.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+#include "fdd_tc.hpp"
+#include "runtime.hpp"
+
+namespace dedisp {
+namespace kern {
+namespace {
+
+constexpr int TC_M = 128;              // DMs per CTA (accumulator lanes)
+constexpr int TC_CHUNK = 64;           // channels per K chunk (K = 128 reals)
+constexpr int TC_STAGES = 3;           // B pipeline depth (smem: 3 x 40 KB + table)
+constexpr int TC_PRODUCER_WARPS = 8;
+constexpr int TC_THREADS = (TC_PRODUCER_WARPS + 2) * 32;
+// Bounded mbarrier waits: give up after TC_WAIT_NS of global time (checked
+// every 16 polls) or TC_WAIT_POLLS polls, whichever comes first.
+constexpr uint64_t TC_WAIT_NS = 2000000000ull;
+constexpr uint32_t TC_WAIT_POLLS = 1u << 28;
+// Dynamic shared memory requested per CTA is at least this much so that only
+// one CTA fits on an SM (each CTA allocates all 512 tensor-memory columns).
+constexpr size_t TC_MIN_SMEM = 120 * 1024;
+constexpr size_t TC_MAX_SMEM = 227 * 1024;
+
+// TMEM column map (512 allocated): A buffers (hi 64 + lo 64 columns) x 2,
+// accumulators x 2.
+constexpr uint32_t TM_A0 = 0, TM_A1 = 128, TM_C0 = 256, TM_C1 = 384;
+
+struct alignas(8) SmemBarriers {
+    uint64_t b_full[TC_STAGES];
+    uint64_t b_empty[TC_STAGES];
+    uint64_t a_full[2];
+    uint64_t a_empty[2];
+    uint64_t c_full[2];
+    uint64_t c_empty[2];
+    uint64_t drain;
+    uint32_t tmem_base;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* b)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait for phase `parity` of barrier b; false if the limit expired.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity)
+{
+    const uint32_t addr = smem_u32(b);
+    uint64_t t0 = 0;
+    for (uint32_t i = 0; i < TC_WAIT_POLLS; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((i & 15u) == 15u) {
+            const uint64_t t = global_ns();
+            if (t0 == 0) t0 = t;
+            else if (t - t0 > TC_WAIT_NS) return false;
+        }
+    }
+    return false;
+}
+
+// The same wait for a whole warp, with one outcome for all its lanes (the
+// tensor-memory loads and stores that follow are warp-collective).
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* b, uint32_t parity)
+{
+    const bool done = mbar_wait(b, parity);
+    return __all_sync(0xFFFFFFFFu, done);
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tma_load_4d(void* smem, const CUtensorMap* map, uint64_t* bar,
+                                            int c0, int c1, int c2, int c3)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5, %6}], [%2];" ::"r"(smem_u32(smem)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t desc_b,
+                                       uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(desc_b), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+// 32 consecutive 32-bit columns of this thread's lane.
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32])
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+        "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
+        "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]),
+        "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]),
+        "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]),
+        "r"(v[29]), "r"(v[30]), "r"(v[31]));
+}
+
+__device__ __forceinline__ float tmem_ld1(uint32_t taddr)
+{
+    uint32_t r;
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
+    return __uint_as_float(r);
+}
+
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart (SBO), LBO unused (1), descriptor version 1.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ int tc_delay(float dm, float delay, int round_delays)
+{
+    const float x = __fmul_rn(dm, delay);
+    return round_delays ? (int)__float2uint_rn(x) : __float2int_rz(x);
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 1)
+fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
+{
+    extern __shared__ __align__(1024) uint8_t smem_dyn[];
+    // layout (from a 1024-byte aligned base, as the 128-byte swizzle needs):
+    // [B stages][barriers][quarter-wave table][delays][sym]
+    uint8_t* smem_raw = smem_dyn + ((1024u - (smem_u32(smem_dyn) & 1023u)) & 1023u);
+    const uint32_t npad = (uint32_t)a.npad;
+    const uint32_t atom_bytes = npad * 128u;           // one 64-kk atom of one split
+    const uint32_t stage_bytes = 4u * atom_bytes;      // hi/lo x 2 atoms
+    uint8_t* s_b = smem_raw;
+    SmemBarriers* bars = reinterpret_cast<SmemBarriers*>(smem_raw + TC_STAGES * stage_bytes);
+    uint2* s_table = reinterpret_cast<uint2*>(reinterpret_cast<uint8_t*>(bars) + 256);
+    const uint32_t qn = a.nfft / 4;                    // quarter-wave entries (+1)
+    float* s_delay = reinterpret_cast<float*>(s_table + (qn + 1));
+    uint2* s_sym = reinterpret_cast<uint2*>(s_delay + a.nact_pad);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int ntiles = (a.ndm + TC_M - 1) / TC_M;
+    const int tile = blockIdx.x % ntiles, group = blockIdx.x / ntiles;
+    const int ngroups = gridDim.x / ntiles;
+    if (group >= ngroups) return;  // whole CTA leaves before touching barriers
+    const size_t k_begin = a.nbins * (size_t)group / ngroups;
+    const size_t k_end = a.nbins * (size_t)(group + 1) / ngroups;
+    const int nchunks = a.nact_pad / TC_CHUNK;
+
+    // --- set-up -------------------------------------------------------------
+    for (uint32_t i = tid; i <= qn; i += blockDim.x) s_table[i] = a.table[i];
+    for (int i = tid; i < a.nact_pad; i += blockDim.x) s_delay[i] = a.delay_act[i];
+    if (tid < 4) {
+        // quadrant q of exp(+i theta): (re, im) = R^q (c, s); in packed
+        // bf16x2 (re low half, im high half): selector swaps halves,
+        // mask flips sign bits.
+        const uint32_t sel[4] = {0x3210u, 0x1032u, 0x3210u, 0x1032u};
+        const uint32_t neg[4] = {0u, 0x00008000u, 0x80008000u, 0x80000000u};
+        s_sym[tid] = make_uint2(sel[tid], neg[tid]);
+    }
+    if (tid == 0) {
+        for (int i = 0; i < TC_STAGES; ++i) {
+            mbar_init(&bars->b_full[i], 1);
+            mbar_init(&bars->b_empty[i], 1);
+        }
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&bars->a_full[i], TC_PRODUCER_WARPS * 32);
+            mbar_init(&bars->a_empty[i], 1);
+            mbar_init(&bars->c_full[i], 1);
+            mbar_init(&bars->c_empty[i], TC_PRODUCER_WARPS * 32);
+        }
+        mbar_init(&bars->drain, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == TC_PRODUCER_WARPS + 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
+                         smem_u32(&bars->tmem_base)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = bars->tmem_base;
+    bool ok = true;
+
+    if (warp < TC_PRODUCER_WARPS) {
+        // --- phasor producers + epilogue ------------------------------------
+        const int quad = warp & 3, half = warp >> 2;
+        const int m = tile * TC_M + quad * 32 + lane;          // this thread's DM row
+        const float dm = a.dms[min(m, a.ndm - 1)];
+        const uint32_t lane_addr = (uint32_t)(quad * 32) << 16;
+        const uint32_t nmask = a.nfft - 1u, qshift = (uint32_t)(31 - __clz((int)qn));
+        uint32_t g = 0;  // global chunk counter
+        int bin_iter = 0;
+        for (size_t k = k_begin; k < k_end && ok; ++k, ++bin_iter) {
+            for (int ch = 0; ch < nchunks && ok; ++ch, ++g) {
+                const uint32_t buf = g & 1u;
+                if (!mbar_wait_warp(&bars->a_empty[buf], ((g >> 1) & 1u) ^ 1u)) { ok = false; break; }
+                tc_fence_after();
+                uint32_t hi[32], lo[32];
+                const int c0 = ch * TC_CHUNK + half * 32;
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    const int d = tc_delay(dm, s_delay[c0 + i], a.round_delays);
+                    const uint32_t idx = ((uint32_t)k * (uint32_t)d) & nmask;
+                    const uint32_t q = idx >> qshift, r = idx & (qn - 1u);
+                    const uint2 t = s_table[r];
+                    const uint2 sy = s_sym[q];
+                    hi[i] = __byte_perm(t.x, 0u, sy.x) ^ sy.y;
+                    lo[i] = __byte_perm(t.y, 0u, sy.x) ^ sy.y;
+                }
+                const uint32_t acol = buf ? TM_A1 : TM_A0;
+                tmem_st32(tmem + lane_addr + acol + half * 32, hi);
+                tmem_st32(tmem + lane_addr + acol + 64 + half * 32, lo);
+                tmem_wait_st();
+                tc_fence_before();
+                mbar_arrive(&bars->a_full[buf]);
+            }
+            if (!ok) break;
+            // epilogue of bin k: accumulator buffer bin_iter & 1
+            const uint32_t cb = (uint32_t)bin_iter & 1u;
+            if (!mbar_wait_warp(&bars->c_full[cb], ((uint32_t)bin_iter >> 1) & 1u)) { ok = false; break; }
+            tc_fence_after();
+            const uint32_t ccol = cb ? TM_C1 : TM_C0;
+            const int sh = (a.nseg + 1) / 2;
+            const int s0 = half * sh, s1 = min(a.nseg, s0 + sh);
+            for (int s = s0; s < s1; ++s) {
+                const float yr = tmem_ld1(tmem + lane_addr + ccol + s);
+                const float yi = tmem_ld1(tmem + lane_addr + ccol + a.nseg + s);
+                tmem_wait_ld();
+                if (m < a.ndm) a.Yt[(k * a.nseg + s) * a.ndm + m] = make_float2(yr, yi);
+            }
+            tc_fence_before();
+            mbar_arrive(&bars->c_empty[cb]);
+        }
+    } else if (warp == TC_PRODUCER_WARPS) {
+        // --- TMA producer ------------------------------------------------------
+        if (lane == 0) {
+            uint32_t g = 0;
+            for (size_t k = k_begin; k < k_end && ok; ++k) {
+                for (int ch = 0; ch < nchunks; ++ch, ++g) {
+                    const uint32_t st = g % TC_STAGES;
+                    if (!mbar_wait(&bars->b_empty[st], ((g / TC_STAGES) & 1u) ^ 1u)) { ok = false; break; }
+                    mbar_expect_tx(&bars->b_full[st], stage_bytes);
+                    uint8_t* dst = s_b + st * stage_bytes;
+                    // coordinates: (kk, n, split, bin)
+                    for (int sp = 0; sp < 2; ++sp)
+                        for (int at = 0; at < 2; ++at)
+                            tma_load_4d(dst + (sp * 2 + at) * atom_bytes, &bmap, &bars->b_full[st],
+                                        ch * 128 + at * 64, 0, sp, (int)k);
+                }
+            }
+            // do not leave while loads are in flight: wait for the last stages
+            const uint32_t issued = g;
+            for (uint32_t j = (issued > TC_STAGES ? issued - TC_STAGES : 0); j < issued; ++j)
+                mbar_wait(&bars->b_full[j % TC_STAGES], (j / TC_STAGES) & 1u);
+        }
+    } else {
+        // --- MMA issuer ----------------------------------------------------------
+        if (lane == 0) {
+            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((npad >> 3) << 17) |
+                                   ((uint32_t)(TC_M >> 4) << 24);
+            uint32_t g = 0;
+            int bin_iter = 0;
+            for (size_t k = k_begin; k < k_end && ok; ++k, ++bin_iter) {
+                const uint32_t cb = (uint32_t)bin_iter & 1u;
+                if (!mbar_wait(&bars->c_empty[cb], (((uint32_t)bin_iter >> 1) & 1u) ^ 1u)) { ok = false; break; }
+                tc_fence_after();
+                const uint32_t dcol = tmem + (cb ? TM_C1 : TM_C0);
+                for (int ch = 0; ch < nchunks; ++ch, ++g) {
+                    const uint32_t buf = g & 1u, st = g % TC_STAGES;
+                    if (!mbar_wait(&bars->a_full[buf], (g >> 1) & 1u)) { ok = false; break; }
+                    if (!mbar_wait(&bars->b_full[st], (g / TC_STAGES) & 1u)) { ok = false; break; }
+                    tc_fence_after();
+                    const uint32_t acol = tmem + (buf ? TM_A1 : TM_A0);
+                    const uint32_t bbase = smem_u32(s_b + st * stage_bytes);
+#pragma unroll
+                    for (int s = 0; s < 8; ++s) {
+                        const uint32_t at = (uint32_t)s >> 2, sub = (uint32_t)s & 3u;
+                        const uint64_t bh = sw128_desc(bbase + (0 * 2 + at) * atom_bytes + sub * 32);
+                        const uint64_t bl = sw128_desc(bbase + (1 * 2 + at) * atom_bytes + sub * 32);
+                        const uint32_t ah = acol + s * 8, al = acol + 64 + s * 8;
+                        const uint32_t first = (ch == 0 && s == 0) ? 0u : 1u;
+                        mma_ts(dcol, ah, bh, idesc, first);
+                        mma_ts(dcol, ah, bl, idesc, 1u);
+                        mma_ts(dcol, al, bh, idesc, 1u);
+                    }
+                    mma_commit(&bars->a_empty[buf]);
+                    mma_commit(&bars->b_empty[st]);
+                }
+                if (!ok) break;
+                mma_commit(&bars->c_full[cb]);
+            }
+            // all issued MMAs complete before the accumulator memory goes away
+            mma_commit(&bars->drain);
+            mbar_wait(&bars->drain, 0);
+        }
+    }
+    if (!ok) atomicExch(a.err, 1u);
+
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == TC_PRODUCER_WARPS + 1) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
+    }
+}
+
+__device__ __forceinline__ uint32_t bf16x2_bits(float lo_half, float hi_half)
+{
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo_half, hi_half);  // .x low, .y high
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// B operand from the spectra: Bsplit[k][split][n][kk] bf16, n < npad,
+// kk < 2*nact_pad (hi = bf16(v), lo = bf16(v - hi)); killmask applied.
+// Element pairs (kk = 2j, 2j+1) are written as one 32-bit word.
+__global__ void __launch_bounds__(256) fdd_prep_b_kernel(const float2* X, size_t bin_pitch, int nseg,
+                                                         size_t nbins, const int32_t* chan,
+                                                         const float* km, int nact, int nact_pad,
+                                                         int npad, uint32_t* B)
+{
+    // one block per (bin tile of 32, channel tile of 32), looping over n
+    __shared__ float2 tile[32][33];
+    const size_t k0 = (size_t)blockIdx.x * 32;
+    const int j0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const size_t words_row = (size_t)nact_pad;  // 2*nact_pad bf16 per row
+    // padding rows n in [2*nseg, npad) are zero
+    for (int r = ty; r < 32; r += 8) {
+        const size_t k = k0 + r;
+        const int j = j0 + tx;
+        if (k >= nbins || j >= nact_pad) continue;
+        for (int n = 2 * nseg; n < npad; ++n)
+            for (int sp = 0; sp < 2; ++sp) B[((k * 2 + sp) * npad + n) * words_row + j] = 0u;
+    }
+    for (int s = 0; s < nseg; ++s) {
+        __syncthreads();
+        for (int r = ty; r < 32; r += 8) {
+            const int j = j0 + r;
+            const size_t k = k0 + tx;
+            float2 v = make_float2(0.f, 0.f);
+            if (j < nact && k < nbins) {
+                v = X[((size_t)chan[j] * nseg + s) * bin_pitch + k];
+                v.x *= km[j];
+                v.y *= km[j];
+            }
+            tile[r][tx] = v;
+        }
+        __syncthreads();
+        for (int r = ty; r < 32; r += 8) {
+            const size_t k = k0 + r;
+            const int j = j0 + tx;
+            if (k >= nbins || j >= nact_pad) continue;
+            const float2 v = tile[tx][r];
+            // real-output column s: (Xr, -Xi); imaginary-output column
+            // nseg + s: (Xi, Xr); element 2j in the low half, 2j+1 high
+            const float vals[2][2] = {{v.x, -v.y}, {v.y, v.x}};
+#pragma unroll
+            for (int part = 0; part < 2; ++part) {
+                const int n = part * nseg + s;
+                const float a0 = vals[part][0], a1 = vals[part][1];
+                const float h0 = __bfloat162float(__float2bfloat16_rn(a0));
+                const float h1 = __bfloat162float(__float2bfloat16_rn(a1));
+                B[((k * 2 + 0) * npad + n) * words_row + j] = bf16x2_bits(h0, h1);
+                B[((k * 2 + 1) * npad + n) * words_row + j] = bf16x2_bits(a0 - h0, a1 - h1);
+            }
+        }
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        RT_CHECK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        if (!p || q != cudaDriverEntryPointSuccess)
+            DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "cuTensorMapEncodeTiled unavailable");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+}  // namespace
+
+size_t tc_b_bytes(size_t nbins, int nact_pad, int npad)
+{
+    return nbins * 2 * (size_t)npad * 2 * (size_t)nact_pad * sizeof(__nv_bfloat16);
+}
+
+int tc_pad_channels(int nact) { return ((nact + TC_CHUNK - 1) / TC_CHUNK) * TC_CHUNK; }
+int tc_pad_n(int nseg) { return ((2 * nseg + 15) / 16) * 16; }
+bool tc_supported(int nseg, unsigned nfft, int nact)
+{
+    if (2 * nseg > 128 || nfft < 256 || (nfft & (nfft - 1)) != 0 || nact <= 0) return false;
+    return tc_smem_bytes(nfft, tc_pad_channels(nact), tc_pad_n(nseg)) <= TC_MAX_SMEM;
+}
+
+void launch_fdd_prep_b(const float2* X, size_t bin_pitch, int nseg, size_t nbins,
+                       const int32_t* chan, const float* km, int nact, int nact_pad, int npad,
+                       void* B, cudaStream_t s)
+{
+    // every word of B is written (zeros for padding rows and channels)
+    dim3 grid((unsigned)((nbins + 31) / 32), (unsigned)((nact_pad + 31) / 32));
+    fdd_prep_b_kernel<<<grid, 256, 0, s>>>(X, bin_pitch, nseg, nbins, chan, km, nact, nact_pad, npad,
+                                           static_cast<uint32_t*>(B));
+    RT_CHECK(cudaGetLastError());
+}
+
+std::vector<uint2> tc_quarter_table(unsigned nfft)
+{
+    // exp(+2 pi i r / nfft), r = 0..nfft/4, split into bf16 hi + lo parts
+    // (re in the low half of each packed word, im in the high half).
+    auto bf16_bits = [](double x) -> uint32_t {
+        const float f = (float)x;
+        uint32_t u;
+        std::memcpy(&u, &f, 4);
+        const uint32_t rounding = 0x7FFFu + ((u >> 16) & 1u);  // round to nearest even
+        return ((u + rounding) >> 16) & 0xFFFFu;
+    };
+    auto bf16_val = [](uint32_t b) -> double {
+        const uint32_t u = b << 16;
+        float f;
+        std::memcpy(&f, &u, 4);
+        return (double)f;
+    };
+    const unsigned qn = nfft / 4;
+    std::vector<uint2> t(qn + 1);
+    for (unsigned r = 0; r <= qn; ++r) {
+        const double th = 2.0 * 3.14159265358979323846 * (double)r / (double)nfft;
+        const double c = std::cos(th), s = std::sin(th);
+        const uint32_t ch = bf16_bits(c), sh = bf16_bits(s);
+        const uint32_t cl = bf16_bits(c - bf16_val(ch)), sl = bf16_bits(s - bf16_val(sh));
+        t[r] = make_uint2(ch | (sh << 16), cl | (sl << 16));
+    }
+    return t;
+}
+
+size_t tc_smem_bytes(unsigned nfft, int nact_pad, int npad)
+{
+    const size_t stage = 4ull * (size_t)npad * 128ull;
+    const size_t need = 1024 /* base alignment */ + TC_STAGES * stage + 256 +
+                        ((size_t)nfft / 4 + 1) * 8 + (size_t)nact_pad * 4 + 4 * 8;
+    return std::max(need, TC_MIN_SMEM);
+}
+
+void launch_fdd_mac_tc(const TcMacArgs& a, const void* B, cudaStream_t s)
+{
+    // Tensor map over Bsplit[bin][split][n][kk]: dims (kk, n, split, bin).
+    CUtensorMap map;
+    const cuuint64_t dims[4] = {(cuuint64_t)(2 * a.nact_pad), (cuuint64_t)a.npad, 2,
+                                (cuuint64_t)a.nbins};
+    const cuuint64_t strides[3] = {(cuuint64_t)(2 * a.nact_pad) * 2,
+                                   (cuuint64_t)(2 * a.nact_pad) * 2 * a.npad,
+                                   (cuuint64_t)(2 * a.nact_pad) * 2 * a.npad * 2};
+    const cuuint32_t box[4] = {64, (cuuint32_t)a.npad, 1, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(B),
+                                   dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                   CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "cuTensorMapEncodeTiled failed");
+    const size_t smem = tc_smem_bytes(a.nfft, a.nact_pad, a.npad);
+    RT_CHECK(cudaFuncSetAttribute(fdd_mac_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    int sms = 148;
+    int dev = 0;
+    RT_CHECK(cudaGetDevice(&dev));
+    RT_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int ntiles = (a.ndm + TC_M - 1) / TC_M;
+    int ngroups = std::max(1, sms / ntiles);
+    ngroups = (int)std::min<size_t>((size_t)ngroups, a.nbins);
+    fdd_mac_tc_kernel<<<ntiles * ngroups, TC_THREADS, smem, s>>>(map, a);
+    RT_CHECK(cudaGetLastError());
+}
+
+}  // namespace kern
+}  // namespace dedisp

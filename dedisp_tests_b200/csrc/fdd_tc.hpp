@@ -1,0 +1,49 @@
+// Launch interface of the tensor-core (tcgen05, 3xBF16) FDD phasor MAC.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include <cuda_bf16.h>
+
+namespace dedisp {
+namespace kern {
+
+struct TcMacArgs {
+    float2* Yt;                // [nbins][nseg][ndm]
+    const float* dms;
+    const float* delay_act;    // nact_pad entries (padding channels 0)
+    const uint2* table;        // quarter-wave table, nfft/4 + 1 entries
+    unsigned* err;             // set to 1 if a bounded wait expired
+    int nact_pad;              // channels, multiple of 64
+    int ndm;
+    int nseg;
+    int npad;                  // 2*nseg rounded up to 16
+    size_t nbins;
+    unsigned nfft;             // power of two
+    int round_delays;
+};
+
+// Shapes the tensor-core MAC handles: 2*nseg <= 128 output columns, a
+// power-of-two nfft >= 256, and its shared-memory footprint within a CTA.
+bool tc_supported(int nseg, unsigned nfft, int nact);
+int tc_pad_channels(int nact);
+int tc_pad_n(int nseg);
+size_t tc_b_bytes(size_t nbins, int nact_pad, int npad);
+size_t tc_smem_bytes(unsigned nfft, int nact_pad, int npad);
+std::vector<uint2> tc_quarter_table(unsigned nfft);
+
+// X [nchans*nseg][bin_pitch] complex spectra -> B operand
+// Bsplit[bin][hi|lo][n < npad][kk < 2*nact_pad] (bf16).
+void launch_fdd_prep_b(const float2* X, size_t bin_pitch, int nseg, size_t nbins,
+                       const int32_t* chan, const float* km, int nact, int nact_pad, int npad,
+                       void* B, cudaStream_t s);
+
+void launch_fdd_mac_tc(const TcMacArgs& a, const void* B, cudaStream_t s);
+
+}  // namespace kern
+}  // namespace dedisp

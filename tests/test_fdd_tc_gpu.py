@@ -1,0 +1,93 @@
+"""FDD with the tensor-core (tcgen05, 3xBF16) phasor MAC against the FP64
+oracle, through the C ABI.
+
+The 3xBF16 form splits phasors and spectra into BF16 hi + lo parts and
+accumulates hi*hi + hi*lo + lo*hi in FP32. Its representation error is about
+2^-16 of each operand, so the stated bound on the dedispersed output is
+rel-L2 <= 1e-5 against FP64 (max-abs, relative to max |ref|, <= 1e-4).
+"""
+import numpy as np
+import pytest
+
+from tests.test_fdd_gpu import _delays, _errs, _input, _oracle_x, _plan
+from oracle import pyoracle as po
+
+pytestmark = pytest.mark.gpu
+
+TC_REL_L2 = 1e-5
+TC_MAX_ABS = 1e-4
+
+
+def _run(p, nsamps, inp, in_nbits, ndm):
+    p.set_timing(True)
+    row = p.output_row_length(nsamps)
+    out = np.zeros((ndm, row), np.float32)
+    p.execute(nsamps, inp, in_nbits, out, 32)
+    assert p.get_timing()["variant"] == 1, "tensor-core MAC did not run"
+    return out
+
+
+def test_tc_whole_series_spectrum_small():
+    """One DM tile, one segment: N = 16384, 64 channels (one K chunk)."""
+    nchans, nsamps = 64, 12000
+    inp, params = _input(nchans, nsamps, 5)
+    dms = np.linspace(0, 60, 18, dtype=np.float32)
+    p = _plan(params, dms, segmented=0, precision=1)
+    out = _run(p, nsamps, inp, 8, len(dms))
+    nfft = out.shape[1]
+    x = _oracle_x(inp, nsamps, params, 8)
+    ref = po.fdd_spectrum(x, _delays(params), np.ones(nchans, np.int32), dms, nfft)
+    rel, mx = _errs(out, ref)
+    print("tc spectrum", rel, mx)
+    assert rel < TC_REL_L2 and mx < TC_MAX_ABS, (rel, mx)
+
+
+@pytest.mark.parametrize("in_nbits", [8, 32])
+def test_tc_segmented_timeseries(in_nbits):
+    """Several segments, padded channel count (96 -> 128), 200 DMs (two tiles)."""
+    nchans, nsamps = 96, 90000
+    inp, params = _input(nchans, nsamps, 3, float_input=(in_nbits == 32))
+    dms = np.linspace(0, 120, 200, dtype=np.float32)
+    p = _plan(params, dms, segmented=1, precision=1)
+    nout = nsamps - p.get_max_delay()
+    out = _run(p, nsamps, inp, in_nbits, len(dms))
+    assert out.shape[1] == nout
+    x = _oracle_x(inp, nsamps, params, in_nbits)
+    ref = po.fdd_timeseries(x, _delays(params), np.ones(nchans, np.int32), dms, nout)
+    rel, mx = _errs(out, ref)
+    print("tc segmented", in_nbits, rel, mx)
+    assert rel < TC_REL_L2 and mx < TC_MAX_ABS, (rel, mx)
+
+
+def test_tc_killmask_rounding_matches_plain():
+    """Killmask and round-half-even delays; the tensor-core and FP32 forms
+    agree with each other and with the oracle."""
+    nchans, nsamps = 128, 14000
+    inp, params = _input(nchans, nsamps, 7)
+    dms = np.linspace(0, 90, 131, dtype=np.float32)
+    km = np.ones(nchans, np.int32)
+    km[3::7] = 0
+    x = _oracle_x(inp, nsamps, params, 8)
+    for rnd in (False, True):
+        p = _plan(params, dms, km=km, segmented=0, timeseries=True, round_delays=rnd, precision=1)
+        out = _run(p, nsamps, inp, 8, len(dms))
+        nout = nsamps - p.get_max_delay()
+        ref = po.fdd_timeseries(x, _delays(params), km, dms, nout, round_delays=rnd)
+        rel, mx = _errs(out[:, :nout], ref)
+        print("tc killmask", rnd, rel, mx)
+        assert rel < TC_REL_L2 and mx < TC_MAX_ABS, (rnd, rel, mx)
+        q = _plan(params, dms, km=km, segmented=0, timeseries=True, round_delays=rnd, precision=0)
+        plain = np.zeros_like(out)
+        q.execute(nsamps, inp, 8, plain, 32)
+        rel2, _ = _errs(out, plain)
+        assert rel2 < TC_REL_L2, rel2
+
+
+def test_tc_repeat_is_deterministic():
+    nchans, nsamps = 64, 30000
+    inp, params = _input(nchans, nsamps, 9)
+    dms = np.linspace(0, 50, 140, dtype=np.float32)
+    p = _plan(params, dms, segmented=1, precision=1)
+    a = _run(p, nsamps, inp, 8, len(dms))
+    b = _run(p, nsamps, inp, 8, len(dms))
+    assert np.array_equal(a, b)
