@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fdd", action="store_true")
+    ap.add_argument("--tile-variant", type=int, default=-1,
+                    help="tiled-kernel tile shape for 8-bit input (-1: time all, use the fastest)")
     ap.add_argument("--fdd-only", action="store_true",
                     help="run only the FDD forms (config 2) and print their JSON object")
     ap.add_argument("--profile-case", default="",
@@ -73,6 +75,7 @@ def profile_case(args):
         cfg = sy.config1(nbits=args.nbits, nsamps=1 << 17)
         p = dd.TDDPlan(cfg.nchans, cfg.dt, cfg.f_top, cfg.df)
         p.generate_dm_list(*cfg.dm_gen)
+        p.set_tile_variant(max(args.tile_variant, 0))
         nbits = args.nbits
     else:
         cfg = sy.config2(nsamps=1 << 18)
@@ -349,6 +352,20 @@ def run_ours(args):
     def step(p, nbits=args.nbits, inp=d_in):
         p.execute(cfg.nsamps, inp, nbits, d_out, 32, flags)
 
+    # --- tile shape: pick the fastest tiled-kernel variant on this workload ---
+    tune = {}
+    if args.nbits == 8 and args.tile_variant < 0:
+        plan.set_timing(True)
+        for v in range(dd.tdd_variant_count(8)):
+            plan.set_tile_variant(v)
+            step(plan)
+            step(plan)
+            tune[v] = plan.get_timing()["kernel_ms"]
+        best = min(tune, key=tune.get)
+    else:
+        best = max(args.tile_variant, 0)
+    plan.set_tile_variant(best)
+
     # --- value: device-resident ---------------------------------------------
     plan.set_timing(True)
     for _ in range(args.warmup):
@@ -454,6 +471,7 @@ def run_ours(args):
                 torch.cuda.empty_cache()
                 hp = dd.TDDPlan(cfg.nchans, cfg.dt, cfg.f_top, cfg.df, local)
                 hp.generate_dm_list(*cfg.dm_gen)
+                hp.set_tile_variant(best)
                 hp.execute(cfg.nsamps, h_in, args.nbits, h_out, 32)  # warm-up
                 torch.cuda.synchronize()
                 barrier()
@@ -497,6 +515,7 @@ def run_ours(args):
                        "parallelism": f"replicas x{world}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches * world, "clocks": clocks, "variants": variants,
+            "tile_variant": {"chosen": best, "k2_ms_by_variant": tune},
             "fdd": fdd,
         }
         print(json.dumps(line), flush=True)

@@ -108,6 +108,8 @@ def lib() -> C.CDLL:
                                       C.c_uint]),
         "dedisp_sync": (err, []),
         "dedisp_b200_set_tdd_kernel": (err, [_vp, C.c_int]),
+        "dedisp_b200_set_tdd_variant": (err, [_vp, C.c_int]),
+        "dedisp_b200_tdd_variant_count": (C.c_int, [_sz]),
         "dedisp_b200_set_stream": (err, [_vp, _vp]),
         "dedisp_b200_set_timing": (err, [_vp, C.c_int]),
         "dedisp_b200_get_timing": (err, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float),
@@ -268,6 +270,10 @@ class DedispPlan(Plan):
         """0 auto, 1 plain (one thread per sample pair), 2 tiled."""
         _check(lib().dedisp_b200_set_tdd_kernel(self._h, kernel))
 
+    def set_tile_variant(self, variant: int) -> None:
+        """Tile shape of the tiled kernel for 8-bit input (same sums)."""
+        _check(lib().dedisp_b200_set_tdd_variant(self._h, variant))
+
 
 class TDDPlan(DedispPlan):
     """Time-domain dedispersion (reference src/tdd/TDDPlan.hpp)."""
@@ -282,3 +288,8 @@ class FDDGPUPlan(Plan):
                     round_delays: bool = False, segment_nfft: int = 0) -> None:
         _check(lib().dedisp_b200_set_fdd_options(self._h, segmented, int(timeseries),
                                                  precision, int(round_delays), segment_nfft))
+
+
+def tdd_variant_count(in_nbits: int = 8) -> int:
+    """Number of tile-shape variants of the tiled TDD kernel for in_nbits."""
+    return int(lib().dedisp_b200_tdd_variant_count(in_nbits))

@@ -15,6 +15,7 @@
 #include "dedisp/DedispPlan.hpp"
 #include "dedisp_b200.h"
 #include "errors.hpp"
+#include "tdd_kernels.hpp"
 #include "fdd/FDDGPUPlan.hpp"
 #include "fdd_engine.hpp"
 #include "gpu_state.hpp"
@@ -278,6 +279,20 @@ dedisp_error dedisp_b200_set_tdd_kernel(dedisp_plan plan, int kernel)
     if (auto* d = as_dedisp(plan)) { d->set_kernel(k); return DEDISP_NO_ERROR; }
     if (auto* t = as_tdd(plan)) { t->set_kernel(k); return DEDISP_NO_ERROR; }
     return DEDISP_INVALID_PLAN;
+}
+
+dedisp_error dedisp_b200_set_tdd_variant(dedisp_plan plan, int variant)
+{
+    if (!plan) return DEDISP_INVALID_PLAN;
+    if (variant < 0 || variant >= dedisp::kern::tiled_variant_count(8)) return DEDISP_UNKNOWN_ERROR;
+    if (auto* d = as_dedisp(plan)) { d->set_tile_variant(variant); return DEDISP_NO_ERROR; }
+    if (auto* t = as_tdd(plan)) { t->set_tile_variant(variant); return DEDISP_NO_ERROR; }
+    return DEDISP_INVALID_PLAN;
+}
+
+int dedisp_b200_tdd_variant_count(dedisp_size in_nbits)
+{
+    return dedisp::kern::tiled_variant_count((int)in_nbits);
 }
 
 dedisp_error dedisp_b200_set_stream(dedisp_plan plan, void* cuda_stream)

@@ -161,9 +161,9 @@ extern "C" dedisp_error dedisp_b200_tdd_execute_noalloc(
     }
     const int nbits = (int)in_nbits;
     const size_t spw = 32 / nbits;
-    const size_t bd = (size_t)kern::tiled_block_dms(nbits);
-    const size_t bt = (size_t)kern::tiled_block_samples(nbits);
-    const size_t J = (size_t)kern::tiled_lane_words(nbits);
+    const size_t bd = (size_t)kern::tiled_block_dms(nbits, 0);
+    const size_t bt = (size_t)kern::tiled_block_samples(nbits, 0);
+    const size_t J = (size_t)kern::tiled_lane_words(nbits, 0);
     uint32_t span = 0;
     for (size_t t = 0; t < dm_count; t += bd) {
         const float f = dms[t], l = dms[std::min(t + bd, (size_t)dm_count) - 1];
@@ -174,8 +174,7 @@ extern "C" dedisp_error dedisp_b200_tdd_execute_noalloc(
         }
     }
     const size_t win = round_up((span + 4 * spw - 1) / spw + 32 * J + 1, 4);
-    int cs = 32;
-    while (cs >= 2 && kern::tiled_smem_bytes(nbits, (int)win, cs) > kern::tiled_max_smem_bytes()) cs -= 2;
+    const int cs = kern::tiled_stage_channels(nbits, (int)win, 0);
     if (cs < 2) return fail(DEDISP_UNKNOWN_ERROR, "DM spacing too wide for the tiled kernel");
     const int nstages = std::max(1, (nact + cs - 1) / cs);
     if ((size_t)nstages * cs > kMaxChans + kListPad)

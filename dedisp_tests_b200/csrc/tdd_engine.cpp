@@ -24,6 +24,7 @@ struct TddEngine::Setup {
     size_t first = ~(size_t)0, count = ~(size_t)0;
     int nbits = -1;
     TddKernel kernel = TddKernel::Auto;
+    int variant = -1;
 
     bool tiled = false;
     int nact = 0;
@@ -58,8 +59,9 @@ rt::Event& TddEngine::event(size_t i)
 void TddEngine::prepare(const TddView& v, const TddCall& c)
 {
     Setup& s = *m_setup;
+    const int eff_variant = c.in_nbits == 8 ? variant : 0;  // other widths have one shape
     if (s.version == v.version && s.first == c.first_dm && s.count == c.dm_count &&
-        s.nbits == c.in_nbits && s.kernel == kernel)
+        s.nbits == c.in_nbits && s.kernel == kernel && s.variant == eff_variant)
         return;
 
     Setup n;
@@ -68,6 +70,7 @@ void TddEngine::prepare(const TddView& v, const TddCall& c)
     n.count = c.dm_count;
     n.nbits = c.in_nbits;
     n.kernel = kernel;
+    n.variant = eff_variant;
 
     // Active channels (killmask != 0) and their multipliers. The reference
     // multiplies every sample by its killmask value (dedisperse_kernel.cuh:
@@ -108,9 +111,9 @@ void TddEngine::prepare(const TddView& v, const TddCall& c)
 
     n.tiled = (kernel != TddKernel::Plain) && !general;
     if (n.tiled) {
-        const int bd = kern::tiled_block_dms(c.in_nbits);
+        const int bd = kern::tiled_block_dms(c.in_nbits, n.variant);
         const int spw = 32 / c.in_nbits;
-        const int J = kern::tiled_lane_words(c.in_nbits);
+        const int J = kern::tiled_lane_words(c.in_nbits, n.variant);
         uint32_t span = 0;
         for (size_t t = 0; t < c.dm_count; t += bd) {
             const float f = n.dms[t], l = n.dms[std::min(t + bd, (size_t)c.dm_count) - 1];
@@ -122,11 +125,8 @@ void TddEngine::prepare(const TddView& v, const TddCall& c)
         }
         const size_t w = (span + 4 * (size_t)spw - 1) / spw + 32 * (size_t)J + 1;
         n.win_words = (int)round_up(w, 4);
-        int cs = 32;
-        while (cs >= 2 && kern::tiled_smem_bytes(c.in_nbits, n.win_words, cs) >
-                              kern::tiled_max_smem_bytes())
-            cs -= 2;
-        if (cs < 2 || w > ((size_t)1 << 26)) {
+        const int cs = w > ((size_t)1 << 26) ? 0 : kern::tiled_stage_channels(c.in_nbits, n.win_words, n.variant);
+        if (cs < 2) {
             n.tiled = false;
         } else {
             n.chan_per_stage = cs;
@@ -181,7 +181,7 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
     if (dev_out && c.out_stride % ob != 0)
         DD_THROW_MSG(DEDISP_INVALID_STRIDE, "device output stride must be a multiple of the sample size");
 
-    const size_t bt = s.tiled ? (size_t)kern::tiled_block_samples(nbits) : 16;
+    const size_t bt = s.tiled ? (size_t)kern::tiled_block_samples(nbits, s.variant) : 16;
     const size_t win = s.tiled ? (size_t)s.win_words : 0;
 
     // Gulp size: the user cap, the grid limit, then device memory.
@@ -224,7 +224,7 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
     const float factor = 3.f * 1024.f / 255.f / 16.f;
 
     // Groups of DM slots whose output rows are contiguous (D2H overlap).
-    const size_t bd = s.tiled ? (size_t)kern::tiled_block_dms(nbits) : 32;
+    const size_t bd = s.tiled ? (size_t)kern::tiled_block_dms(nbits, s.variant) : 32;
     const size_t ntile = (ndm + bd - 1) / bd;
     const size_t ngroups = (!dev_out && s.identity) ? std::min<size_t>(kMaxOutGroups, ntile) : 1;
 
@@ -312,6 +312,7 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
             da.factor = factor;
             da.win_words = s.win_words;
             da.chan_per_stage = s.chan_per_stage;
+            da.variant = s.variant;
             if (s.identity) {
                 da.perm = nullptr;
                 da.out = out_base + s0 * out_elems_stride * ob;

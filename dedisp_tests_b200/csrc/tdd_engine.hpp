@@ -63,6 +63,7 @@ public:
 
     size_t gulp_size = kDefaultGulp;
     TddKernel kernel = TddKernel::Auto;
+    int variant = 0;  // tile-shape variant of the tiled kernel (8-bit input)
     bool record_timing = false;
     TddStats stats;
 

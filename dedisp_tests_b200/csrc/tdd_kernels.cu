@@ -166,13 +166,15 @@ template <int NBITS>
 struct Tiled;
 // J: words per lane (odd); DPW: DMs per warp; FLP: channel pairs per narrow
 // flush (narrow lane capacity / (2 * max sample)).
-template <> struct Tiled<8>  { static constexpr int J = 5, DPW = 2, NN = 2, FLP = 128; };
-template <> struct Tiled<4>  { static constexpr int J = 3, DPW = 2, NN = 2, FLP = 8; };
-template <> struct Tiled<2>  { static constexpr int J = 1, DPW = 2, NN = 4, FLP = 42; };
-template <> struct Tiled<1>  { static constexpr int J = 1, DPW = 1, NN = 8, FLP = 127; };
-template <> struct Tiled<16> { static constexpr int J = 7, DPW = 2, NN = 1, FLP = 0; };
-template <> struct Tiled<32> { static constexpr int J = 7, DPW = 2, NN = 1, FLP = 0; };
-constexpr int TILED_NW = 16;
+// NW: warps per block. The 8-bit kernel runs 32 warps of one DM each (more
+// warps per scheduler to hide shared-memory latency); the generic kernel 16
+// warps of two DMs.
+template <> struct Tiled<8>  { static constexpr int J = 5, DPW = 1, NW = 32, NN = 2, FLP = 128; };
+template <> struct Tiled<4>  { static constexpr int J = 3, DPW = 2, NW = 16, NN = 2, FLP = 8; };
+template <> struct Tiled<2>  { static constexpr int J = 1, DPW = 2, NW = 16, NN = 4, FLP = 42; };
+template <> struct Tiled<1>  { static constexpr int J = 1, DPW = 1, NW = 16, NN = 8, FLP = 127; };
+template <> struct Tiled<16> { static constexpr int J = 7, DPW = 2, NW = 16, NN = 1, FLP = 0; };
+template <> struct Tiled<32> { static constexpr int J = 7, DPW = 2, NW = 16, NN = 1, FLP = 0; };
 
 template <int NBITS>
 struct TiledGeom {
@@ -181,8 +183,9 @@ struct TiledGeom {
     static constexpr int R = J * SPW;       // samples per lane
     static constexpr int BT = 32 * R;       // samples per block
     static constexpr int DPW = Tiled<NBITS>::DPW;
-    static constexpr int BD = TILED_NW * DPW;
-    static constexpr int NT = TILED_NW * 32;
+    static constexpr int NW = Tiled<NBITS>::NW;
+    static constexpr int BD = NW * DPW;
+    static constexpr int NT = NW * 32;
 };
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
@@ -277,7 +280,7 @@ __global__ void __launch_bounds__(TiledGeom<NBITS>::NT, 1) dedisperse_tiled_kern
     // Stage `stage` of the channel list into buffer `buf`.
     auto prep = [&](int stage, int buf) {
         const int32_t* cl = a.chan_list + (size_t)stage * CS;
-        for (int j = warp; j < CS; j += TILED_NW) {
+        for (int j = warp; j < CS; j += G::NW) {
             const int c = cl[j];
             const float dl = a.delay_table[c];
             const uint32_t lo = min(delay_rn(dm_first, dl), delay_rn(dm_last, dl));
@@ -386,18 +389,22 @@ __global__ void __launch_bounds__(TiledGeom<NBITS>::NT, 1) dedisperse_tiled_kern
 }
 
 // ---------------------------------------------------------------------------
-// K2 for 8-bit input: integer work balanced across the ALU and FMA pipes.
+// K2 for 8-bit input.
 //
-// The 32-bit integer ALU pipe issues at half the rate of the FMA pipe, and
-// the generic kernel keeps it ~80% busy (funnel shift, mask, byte permute,
-// 3-input add per word). Here:
-//   * each staged channel window is also stored shifted by 1, 2 and 3
-//     bytes (built once per stage, reused by all BD DMs), so a lane reads
-//     already-aligned words and no per-word funnel shift is needed;
-//   * the 16-bit-lane sums are accumulated with IMAD (multiplier `one` = 1,
-//     a kernel argument, so the multiply-add stays on the FMA pipe).
-// Per word and channel: 1 LOP (even bytes) + 1 PRMT (odd bytes) on the ALU
-// pipe, 2 IMAD on the FMA pipe.
+// Byte alignment: each staged channel window is also stored shifted by 1, 2
+// and 3 bytes (built once per stage with 16-byte shared loads/stores, reused
+// by all BD DMs), so a lane reads already-aligned words.
+//
+// Accumulation (two accumulators per word of 4 samples b0..b3, exact):
+//   S += w1 + w2                          raw words, carries run across bytes
+//   O += prmt(w1) + prmt(w2)              odd bytes (b1, b3) in 16-bit lanes
+// After at most 256 channels, E = S - 256*O holds the even bytes (b0, b2) in
+// 16-bit lanes: S = sum(b0 + b1 2^8 + b2 2^16 + b3 2^24) and
+// 256*O = sum(b1 2^8 + b3 2^24) modulo 2^32, and each lane sum of E and O is
+// at most 256*255 < 2^16, so E < 2^32 and every lane is exact. Per word and
+// channel pair: one 3-input add and two byte permutes on the ALU pipe, two
+// IMAD (multiplier `one` = 1, a kernel argument) on the FMA pipe, two
+// shared loads.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t imad(uint32_t a, uint32_t b, uint32_t c)
 {
@@ -406,12 +413,18 @@ __device__ __forceinline__ uint32_t imad(uint32_t a, uint32_t b, uint32_t c)
     return d;
 }
 
-__global__ void __launch_bounds__(TiledGeom<8>::NT, 1) dedisperse_tiled8_kernel(DedisperseArgs a,
-                                                                                uint32_t one)
+constexpr int T8_FLUSH_CHANNELS = 256;
+
+// Tile shapes of the 8-bit kernel (one DM per warp): J words (4J samples)
+// per lane, NW warps = NW DMs per block. Index = the plan's `variant`.
+struct T8Shape { int J, NW; };
+constexpr T8Shape T8_SHAPES[] = {{5, 28}, {5, 32}, {5, 24}, {3, 32}, {7, 16}};
+constexpr int T8_NSHAPES = sizeof(T8_SHAPES) / sizeof(T8_SHAPES[0]);
+
+template <int J, int NW>
+__global__ void __launch_bounds__(NW * 32, 1) dedisperse_tiled8_kernel(DedisperseArgs a, uint32_t one)
 {
-    using G = TiledGeom<8>;
-    constexpr int J = G::J, R = G::R, BT = G::BT, DPW = G::DPW, BD = G::BD, NT = G::NT;
-    constexpr int FLP = Tiled<8>::FLP;
+    constexpr int R = 4 * J, BT = 32 * R, BD = NW, NT = NW * 32;
 
     extern __shared__ __align__(16) uint32_t smem[];
     const int W = a.win_words, CS = a.chan_per_stage;
@@ -419,7 +432,8 @@ __global__ void __launch_bounds__(TiledGeom<8>::NT, 1) dedisperse_tiled8_kernel(
     uint32_t* s_win = smem;                        // [2][CS][W]   raw windows
     uint32_t* s_shift = s_win + 2 * CSW;           // [3][CS][W]   shifted by 1..3 bytes
     uint32_t* s_info = s_shift + 3 * CSW;          // [2][BD][CS]  word offset into smem
-    float* s_dm = reinterpret_cast<float*>(s_info + 2 * BD * CS);  // [BD]
+    int* s_need = reinterpret_cast<int*>(s_info + 2 * BD * CS);    // [2][CS] words used per row
+    float* s_dm = reinterpret_cast<float*>(s_need + 2 * CS);       // [BD]
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int i0 = blockIdx.x * BD;
@@ -430,16 +444,23 @@ __global__ void __launch_bounds__(TiledGeom<8>::NT, 1) dedisperse_tiled8_kernel(
     if (tid < BD) s_dm[tid] = a.dms[i0 + min(tid, nvalid - 1)];
     __syncthreads();
 
+    // Window of channel row j: words [A/4, A/4 + need) of the channel, where
+    // A is the block's earliest read rounded down to 16 samples and need
+    // covers the latest DM's read of the last lane (plus the one word the
+    // shifted copies look ahead). need <= W (W is the maximum over blocks).
     auto prep = [&](int stage, int buf) {
         const int32_t* cl = a.chan_list + (size_t)stage * CS;
-        for (int j = warp; j < CS; j += TILED_NW) {
+        for (int j = warp; j < CS; j += NW) {
             const int c = cl[j];
             const float dl = a.delay_table[c];
-            const uint32_t lo = min(delay_rn(dm_first, dl), delay_rn(dm_last, dl));
+            const uint32_t d0 = delay_rn(dm_first, dl), d1 = delay_rn(dm_last, dl);
+            const uint32_t lo = min(d0, d1), hi = max(d0, d1);
             const size_t A = ((t0 + lo) / 16) * 16;
+            const int need = min(W, (int)((t0 + hi - A) / 4) + 32 * J + 1);
             const uint32_t* src = a.tr + (size_t)c * a.tr_pitch_words + A / 4;
             uint32_t* dst = s_win + buf * CSW + j * W;
-            for (int k = lane * 4; k < W; k += 128) cp_async16(dst + k, src + k);
+            for (int k = lane * 4; k < need; k += 128) cp_async16(dst + k, src + k);
+            if (lane == 0) s_need[buf * CS + j] = need;
         }
         for (int idx = tid; idx < BD * CS; idx += NT) {
             const int slot = idx / CS, j = idx - slot * CS;
@@ -454,34 +475,58 @@ __global__ void __launch_bounds__(TiledGeom<8>::NT, 1) dedisperse_tiled8_kernel(
         }
     };
 
-    uint32_t acc[DPW][R];
-    uint32_t nar[DPW][J][2];
+    uint32_t acc[R];
+    uint32_t sw[J], so[J];
 #pragma unroll
-    for (int di = 0; di < DPW; ++di) {
+    for (int k = 0; k < R; ++k) acc[k] = 0;
 #pragma unroll
-        for (int k = 0; k < R; ++k) acc[di][k] = 0;
+    for (int k = 0; k < J; ++k) sw[k] = so[k] = 0;
+    auto flush = [&]() {
 #pragma unroll
-        for (int k = 0; k < J; ++k) nar[di][k][0] = nar[di][k][1] = 0;
-    }
+        for (int k = 0; k < J; ++k) {
+            const uint32_t e = imad(so[k], 0xFFFFFF00u, sw[k]);  // S - 256*O
+            acc[4 * k + 0] += e & 0xFFFFu;
+            acc[4 * k + 2] += e >> 16;
+            acc[4 * k + 1] += so[k] & 0xFFFFu;
+            acc[4 * k + 3] += so[k] >> 16;
+            sw[k] = so[k] = 0;
+        }
+    };
 
     prep(0, 0);
     cp_async_commit();
-    int pairs = 0;
+    int since_flush = 0;  // channels accumulated since the last flush
+    const int slot = warp;
     for (int s = 0; s < a.nstages; ++s) {
         const int buf = s & 1;
         asm volatile("cp.async.wait_group 0;\n" ::);
         __syncthreads();
-        // shifted copies of this stage's windows (the last word of each
-        // shifted row is never read)
+        // Shifted copies of this stage's windows, 4 words per lane step; the
+        // word after a lane's four comes from the next lane (or, for lane 31,
+        // from shared memory). The last word of each shifted row is never read.
         {
             const uint32_t* src = s_win + buf * CSW;
-            for (int i = tid; i < CSW; i += NT) {
-                const int w = i % W;
-                if (w + 1 < W) {
-                    const uint32_t lo = src[i], hi = src[i + 1];
-                    s_shift[i] = __funnelshift_r(lo, hi, 8);
-                    s_shift[CSW + i] = __funnelshift_r(lo, hi, 16);
-                    s_shift[2 * CSW + i] = __funnelshift_r(lo, hi, 24);
+            for (int j = warp; j < CS; j += NW) {
+                const uint32_t* row = src + j * W;
+                const int need = s_need[buf * CS + j];
+                for (int k0 = 0; k0 < need; k0 += 128) {
+                    const int k = k0 + lane * 4;
+                    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                    if (k < need) v = *reinterpret_cast<const uint4*>(row + k);
+                    uint32_t nx = __shfl_down_sync(0xFFFFFFFFu, v.x, 1);
+                    if (lane == 31) nx = (k + 4 < W) ? row[k + 4] : 0u;
+                    if (k < need) {
+                        const int o = j * W + k;
+                        *reinterpret_cast<uint4*>(s_shift + o) =
+                            make_uint4(__funnelshift_r(v.x, v.y, 8), __funnelshift_r(v.y, v.z, 8),
+                                       __funnelshift_r(v.z, v.w, 8), __funnelshift_r(v.w, nx, 8));
+                        *reinterpret_cast<uint4*>(s_shift + CSW + o) =
+                            make_uint4(__funnelshift_r(v.x, v.y, 16), __funnelshift_r(v.y, v.z, 16),
+                                       __funnelshift_r(v.z, v.w, 16), __funnelshift_r(v.w, nx, 16));
+                        *reinterpret_cast<uint4*>(s_shift + 2 * CSW + o) =
+                            make_uint4(__funnelshift_r(v.x, v.y, 24), __funnelshift_r(v.y, v.z, 24),
+                                       __funnelshift_r(v.z, v.w, 24), __funnelshift_r(v.w, nx, 24));
+                    }
                 }
             }
         }
@@ -489,70 +534,98 @@ __global__ void __launch_bounds__(TiledGeom<8>::NT, 1) dedisperse_tiled8_kernel(
         if (s + 1 < a.nstages) prep(s + 1, buf ^ 1);
         cp_async_commit();
 
-        const uint32_t* info = s_info + buf * BD * CS;
+        // 16-bit lanes hold at most 256 channels of 8-bit samples
+        if (since_flush + CS > T8_FLUSH_CHANNELS) {
+            flush();
+            since_flush = 0;
+        }
+        const uint32_t* info = s_info + (buf * BD + slot) * CS;
+#pragma unroll 1
         for (int j = 0; j < CS; j += 2) {
+            const uint2 f = *reinterpret_cast<const uint2*>(info + j);
+            const uint32_t* p1 = smem + f.x + lane * J;
+            const uint32_t* p2 = smem + f.y + lane * J;
+            uint32_t w1[J], w2[J];
 #pragma unroll
-            for (int di = 0; di < DPW; ++di) {
-                const int slot = warp * DPW + di;
-                const uint32_t* p1 = smem + info[slot * CS + j] + lane * J;
-                const uint32_t* p2 = smem + info[slot * CS + j + 1] + lane * J;
-                uint32_t w1[J], w2[J];
-#pragma unroll
-                for (int k = 0; k < J; ++k) {
-                    w1[k] = p1[k];
-                    w2[k] = p2[k];
-                }
-#pragma unroll
-                for (int k = 0; k < J; ++k) {
-                    nar[di][k][0] = imad(w1[k] & 0x00FF00FFu, one, nar[di][k][0]);
-                    nar[di][k][0] = imad(w2[k] & 0x00FF00FFu, one, nar[di][k][0]);
-                    nar[di][k][1] = imad(__byte_perm(w1[k], 0u, 0x4341), one, nar[di][k][1]);
-                    nar[di][k][1] = imad(__byte_perm(w2[k], 0u, 0x4341), one, nar[di][k][1]);
-                }
+            for (int k = 0; k < J; ++k) {
+                w1[k] = p1[k];
+                w2[k] = p2[k];
             }
-            if (++pairs == FLP) {
 #pragma unroll
-                for (int di = 0; di < DPW; ++di) narrow_flush<8, J, 2, R>(nar[di], acc[di]);
-                pairs = 0;
+            for (int k = 0; k < J; ++k) {
+                sw[k] = sw[k] + w1[k] + w2[k];
+                so[k] = imad(__byte_perm(w1[k], 0u, 0x4341), one, so[k]);
+                so[k] = imad(__byte_perm(w2[k], 0u, 0x4341), one, so[k]);
             }
         }
+        since_flush += CS;
     }
-#pragma unroll
-    for (int di = 0; di < DPW; ++di) narrow_flush<8, J, 2, R>(nar[di], acc[di]);
+    flush();
 
-#pragma unroll
-    for (int di = 0; di < DPW; ++di) {
-        const int slot = warp * DPW + di;
-        if (slot >= nvalid) continue;
+    if (slot < nvalid) {
         const int row = a.perm ? a.perm[i0 + slot] : i0 + slot;
         const size_t base = (size_t)row * a.out_stride;
         const size_t tl = t0 + (size_t)lane * R;
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const size_t t = tl + k;
-            if (t < a.nsamp_out) store_out(a.out, base + t, a.out_nbits, acc[di][k], a.den, a.factor);
+            if (t < a.nsamp_out) store_out(a.out, base + t, a.out_nbits, acc[k], a.den, a.factor);
         }
     }
+}
+
+// cudaFuncSetAttribute is per device context; remember what each device has
+// been given, per kernel.
+template <typename K>
+void ensure_smem(K kfn, size_t smem, size_t (&configured)[64])
+{
+    int dev = 0;
+    RT_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64 || smem > configured[dev]) {
+        RT_CHECK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if (dev >= 0 && dev < 64) configured[dev] = smem;
+    }
+}
+
+template <int J, int NW>
+void launch_tiled8_shape(const DedisperseArgs& a, cudaStream_t s)
+{
+    static size_t configured[64] = {};
+    const size_t smem = tiled_smem_bytes(8, a.win_words, a.chan_per_stage, a.variant);
+    ensure_smem(dedisperse_tiled8_kernel<J, NW>, smem, configured);
+    dim3 grid((a.ndm + NW - 1) / NW, (unsigned)((a.nsamp_out + 128 * J - 1) / (128 * J)));
+    dedisperse_tiled8_kernel<J, NW><<<grid, NW * 32, smem, s>>>(a, 1u);
+    RT_CHECK(cudaGetLastError());
+}
+
+template <int V>
+void launch_tiled8_variant(const DedisperseArgs& a, cudaStream_t s)
+{
+    launch_tiled8_shape<T8_SHAPES[V].J, T8_SHAPES[V].NW>(a, s);
 }
 
 template <int NBITS>
 void launch_tiled_n(const DedisperseArgs& a, cudaStream_t s)
 {
-    using G = TiledGeom<NBITS>;
-    const size_t smem = tiled_smem_bytes(NBITS, a.win_words, a.chan_per_stage);
-    // The attribute is per device context; remember what each device has.
-    static size_t configured[64] = {};
-    int dev = 0;
-    RT_CHECK(cudaGetDevice(&dev));
-    auto kfn = (NBITS == 8) ? (void*)dedisperse_tiled8_kernel : (void*)dedisperse_tiled_kernel<NBITS>;
-    if (dev < 0 || dev >= 64 || smem > configured[dev]) {
-        RT_CHECK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        if (dev >= 0 && dev < 64) configured[dev] = smem;
+    if constexpr (NBITS == 8) {
+        static_assert(T8_NSHAPES == 5, "dispatch below lists every shape");
+        switch (a.variant) {
+        case 0: launch_tiled8_variant<0>(a, s); break;
+        case 1: launch_tiled8_variant<1>(a, s); break;
+        case 2: launch_tiled8_variant<2>(a, s); break;
+        case 3: launch_tiled8_variant<3>(a, s); break;
+        case 4: launch_tiled8_variant<4>(a, s); break;
+        default: DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unknown tiled kernel variant");
+        }
+    } else {
+        using G = TiledGeom<NBITS>;
+        static size_t configured[64] = {};
+        const size_t smem = tiled_smem_bytes(NBITS, a.win_words, a.chan_per_stage, 0);
+        ensure_smem(dedisperse_tiled_kernel<NBITS>, smem, configured);
+        dim3 grid((a.ndm + G::BD - 1) / G::BD, (unsigned)((a.nsamp_out + G::BT - 1) / G::BT));
+        dedisperse_tiled_kernel<NBITS><<<grid, G::NT, smem, s>>>(a);
+        RT_CHECK(cudaGetLastError());
     }
-    dim3 grid((a.ndm + G::BD - 1) / G::BD, (unsigned)((a.nsamp_out + G::BT - 1) / G::BT));
-    if constexpr (NBITS == 8) dedisperse_tiled8_kernel<<<grid, G::NT, smem, s>>>(a, 1u);
-    else dedisperse_tiled_kernel<NBITS><<<grid, G::NT, smem, s>>>(a);
-    RT_CHECK(cudaGetLastError());
 }
 
 template <int NBITS>
@@ -577,51 +650,73 @@ void launch_transpose_n(const TransposeArgs& a, cudaStream_t s)
 
 }  // namespace
 
-int tiled_block_samples(int nbits)
+int tiled_variant_count(int nbits) { return nbits == 8 ? T8_NSHAPES : 1; }
+
+static int checked_variant(int nbits, int variant)
 {
+    if (variant < 0 || variant >= tiled_variant_count(nbits))
+        DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unknown tiled kernel variant");
+    return variant;
+}
+
+int tiled_block_samples(int nbits, int variant)
+{
+    checked_variant(nbits, variant);
     switch (nbits) {
     case 1: return TiledGeom<1>::BT;
     case 2: return TiledGeom<2>::BT;
     case 4: return TiledGeom<4>::BT;
-    case 8: return TiledGeom<8>::BT;
+    case 8: return 128 * T8_SHAPES[variant].J;
     case 16: return TiledGeom<16>::BT;
     default: return TiledGeom<32>::BT;
     }
 }
 
-int tiled_block_dms(int nbits)
+int tiled_block_dms(int nbits, int variant)
 {
+    checked_variant(nbits, variant);
     switch (nbits) {
     case 1: return TiledGeom<1>::BD;
     case 2: return TiledGeom<2>::BD;
     case 4: return TiledGeom<4>::BD;
-    case 8: return TiledGeom<8>::BD;
+    case 8: return T8_SHAPES[variant].NW;
     case 16: return TiledGeom<16>::BD;
     default: return TiledGeom<32>::BD;
     }
 }
 
-int tiled_lane_words(int nbits)
+int tiled_lane_words(int nbits, int variant)
 {
+    checked_variant(nbits, variant);
     switch (nbits) {
     case 1: return TiledGeom<1>::J;
     case 2: return TiledGeom<2>::J;
     case 4: return TiledGeom<4>::J;
-    case 8: return TiledGeom<8>::J;
+    case 8: return T8_SHAPES[variant].J;
     case 16: return TiledGeom<16>::J;
     default: return TiledGeom<32>::J;
     }
 }
 
-size_t tiled_smem_bytes(int nbits, int win_words, int chan_per_stage)
+size_t tiled_smem_bytes(int nbits, int win_words, int chan_per_stage, int variant)
 {
-    const size_t bd = (size_t)tiled_block_dms(nbits);
-    // 8-bit: two raw buffers plus three byte-shifted copies per stage
+    const size_t bd = (size_t)tiled_block_dms(nbits, variant);
+    // 8-bit: two raw buffers plus three byte-shifted copies per stage, and
+    // the per-row window lengths
     const size_t windows = nbits == 8 ? 5ull : 2ull;
-    return (windows * chan_per_stage * win_words + 2ull * bd * chan_per_stage + bd) * 4ull;
+    const size_t extra = nbits == 8 ? 2ull * chan_per_stage : 0ull;
+    return (windows * chan_per_stage * win_words + 2ull * bd * chan_per_stage + extra + bd) * 4ull;
 }
 
-size_t tiled_max_smem_bytes() { return 200 * 1024; }
+// The opt-in maximum of dynamic shared memory per block on sm_100.
+size_t tiled_max_smem_bytes() { return 227 * 1024; }
+
+int tiled_stage_channels(int nbits, int win_words, int variant)
+{
+    int cs = 32;
+    while (cs >= 2 && tiled_smem_bytes(nbits, win_words, cs, variant) > tiled_max_smem_bytes()) cs -= 2;
+    return cs >= 2 ? cs : 0;
+}
 
 void launch_transpose(const TransposeArgs& a, cudaStream_t s)
 {

@@ -52,14 +52,19 @@ struct DedisperseArgs {
     float factor;               // (3.f*1024.f)/255.f/16.f
     int win_words;              // tiled: staged window per channel (words)
     int chan_per_stage;         // tiled: channels per pipeline stage (even)
+    int variant;                // tiled: tile-shape variant (8-bit input)
 };
 
-// Tile geometry of the tiled kernel for a given input width.
-int tiled_block_samples(int nbits);  // output samples per block
-int tiled_block_dms(int nbits);      // DMs per block
-int tiled_lane_words(int nbits);     // J: words per lane
-size_t tiled_smem_bytes(int nbits, int win_words, int chan_per_stage);
+// Tile geometry of the tiled kernel for a given input width and tile-shape
+// variant (8-bit input has several, see tiled_variant_count; other widths 1).
+int tiled_variant_count(int nbits);
+int tiled_block_samples(int nbits, int variant);  // output samples per block
+int tiled_block_dms(int nbits, int variant);      // DMs per block
+int tiled_lane_words(int nbits, int variant);     // J: words per lane
+size_t tiled_smem_bytes(int nbits, int win_words, int chan_per_stage, int variant);
 size_t tiled_max_smem_bytes();
+// Channels per pipeline stage for a window of win_words (0: does not fit).
+int tiled_stage_channels(int nbits, int win_words, int variant);
 
 void launch_dedisperse_plain(const DedisperseArgs& a, cudaStream_t s);
 void launch_dedisperse_tiled(const DedisperseArgs& a, cudaStream_t s);

@@ -61,6 +61,7 @@ TDDPlan::~TDDPlan() {}
 void TDDPlan::set_gulp_size(size_type gulp_size) { m_engine->gulp_size = gulp_size; }
 dedisp_size TDDPlan::get_gulp_size() const { return m_engine->gulp_size; }
 void TDDPlan::set_kernel(TddKernel k) { m_engine->kernel = k; }
+void TDDPlan::set_tile_variant(int variant) { m_engine->variant = variant; }
 void TDDPlan::set_timing(bool enable) { m_engine->record_timing = enable; }
 ExecTiming TDDPlan::last_timing() const
 {
@@ -130,6 +131,7 @@ DedispPlan::~DedispPlan() {}
 void DedispPlan::set_gulp_size(size_type gulp_size) { m_engine->gulp_size = gulp_size; }
 DedispPlan::size_type DedispPlan::get_gulp_size() const { return m_engine->gulp_size; }
 void DedispPlan::set_kernel(TddKernel k) { m_engine->kernel = k; }
+void DedispPlan::set_tile_variant(int variant) { m_engine->variant = variant; }
 void DedispPlan::set_timing(bool enable) { m_engine->record_timing = enable; }
 ExecTiming DedispPlan::last_timing() const
 {

@@ -184,3 +184,26 @@ def config2(seed: int = 20261205, nsamps: int = 1 << 20) -> Config:
                   0.0, 1.0, pulses,
                   dm_list=(1000.0 * np.arange(2048) / 2047.0).astype(np.float32), seed=seed,
                   float_input=True)
+
+
+def config3(seed: int = 20261206, nbeams: int = 96, nsamp_range: Tuple[int, int] = (1 << 17, 1 << 20),
+            dm_max_range: Tuple[float, float] = (500.0, 3000.0),
+            ndm_range: Tuple[int, int] = (1024, 4096)) -> List[Config]:
+    """Batched multi-beam TDD: `nbeams` beams of 1536 ch (f_top 1670 MHz,
+    df -0.25 MHz, dt 81.92 us), 8-bit noise round(N(128, 16)); per beam a
+    seeded nsamp, maximum DM and linear DM-trial count, and 3 pulses."""
+    rng = np.random.default_rng(seed)
+    beams = []
+    for b in range(nbeams):
+        ns = int(rng.integers(nsamp_range[0], nsamp_range[1] + 1))
+        dm_max = float(rng.uniform(*dm_max_range))
+        ndm = int(rng.integers(ndm_range[0], ndm_range[1] + 1))
+        dur = ns * 81.92e-6
+        pulses = [Pulse(float(rng.uniform(20.0, 0.9 * dm_max)), float(rng.uniform(0.05, 0.6) * dur),
+                        float(rng.uniform(0.5e-3, 3e-3)), float(rng.uniform(24.0, 64.0)))
+                  for _ in range(3)]
+        beams.append(Config(f"beam{b:02d}-1536ch-{ns}s-{ndm}dm", 1536, 1670.0, -0.25, 81.92e-6, ns, 8,
+                            128.0, 16.0, pulses,
+                            dm_list=(dm_max * np.arange(ndm) / max(ndm - 1, 1)).astype(np.float32),
+                            seed=seed + 1 + b))
+    return beams

@@ -39,6 +39,7 @@ public:
                       dedisp_size dm_count, unsigned flags);
 
     void set_kernel(TddKernel k);
+    void set_tile_variant(int variant);
     void set_timing(bool enable) override;
     ExecTiming last_timing() const override;
 

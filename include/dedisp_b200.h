@@ -24,6 +24,13 @@ typedef enum {
 
 dedisp_error dedisp_b200_set_tdd_kernel(dedisp_plan plan, int kernel);
 
+/* Tile shape of the tiled TDD kernel (8-bit input: DMs per block, samples
+ * per thread); variant in [0, dedisp_b200_tdd_variant_count(in_nbits)).
+ * Every variant computes the same bit-exact sums; they differ in speed.
+ * Other input widths have a single shape and ignore the setting. */
+dedisp_error dedisp_b200_set_tdd_variant(dedisp_plan plan, int variant);
+int dedisp_b200_tdd_variant_count(dedisp_size in_nbits);
+
 /* Runs the plan's device work on a caller-provided cudaStream_t (NULL
  * restores the plan's own stream). */
 dedisp_error dedisp_b200_set_stream(dedisp_plan plan, void* cuda_stream);

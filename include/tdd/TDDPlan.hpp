@@ -55,6 +55,7 @@ public:
                             size_type out_stride, dedisp_size first_dm_idx,
                             dedisp_size dm_count, unsigned flags);
     void set_kernel(TddKernel k);
+    void set_tile_variant(int variant);
     void set_timing(bool enable) override;
     ExecTiming last_timing() const override;
 

@@ -64,6 +64,45 @@ def test_all_widths_bit_exact(nbits, nchans, kernel):
         assert np.array_equal(ours.view(np.uint8), ref.view(np.uint8)), (nbits, out_nbits)
 
 
+@pytest.mark.parametrize("variant", range(5))
+def test_tiled8_tile_variants_bit_exact(variant):
+    """Every tile shape of the 8-bit kernel; > 256 channels so the 16-bit
+    lanes are flushed several times, with a killmask thinning the list."""
+    assert dd.tdd_variant_count(8) == 5
+    nchans, nsamps = 1100, 12000
+    packed, dms, params = _case(8, nchans, nsamps, 75, 600.0, 900 + variant, df=-0.25)
+    km = np.ones(nchans, np.int32)
+    km[7::31] = 0
+    p = dd.TDDPlan(*params)
+    p.set_dm_list(dms)
+    p.set_killmask(km)
+    p.set_kernel(2)
+    p.set_tile_variant(variant)
+    nout = nsamps - p.get_max_delay()
+    out = np.zeros((len(dms), nout), np.float32)
+    p.execute(nsamps, packed, 8, out, 32)
+    ref = _oracle(packed, nsamps, 8, params, dms, km, 32, nout)
+    assert np.array_equal(out.view(np.uint32), ref.view(np.uint32))
+
+
+def test_tiled8_saturated_bytes():
+    """All samples 255: every 16-bit lane reaches 256 * 255 before a flush."""
+    nchans, nsamps = 1024, 6000
+    packed = np.full((nsamps, nchans), 255, np.uint8)
+    params = (nchans, 250e-6, 1500.0, -0.5)
+    dms = np.linspace(0, 300, 45, dtype=np.float32)
+    for variant in range(dd.tdd_variant_count(8)):
+        p = dd.TDDPlan(*params)
+        p.set_dm_list(dms)
+        p.set_kernel(2)
+        p.set_tile_variant(variant)
+        nout = nsamps - p.get_max_delay()
+        out = np.zeros((len(dms), nout), np.float32)
+        p.execute(nsamps, packed, 8, out, 32)
+        ref = _oracle(packed, nsamps, 8, params, dms, np.ones(nchans, np.int32), 32, nout)
+        assert np.array_equal(out.view(np.uint32), ref.view(np.uint32)), variant
+
+
 @pytest.mark.parametrize("nbits", [2, 8])
 def test_killmask_zero_one_and_general(nbits):
     nchans, nsamps = 256, 6000
