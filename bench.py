@@ -59,6 +59,9 @@ def parse():
                     help="tiled-kernel tile shape for 8-bit input (-1: time all, use the fastest)")
     ap.add_argument("--fdd-only", action="store_true",
                     help="run only the FDD forms (config 2) and print their JSON object")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="run only the batched multi-beam TDD (config 3) and print its JSON object")
     ap.add_argument("--profile-case", default="",
                     help="run one small case for ncu and exit: tdd (the TDD workload with "
                          "2^17 samples) or fdd (config-2 geometry with 2^18 samples)")
@@ -284,6 +287,138 @@ def run_fdd(args, local, world, stream, max_over_ranks):
     return out
 
 
+def run_batched(args, local, world, stream, max_over_ranks):
+    """Config 3: 96 beams of 1536 ch (8-bit), each with its own sample count,
+    DM range and trial count, dedispersed by the batch engine (one persistent
+    launch per wave of beams, each wave a replayed CUDA graph, tile shape
+    from the autotuner). Outputs of a wave go to a device pool that the next
+    wave reuses (all outputs together, 577 GB, exceed HBM; a consumer would
+    take each wave's rows before the next). The plain single-beam form and
+    per-beam tiled plans are timed on the first four beams."""
+    import torch
+    import dedisp_tests_b200 as dd
+    from dedisp_tests_b200 import synthetic as sy
+    beams = sy.config3()
+    c0 = beams[0]
+    dev = f"cuda:{local}"
+    mds = []
+    for c in beams:
+        p = dd.TDDPlan(c.nchans, c.dt, c.f_top, c.df)
+        p.set_dm_list(c.dm_list)
+        mds.append(p.get_max_delay())
+        p.close()
+    nouts = [c.nsamps - m for c, m in zip(beams, mds)]
+    units = [len(c.dm_list) * n for c, n in zip(beams, nouts)]
+    out_bytes = [u * 4 for u in units]
+    d_in = [sy.make_input_torch(c, device=dev) for c in beams]
+    torch.cuda.synchronize()
+    free, _ = torch.cuda.mem_get_info(local)
+    budget = free - 12e9  # output pool + transposed-input workspace
+    in_bytes = [x.numel() * 1.1 for x in d_in]
+
+    def partition(cap):
+        waves, cur, acc = [], [], 0.0
+        for i in range(len(beams)):
+            cost = out_bytes[i] + in_bytes[i]
+            if cur and acc + cost > cap:
+                waves.append(cur)
+                cur, acc = [], 0.0
+            cur.append(i)
+            acc += cost
+        waves.append(cur)
+        return waves
+
+    cap = budget
+    while True:
+        waves = partition(cap)
+        need = (max(sum(out_bytes[i] for i in w) for w in waves) +
+                max(sum(in_bytes[i] for i in w) for w in waves))
+        if need <= budget or cap < 1e9:
+            break
+        cap *= 0.9
+    pool = torch.empty(max(sum(out_bytes[i] for i in w) for w in waves), dtype=torch.uint8, device=dev)
+    batches = []
+    for w in waves:
+        b = dd.Batch(c0.nchans, c0.dt, c0.f_top, c0.df, in_nbits=8, out_nbits=32, device=local)
+        spec, off = [], 0
+        for i in w:
+            c = beams[i]
+            y = pool[off:off + out_bytes[i]]
+            off += out_bytes[i]
+            spec.append((d_in[i], c.nchans, c.nsamps, c.dm_list, y, nouts[i] * 4))
+        b.set_beams(spec)
+        batches.append(b)
+    ws_bytes = max(b.workspace_size() for b in batches)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    for b in batches:
+        b.set_workspace(ws, ws_bytes)
+    shape = batches[0].autotune(stream.cuda_stream)
+    for b in batches:
+        b.set_shape(*shape)
+
+    def batched_step():
+        for b in batches:
+            b.execute(stream.cuda_stream, use_graph=True)
+
+    batched_step()  # warm-up: captures each wave's graph
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    steps = 1
+    e0.record(stream)
+    for _ in range(steps):
+        batched_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1)) / steps
+    total_units = float(sum(units))
+    res = {"workload": "96 beams x 1536 ch 8-bit, nsamp U[2^17,2^20], DM max U[500,3000], "
+                       "ndm U[1024,4096] linear (seeded), f32 out",
+           "units": total_units, "waves": len(waves), "beams_per_wave": [len(w) for w in waves],
+           "shape": {"variant": shape[0], "chan_per_stage": shape[1]},
+           "batched": {"value": total_units * world / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+                       "launches_per_step": sum(2 * len(w) + 1 for w in waves)}}
+    for b in batches:
+        b.close()
+    del pool, ws, batches, spec, y
+    torch.cuda.empty_cache()
+
+    # single-beam comparators on the first four beams
+    sub = list(range(4))
+    sub_units = float(sum(units[i] for i in sub))
+    for name, kernel in (("plain_single_beam", 1), ("tiled_single_beam", 2)):
+        outs = [torch.empty((len(beams[i].dm_list), nouts[i]), dtype=torch.float32, device=dev)
+                for i in sub]
+        plans = []
+        for i in sub:
+            c = beams[i]
+            p = dd.TDDPlan(c.nchans, c.dt, c.f_top, c.df, local)
+            p.set_dm_list(c.dm_list)
+            p.set_kernel(kernel)
+            p.set_stream(stream.cuda_stream)
+            plans.append(p)
+        if kernel == 2:
+            for i, p in zip(sub, plans):  # warm-up
+                p.execute(beams[i].nsamps, d_in[i], 8, outs[sub.index(i)], 32, dd.DEDISP_DEVICE_POINTERS)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for i, p in zip(sub, plans):
+            p.execute(beams[i].nsamps, d_in[i], 8, outs[sub.index(i)], 32, dd.DEDISP_DEVICE_POINTERS)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = max_over_ranks(e0.elapsed_time(e1))
+        res[name] = {"value": sub_units * world / (t * 1e-3), "unit": UNIT, "ms": t,
+                     "sample": f"beams {sub} ({sub_units:.3e} DM-trials x samples), one plan "
+                               f"execute per beam"}
+        for p in plans:
+            p.close()
+        del outs
+    res["batched_vs_plain"] = res["batched"]["value"] / res["plain_single_beam"]["value"]
+    del d_in
+    torch.cuda.empty_cache()
+    return res
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -323,6 +458,13 @@ def run_ours(args):
         return float(t.item())
 
     stream = torch.cuda.current_stream()
+    if args.batched_only:
+        res = run_batched(args, local, world, stream, max_over_ranks)
+        if rank == 0:
+            print(json.dumps({"batched": res}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
     if args.fdd_only:
         fdd = run_fdd(args, local, world, stream, max_over_ranks)
         if rank == 0:
@@ -502,6 +644,15 @@ def run_ours(args):
         torch.cuda.empty_cache()
         fdd = run_fdd(args, local, world, stream, max_over_ranks)
 
+    # --- batched multi-beam TDD (config 3) ----------------------------------------
+    batched = None
+    if not args.no_batched:
+        if args.no_fdd:
+            del plan, d_in
+            d_out = None
+            torch.cuda.empty_cache()
+        batched = run_batched(args, local, world, stream, max_over_ranks)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -516,7 +667,7 @@ def run_ours(args):
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches * world, "clocks": clocks, "variants": variants,
             "tile_variant": {"chosen": best, "k2_ms_by_variant": tune},
-            "fdd": fdd,
+            "fdd": fdd, "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

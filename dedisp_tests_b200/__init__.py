@@ -293,3 +293,124 @@ class FDDGPUPlan(Plan):
 def tdd_variant_count(in_nbits: int = 8) -> int:
     """Number of tile-shape variants of the tiled TDD kernel for in_nbits."""
     return int(lib().dedisp_b200_tdd_variant_count(in_nbits))
+
+
+# ---------------------------------------------------------------------------
+# Batched multi-beam TDD (dedisp_b200_batch_*; device buffers only)
+# ---------------------------------------------------------------------------
+
+class _Beam(C.Structure):
+    _fields_ = [("in_", _vp), ("in_stride", _sz), ("nsamps", _sz), ("dm_list", _vp),
+                ("dm_count", _sz), ("out", _vp), ("out_stride", _sz)]
+
+
+_BATCH_SIGS = {
+    "dedisp_b200_batch_create": (C.c_int, [C.POINTER(_vp), _sz, C.c_float, C.c_float, C.c_float,
+                                           _sz, _sz, C.c_int]),
+    "dedisp_b200_batch_destroy": (None, [_vp]),
+    "dedisp_b200_batch_set_killmask": (C.c_int, [_vp, _vp]),
+    "dedisp_b200_batch_set_beams": (C.c_int, [_vp, C.POINTER(_Beam), _sz]),
+    "dedisp_b200_batch_workspace_size": (_sz, [_vp]),
+    "dedisp_b200_batch_set_workspace": (C.c_int, [_vp, _vp, _sz]),
+    "dedisp_b200_batch_set_shape": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "dedisp_b200_batch_autotune": (C.c_int, [_vp, _vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "dedisp_b200_batch_execute": (C.c_int, [_vp, _vp, C.c_int]),
+    "dedisp_b200_batch_set_timing": (C.c_int, [_vp, C.c_int]),
+    "dedisp_b200_batch_get_timing": (C.c_int, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                               C.POINTER(C.c_int)]),
+    "dedisp_b200_batch_max_delay": (_sz, [_vp, _sz]),
+}
+
+
+def _batch_lib() -> C.CDLL:
+    L = lib()
+    if not getattr(L, "_batch_sigs", False):
+        for name, (res, args) in _BATCH_SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        L._batch_sigs = True
+    return L
+
+
+def _bcheck(code: int) -> None:
+    if code != 0:
+        buf = C.create_string_buffer(512)
+        lib().dedisp_b200_last_error(buf, 512)
+        raise DedispError(code, code, buf.value.decode(errors="replace"))
+
+
+class Batch:
+    """Many beams with one channel setup, dedispersed by one graph-captured
+    persistent launch. Beams are (device input, nsamps, DM list, device
+    output) with torch CUDA tensors or raw device addresses."""
+
+    def __init__(self, nchans: int, dt: float, f0: float, df: float, in_nbits: int = 8,
+                 out_nbits: int = 32, device: int = 0):
+        self._h = _vp()
+        _bcheck(_batch_lib().dedisp_b200_batch_create(C.byref(self._h), nchans, dt, f0, df,
+                                                      in_nbits, out_nbits, device))
+        self.nchans, self.in_nbits, self.out_nbits = nchans, in_nbits, out_nbits
+        self._keep = []
+
+    def close(self) -> None:
+        if self._h:
+            _batch_lib().dedisp_b200_batch_destroy(self._h)
+            self._h = _vp()
+        self._keep = []
+        self._ws = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_killmask(self, killmask=None) -> None:
+        if killmask is None:
+            _bcheck(_batch_lib().dedisp_b200_batch_set_killmask(self._h, None))
+            return
+        km = np.ascontiguousarray(killmask, dtype=np.int32)
+        _bcheck(_batch_lib().dedisp_b200_batch_set_killmask(self._h, km.ctypes.data))
+
+    def set_beams(self, beams) -> None:
+        """beams: sequence of (d_in, in_stride, nsamps, dm_list, d_out, out_stride)."""
+        arr = (_Beam * max(len(beams), 1))()
+        keep = []
+        for i, (d_in, in_stride, nsamps, dms, d_out, out_stride) in enumerate(beams):
+            dm = np.ascontiguousarray(dms, dtype=np.float32)
+            keep.append(dm)
+            arr[i] = _Beam(_addr(d_in), in_stride, nsamps, dm.ctypes.data, len(dm), _addr(d_out),
+                           out_stride)
+        _bcheck(_batch_lib().dedisp_b200_batch_set_beams(self._h, arr, len(beams)))
+        self._keep = [b[0] for b in beams] + [b[4] for b in beams]
+
+    def workspace_size(self) -> int:
+        return int(_batch_lib().dedisp_b200_batch_workspace_size(self._h))
+
+    def set_workspace(self, buf, nbytes: int) -> None:
+        _bcheck(_batch_lib().dedisp_b200_batch_set_workspace(self._h, _addr(buf), nbytes))
+        self._ws = buf
+
+    def set_shape(self, variant: int, chan_per_stage: int = 0) -> None:
+        _bcheck(_batch_lib().dedisp_b200_batch_set_shape(self._h, variant, chan_per_stage))
+
+    def autotune(self, stream: int = 0):
+        v, cs = C.c_int(), C.c_int()
+        _bcheck(_batch_lib().dedisp_b200_batch_autotune(self._h, stream, C.byref(v), C.byref(cs)))
+        return v.value, cs.value
+
+    def execute(self, stream: int = 0, use_graph: bool = True) -> None:
+        _bcheck(_batch_lib().dedisp_b200_batch_execute(self._h, stream, int(use_graph)))
+
+    def set_timing(self, enable: bool = True) -> None:
+        _bcheck(_batch_lib().dedisp_b200_batch_set_timing(self._h, int(enable)))
+
+    def get_timing(self) -> dict:
+        a, b, n = C.c_float(), C.c_float(), C.c_int()
+        _bcheck(_batch_lib().dedisp_b200_batch_get_timing(self._h, C.byref(a), C.byref(b),
+                                                          C.byref(n)))
+        return {"transpose_ms": a.value, "dedisperse_ms": b.value, "launches": n.value}
+
+    def max_delay(self, beam: int) -> int:
+        return int(_batch_lib().dedisp_b200_batch_max_delay(self._h, beam))

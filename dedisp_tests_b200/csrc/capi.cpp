@@ -68,6 +68,11 @@ dedisp::DedispPlan* as_dedisp(dedisp_plan p)
 dedisp::FDDGPUPlan* as_fdd(dedisp_plan p) { return dynamic_cast<dedisp::FDDGPUPlan*>(p->ptr.get()); }
 }  // namespace
 
+namespace dedisp {
+// Used by the other C entry points of the library (not exported in a header).
+void note_last_error(dedisp_error code, const char* msg) { note(code, msg); }
+}  // namespace dedisp
+
 extern "C" {
 
 dedisp_error dedisp_create_plan(dedisp_plan* plan, dedisp_size nchans, dedisp_float dt,

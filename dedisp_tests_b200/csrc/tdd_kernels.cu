@@ -14,6 +14,8 @@
 // intrinsics (dedisperse_kernel.cuh:45-64).
 #include "tdd_kernels.hpp"
 
+#include <algorithm>
+
 #include "runtime.hpp"
 
 namespace dedisp {
@@ -421,8 +423,11 @@ struct T8Shape { int J, NW; };
 constexpr T8Shape T8_SHAPES[] = {{5, 28}, {5, 32}, {5, 24}, {3, 32}, {7, 16}};
 constexpr int T8_NSHAPES = sizeof(T8_SHAPES) / sizeof(T8_SHAPES[0]);
 
+// One block tile: DMs [bx*NW, bx*NW + NW) x samples [by*BT, by*BT + BT) of
+// the series described by `a`. Called by the one-tile-per-block kernel and
+// by the persistent multi-beam kernel.
 template <int J, int NW>
-__global__ void __launch_bounds__(NW * 32, 1) dedisperse_tiled8_kernel(DedisperseArgs a, uint32_t one)
+__device__ __forceinline__ void tiled8_tile(const DedisperseArgs& a, int bx, size_t by, uint32_t one)
 {
     constexpr int R = 4 * J, BT = 32 * R, BD = NW, NT = NW * 32;
 
@@ -436,8 +441,8 @@ __global__ void __launch_bounds__(NW * 32, 1) dedisperse_tiled8_kernel(Dedispers
     float* s_dm = reinterpret_cast<float*>(s_need + 2 * CS);       // [BD]
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int i0 = blockIdx.x * BD;
-    const size_t t0 = (size_t)blockIdx.y * BT;
+    const int i0 = bx * BD;
+    const size_t t0 = by * BT;
     const int nvalid = min(BD, a.ndm - i0);
     const float dm_first = a.dms[i0];
     const float dm_last = a.dms[i0 + nvalid - 1];
@@ -574,6 +579,55 @@ __global__ void __launch_bounds__(NW * 32, 1) dedisperse_tiled8_kernel(Dedispers
     }
 }
 
+template <int J, int NW>
+__global__ void __launch_bounds__(NW * 32, 1) dedisperse_tiled8_kernel(DedisperseArgs a, uint32_t one)
+{
+    tiled8_tile<J, NW>(a, blockIdx.x, blockIdx.y, one);
+}
+
+// Persistent form over many series (beams): block b takes work items b,
+// b + gridDim.x, ...; item i belongs to the beam with
+// item_start[beam] <= i < item_start[beam + 1] and is tile
+// (bx, by) = (local % nbx, local / nbx) of that beam. Each beam's arguments
+// are copied to shared memory before its tiles run.
+template <int J, int NW>
+__global__ void __launch_bounds__(NW * 32, 1)
+dedisperse_tiled8_batch_kernel(const DedisperseArgs* __restrict__ args,
+                               const unsigned long long* __restrict__ item_start,
+                               const int* __restrict__ nbx, int nbeams, uint32_t one)
+{
+    __shared__ DedisperseArgs s_a;
+    __shared__ int s_beam;
+    const unsigned long long total = item_start[nbeams];
+    int cur = -1;
+    for (unsigned long long item = blockIdx.x; item < total; item += gridDim.x) {
+        if (threadIdx.x == 0) {
+            int lo = 0, hi = nbeams - 1;  // last beam with item_start <= item
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) / 2;
+                if (item_start[mid] <= item) lo = mid;
+                else hi = mid - 1;
+            }
+            s_beam = lo;
+        }
+        __syncthreads();
+        const int beam = s_beam;
+        if (beam != cur) {
+            constexpr int NWORDS = (int)(sizeof(DedisperseArgs) / 4);
+            static_assert(sizeof(DedisperseArgs) % 4 == 0, "argument block is copied as words");
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(args + beam);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&s_a);
+            for (int w = threadIdx.x; w < NWORDS; w += blockDim.x) dst[w] = src[w];
+            cur = beam;
+        }
+        __syncthreads();
+        const unsigned long long local = item - item_start[beam];
+        const int n = nbx[beam];
+        tiled8_tile<J, NW>(s_a, (int)(local % (unsigned long long)n), (size_t)(local / (unsigned long long)n), one);
+        __syncthreads();  // shared memory is reused by the next item
+    }
+}
+
 // cudaFuncSetAttribute is per device context; remember what each device has
 // been given, per kernel.
 template <typename K>
@@ -602,6 +656,29 @@ template <int V>
 void launch_tiled8_variant(const DedisperseArgs& a, cudaStream_t s)
 {
     launch_tiled8_shape<T8_SHAPES[V].J, T8_SHAPES[V].NW>(a, s);
+}
+
+template <int J, int NW>
+void launch_tiled8_batch_shape(const BatchLaunch& b, cudaStream_t s)
+{
+    static size_t configured[64] = {};
+    auto kfn = dedisperse_tiled8_batch_kernel<J, NW>;
+    ensure_smem(kfn, b.smem_bytes, configured);
+    int dev = 0, sms = 0, per_sm = 0;
+    RT_CHECK(cudaGetDevice(&dev));
+    RT_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    RT_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, NW * 32, b.smem_bytes));
+    if (per_sm < 1) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "batch kernel does not fit on an SM");
+    const unsigned long long want = (unsigned long long)sms * per_sm;
+    const unsigned grid = (unsigned)std::max<unsigned long long>(1, std::min(want, b.total_items));
+    kfn<<<grid, NW * 32, b.smem_bytes, s>>>(b.args, b.item_start, b.nbx, b.nbeams, 1u);
+    RT_CHECK(cudaGetLastError());
+}
+
+template <int V>
+void launch_tiled8_batch_variant(const BatchLaunch& b, cudaStream_t s)
+{
+    launch_tiled8_batch_shape<T8_SHAPES[V].J, T8_SHAPES[V].NW>(b, s);
 }
 
 template <int NBITS>
@@ -741,6 +818,20 @@ void launch_dedisperse_plain(const DedisperseArgs& a, cudaStream_t s)
     case 16: launch_plain_n<16>(a, s); break;
     case 32: launch_plain_n<32>(a, s); break;
     default: DD_THROW(DEDISP_UNSUPPORTED_IN_NBITS);
+    }
+}
+
+void launch_dedisperse_tiled8_batch(const BatchLaunch& b, int variant, cudaStream_t s)
+{
+    if (b.total_items == 0) return;
+    static_assert(T8_NSHAPES == 5, "dispatch below lists every shape");
+    switch (variant) {
+    case 0: launch_tiled8_batch_variant<0>(b, s); break;
+    case 1: launch_tiled8_batch_variant<1>(b, s); break;
+    case 2: launch_tiled8_batch_variant<2>(b, s); break;
+    case 3: launch_tiled8_batch_variant<3>(b, s); break;
+    case 4: launch_tiled8_batch_variant<4>(b, s); break;
+    default: DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unknown tiled kernel variant");
     }
 }
 

@@ -69,5 +69,19 @@ int tiled_stage_channels(int nbits, int win_words, int variant);
 void launch_dedisperse_plain(const DedisperseArgs& a, cudaStream_t s);
 void launch_dedisperse_tiled(const DedisperseArgs& a, cudaStream_t s);
 
+// Persistent 8-bit tiled kernel over many series: args[beam] describes beam
+// `beam` (device array), its tiles are items item_start[beam] ..
+// item_start[beam+1]-1 (nbeams+1 entries, device), nbx[beam] DM blocks per
+// time tile (device). smem_bytes: the largest tiled_smem_bytes of the beams.
+struct BatchLaunch {
+    const DedisperseArgs* args;
+    const unsigned long long* item_start;
+    const int* nbx;
+    int nbeams;
+    unsigned long long total_items;
+    size_t smem_bytes;
+};
+void launch_dedisperse_tiled8_batch(const BatchLaunch& b, int variant, cudaStream_t s);
+
 }  // namespace kern
 }  // namespace dedisp

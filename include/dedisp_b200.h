@@ -91,6 +91,62 @@ dedisp_error dedisp_b200_tdd_execute_noalloc(
     dedisp_byte* d_out, dedisp_size out_nbits, dedisp_size out_stride, void* stream);
 const char* dedisp_b200_noalloc_last_message(void);
 
+/* ------------------------------------------------------------------------
+ * Batched multi-beam TDD. No counterpart in the reference (its plans take one
+ * series per execute call). Beams share the channel setup and widths; each
+ * has its own DEVICE input (time-major packed rows), sample count, DM list
+ * and DEVICE output (dm_count rows of nsamps - max_delay samples, out_stride
+ * bytes apart; max_delay follows the reference rule: last DM of the list x
+ * delay of the last channel). One execute enqueues the transposes of all
+ * beams and one persistent dedispersion launch over all of them (8-bit input,
+ * 0/1 killmask; otherwise one launch per beam), captured once into a CUDA
+ * graph when use_graph != 0 and replayed on later calls. Results are
+ * bit-identical to a TDD plan run per beam.
+ * ---------------------------------------------------------------------- */
+typedef struct dedisp_b200_batch_struct* dedisp_b200_batch;
+
+typedef struct {
+    const dedisp_byte* in;      /* device */
+    dedisp_size in_stride;      /* bytes per input row */
+    dedisp_size nsamps;
+    const dedisp_float* dm_list;  /* host, dm_count entries (copied) */
+    dedisp_size dm_count;
+    dedisp_byte* out;           /* device */
+    dedisp_size out_stride;     /* bytes per output row */
+} dedisp_b200_beam;
+
+dedisp_error dedisp_b200_batch_create(dedisp_b200_batch* batch, dedisp_size nchans, dedisp_float dt,
+                                      dedisp_float f0, dedisp_float df, dedisp_size in_nbits,
+                                      dedisp_size out_nbits, int device);
+void dedisp_b200_batch_destroy(dedisp_b200_batch batch);
+dedisp_error dedisp_b200_batch_set_killmask(dedisp_b200_batch batch, const dedisp_bool* killmask);
+dedisp_error dedisp_b200_batch_set_beams(dedisp_b200_batch batch, const dedisp_b200_beam* beams,
+                                         dedisp_size nbeams);
+/* Scratch for the transposed inputs (any tile shape); a caller may hand the
+ * same buffer to several batches that it runs one after another on one
+ * stream. Without one the batch allocates its own. */
+dedisp_size dedisp_b200_batch_workspace_size(dedisp_b200_batch batch);
+dedisp_error dedisp_b200_batch_set_workspace(dedisp_b200_batch batch, void* d_workspace,
+                                             dedisp_size bytes);
+/* Tile shape: variant < dedisp_b200_tdd_variant_count(in_nbits), channels
+ * per stage even and <= 32 (0: the largest that fits shared memory). */
+dedisp_error dedisp_b200_batch_set_shape(dedisp_b200_batch batch, int variant, int chan_per_stage);
+/* Times every candidate shape on the leading 8192 output samples of each
+ * beam (CUDA events, on `stream`, synchronous) and keeps the fastest. */
+dedisp_error dedisp_b200_batch_autotune(dedisp_b200_batch batch, void* stream, int* variant,
+                                        int* chan_per_stage);
+dedisp_error dedisp_b200_batch_execute(dedisp_b200_batch batch, void* stream, int use_graph);
+/* Device time of the last execute's transposes and dedispersion (with
+ * timing enabled; execute then waits for its work). With use_graph the
+ * transposes are inside the graph: transpose_ms is -1 and dedisperse_ms is
+ * the whole graph. */
+dedisp_error dedisp_b200_batch_set_timing(dedisp_b200_batch batch, int enable);
+dedisp_error dedisp_b200_batch_get_timing(dedisp_b200_batch batch, float* transpose_ms,
+                                          float* dedisperse_ms, int* launches);
+dedisp_size dedisp_b200_batch_max_delay(dedisp_b200_batch batch, dedisp_size beam);
+/* The batch functions return their specific error code; the message of the
+ * last failure on the calling thread is available from dedisp_b200_last_error. */
+
 /* Floats per DM row that execute() writes for nsamps input samples. */
 dedisp_size dedisp_b200_output_row_length(dedisp_plan plan, dedisp_size nsamps);
 

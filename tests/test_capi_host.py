@@ -163,3 +163,28 @@ def test_fdd_output_row_length_follows_reference_geometry():
     assert p.output_row_length(n) == n - 5243           # segmented: time series
     p.set_options(segmented=0, timeseries=True)
     assert p.output_row_length(n) == n - 5243
+
+
+def test_batch_api_argument_checks():
+    """Host-side checks of the batch interface; no GPU work is launched."""
+    L = dd._batch_lib()
+    h = C.c_void_p()
+    assert L.dedisp_b200_batch_create(None, 64, 1e-4, 1500.0, -1.0, 8, 32, 0) == 5  # invalid pointer
+    assert L.dedisp_b200_batch_execute(None, None, 1) == 4                        # invalid plan
+    assert L.dedisp_b200_batch_set_beams(None, None, 0) == 4
+    assert L.dedisp_b200_batch_workspace_size(None) == 0
+    L.dedisp_b200_batch_destroy(None)
+    # unsupported widths are rejected before any device work
+    assert L.dedisp_b200_batch_create(C.byref(h), 64, 1e-4, 1500.0, -1.0, 3, 32, 0) == 10
+    assert L.dedisp_b200_batch_create(C.byref(h), 64, 1e-4, 1500.0, -1.0, 8, 12, 0) == 11
+    assert not h.value
+
+
+@pytest.mark.skipif(__import__("torch").cuda.is_available(), reason="checks the no-GPU path")
+def test_batch_create_without_gpu_fails_cleanly():
+    L = dd._batch_lib()
+    h = C.c_void_p()
+    rc = L.dedisp_b200_batch_create(C.byref(h), 64, 1e-4, 1500.0, -1.0, 8, 32, 0)
+    assert rc != 0 and not h.value
+    with pytest.raises(dd.DedispError):
+        dd.Batch(64, 1e-4, 1500.0, -1.0)
