@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--fdd-only", action="store_true",
                     help="run only the FDD forms (config 2) and print their JSON object")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-only", action="store_true",
+                    help="run only the streaming server (config 4) and print its JSON object")
     ap.add_argument("--batched-only", action="store_true",
                     help="run only the batched multi-beam TDD (config 3) and print its JSON object")
     ap.add_argument("--profile-case", default="",
@@ -419,6 +422,73 @@ def run_batched(args, local, world, stream, max_over_ranks):
     return res
 
 
+def run_serving(args, local, world):
+    """Config 4: 32 beams of 4096 ch 2-bit (f_top 1500 MHz, df -0.078125 MHz,
+    dt 64 us), 2048 DM trials over 0-1500, through the streaming server: 28
+    TDD beams (gulps of 16384, 65536 or 262144 samples) and 4 FDD beams (3xBF16
+    tensor-core MAC, 32768-point segments, gulps of 16384 or 65536). Gulps
+    arrive as a Poisson process at 1x, 2x, 4x and 8x the aggregate real-time
+    sample rate (32 x 15625 samples/s) for a fixed window each; outputs stay
+    on the device (a GPU consumer reads each worker's buffer). All beams read
+    the same pinned host gulp (its contents do not affect the work)."""
+    import torch
+    import dedisp_tests_b200 as dd
+    from dedisp_tests_b200 import synthetic as sy
+    nch, f0, df, dt, nbits = 4096, 1500.0, -0.078125, 64e-6, 2
+    dms = (1500.0 * np.arange(2048) / 2047.0).astype(np.float32)
+    nbeams, n_fdd = 32, 4
+    sizes_tdd, sizes_fdd = [16384, 65536, 262144], [16384, 65536]
+    srv = dd.StreamServer(nch, dt, f0, df, in_nbits=nbits, device=local, hbm_budget=int(120e9),
+                          max_gulp=max(sizes_tdd), tdd_workers=4, fdd_workers=1, fdd_precision=1,
+                          fdd_segment=32768, fdd_max_gulp=max(sizes_fdd))
+    kinds = [0] * (nbeams - n_fdd) + [1] * n_fdd
+    for k in kinds:
+        srv.add_beam(dms, k)
+    held = srv.start()
+    cfg = sy.Config("serve-gulp", nch, f0, df, dt, max(sizes_tdd), nbits, 1.5, 1.0,
+                    [sy.Pulse(700.0, 8.0, 1e-3, 3.0)], seed=20261207)
+    host = torch.empty((cfg.nsamps, nch * nbits // 8), dtype=torch.uint8, pin_memory=True)
+    host.copy_(sy.make_input_torch(cfg, device=f"cuda:{local}").cpu())
+    rt_rate = nbeams * 15625.0
+    rng = np.random.default_rng(7)
+    window = 6.0
+    out = {"workload": "32 beams x 4096 ch 2-bit, 2048 DMs 0-1500, 28 TDD + 4 FDD beams",
+           "hbm_budget_bytes": int(120e9), "device_bytes_held": held, "workers": "4 TDD + 1 FDD",
+           "window_s": window, "rates": {}}
+    mean_n = ((nbeams - n_fdd) * np.mean(sizes_tdd) + n_fdd * np.mean(sizes_fdd)) / nbeams
+    for rate in (1, 2, 4, 8):
+        lam = rate * rt_rate / mean_n
+        n0 = len(srv.records())
+        t0 = time.perf_counter()
+        t_next = t0
+        while True:
+            t_next += rng.exponential(1.0 / lam)
+            if t_next - t0 > window:
+                break
+            b = int(rng.integers(0, nbeams))
+            n = int(rng.choice(sizes_tdd if kinds[b] == 0 else sizes_fdd))
+            dly = t_next - time.perf_counter()
+            if dly > 0:
+                time.sleep(dly)
+            srv.submit(b, host, n)
+        srv.drain()
+        recs = srv.records()[n0:]
+        lat = np.array([r["t_done"] - r["t_submit"] for r in recs])
+        samples = float(sum(r["nsamps"] for r in recs))
+        wall = max(r["t_done"] for r in recs) - min(r["t_submit"] for r in recs)
+        out["rates"][f"{rate}x"] = {
+            "gulps": len(recs), "samples": samples,
+            "latency_p50_ms": float(np.percentile(lat, 50) * 1e3),
+            "latency_p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "throughput": samples * len(dms) / wall, "unit": UNIT,
+            "real_time_factor": samples / wall / rt_rate,
+            "offered_real_time_factor": float(rate)}
+    srv.close()
+    del host
+    torch.cuda.empty_cache()
+    return out
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -458,6 +528,13 @@ def run_ours(args):
         return float(t.item())
 
     stream = torch.cuda.current_stream()
+    if args.serve_only:
+        res = run_serving(args, local, world)
+        if rank == 0:
+            print(json.dumps({"serving": res}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
     if args.batched_only:
         res = run_batched(args, local, world, stream, max_over_ranks)
         if rank == 0:
@@ -653,6 +730,11 @@ def run_ours(args):
             torch.cuda.empty_cache()
         batched = run_batched(args, local, world, stream, max_over_ranks)
 
+    # --- streaming server (config 4) -----------------------------------------------
+    serving = None
+    if not args.no_serve:
+        serving = run_serving(args, local, world)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -667,7 +749,7 @@ def run_ours(args):
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches * world, "clocks": clocks, "variants": variants,
             "tile_variant": {"chosen": best, "k2_ms_by_variant": tune},
-            "fdd": fdd, "batched": batched,
+            "fdd": fdd, "batched": batched, "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -46,6 +46,7 @@ ERROR_NAMES = [
     "DEDISP_DEVICE_ALREADY_SET", "DEDISP_PRIOR_GPU_ERROR", "DEDISP_INTERNAL_GPU_ERROR",
     "DEDISP_UNKNOWN_ERROR",
 ]
+DEDISP_UNKNOWN_ERROR = ERROR_NAMES.index("DEDISP_UNKNOWN_ERROR")
 
 
 class DedispError(RuntimeError):
@@ -414,3 +415,121 @@ class Batch:
 
     def max_delay(self, beam: int) -> int:
         return int(_batch_lib().dedisp_b200_batch_max_delay(self._h, beam))
+
+
+# ---------------------------------------------------------------------------
+# Streaming server (dedisp_b200_server_*)
+# ---------------------------------------------------------------------------
+
+class _GulpRecord(C.Structure):
+    _fields_ = [("beam", C.c_int), ("worker", C.c_int), ("nsamps", _sz), ("t_submit", C.c_double),
+                ("t_start", C.c_double), ("t_done", C.c_double), ("device_ms", C.c_float)]
+
+
+_SERVER_SIGS = {
+    "dedisp_b200_server_create": (C.c_int, [C.POINTER(_vp), _sz, C.c_float, C.c_float, C.c_float,
+                                            _sz, C.c_int, _sz, _sz, C.c_int, C.c_int, C.c_int, _sz,
+                                            _sz]),
+    "dedisp_b200_server_destroy": (None, [_vp]),
+    "dedisp_b200_server_add_beam": (C.c_int, [_vp, _vp, _sz, C.c_int]),
+    "dedisp_b200_server_max_delay": (_sz, [_vp, C.c_int]),
+    "dedisp_b200_server_start": (C.c_int, [_vp, C.POINTER(_sz)]),
+    "dedisp_b200_server_submit": (C.c_long, [_vp, C.c_int, _vp, _sz, _vp]),
+    "dedisp_b200_server_done": (C.c_int, [_vp, C.c_long]),
+    "dedisp_b200_server_wait": (C.c_int, [_vp, C.c_long]),
+    "dedisp_b200_server_drain": (C.c_int, [_vp]),
+    "dedisp_b200_server_record_count": (_sz, [_vp]),
+    "dedisp_b200_server_records": (C.c_int, [_vp, C.POINTER(_GulpRecord), _sz]),
+}
+
+
+def _server_lib() -> C.CDLL:
+    L = lib()
+    if not getattr(L, "_server_sigs", False):
+        for name, (res, args) in _SERVER_SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        L._server_sigs = True
+    return L
+
+
+def _last_message() -> str:
+    buf = C.create_string_buffer(512)
+    lib().dedisp_b200_last_error(buf, 512)
+    return buf.value.decode(errors="replace")
+
+
+class StreamServer:
+    """Streaming dedispersion of many beams' gulps with device-resident
+    overlap tails (kind 0: TDD, 1: FDD). See include/dedisp_b200.h."""
+
+    TDD, FDD = 0, 1
+
+    def __init__(self, nchans: int, dt: float, f0: float, df: float, in_nbits: int = 8,
+                 device: int = 0, hbm_budget: int = 0, max_gulp: int = 1 << 18,
+                 tdd_workers: int = 2, fdd_workers: int = 0, fdd_precision: int = 1,
+                 fdd_segment: int = 0, fdd_max_gulp: int = 0):
+        self._h = _vp()
+        _bcheck(_server_lib().dedisp_b200_server_create(
+            C.byref(self._h), nchans, dt, f0, df, in_nbits, device, int(hbm_budget), max_gulp,
+            tdd_workers, fdd_workers, fdd_precision, fdd_segment, fdd_max_gulp))
+        self.nchans, self.in_nbits = nchans, in_nbits
+        self._rows = {}
+
+    def close(self) -> None:
+        if self._h:
+            _server_lib().dedisp_b200_server_destroy(self._h)
+            self._h = _vp()
+        self._rows = {}
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_beam(self, dms, kind: int = 0) -> int:
+        dm = np.ascontiguousarray(dms, dtype=np.float32)
+        b = _server_lib().dedisp_b200_server_add_beam(self._h, dm.ctypes.data, len(dm), kind)
+        if b < 0:
+            raise DedispError(DEDISP_UNKNOWN_ERROR, DEDISP_UNKNOWN_ERROR, _last_message())
+        return b
+
+    def max_delay(self, beam: int) -> int:
+        return int(_server_lib().dedisp_b200_server_max_delay(self._h, beam))
+
+    def start(self) -> int:
+        n = _sz()
+        _bcheck(_server_lib().dedisp_b200_server_start(self._h, C.byref(n)))
+        return int(n.value)
+
+    def submit(self, beam: int, rows, nsamps: int, d_out=None) -> int:
+        t = _server_lib().dedisp_b200_server_submit(self._h, beam, _addr(rows), nsamps, _addr(d_out))
+        if t < 0:
+            raise DedispError(DEDISP_UNKNOWN_ERROR, DEDISP_UNKNOWN_ERROR, _last_message())
+        self._rows[t] = (rows, d_out)
+        return t
+
+    def done(self, ticket: int) -> bool:
+        d = _server_lib().dedisp_b200_server_done(self._h, ticket)
+        if d < 0:
+            raise DedispError(DEDISP_UNKNOWN_ERROR, DEDISP_UNKNOWN_ERROR, _last_message())
+        return bool(d)
+
+    def wait(self, ticket: int) -> None:
+        _bcheck(_server_lib().dedisp_b200_server_wait(self._h, ticket))
+        self._rows.pop(ticket, None)
+
+    def drain(self) -> None:
+        _bcheck(_server_lib().dedisp_b200_server_drain(self._h))
+        self._rows = {}
+
+    def records(self) -> list:
+        L = _server_lib()
+        n = int(L.dedisp_b200_server_record_count(self._h))
+        arr = (_GulpRecord * max(n, 1))()
+        _bcheck(L.dedisp_b200_server_records(self._h, arr, n))
+        return [{"beam": r.beam, "worker": r.worker, "nsamps": int(r.nsamps),
+                 "t_submit": r.t_submit, "t_start": r.t_start, "t_done": r.t_done,
+                 "device_ms": r.device_ms} for r in arr[:n]]

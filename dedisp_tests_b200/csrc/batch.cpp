@@ -66,7 +66,8 @@ TddBatch::TddBatch(size_t nchans, float dt, float f0, float df, int in_nbits, in
 
 TddBatch::~TddBatch()
 {
-    rt::DeviceGuard g(m_device);
+    int cur = -1;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur != m_device) cudaSetDevice(m_device);
     cudaDeviceSynchronize();
     drop_graph();
 }

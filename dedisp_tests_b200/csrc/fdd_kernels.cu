@@ -232,8 +232,8 @@ __global__ void __launch_bounds__(512) fft_c2r_kernel(const float2* Y, size_t bi
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) fdd_unpack_kernel(const uint8_t* in, size_t in_stride,
                                                          int in_nbits, size_t nsamps, size_t nchans,
-                                                         float scale, float* x, size_t x_pitch,
-                                                         size_t x_len)
+                                                         float scale, float mid, float* x,
+                                                         size_t x_pitch, size_t x_len)
 {
     __shared__ float tile[32][33];
     const size_t t0 = (size_t)blockIdx.x * 32, c0 = (size_t)blockIdx.y * 32;
@@ -244,11 +244,19 @@ __global__ void __launch_bounds__(256) fdd_unpack_kernel(const uint8_t* in, size
         if (t < nsamps && c < nchans) {
             if (in_nbits == 8) {
                 v = ((float)in[t * in_stride + c] - 127.5f) * scale;
-            } else {
+            } else if (in_nbits == 32) {
                 const uint8_t* p = in + t * in_stride + 4 * c;
                 uint32_t u = (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) |
                              ((uint32_t)p[3] << 24);
                 v = __uint_as_float(u) * scale;
+            } else if (in_nbits == 16) {
+                const uint8_t* p = in + t * in_stride + 2 * c;
+                v = ((float)((uint32_t)p[0] | ((uint32_t)p[1] << 8)) - mid) * scale;
+            } else {
+                // 1/2/4-bit samples packed LSB-first within each byte
+                const size_t bit = c * (size_t)in_nbits;
+                const uint32_t u = (in[t * in_stride + (bit >> 3)] >> (bit & 7)) & ((1u << in_nbits) - 1u);
+                v = ((float)u - mid) * scale;
             }
         }
         tile[r][tx] = v;
@@ -482,8 +490,11 @@ void launch_fdd_unpack(const uint8_t* in, size_t in_stride, int in_nbits, size_t
                        size_t nchans, float scale, float* x, size_t x_pitch, size_t x_len,
                        cudaStream_t s)
 {
+    // packed unsigned samples are centred at mid-scale, (2^nbits - 1) / 2
+    // (127.5 for 8-bit, as the reference's unpack_kernel.cuh:60)
+    const float mid = in_nbits == 32 ? 0.f : (float)((1u << in_nbits) - 1u) * 0.5f;
     dim3 grid((unsigned)((x_len + 31) / 32), (unsigned)((nchans + 31) / 32));
-    fdd_unpack_kernel<<<grid, 256, 0, s>>>(in, in_stride, in_nbits, nsamps, nchans, scale, x,
+    fdd_unpack_kernel<<<grid, 256, 0, s>>>(in, in_stride, in_nbits, nsamps, nchans, scale, mid, x,
                                            x_pitch, x_len);
     RT_CHECK(cudaGetLastError());
 }

@@ -71,11 +71,16 @@ void FDDGPUPlan::execute(size_type nsamps, const byte_type* in, size_type in_nbi
                          byte_type* out, size_type out_nbits, unsigned flags)
 {
     // The reference asserts 8-bit input and float output (FDDGPUPlan.cpp:
-    // 66-67); in_nbits 32 (IEEE float samples) is an extension.
+    // 66-67); in_nbits 32 (IEEE float samples) and 1/2/4/16-bit packed
+    // samples (centred at (2^nbits - 1) / 2 like the 8-bit 127.5) are
+    // extensions.
     if (in == nullptr || out == nullptr) DD_THROW(DEDISP_INVALID_POINTER);
     if (m_dm_count == 0) DD_THROW(DEDISP_NO_DM_LIST_SET);
     if (nsamps < m_max_delay) DD_THROW(DEDISP_TOO_FEW_NSAMPS);
-    if (in_nbits != 8 && in_nbits != 32) DD_THROW(DEDISP_UNSUPPORTED_IN_NBITS);
+    if (in_nbits != 1 && in_nbits != 2 && in_nbits != 4 && in_nbits != 8 && in_nbits != 16 &&
+        in_nbits != 32)
+        DD_THROW(DEDISP_UNSUPPORTED_IN_NBITS);
+    if ((m_nchans * in_nbits) % 8 != 0) DD_THROW(DEDISP_INVALID_STRIDE);
     if (out_nbits != 32) DD_THROW(DEDISP_UNSUPPORTED_OUT_NBITS);
     detail::FddView v{m_nchans, m_dt, h_delay_table.data(), h_killmask.data(),
                       h_dm_list.data(), m_dm_count, m_max_delay, m_state_version};

@@ -147,6 +147,56 @@ dedisp_size dedisp_b200_batch_max_delay(dedisp_b200_batch batch, dedisp_size bea
 /* The batch functions return their specific error code; the message of the
  * last failure on the calling thread is available from dedisp_b200_last_error. */
 
+/* ------------------------------------------------------------------------
+ * Streaming server. No counterpart in the reference. Beams deliver host
+ * gulps of any length (<= max_gulp); the server keeps each beam's last
+ * max_delay input rows on the device, so a gulp of n rows yields n output
+ * samples per DM (the dedispersion of tail + gulp; tails start as zero
+ * rows). kind 0 beams run on TDD workers, kind 1 on FDD workers (segmented
+ * time-series output; fdd_precision 0 FP32, 1 3xBF16 tensor cores;
+ * fdd_segment 0 = the plan's FFT-length rule; FDD gulps at most
+ * fdd_max_gulp samples, 0 = max_gulp). Each worker is a host thread
+ * with its own CUDA stream and plans; start() allocates everything and
+ * fails with DEDISP_MEM_ALLOC_FAILED above hbm_budget bytes (0: no limit),
+ * after which submit() does not allocate. Gulps of one beam run in order.
+ * d_out: device buffer of dm_count x nsamps floats, or NULL (the worker's
+ * own buffer, reused by its next gulp). Host rows must stay valid until the
+ * gulp is done; pinned memory makes the copy asynchronous.
+ * ---------------------------------------------------------------------- */
+typedef struct dedisp_b200_server_struct* dedisp_b200_server;
+
+typedef struct {
+    int beam;
+    int worker;
+    dedisp_size nsamps;
+    double t_submit;   /* seconds, monotonic host clock */
+    double t_start;
+    double t_done;
+    float device_ms;   /* H2D + dedispersion + tail copy, CUDA events */
+} dedisp_b200_gulp_record;
+
+dedisp_error dedisp_b200_server_create(dedisp_b200_server* server, dedisp_size nchans, dedisp_float dt,
+                                       dedisp_float f0, dedisp_float df, dedisp_size in_nbits, int device,
+                                       dedisp_size hbm_budget, dedisp_size max_gulp, int tdd_workers,
+                                       int fdd_workers, int fdd_precision, dedisp_size fdd_segment,
+                                       dedisp_size fdd_max_gulp);
+void dedisp_b200_server_destroy(dedisp_b200_server server);
+/* Returns the beam index, or -1 (dedisp_b200_last_error has the reason). */
+int dedisp_b200_server_add_beam(dedisp_b200_server server, const dedisp_float* dm_list,
+                                dedisp_size dm_count, int kind);
+dedisp_size dedisp_b200_server_max_delay(dedisp_b200_server server, int beam);
+dedisp_error dedisp_b200_server_start(dedisp_b200_server server, dedisp_size* bytes_held);
+/* Returns a ticket >= 0, or -1. */
+long dedisp_b200_server_submit(dedisp_b200_server server, int beam, const dedisp_byte* rows,
+                               dedisp_size nsamps, dedisp_float* d_out);
+/* 1 done, 0 pending, -1 error. */
+int dedisp_b200_server_done(dedisp_b200_server server, long ticket);
+dedisp_error dedisp_b200_server_wait(dedisp_b200_server server, long ticket);
+dedisp_error dedisp_b200_server_drain(dedisp_b200_server server);
+dedisp_size dedisp_b200_server_record_count(dedisp_b200_server server);
+dedisp_error dedisp_b200_server_records(dedisp_b200_server server, dedisp_b200_gulp_record* records,
+                                        dedisp_size count);
+
 /* Floats per DM row that execute() writes for nsamps input samples. */
 dedisp_size dedisp_b200_output_row_length(dedisp_plan plan, dedisp_size nsamps);
 

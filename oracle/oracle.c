@@ -289,19 +289,32 @@ int orc_tdd(const uint8_t* in, size_t nsamps, size_t in_stride, int in_nbits,
 int orc_fdd_unpack(const uint8_t* in, size_t nsamps, size_t in_stride,
                    int in_nbits, size_t nchans, float* x)
 {
-    if (in_nbits != 8 && in_nbits != 32) return -1;
+    if (in_nbits != 1 && in_nbits != 2 && in_nbits != 4 && in_nbits != 8 && in_nbits != 16 &&
+        in_nbits != 32)
+        return -1;
     /* FDDGPUPlan.cpp:472 passes 1.0/nchan to a float parameter. */
     float scale = (float)(1.0 / (double)nchans);
+    /* 8-bit: (v - 127.5) * scale (unpack_kernel.cuh:60); other packed widths
+       (an extension of this library) are centred at (2^nbits - 1) / 2. */
+    float mid = in_nbits == 32 ? 0.f : (float)((1u << in_nbits) - 1u) * 0.5f;
     for (size_t c = 0; c < nchans; ++c) {
         for (size_t t = 0; t < nsamps; ++t) {
             float v;
             if (in_nbits == 8) {
                 uint32_t u = in[t * in_stride + c];
                 v = ((float)u - 127.5f) * scale;
-            } else {
+            } else if (in_nbits == 32) {
                 float f;
                 memcpy(&f, in + t * in_stride + 4 * c, 4);
                 v = f * scale;
+            } else if (in_nbits == 16) {
+                const uint8_t* p = in + t * in_stride + 2 * c;
+                uint32_t u = (uint32_t)p[0] | ((uint32_t)p[1] << 8);
+                v = ((float)u - mid) * scale;
+            } else {
+                size_t bit = c * (size_t)in_nbits;
+                uint32_t u = (in[t * in_stride + bit / 8] >> (bit % 8)) & ((1u << in_nbits) - 1u);
+                v = ((float)u - mid) * scale;
             }
             x[c * nsamps + t] = v;
         }

@@ -188,3 +188,20 @@ def test_batch_create_without_gpu_fails_cleanly():
     assert rc != 0 and not h.value
     with pytest.raises(dd.DedispError):
         dd.Batch(64, 1e-4, 1500.0, -1.0)
+
+
+def test_server_api_host_checks():
+    """Streaming-server argument checks that need no GPU work."""
+    s = dd.StreamServer(256, 64e-6, 1500.0, -0.25, in_nbits=8, max_gulp=4096, tdd_workers=1)
+    b = s.add_beam(np.linspace(0, 100, 20, dtype=np.float32), 0)
+    assert b == 0 and s.max_delay(0) > 0
+    with pytest.raises(dd.DedispError):
+        s.add_beam(np.linspace(0, 100, 20, dtype=np.float32), 1)  # no FDD workers
+    with pytest.raises(dd.DedispError):
+        s.submit(0, np.zeros((10, 256), np.uint8), 10)            # before start()
+    s.close()
+    L = dd._server_lib()
+    h = C.c_void_p()
+    assert L.dedisp_b200_server_create(C.byref(h), 256, 64e-6, 1500.0, -0.25, 3, 0, 0, 4096, 1, 0, 1, 0, 0) == 10
+    assert L.dedisp_b200_server_create(C.byref(h), 256, 64e-6, 1500.0, -0.25, 8, 0, 0, 4096, 0, 0, 1, 0, 0) != 0
+    assert L.dedisp_b200_server_drain(None) == 4

@@ -192,3 +192,24 @@ def test_against_reference_fdd_outputs():
         our_err = _errs(out[rows][:, sl], f64[rows][:, sl])[0]
         assert ref_err < 5e-2, ref_err
         assert our_err < FP32_REL_L2 and our_err * 5 < ref_err, (our_err, ref_err)
+
+
+@pytest.mark.parametrize("nbits,precision", [(2, 0), (4, 0), (2, 1), (16, 0)])
+def test_packed_input_widths(nbits, precision):
+    """1/2/4/16-bit packed input (an extension; samples centred at
+    (2^nbits - 1) / 2), both MAC forms."""
+    nchans, nsamps = 128, 40000
+    rng = np.random.default_rng(40 + nbits)
+    vals = rng.integers(0, 1 << nbits, (nsamps, nchans), dtype=np.uint32)
+    inp = sy.pack(vals, nbits)
+    params = (nchans, 250e-6, 1581.8, -1.5625)
+    dms = np.linspace(0, 90, 21, dtype=np.float32)
+    p = _plan(params, dms, segmented=1, precision=precision)
+    nout = nsamps - p.get_max_delay()
+    out = np.zeros((len(dms), nout), np.float32)
+    p.execute(nsamps, inp, nbits, out, 32)
+    x = _oracle_x(inp, nsamps, params, nbits)
+    ref = po.fdd_timeseries(x, _delays(params), np.ones(nchans, np.int32), dms, nout)
+    rel, mx = _errs(out, ref)
+    tol = (FP32_REL_L2, FP32_MAX_ABS) if precision == 0 else (1e-5, 1e-4)
+    assert rel < tol[0] and mx < tol[1], (rel, mx)

@@ -122,3 +122,17 @@ def test_segment_geometry_matches_reference_rule():
     # config 2: max delay 5243 -> nfft 32768, nsamp_good 27525, 39 chunks
     assert po.fdd_segment_geometry(1 << 20, 5243) == (32768, 27525, 39)
     assert po.fdd_nfft_spectrum(1 << 20, 5243) == 1064960
+
+
+@pytest.mark.parametrize("nbits", [1, 2, 4, 8, 16])
+def test_oracle_fdd_unpack_packed_widths(nbits):
+    """Packed samples are centred at (2^nbits - 1) / 2 and scaled by 1/nchans
+    (8-bit: the reference's (v - 127.5) / nchan)."""
+    rng = np.random.default_rng(nbits)
+    nchans, nsamps = 64, 50
+    vals = rng.integers(0, 1 << nbits, (nsamps, nchans), dtype=np.uint32)
+    packed = sy.pack(vals, nbits)
+    x = po.fdd_unpack(packed, nsamps, packed.shape[1], nbits, nchans)
+    mid = np.float32(((1 << nbits) - 1) * 0.5)
+    want = ((vals.astype(np.float32) - mid) * np.float32(1.0 / nchans)).T
+    assert np.array_equal(x, want)
