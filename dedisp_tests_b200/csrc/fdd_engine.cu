@@ -28,6 +28,9 @@ struct FddEngine::Impl {
     unsigned tw_n = 0;
     unsigned long version = ~0ul;
     unsigned long pad_version = ~0ul;
+    unsigned long dmax_version = ~0ul;
+    int dmax_round = -1;
+    int dmax = -1;               // largest delay index, -1 if any DM is negative or NaN
     int nact = 0;
     std::vector<float> delays_active;
 };
@@ -182,6 +185,8 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
         ta.dms = m.dms.get<float>();
         ta.delay_act = m.delay_pad.get<float>();
         ta.table = m.qtable.get<uint2>();
+        ta.tw_lo = m.tw_lo.get<float2>();
+        ta.tw_hi = m.tw_hi.get<float2>();
         ta.err = m.err.get<unsigned>();
         ta.nact_pad = nact_pad;
         ta.ndm = (int)ndm;
@@ -190,6 +195,27 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
         ta.nbins = nbins;
         ta.nfft = (unsigned)g.nfft;
         ta.round_delays = opt.round_delays ? 1 : 0;
+        // Largest delay index over all DMs and active channels (same float
+        // operations as the kernel); the kernel then builds a per-bin
+        // phasor table over 0..dmax when it fits shared memory.
+        if (m.dmax_version != v.version || m.dmax_round != ta.round_delays) {
+            long dmax = 0;
+            bool ok = true;
+            for (size_t i = 0; i < ndm && ok; ++i) {
+                const float d = v.dms[i];
+                if (!(d >= 0.f)) { ok = false; break; }
+                for (float dl : m.delays_active) {
+                    const long x = ta.round_delays ? (long)hostmath::delay_rn(d, dl)
+                                                   : (long)hostmath::delay_trunc(d, dl);
+                    dmax = std::max(dmax, x);
+                }
+            }
+            m.dmax = (ok && dmax < (1l << 30)) ? (int)dmax : -1;
+            m.dmax_version = v.version;
+            m.dmax_round = ta.round_delays;
+        }
+        ta.dmax = kern::tc_table_mode_dmax(m.dmax, ta.nfft, nact_pad, npad);
+        ta.stages = kern::tc_stages(ta.nfft, nact_pad, npad, ta.dmax);
         kern::launch_fdd_mac_tc(ta, m.B.get(), st);
         stats.launches = 1;
     } else if (m.nact > 0) {

@@ -12,14 +12,14 @@
 //   D = Ah Bh + Ah Bl + Al Bh   (FP32 accumulation in tensor memory).
 //
 // Roles (one CTA per SM, 128 DMs per CTA, a range of bins per CTA):
-//   warps 0-7   phasor producers: each thread owns one DM row (its TMEM
-//               lane) and half of every 64-channel chunk; phasors come from
+//   warps 0-15  phasor producers: each thread owns one DM row (its TMEM
+//               lane) and a quarter of every 64-channel chunk; phasors come from
 //               the exact integer phase index (k*d) mod nfft and a quarter-
 //               wave table of pre-split BF16 (cos, sin) pairs, and are stored
 //               into tensor memory as the A operand; the same warps read the
 //               accumulator of each finished bin and write Yt[k][s][dm].
-//   warp 8      TMA producer for the B chunks (pre-split BF16, 128B swizzle).
-//   warp 9      TMEM allocation and the single-thread MMA issuer.
+//   warp 16     TMA producer for the B chunks (pre-split BF16, 128B swizzle).
+//   warp 17     TMEM allocation and the single-thread MMA issuer.
 // Every wait on an mbarrier is bounded; on expiry the kernel records an
 // error code and winds down without waiting further.
 #include <cuda.h>
@@ -40,8 +40,10 @@ namespace {
 
 constexpr int TC_M = 128;              // DMs per CTA (accumulator lanes)
 constexpr int TC_CHUNK = 64;           // channels per K chunk (K = 128 reals)
-constexpr int TC_STAGES = 3;           // B pipeline depth (smem: 3 x 40 KB + table)
-constexpr int TC_PRODUCER_WARPS = 8;
+constexpr int TC_MAX_STAGES = 6;       // B pipeline depth: as many as shared memory allows, 2..6
+constexpr int TC_PRODUCER_WARPS = 16;  // 4 per TMEM lane quadrant
+constexpr int TC_PARTS = TC_PRODUCER_WARPS / 4;  // producers sharing one DM row
+constexpr int TC_PART_CH = 64 / TC_PARTS;        // channels per producer per chunk
 constexpr int TC_THREADS = (TC_PRODUCER_WARPS + 2) * 32;
 // Bounded mbarrier waits: give up after TC_WAIT_NS of global time (checked
 // every 16 polls) or TC_WAIT_POLLS polls, whichever comes first.
@@ -57,14 +59,15 @@ constexpr size_t TC_MAX_SMEM = 227 * 1024;
 constexpr uint32_t TM_A0 = 0, TM_A1 = 128, TM_C0 = 256, TM_C1 = 384;
 
 struct alignas(8) SmemBarriers {
-    uint64_t b_full[TC_STAGES];
-    uint64_t b_empty[TC_STAGES];
+    uint64_t b_full[TC_MAX_STAGES];
+    uint64_t b_empty[TC_MAX_STAGES];
     uint64_t a_full[2];
     uint64_t a_empty[2];
     uint64_t c_full[2];
     uint64_t c_empty[2];
     uint64_t drain;
     uint32_t tmem_base;
+    uint32_t abort_flag;  // a producer gave up a bounded wait (delay-table mode)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
@@ -159,6 +162,17 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar)
 }
 
 // 32 consecutive 32-bit columns of this thread's lane.
+// 16 consecutive 32-bit columns of this thread's lane.
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&v)[16])
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+        "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(taddr),
+        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
+        "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]),
+        "r"(v[15]));
+}
+
 __device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32])
 {
     asm volatile(
@@ -196,21 +210,50 @@ __device__ __forceinline__ int tc_delay(float dm, float delay, int round_delays)
     return round_delays ? (int)__float2uint_rn(x) : __float2int_rz(x);
 }
 
+// The same delay for 0 <= dm*delay < 2^22 without a conversion instruction:
+// adding 2^23 leaves the integer part (rounded toward zero, or to nearest
+// even) in the low mantissa bits.
+__device__ __forceinline__ int tc_delay_small(float dm, float delay, int round_delays)
+{
+    const float x = __fmul_rn(dm, delay);
+    const float y = round_delays ? __fadd_rn(x, 8388608.0f) : __fadd_rz(x, 8388608.0f);
+    return (int)(__float_as_uint(y) - 0x4B000000u);
+}
+
+// (re, im) -> packed bf16x2 hi parts (re low half) and lo parts
+// (bf16(x - hi)).
+__device__ __forceinline__ uint2 split_bf16x2(float re, float im)
+{
+    const __nv_bfloat162 hi = __floats2bfloat162_rn(re, im);
+    const float2 hf = __bfloat1622float2(hi);
+    const __nv_bfloat162 lo = __floats2bfloat162_rn(__fsub_rn(re, hf.x), __fsub_rn(im, hf.y));
+    return make_uint2(*reinterpret_cast<const uint32_t*>(&hi), *reinterpret_cast<const uint32_t*>(&lo));
+}
+
 __global__ void __launch_bounds__(TC_THREADS, 1)
 fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
 {
     extern __shared__ __align__(1024) uint8_t smem_dyn[];
     // layout (from a 1024-byte aligned base, as the 128-byte swizzle needs):
-    // [B stages][barriers][quarter-wave table][delays][sym]
+    // [B stages][barriers][phasor table][delays][sym]; the phasor table is
+    // the quarter-wave table (nfft/4 + 1 entries) or, in delay-table mode
+    // (a.dmax >= 0), the phasors of the current bin for every delay 0..dmax
     uint8_t* smem_raw = smem_dyn + ((1024u - (smem_u32(smem_dyn) & 1023u)) & 1023u);
     const uint32_t npad = (uint32_t)a.npad;
     const uint32_t atom_bytes = npad * 128u;           // one 64-kk atom of one split
     const uint32_t stage_bytes = 4u * atom_bytes;      // hi/lo x 2 atoms
     uint8_t* s_b = smem_raw;
-    SmemBarriers* bars = reinterpret_cast<SmemBarriers*>(smem_raw + TC_STAGES * stage_bytes);
+    const int nst = a.stages;
+    SmemBarriers* bars = reinterpret_cast<SmemBarriers*>(smem_raw + nst * stage_bytes);
     uint2* s_table = reinterpret_cast<uint2*>(reinterpret_cast<uint8_t*>(bars) + 256);
     const uint32_t qn = a.nfft / 4;                    // quarter-wave entries (+1)
-    float* s_delay = reinterpret_cast<float*>(s_table + (qn + 1));
+    const bool ptab = a.dmax >= 0;
+    const uint32_t tab_n = ptab ? (uint32_t)a.dmax + 1u : qn + 1u;
+    // table mode: exp(-2 pi i t / N) = tw_hi[t >> 8] * tw_lo[t & 255] (FP32)
+    const uint32_t nhi = a.nfft / 256;
+    float2* s_tw_lo = reinterpret_cast<float2*>(s_table + tab_n);
+    float2* s_tw_hi = s_tw_lo + (ptab ? 256 : 0);
+    float* s_delay = reinterpret_cast<float*>(s_tw_hi + (ptab ? nhi : 0));
     uint2* s_sym = reinterpret_cast<uint2*>(s_delay + a.nact_pad);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -223,7 +266,12 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
     const int nchunks = a.nact_pad / TC_CHUNK;
 
     // --- set-up -------------------------------------------------------------
-    for (uint32_t i = tid; i <= qn; i += blockDim.x) s_table[i] = a.table[i];
+    if (!ptab) {
+        for (uint32_t i = tid; i <= qn; i += blockDim.x) s_table[i] = a.table[i];
+    } else {
+        for (uint32_t i = tid; i < 256; i += blockDim.x) s_tw_lo[i] = a.tw_lo[i];
+        for (uint32_t i = tid; i < nhi; i += blockDim.x) s_tw_hi[i] = a.tw_hi[i];
+    }
     for (int i = tid; i < a.nact_pad; i += blockDim.x) s_delay[i] = a.delay_act[i];
     if (tid < 4) {
         // quadrant q of exp(+i theta): (re, im) = R^q (c, s); in packed
@@ -234,17 +282,18 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
         s_sym[tid] = make_uint2(sel[tid], neg[tid]);
     }
     if (tid == 0) {
-        for (int i = 0; i < TC_STAGES; ++i) {
+        for (int i = 0; i < nst; ++i) {
             mbar_init(&bars->b_full[i], 1);
             mbar_init(&bars->b_empty[i], 1);
         }
         for (int i = 0; i < 2; ++i) {
-            mbar_init(&bars->a_full[i], TC_PRODUCER_WARPS * 32);
+            mbar_init(&bars->a_full[i], TC_PRODUCER_WARPS);   // one arrive per producer warp
             mbar_init(&bars->a_empty[i], 1);
             mbar_init(&bars->c_full[i], 1);
-            mbar_init(&bars->c_empty[i], TC_PRODUCER_WARPS * 32);
+            mbar_init(&bars->c_empty[i], TC_PRODUCER_WARPS);
         }
         mbar_init(&bars->drain, 1);
+        bars->abort_flag = 0u;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == TC_PRODUCER_WARPS + 1) {
@@ -260,62 +309,117 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
 
     if (warp < TC_PRODUCER_WARPS) {
         // --- phasor producers + epilogue ------------------------------------
-        const int quad = warp & 3, half = warp >> 2;
+        // Order per bin k: (delay-table mode: rebuild the table for k), store
+        // the A chunks of k, then read out the accumulator of bin k-1 while
+        // the tensor cores work on k.
+        const int quad = warp & 3, part = warp >> 2;
         const int m = tile * TC_M + quad * 32 + lane;          // this thread's DM row
         const float dm = a.dms[min(m, a.ndm - 1)];
         const uint32_t lane_addr = (uint32_t)(quad * 32) << 16;
         const uint32_t nmask = a.nfft - 1u, qshift = (uint32_t)(31 - __clz((int)qn));
+        const int ptid = warp * 32 + lane;                      // 0..255
+        volatile uint32_t* abort_flag = &bars->abort_flag;
         uint32_t g = 0;  // global chunk counter
         int bin_iter = 0;
-        for (size_t k = k_begin; k < k_end && ok; ++k, ++bin_iter) {
-            for (int ch = 0; ch < nchunks && ok; ++ch, ++g) {
-                const uint32_t buf = g & 1u;
-                if (!mbar_wait_warp(&bars->a_empty[buf], ((g >> 1) & 1u) ^ 1u)) { ok = false; break; }
-                tc_fence_after();
-                uint32_t hi[32], lo[32];
-                const int c0 = ch * TC_CHUNK + half * 32;
-#pragma unroll
-                for (int i = 0; i < 32; ++i) {
-                    const int d = tc_delay(dm, s_delay[c0 + i], a.round_delays);
-                    const uint32_t idx = ((uint32_t)k * (uint32_t)d) & nmask;
-                    const uint32_t q = idx >> qshift, r = idx & (qn - 1u);
-                    const uint2 t = s_table[r];
-                    const uint2 sy = s_sym[q];
-                    hi[i] = __byte_perm(t.x, 0u, sy.x) ^ sy.y;
-                    lo[i] = __byte_perm(t.y, 0u, sy.x) ^ sy.y;
-                }
-                const uint32_t acol = buf ? TM_A1 : TM_A0;
-                tmem_st32(tmem + lane_addr + acol + half * 32, hi);
-                tmem_st32(tmem + lane_addr + acol + 64 + half * 32, lo);
-                tmem_wait_st();
-                tc_fence_before();
-                mbar_arrive(&bars->a_full[buf]);
-            }
-            if (!ok) break;
-            // epilogue of bin k: accumulator buffer bin_iter & 1
-            const uint32_t cb = (uint32_t)bin_iter & 1u;
-            if (!mbar_wait_warp(&bars->c_full[cb], ((uint32_t)bin_iter >> 1) & 1u)) { ok = false; break; }
+
+        auto epilogue = [&](int it, size_t kk) -> bool {
+            const uint32_t cb = (uint32_t)it & 1u;
+            if (!mbar_wait_warp(&bars->c_full[cb], ((uint32_t)it >> 1) & 1u)) return false;
             tc_fence_after();
             const uint32_t ccol = cb ? TM_C1 : TM_C0;
-            const int sh = (a.nseg + 1) / 2;
-            const int s0 = half * sh, s1 = min(a.nseg, s0 + sh);
-            for (int s = s0; s < s1; ++s) {
-                const float yr = tmem_ld1(tmem + lane_addr + ccol + s);
-                const float yi = tmem_ld1(tmem + lane_addr + ccol + a.nseg + s);
+            const int sh = (a.nseg + TC_PARTS - 1) / TC_PARTS;
+            const int s0 = min(a.nseg, part * sh), s1 = min(a.nseg, s0 + sh);
+            for (int sb = s0; sb < s1; sb += 8) {
+                const int cnt = min(8, s1 - sb);  // the same for the whole warp
+                float yr[8], yi[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    if (i < cnt) {
+                        yr[i] = tmem_ld1(tmem + lane_addr + ccol + sb + i);
+                        yi[i] = tmem_ld1(tmem + lane_addr + ccol + a.nseg + sb + i);
+                    }
+                }
                 tmem_wait_ld();
-                if (m < a.ndm) a.Yt[(k * a.nseg + s) * a.ndm + m] = make_float2(yr, yi);
+                if (m < a.ndm) {
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+                        if (i < cnt) a.Yt[(kk * a.nseg + sb + i) * a.ndm + m] = make_float2(yr[i], yi[i]);
+                }
             }
             tc_fence_before();
-            mbar_arrive(&bars->c_empty[cb]);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bars->c_empty[cb]);
+            return true;
+        };
+
+        bool aborted = false;
+        for (size_t k = k_begin; k < k_end; ++k, ++bin_iter) {
+            if (ptab) {
+                // All producers are done with the previous bin's table, and
+                // every abort raised before this point is visible to all.
+                asm volatile("bar.sync 1, %0;" ::"n"(TC_PRODUCER_WARPS * 32) : "memory");
+                if (*abort_flag) { aborted = true; break; }
+                for (int d = ptid; d <= a.dmax; d += TC_PRODUCER_WARPS * 32) {
+                    // exp(+2 pi i idx / N) = conj(tw_hi[idx >> 8] * tw_lo[idx & 255])
+                    const uint32_t idx = ((uint32_t)k * (uint32_t)d) & nmask;
+                    const float2 h = s_tw_hi[idx >> 8], l = s_tw_lo[idx & 255u];
+                    const float c = __fsub_rn(__fmul_rn(h.x, l.x), __fmul_rn(h.y, l.y));
+                    const float sn = -__fadd_rn(__fmul_rn(h.x, l.y), __fmul_rn(h.y, l.x));
+                    s_table[d] = split_bf16x2(c, sn);
+                }
+                asm volatile("bar.sync 1, %0;" ::"n"(TC_PRODUCER_WARPS * 32) : "memory");
+            } else if (!ok) {
+                break;
+            }
+            if (ok) {
+                for (int ch = 0; ch < nchunks; ++ch, ++g) {
+                    const uint32_t buf = g & 1u;
+                    if (!mbar_wait_warp(&bars->a_empty[buf], ((g >> 1) & 1u) ^ 1u)) { ok = false; break; }
+                    tc_fence_after();
+                    uint32_t hi[TC_PART_CH], lo[TC_PART_CH];
+                    const int c0 = ch * TC_CHUNK + part * TC_PART_CH;
+                    if (ptab) {
+#pragma unroll
+                        for (int i = 0; i < TC_PART_CH; ++i) {
+                            const int d = min(max(tc_delay_small(dm, s_delay[c0 + i], a.round_delays), 0), a.dmax);
+                            const uint2 v = s_table[d];
+                            hi[i] = v.x;
+                            lo[i] = v.y;
+                        }
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < TC_PART_CH; ++i) {
+                            const int d = tc_delay(dm, s_delay[c0 + i], a.round_delays);
+                            const uint32_t idx = ((uint32_t)k * (uint32_t)d) & nmask;
+                            const uint32_t q = idx >> qshift, r = idx & (qn - 1u);
+                            const uint2 t = s_table[r];
+                            const uint2 sy = s_sym[q];
+                            hi[i] = __byte_perm(t.x, 0u, sy.x) ^ sy.y;
+                            lo[i] = __byte_perm(t.y, 0u, sy.x) ^ sy.y;
+                        }
+                    }
+                    const uint32_t acol = buf ? TM_A1 : TM_A0;
+                    tmem_st16(tmem + lane_addr + acol + part * TC_PART_CH, hi);
+                    tmem_st16(tmem + lane_addr + acol + 64 + part * TC_PART_CH, lo);
+                    tmem_wait_st();
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&bars->a_full[buf]);
+                }
+            }
+            if (ok && bin_iter > 0) ok = epilogue(bin_iter - 1, k - 1);
+            if (!ok && ptab) *abort_flag = 1u;  // the others stop at the next barrier
         }
+        if (ok && !aborted && bin_iter > 0) ok = epilogue(bin_iter - 1, k_end - 1);
+        if (aborted) ok = false;
     } else if (warp == TC_PRODUCER_WARPS) {
         // --- TMA producer ------------------------------------------------------
         if (lane == 0) {
             uint32_t g = 0;
             for (size_t k = k_begin; k < k_end && ok; ++k) {
                 for (int ch = 0; ch < nchunks; ++ch, ++g) {
-                    const uint32_t st = g % TC_STAGES;
-                    if (!mbar_wait(&bars->b_empty[st], ((g / TC_STAGES) & 1u) ^ 1u)) { ok = false; break; }
+                    const uint32_t st = g % (uint32_t)nst;
+                    if (!mbar_wait(&bars->b_empty[st], ((g / nst) & 1u) ^ 1u)) { ok = false; break; }
                     mbar_expect_tx(&bars->b_full[st], stage_bytes);
                     uint8_t* dst = s_b + st * stage_bytes;
                     // coordinates: (kk, n, split, bin)
@@ -327,8 +431,8 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
             }
             // do not leave while loads are in flight: wait for the last stages
             const uint32_t issued = g;
-            for (uint32_t j = (issued > TC_STAGES ? issued - TC_STAGES : 0); j < issued; ++j)
-                mbar_wait(&bars->b_full[j % TC_STAGES], (j / TC_STAGES) & 1u);
+            for (uint32_t j = (issued > (uint32_t)nst ? issued - nst : 0); j < issued; ++j)
+                mbar_wait(&bars->b_full[j % nst], (j / nst) & 1u);
         }
     } else {
         // --- MMA issuer ----------------------------------------------------------
@@ -343,9 +447,9 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
                 tc_fence_after();
                 const uint32_t dcol = tmem + (cb ? TM_C1 : TM_C0);
                 for (int ch = 0; ch < nchunks; ++ch, ++g) {
-                    const uint32_t buf = g & 1u, st = g % TC_STAGES;
+                    const uint32_t buf = g & 1u, st = g % (uint32_t)nst;
                     if (!mbar_wait(&bars->a_full[buf], (g >> 1) & 1u)) { ok = false; break; }
-                    if (!mbar_wait(&bars->b_full[st], (g / TC_STAGES) & 1u)) { ok = false; break; }
+                    if (!mbar_wait(&bars->b_full[st], (g / nst) & 1u)) { ok = false; break; }
                     tc_fence_after();
                     const uint32_t acol = tmem + (buf ? TM_A1 : TM_A0);
                     const uint32_t bbase = smem_u32(s_b + st * stage_bytes);
@@ -470,7 +574,7 @@ int tc_pad_n(int nseg) { return ((2 * nseg + 15) / 16) * 16; }
 bool tc_supported(int nseg, unsigned nfft, int nact)
 {
     if (2 * nseg > 128 || nfft < 256 || (nfft & (nfft - 1)) != 0 || nact <= 0) return false;
-    return tc_smem_bytes(nfft, tc_pad_channels(nact), tc_pad_n(nseg)) <= TC_MAX_SMEM;
+    return tc_smem_bytes(nfft, tc_pad_channels(nact), tc_pad_n(nseg), -1, 2) <= TC_MAX_SMEM;
 }
 
 void launch_fdd_prep_b(const float2* X, size_t bin_pitch, int nseg, size_t nbins,
@@ -513,12 +617,27 @@ std::vector<uint2> tc_quarter_table(unsigned nfft)
     return t;
 }
 
-size_t tc_smem_bytes(unsigned nfft, int nact_pad, int npad)
+size_t tc_smem_bytes(unsigned nfft, int nact_pad, int npad, int dmax, int stages)
 {
     const size_t stage = 4ull * (size_t)npad * 128ull;
-    const size_t need = 1024 /* base alignment */ + TC_STAGES * stage + 256 +
-                        ((size_t)nfft / 4 + 1) * 8 + (size_t)nact_pad * 4 + 4 * 8;
+    // table mode: dmax + 1 phasors + the two twiddle tables (256 + nfft/256 float2)
+    const size_t table = dmax >= 0 ? (size_t)dmax + 1 + 256 + nfft / 256 : (size_t)nfft / 4 + 1;
+    const size_t need = 1024 /* base alignment */ + (size_t)stages * stage + 256 + table * 8 +
+                        (size_t)nact_pad * 4 + 4 * 8;
     return std::max(need, TC_MIN_SMEM);
+}
+
+int tc_table_mode_dmax(int dmax, unsigned nfft, int nact_pad, int npad)
+{
+    if (dmax < 0) return -1;
+    return tc_smem_bytes(nfft, nact_pad, npad, dmax, 2) <= TC_MAX_SMEM ? dmax : -1;
+}
+
+int tc_stages(unsigned nfft, int nact_pad, int npad, int dmax)
+{
+    int st = TC_MAX_STAGES;
+    while (st > 2 && tc_smem_bytes(nfft, nact_pad, npad, dmax, st) > TC_MAX_SMEM) --st;
+    return st;
 }
 
 void launch_fdd_mac_tc(const TcMacArgs& a, const void* B, cudaStream_t s)
@@ -537,7 +656,8 @@ void launch_fdd_mac_tc(const TcMacArgs& a, const void* B, cudaStream_t s)
                                    CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "cuTensorMapEncodeTiled failed");
-    const size_t smem = tc_smem_bytes(a.nfft, a.nact_pad, a.npad);
+    if (a.stages < 2 || a.stages > TC_MAX_STAGES) DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "bad stage count");
+    const size_t smem = tc_smem_bytes(a.nfft, a.nact_pad, a.npad, a.dmax, a.stages);
     RT_CHECK(cudaFuncSetAttribute(fdd_mac_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem));
     int sms = 148;

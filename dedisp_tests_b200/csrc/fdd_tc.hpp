@@ -18,6 +18,8 @@ struct TcMacArgs {
     const float* dms;
     const float* delay_act;    // nact_pad entries (padding channels 0)
     const uint2* table;        // quarter-wave table, nfft/4 + 1 entries
+    const float2* tw_lo;       // exp(-2 pi i t / nfft), t < 256
+    const float2* tw_hi;       // exp(-2 pi i 256 h / nfft), h < nfft / 256
     unsigned* err;             // set to 1 if a bounded wait expired
     int nact_pad;              // channels, multiple of 64
     int ndm;
@@ -26,6 +28,8 @@ struct TcMacArgs {
     size_t nbins;
     unsigned nfft;             // power of two
     int round_delays;
+    int dmax;                  // >= 0: delay-table mode, every delay in 0..dmax; -1: quarter-wave mode
+    int stages;                // B pipeline depth (tc_stages)
 };
 
 // Shapes the tensor-core MAC handles: 2*nseg <= 128 output columns, a
@@ -34,7 +38,12 @@ bool tc_supported(int nseg, unsigned nfft, int nact);
 int tc_pad_channels(int nact);
 int tc_pad_n(int nseg);
 size_t tc_b_bytes(size_t nbins, int nact_pad, int npad);
-size_t tc_smem_bytes(unsigned nfft, int nact_pad, int npad);
+size_t tc_smem_bytes(unsigned nfft, int nact_pad, int npad, int dmax, int stages);
+// Deepest B pipeline (2..6 stages) that fits shared memory.
+int tc_stages(unsigned nfft, int nact_pad, int npad, int dmax);
+// dmax if the per-bin delay table (dmax + 1 phasors) fits shared memory,
+// else -1 (the kernel then indexes the quarter-wave table per phasor).
+int tc_table_mode_dmax(int dmax, unsigned nfft, int nact_pad, int npad);
 std::vector<uint2> tc_quarter_table(unsigned nfft);
 
 // X [nchans*nseg][bin_pitch] complex spectra -> B operand

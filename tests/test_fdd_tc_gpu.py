@@ -91,3 +91,17 @@ def test_tc_repeat_is_deterministic():
     a = _run(p, nsamps, inp, 8, len(dms))
     b = _run(p, nsamps, inp, 8, len(dms))
     assert np.array_equal(a, b)
+
+
+def test_tc_negative_dms_use_quarter_wave_phasors():
+    """Negative DMs (negative delays) take the kernel's quarter-wave phasor
+    path instead of the per-bin delay table; spectrum output, circular shifts."""
+    nchans, nsamps = 64, 12000
+    inp, params = _input(nchans, nsamps, 6)
+    dms = np.linspace(-30, 60, 45, dtype=np.float32)
+    p = _plan(params, dms, segmented=0, precision=1)
+    out = _run(p, nsamps, inp, 8, len(dms))
+    x = _oracle_x(inp, nsamps, params, 8)
+    ref = po.fdd_spectrum(x, _delays(params), np.ones(nchans, np.int32), dms, out.shape[1])
+    rel, mx = _errs(out, ref)
+    assert rel < TC_REL_L2 and mx < TC_MAX_ABS, (rel, mx)
