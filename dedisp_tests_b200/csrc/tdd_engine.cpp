@@ -257,6 +257,7 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
             kern::TransposeArgs ta{c.in + g0 * c.in_stride, c.in_stride, rows_avail, v.nchans, nbits,
                                    tr, pitch, 0, pitch};
             kern::launch_transpose(ta, ex);
+            ++stats.launches;
         } else {
             const size_t nchunks = std::max<size_t>(1, (rows_avail + chunk_rows - 1) / chunk_rows);
             for (size_t k = 0; k < nchunks; ++k) {
@@ -277,6 +278,7 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
                 kern::TransposeArgs ta{m_stage[b].get<uint8_t>(), row_bytes, nr, v.nchans, nbits,
                                        tr, pitch, w0, nw};
                 kern::launch_transpose(ta, ex);
+                ++stats.launches;
                 ev_free[b]->record(ex);
                 stage_used[b] = true;
             }
