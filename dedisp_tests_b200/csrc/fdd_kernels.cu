@@ -32,18 +32,24 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 }
 __device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
 
-// exp(-2 pi i t / 16), t = 0..7 (forward); conjugated for the inverse.
-__device__ __forceinline__ float2 w16(int t, bool inv)
+// exp(-2 pi i t / 32), t = 0..15 (forward); conjugated for the inverse.
+__device__ __forceinline__ float2 w32(int t, bool inv)
 {
-    const float c[8] = {1.0f, 0.92387953251128674f, 0.70710678118654752f, 0.38268343236508977f,
-                        0.0f, -0.38268343236508977f, -0.70710678118654752f, -0.92387953251128674f};
-    const float s[8] = {0.0f, 0.38268343236508977f, 0.70710678118654752f, 0.92387953251128674f,
-                        1.0f, 0.92387953251128674f, 0.70710678118654752f, 0.38268343236508977f};
+    const float c[16] = {1.0f, 0.98078528040323044f, 0.92387953251128674f, 0.83146961230254524f,
+                         0.70710678118654752f, 0.55557023301960218f, 0.38268343236508977f,
+                         0.19509032201612826f, 0.0f, -0.19509032201612826f, -0.38268343236508977f,
+                         -0.55557023301960218f, -0.70710678118654752f, -0.83146961230254524f,
+                         -0.92387953251128674f, -0.98078528040323044f};
+    const float s[16] = {0.0f, 0.19509032201612826f, 0.38268343236508977f, 0.55557023301960218f,
+                         0.70710678118654752f, 0.83146961230254524f, 0.92387953251128674f,
+                         0.98078528040323044f, 1.0f, 0.98078528040323044f, 0.92387953251128674f,
+                         0.83146961230254524f, 0.70710678118654752f, 0.55557023301960218f,
+                         0.38268343236508977f, 0.19509032201612826f};
     return make_float2(c[t], inv ? s[t] : -s[t]);
 }
 
-// In-register DFT of R = 2,4,8,16 points (radix-2 DIF network), output in
-// natural order.
+// In-register DFT of R = 2,4,8,16,32 points (radix-2 DIF network), output
+// in natural order.
 template <int R, bool INV>
 __device__ __forceinline__ void dft_reg(float2 (&v)[R])
 {
@@ -56,8 +62,8 @@ __device__ __forceinline__ void dft_reg(float2 (&v)[R])
                 const float2 a = v[i], b = v[j];
                 v[i] = a + b;
                 const float2 d = a - b;
-                const int t = (i & (span - 1)) * (8 / span);  // W_{2 span}^t' in units of W_16
-                v[j] = (t == 0) ? d : cmul(d, w16(t, INV));
+                const int t = (i & (span - 1)) * (16 / span);  // W_{2 span}^t' in units of W_32
+                v[j] = (t == 0) ? d : cmul(d, w32(t, INV));
             }
         }
     }
@@ -74,13 +80,24 @@ __device__ __forceinline__ void dft_reg(float2 (&v)[R])
     for (int q = 0; q < R; ++q) v[q] = o[q];
 }
 
-// Radix of pass p for M = 2^LOGM: radix 16 while possible, the remainder last.
+// Radix of pass p for M = 2^LOGM: radix 2^FFT_RB while possible, the
+// remainder last (16384 points: 16 x 16 x 16 x 4).
+constexpr int FFT_RB = 4;
 template <int LOGM>
 struct FftPlan {
-    static constexpr int NP = (LOGM + 3) / 4;
-    __host__ __device__ static constexpr int last_bits() { return LOGM - 4 * (NP - 1); }
-    __host__ __device__ static constexpr int bits(int p) { return p < NP - 1 ? 4 : last_bits(); }
+    static constexpr int NP = (LOGM + FFT_RB - 1) / FFT_RB;
+    __host__ __device__ static constexpr int last_bits() { return LOGM - FFT_RB * (NP - 1); }
+    __host__ __device__ static constexpr int bits(int p) { return p < NP - 1 ? FFT_RB : last_bits(); }
+    // threads per transform: one radix-32 group each
+    __host__ __device__ static constexpr unsigned threads() { return (1u << LOGM) / 32 > 32 ? (1u << LOGM) / 32 : 32; }
 };
+
+// Shared-memory slot of element a: the low 4 index bits are XORed with bits
+// 4-7, 8-11 and 12-15 (a bijection on [0, M), no padding), so 16 lanes that
+// access a power-of-two stride up to 2^12 elements hit 16 different 8-byte
+// bank pairs (the passes' strides and the digit-reversed final gather).
+__device__ __forceinline__ unsigned pa(unsigned a) { return a ^ (((a >> 4) ^ (a >> 8) ^ (a >> 12)) & 15u); }
+__host__ __device__ constexpr unsigned padded_len(unsigned m) { return m; }
 
 // Smem position of frequency k after all DIF passes (mixed-radix digit
 // reversal; each pass's output digit is the next frequency digit).
@@ -118,16 +135,21 @@ __device__ __forceinline__ void fft_pass(float2* s, unsigned M, unsigned L, int 
         const unsigned base = blk * L + j;
         float2 v[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = s[base + r * sub];
+        for (int r = 0; r < R; ++r) v[r] = s[pa(base + r * sub)];
         dft_reg<R, INV>(v);
+        if (j) {
+            // W_L^{j q} = W_N^{j q N / L} (N = 2M) as powers of one looked-up
+            // W_L^j: squarings for even q, one more factor for odd q (at
+            // most 4 roundings per factor for R <= 16).
+            float2 p[R];
+            p[1] = twiddle(lo, hi, j << log_nl, INV);
 #pragma unroll
-        for (int q = 1; q < R; ++q) {
-            // W_L^{j q} = W_N^{j q N / L}, N = 2M
-            const unsigned t = (j * q) << log_nl;
-            if (j) v[q] = cmul(v[q], twiddle(lo, hi, t, INV));
+            for (int q = 2; q < R; ++q) p[q] = (q & 1) ? cmul(p[q - 1], p[1]) : cmul(p[q / 2], p[q / 2]);
+#pragma unroll
+            for (int q = 1; q < R; ++q) v[q] = cmul(v[q], p[q]);
         }
 #pragma unroll
-        for (int q = 0; q < R; ++q) s[base + q * sub] = v[q];
+        for (int q = 0; q < R; ++q) s[pa(base + q * sub)] = v[q];
     }
 }
 
@@ -142,7 +164,8 @@ __device__ __forceinline__ void fft_smem(float2* s, const float2* lo, const floa
     for (int p = 0; p < P::NP; ++p) {
         const int b = P::bits(p);
         __syncthreads();
-        if (b == 4) fft_pass<16, INV>(s, M, L, log_nl, lo, hi);
+        if (b == 5) fft_pass<32, INV>(s, M, L, log_nl, lo, hi);
+        else if (b == 4) fft_pass<16, INV>(s, M, L, log_nl, lo, hi);
         else if (b == 3) fft_pass<8, INV>(s, M, L, log_nl, lo, hi);
         else if (b == 2) fft_pass<4, INV>(s, M, L, log_nl, lo, hi);
         else if (b == 1) fft_pass<2, INV>(s, M, L, log_nl, lo, hi);
@@ -153,14 +176,14 @@ __device__ __forceinline__ void fft_smem(float2* s, const float2* lo, const floa
 }
 
 template <int LOGM>
-__global__ void __launch_bounds__(512) fft_r2c_kernel(const float* x, size_t x_pitch, size_t nseg,
-                                                      size_t seg_stride, float2* X, size_t bin_pitch,
-                                                      TwiddleTable tw)
+__global__ void __launch_bounds__(FftPlan<LOGM>::threads()) fft_r2c_kernel(
+    const float* x, size_t x_pitch, size_t nseg, size_t seg_stride, float2* X, size_t bin_pitch,
+    TwiddleTable tw)
 {
     constexpr unsigned M = 1u << LOGM;
     extern __shared__ __align__(16) float2 s_fft[];
     float2* s = s_fft;
-    float2* lo = s + M;
+    float2* lo = s + padded_len(M);
     float2* hi = lo + 256;
     const unsigned nhi = (2 * M) / 256;
     for (unsigned i = threadIdx.x; i < 256; i += blockDim.x) lo[i] = tw.lo[i];
@@ -169,14 +192,31 @@ __global__ void __launch_bounds__(512) fft_r2c_kernel(const float* x, size_t x_p
     const size_t row = blockIdx.x;
     const size_t c = row / nseg, seg = row - c * nseg;
     const float* src = x + c * x_pitch + seg * seg_stride;
-    for (unsigned n = threadIdx.x; n < M; n += blockDim.x)
-        s[n] = make_float2(src[2 * n], src[2 * n + 1]);
+    // Batches of loads in flight per thread (the trip count is a compile-time
+    // constant, so each batch is issued before any of its values is used).
+    constexpr unsigned T = FftPlan<LOGM>::threads();
+    constexpr unsigned PER = M / T, BATCH = PER < 16 ? (PER ? PER : 1) : 16;
+    for (unsigned i0 = 0; i0 < PER; i0 += BATCH) {
+        float2 v[BATCH];
+#pragma unroll
+        for (unsigned i = 0; i < BATCH; ++i) {
+            const unsigned n = threadIdx.x + (i0 + i) * T;
+            v[i] = n < M ? make_float2(src[2 * n], src[2 * n + 1]) : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (unsigned i = 0; i < BATCH; ++i) {
+            const unsigned n = threadIdx.x + (i0 + i) * T;
+            if (n < M) s[pa(n)] = v[i];
+        }
+    }
+    for (unsigned n = threadIdx.x + PER * T; n < M; n += T)  // M < T only
+        s[pa(n)] = make_float2(src[2 * n], src[2 * n + 1]);
     fft_smem<LOGM, false>(s, lo, hi);
 
     float2* dst = X + row * bin_pitch;
     for (unsigned k = threadIdx.x; k <= M; k += blockDim.x) {
-        const float2 zk = s[fft_pos<LOGM>(k & (M - 1))];
-        const float2 zm = s[fft_pos<LOGM>((M - k) & (M - 1))];
+        const float2 zk = s[pa(fft_pos<LOGM>(k & (M - 1)))];
+        const float2 zm = s[pa(fft_pos<LOGM>((M - k) & (M - 1)))];
         const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
         const float2 d = make_float2(zk.x - zm.x, zk.y + zm.y);  // zk - conj(zm)
         const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);   // d / (2i)
@@ -186,14 +226,14 @@ __global__ void __launch_bounds__(512) fft_r2c_kernel(const float* x, size_t x_p
 }
 
 template <int LOGM>
-__global__ void __launch_bounds__(512) fft_c2r_kernel(const float2* Y, size_t bin_pitch, size_t nseg,
-                                                      float* out, size_t out_stride, size_t keep,
-                                                      size_t out_len, TwiddleTable tw)
+__global__ void __launch_bounds__(FftPlan<LOGM>::threads()) fft_c2r_kernel(
+    const float2* Y, size_t bin_pitch, size_t nseg, float* out, size_t out_stride, size_t keep,
+    size_t out_len, TwiddleTable tw)
 {
     constexpr unsigned M = 1u << LOGM;
     extern __shared__ __align__(16) float2 s_fft[];
     float2* s = s_fft;
-    float2* lo = s + M;
+    float2* lo = s + padded_len(M);
     float2* hi = lo + 256;
     const unsigned nhi = (2 * M) / 256;
     for (unsigned i = threadIdx.x; i < 256; i += blockDim.x) lo[i] = tw.lo[i];
@@ -203,16 +243,30 @@ __global__ void __launch_bounds__(512) fft_c2r_kernel(const float2* Y, size_t bi
     const size_t row = blockIdx.x;
     const size_t dm = row / nseg, seg = row - dm * nseg;
     const float2* src = Y + row * bin_pitch;
-    for (unsigned k = threadIdx.x; k < M; k += blockDim.x) {
-        float2 xk = src[k], xm = src[M - k];
-        if (k == 0) {  // the DC and Nyquist imaginary parts are ignored (C2R)
-            xk.y = 0.f;
-            xm.y = 0.f;
+    constexpr unsigned T = FftPlan<LOGM>::threads();
+    constexpr unsigned PER = (M + T - 1) / T, BATCH = PER < 8 ? PER : 8;
+    for (unsigned i0 = 0; i0 < PER; i0 += BATCH) {
+        float2 xk[BATCH], xm[BATCH];
+#pragma unroll
+        for (unsigned i = 0; i < BATCH; ++i) {
+            const unsigned k = threadIdx.x + (i0 + i) * T;
+            xk[i] = k < M ? src[k] : make_float2(0.f, 0.f);
+            xm[i] = k < M ? src[M - k] : make_float2(0.f, 0.f);
         }
-        const float2 e = make_float2(0.5f * (xk.x + xm.x), 0.5f * (xk.y - xm.y));
-        const float2 d = make_float2(0.5f * (xk.x - xm.x), 0.5f * (xk.y + xm.y));
-        const float2 o = cmul(d, conjf2(twiddle(lo, hi, k, false)));
-        s[k] = make_float2(e.x - o.y, e.y + o.x);  // E + i O
+#pragma unroll
+        for (unsigned i = 0; i < BATCH; ++i) {
+            const unsigned k = threadIdx.x + (i0 + i) * T;
+            if (k >= M) continue;
+            float2 a = xk[i], b = xm[i];
+            if (k == 0) {  // the DC and Nyquist imaginary parts are ignored (C2R)
+                a.y = 0.f;
+                b.y = 0.f;
+            }
+            const float2 e = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
+            const float2 d = make_float2(0.5f * (a.x - b.x), 0.5f * (a.y + b.y));
+            const float2 o = cmul(d, conjf2(twiddle(lo, hi, k, false)));
+            s[pa(k)] = make_float2(e.x - o.y, e.y + o.x);  // E + i O
+        }
     }
     fft_smem<LOGM, true>(s, lo, hi);
 
@@ -220,7 +274,7 @@ __global__ void __launch_bounds__(512) fft_c2r_kernel(const float2* Y, size_t bi
     float* dst = out + dm * out_stride;
     const size_t o0 = seg * keep;
     for (unsigned n = threadIdx.x; n < M; n += blockDim.x) {
-        const float2 z = s[fft_pos<LOGM>(n)];
+        const float2 z = s[pa(fft_pos<LOGM>(n))];
         const size_t i0 = 2 * (size_t)n, i1 = i0 + 1;
         if (i0 < keep && o0 + i0 < out_len) dst[o0 + i0] = z.x * scale;
         if (i1 < keep && o0 + i1 < out_len) dst[o0 + i1] = z.y * scale;
@@ -453,10 +507,10 @@ void launch_r2c_n(const float* x, size_t x_pitch, size_t nchans, size_t nseg, si
                   float2* X, size_t bin_pitch, const TwiddleTable& tw, cudaStream_t s)
 {
     constexpr unsigned M = 1u << LOGM;
-    const size_t smem = (M + 256 + 2 * M / 256) * sizeof(float2);
+    const size_t smem = (padded_len(M) + 256 + 2 * M / 256) * sizeof(float2);
     RT_CHECK(cudaFuncSetAttribute(fft_r2c_kernel<LOGM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem));
-    const unsigned threads = M >= 8192 ? 512 : (M >= 1024 ? 256 : 128);
+    const unsigned threads = FftPlan<LOGM>::threads();
     fft_r2c_kernel<LOGM><<<(unsigned)(nchans * nseg), threads, smem, s>>>(x, x_pitch, nseg,
                                                                         seg_stride, X, bin_pitch, tw);
     RT_CHECK(cudaGetLastError());
@@ -468,10 +522,10 @@ void launch_c2r_n(const float2* Y, size_t bin_pitch, size_t ndm, size_t nseg, fl
                   cudaStream_t s)
 {
     constexpr unsigned M = 1u << LOGM;
-    const size_t smem = (M + 256 + 2 * M / 256) * sizeof(float2);
+    const size_t smem = (padded_len(M) + 256 + 2 * M / 256) * sizeof(float2);
     RT_CHECK(cudaFuncSetAttribute(fft_c2r_kernel<LOGM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem));
-    const unsigned threads = M >= 8192 ? 512 : (M >= 1024 ? 256 : 128);
+    const unsigned threads = FftPlan<LOGM>::threads();
     fft_c2r_kernel<LOGM><<<(unsigned)(ndm * nseg), threads, smem, s>>>(Y, bin_pitch, nseg, out,
                                                                       out_stride, keep, out_len, tw);
     RT_CHECK(cudaGetLastError());

@@ -343,7 +343,13 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
                 if (m < a.ndm) {
 #pragma unroll
                     for (int i = 0; i < 8; ++i)
-                        if (i < cnt) a.Yt[(kk * a.nseg + sb + i) * a.ndm + m] = make_float2(yr[i], yi[i]);
+                        if (i < cnt) {
+                            // DM-major rows for the inverse FFT (successive bins of
+                            // this CTA fill the same L2 sectors), else bin-major
+                            const float2 y = make_float2(yr[i], yi[i]);
+                            if (a.Y) a.Y[((size_t)m * a.nseg + sb + i) * a.y_pitch + kk] = y;
+                            else a.Yt[(kk * a.nseg + sb + i) * a.ndm + m] = y;
+                        }
                 }
             }
             tc_fence_before();

@@ -14,7 +14,9 @@ namespace dedisp {
 namespace kern {
 
 struct TcMacArgs {
-    float2* Yt;                // [nbins][nseg][ndm]
+    float2* Yt;                // [nbins][nseg][ndm] (Y == nullptr)
+    float2* Y;                 // DM-major [ndm * nseg][y_pitch] (time-series output), or nullptr
+    size_t y_pitch;
     const float* dms;
     const float* delay_act;    // nact_pad entries (padding channels 0)
     const uint2* table;        // quarter-wave table, nfft/4 + 1 entries
