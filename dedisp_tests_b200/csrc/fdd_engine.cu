@@ -23,6 +23,7 @@ struct FddEngine::Impl {
     rt::DeviceBuffer in, x, X, Xt, Yt, Y, out, tw_lo, tw_hi, dms, chan, km, delay_act;
     // tensor-core form
     rt::DeviceBuffer B, delay_pad, qtable, err;
+    rt::DeviceBuffer fft_tmp;  // four-step FFT scratch (nfft > 32768)
     unsigned qtable_n = 0;
     int delay_pad_n = -1;
     unsigned tw_n = 0;
@@ -52,9 +53,9 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
     stats = ExecTiming();
 
     const FddGeometry g = fdd_geometry(opt, c.nsamps, v.max_delay);
-    if (g.nfft > (size_t)kern::kMaxSmemFft || g.nfft < 512)
+    if (g.nfft > (size_t)kern::kMaxFft || g.nfft < 512 || (g.nfft & (g.nfft - 1)) != 0)
         DD_THROW_MSG(DEDISP_UNKNOWN_ERROR,
-                     "FDD transform length outside the supported range (512..32768)");
+                     "FDD transform length must be a power of two in 512..2^20");
     const bool dev = (c.flags & DEDISP_DEVICE_POINTERS) != 0;
     cudaStream_t st = m_gpu.stream();
     const size_t nchans = v.nchans, ndm = v.ndm, nseg = g.nchunk;
@@ -172,8 +173,10 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
     const float scale = (float)(1.0 / (double)nchans);
     kern::launch_fdd_unpack(d_in, in_stride, c.in_nbits, c.nsamps, nchans, scale, m.x.get<float>(),
                             x_len, x_len, st);
+    const size_t tmp_elems = kern::fft_scratch_elems((int)g.nfft, std::max(nchans, ndm) * nseg);
+    if (tmp_elems) m.fft_tmp.reserve(tmp_elems * sizeof(float2));
     kern::launch_fft_r2c(m.x.get<float>(), x_len, nchans, nseg, seg_stride, (int)g.nfft,
-                         m.X.get<float2>(), bin_pitch, tw, st);
+                         m.X.get<float2>(), bin_pitch, tw, m.fft_tmp.get<float2>(), st);
     if (use_tc)
         kern::launch_fdd_prep_b(m.X.get<float2>(), bin_pitch, (int)nseg, nbins, m.chan.get<int32_t>(),
                                 m.km.get<float>(), m.nact, nact_pad, npad, m.B.get(), st);
@@ -253,7 +256,7 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
                                         bin_pitch, st);
         const size_t keep = g.segmented ? g.nsamp_good : g.nfft;
         kern::launch_fft_c2r(m.Y.get<float2>(), bin_pitch, ndm, nseg, (int)g.nfft, d_out, g.row_len,
-                             keep, g.row_len, tw, st);
+                             keep, g.row_len, tw, m.fft_tmp.get<float2>(), st);
     }
     if (e3) e3->record(st);
     if (!dev)

@@ -282,6 +282,219 @@ __global__ void __launch_bounds__(FftPlan<LOGM>::threads()) fft_c2r_kernel(
 }
 
 // ---------------------------------------------------------------------------
+// Four-step FFT for M = M1 * M2 complex points (M > 16384): the columns
+// n2 of z[n1 M2 + n2] are transformed (length M1) in tiles of FT_TILE columns
+// per CTA, multiplied by W_M^{n2 k1} and stored as Z1[n2][k1]; then the rows
+// k1 (length M2) in tiles of FT_TILE, giving X[k1 + M1 k2]. Each tile is a
+// batch of independent transforms in shared memory; every global access is a
+// run of FT_TILE consecutive complex values (128 bytes). Real input/output
+// use the same half-length packing as the single-CTA kernels, with the
+// real<->complex step as separate in-place passes over (k, M - k) pairs.
+// ---------------------------------------------------------------------------
+constexpr int FT_TILE = 16;
+constexpr int FT_THREADS = 512;
+
+// DIF passes over nb concatenated transforms of 2^LOG points each.
+template <int LOG, bool INV>
+__device__ __forceinline__ void fft_smem_multi(float2* s, unsigned nb, int log_nl0, const float2* lo,
+                                               const float2* hi)
+{
+    using P = FftPlan<LOG>;
+    const unsigned M = nb << LOG;
+    unsigned L = 1u << LOG;
+    int log_nl = log_nl0;  // log2(N / L) for the twiddle table's N
+#pragma unroll
+    for (int p = 0; p < P::NP; ++p) {
+        const int b = P::bits(p);
+        __syncthreads();
+        if (b == 4) fft_pass<16, INV>(s, M, L, log_nl, lo, hi);
+        else if (b == 3) fft_pass<8, INV>(s, M, L, log_nl, lo, hi);
+        else if (b == 2) fft_pass<4, INV>(s, M, L, log_nl, lo, hi);
+        else if (b == 1) fft_pass<2, INV>(s, M, L, log_nl, lo, hi);
+        L >>= b;
+        log_nl += b;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void load_twiddles(float2* lo, float2* hi, const TwiddleTable& tw)
+{
+    const unsigned nhi = tw.n / 256;
+    for (unsigned i = threadIdx.x; i < 256; i += blockDim.x) lo[i] = tw.lo[i];
+    for (unsigned i = threadIdx.x; i < nhi; i += blockDim.x) hi[i] = tw.hi[i];
+}
+
+// Step A. REAL_IN: row r = (c, seg) of real samples x (pairs packed as
+// complex); else complex rows `zin` (pitch zin_pitch). Output Z1 rows of M.
+template <int L1, int L2, bool REAL_IN, bool INV>
+__global__ void __launch_bounds__(FT_THREADS) fft4_cols_kernel(
+    const float* x, size_t x_pitch, size_t nseg, size_t seg_stride, const float2* zin, size_t zin_pitch,
+    float2* Z1, TwiddleTable tw)
+{
+    constexpr unsigned M1 = 1u << L1, M2 = 1u << L2, M = M1 * M2;
+    extern __shared__ __align__(16) float2 s_ft[];
+    float2* s = s_ft;
+    float2* lo = s + FT_TILE * M1;
+    float2* hi = lo + 256;
+    load_twiddles(lo, hi, tw);
+    const size_t row = blockIdx.y;
+    const unsigned c0 = blockIdx.x * FT_TILE;
+    const float* xr = nullptr;
+    const float2* zr = nullptr;
+    if (REAL_IN) {
+        const size_t c = row / nseg, seg = row - c * nseg;
+        xr = x + c * x_pitch + seg * seg_stride;
+    } else {
+        zr = zin + row * zin_pitch;
+    }
+    for (unsigned idx = threadIdx.x; idx < FT_TILE * M1; idx += FT_THREADS) {
+        const unsigned col = idx % FT_TILE, n1 = idx / FT_TILE;
+        const size_t n = (size_t)n1 * M2 + c0 + col;
+        s[pa(col * M1 + n1)] = REAL_IN ? make_float2(xr[2 * n], xr[2 * n + 1]) : zr[n];
+    }
+    fft_smem_multi<L1, INV>(s, FT_TILE, L1 + L2 + 1 - L1, lo, hi);
+    float2* zo = Z1 + row * (size_t)M;
+    const unsigned nmask = 2 * M - 1;
+    for (unsigned idx = threadIdx.x; idx < FT_TILE * M1; idx += FT_THREADS) {
+        const unsigned col = idx / M1, k1 = idx - col * M1;
+        const unsigned n2 = c0 + col;
+        const float2 v = s[pa(col * M1 + fft_pos<L1>(k1))];
+        // W_M^{n2 k1} = W_N^{2 n2 k1}, N = 2M
+        const float2 w = twiddle(lo, hi, (2u * n2 * k1) & nmask, INV);
+        zo[(size_t)n2 * M1 + k1] = cmul(v, w);
+    }
+}
+
+// Step B. REAL_OUT: time samples x[2n], x[2n+1] = Re, Im of z[n] / M into
+// out rows (segment `seg` at column seg * keep, the first `keep` samples,
+// at most out_len), else complex rows X (pitch x_pitch).
+template <int L1, int L2, bool REAL_OUT, bool INV>
+__global__ void __launch_bounds__(FT_THREADS) fft4_rows_kernel(
+    const float2* Z1, float2* X, size_t x_pitch, float* out, size_t out_stride, size_t nseg, size_t keep,
+    size_t out_len, TwiddleTable tw)
+{
+    constexpr unsigned M1 = 1u << L1, M2 = 1u << L2, M = M1 * M2;
+    extern __shared__ __align__(16) float2 s_ft[];
+    float2* s = s_ft;
+    float2* lo = s + FT_TILE * M2;
+    float2* hi = lo + 256;
+    load_twiddles(lo, hi, tw);
+    const size_t row = blockIdx.y;
+    const unsigned t0 = blockIdx.x * FT_TILE;
+    const float2* zr = Z1 + row * (size_t)M;
+    for (unsigned idx = threadIdx.x; idx < FT_TILE * M2; idx += FT_THREADS) {
+        const unsigned col = idx % FT_TILE, n2 = idx / FT_TILE;
+        s[pa(col * M2 + n2)] = zr[(size_t)n2 * M1 + t0 + col];
+    }
+    fft_smem_multi<L2, INV>(s, FT_TILE, L1 + L2 + 1 - L2, lo, hi);
+    if (REAL_OUT) {
+        const float scale = 1.0f / (float)M;
+        const size_t dm = row / nseg, seg = row - dm * nseg;
+        float* dst = out + dm * out_stride;
+        const size_t o0 = seg * keep;
+        for (unsigned idx = threadIdx.x; idx < FT_TILE * M2; idx += FT_THREADS) {
+            const unsigned col = idx % FT_TILE, k2 = idx / FT_TILE;
+            const float2 z = s[pa(col * M2 + fft_pos<L2>(k2))];
+            const size_t n = (size_t)t0 + col + (size_t)M1 * k2;
+            const size_t i0 = 2 * n, i1 = i0 + 1;
+            if (i0 < keep && o0 + i0 < out_len) dst[o0 + i0] = z.x * scale;
+            if (i1 < keep && o0 + i1 < out_len) dst[o0 + i1] = z.y * scale;
+        }
+    } else {
+        float2* xo = X + row * x_pitch;
+        for (unsigned idx = threadIdx.x; idx < FT_TILE * M2; idx += FT_THREADS) {
+            const unsigned col = idx % FT_TILE, k2 = idx / FT_TILE;
+            xo[(size_t)t0 + col + (size_t)M1 * k2] = s[pa(col * M2 + fft_pos<L2>(k2))];
+        }
+    }
+}
+
+// Real-FFT post step in place: rows of M complex z -> M + 1 bins (same
+// formula as fft_r2c_kernel), one thread per pair (k, M - k).
+__global__ void __launch_bounds__(256) r2c_post_kernel(float2* X, size_t x_pitch, unsigned M, TwiddleTable tw)
+{
+    const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > M / 2) return;
+    float2* r = X + (size_t)blockIdx.y * x_pitch;
+    const float2 a = r[k & (M - 1)], b = r[(M - k) & (M - 1)];
+    auto bin = [&](float2 zk, float2 zm, unsigned kk) {
+        const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+        const float2 d = make_float2(zk.x - zm.x, zk.y + zm.y);
+        const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
+        const float2 w = (kk == M) ? make_float2(-1.f, 0.f) : cmul(tw.hi[kk >> 8], tw.lo[kk & 255]);
+        return e + cmul(w, o);
+    };
+    const float2 xk = bin(a, b, k);
+    const float2 xm = bin(b, a, M - k);
+    r[k] = xk;
+    if (M - k != k) r[M - k] = xm;
+}
+
+// Inverse real-FFT pre step in place: M + 1 bins -> M complex z (same
+// formula as fft_c2r_kernel), one thread per pair (k, M - k).
+__global__ void __launch_bounds__(256) c2r_pre_kernel(float2* Y, size_t y_pitch, unsigned M, TwiddleTable tw)
+{
+    const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > M / 2) return;
+    float2* r = Y + (size_t)blockIdx.y * y_pitch;
+    float2 a = r[k], b = r[M - k];
+    if (k == 0) {  // the DC and Nyquist imaginary parts are ignored (C2R)
+        a.y = 0.f;
+        b.y = 0.f;
+    }
+    auto pre = [&](float2 xk, float2 xm, unsigned kk) {
+        const float2 e = make_float2(0.5f * (xk.x + xm.x), 0.5f * (xk.y - xm.y));
+        const float2 d = make_float2(0.5f * (xk.x - xm.x), 0.5f * (xk.y + xm.y));
+        const float2 w = cmul(tw.hi[kk >> 8], tw.lo[kk & 255]);
+        const float2 o = cmul(d, conjf2(w));
+        return make_float2(e.x - o.y, e.y + o.x);
+    };
+    const float2 zk = pre(a, b, k);
+    if (k != 0 && M - k != k) r[M - k] = pre(b, a, M - k);
+    r[k] = zk;
+}
+
+template <int L1, int L2>
+void launch_r2c_4step(const float* x, size_t x_pitch, size_t rows, size_t nseg, size_t seg_stride,
+                      float2* X, size_t bin_pitch, float2* Z1, const TwiddleTable& tw, cudaStream_t s)
+{
+    constexpr unsigned M1 = 1u << L1, M2 = 1u << L2, M = M1 * M2;
+    const size_t tws = (256 + (size_t)tw.n / 256) * sizeof(float2);
+    const size_t sa = FT_TILE * M1 * sizeof(float2) + tws, sb = FT_TILE * M2 * sizeof(float2) + tws;
+    auto ka = fft4_cols_kernel<L1, L2, true, false>;
+    auto kb = fft4_rows_kernel<L1, L2, false, false>;
+    RT_CHECK(cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sa));
+    RT_CHECK(cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb));
+    ka<<<dim3(M2 / FT_TILE, (unsigned)rows), FT_THREADS, sa, s>>>(x, x_pitch, nseg, seg_stride, nullptr, 0,
+                                                                Z1, tw);
+    RT_CHECK(cudaGetLastError());
+    kb<<<dim3(M1 / FT_TILE, (unsigned)rows), FT_THREADS, sb, s>>>(Z1, X, bin_pitch, nullptr, 0, 1, 0, 0, tw);
+    RT_CHECK(cudaGetLastError());
+    r2c_post_kernel<<<dim3((M / 2 + 256) / 256, (unsigned)rows), 256, 0, s>>>(X, bin_pitch, M, tw);
+    RT_CHECK(cudaGetLastError());
+}
+
+template <int L1, int L2>
+void launch_c2r_4step(float2* Y, size_t bin_pitch, size_t rows, size_t nseg, float* out, size_t out_stride,
+                      size_t keep, size_t out_len, float2* Z1, const TwiddleTable& tw, cudaStream_t s)
+{
+    constexpr unsigned M1 = 1u << L1, M2 = 1u << L2, M = M1 * M2;
+    const size_t tws = (256 + (size_t)tw.n / 256) * sizeof(float2);
+    const size_t sa = FT_TILE * M1 * sizeof(float2) + tws, sb = FT_TILE * M2 * sizeof(float2) + tws;
+    c2r_pre_kernel<<<dim3((M / 2 + 256) / 256, (unsigned)rows), 256, 0, s>>>(Y, bin_pitch, M, tw);
+    RT_CHECK(cudaGetLastError());
+    auto ka = fft4_cols_kernel<L1, L2, false, true>;
+    auto kb = fft4_rows_kernel<L1, L2, true, true>;
+    RT_CHECK(cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sa));
+    RT_CHECK(cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb));
+    ka<<<dim3(M2 / FT_TILE, (unsigned)rows), FT_THREADS, sa, s>>>(nullptr, 0, 1, 0, Y, bin_pitch, Z1, tw);
+    RT_CHECK(cudaGetLastError());
+    kb<<<dim3(M1 / FT_TILE, (unsigned)rows), FT_THREADS, sb, s>>>(Z1, nullptr, 0, out, out_stride, nseg, keep,
+                                                                out_len, tw);
+    RT_CHECK(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
 // unpack / transposes
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) fdd_unpack_kernel(const uint8_t* in, size_t in_stride,
@@ -554,27 +767,40 @@ void launch_fdd_unpack(const uint8_t* in, size_t in_stride, int in_nbits, size_t
 }
 
 void launch_fft_r2c(const float* x, size_t x_pitch, size_t nchans, size_t nseg, size_t seg_stride,
-                    int nfft, float2* X, size_t bin_pitch, const TwiddleTable& tw, cudaStream_t s)
+                    int nfft, float2* X, size_t bin_pitch, const TwiddleTable& tw, float2* scratch,
+                    cudaStream_t s)
 {
+    const size_t rows = nchans * nseg;
+    if (rows > 65535 && log2_exact(nfft) > 15) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "too many FFT rows");
     switch (log2_exact(nfft)) {
 #define R2C(L) case L + 1: launch_r2c_n<L>(x, x_pitch, nchans, nseg, seg_stride, X, bin_pitch, tw, s); break;
         R2C(4) R2C(5) R2C(6) R2C(7) R2C(8) R2C(9) R2C(10) R2C(11) R2C(12) R2C(13) R2C(14)
 #undef R2C
+#define R4(L1, L2) case L1 + L2 + 1: launch_r2c_4step<L1, L2>(x, x_pitch, rows, nseg, seg_stride, X, bin_pitch, scratch, tw, s); break;
+        R4(8, 7) R4(8, 8) R4(9, 8) R4(9, 9) R4(10, 9)
+#undef R4
     default: DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unsupported FFT length");
     }
 }
 
-void launch_fft_c2r(const float2* Y, size_t bin_pitch, size_t ndm, size_t nseg, int nfft,
+void launch_fft_c2r(float2* Y, size_t bin_pitch, size_t ndm, size_t nseg, int nfft,
                     float* out, size_t out_stride, size_t keep, size_t out_len,
-                    const TwiddleTable& tw, cudaStream_t s)
+                    const TwiddleTable& tw, float2* scratch, cudaStream_t s)
 {
+    const size_t rows = ndm * nseg;
+    if (rows > 65535 && log2_exact(nfft) > 15) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "too many FFT rows");
     switch (log2_exact(nfft)) {
 #define C2R(L) case L + 1: launch_c2r_n<L>(Y, bin_pitch, ndm, nseg, out, out_stride, keep, out_len, tw, s); break;
         C2R(4) C2R(5) C2R(6) C2R(7) C2R(8) C2R(9) C2R(10) C2R(11) C2R(12) C2R(13) C2R(14)
 #undef C2R
+#define C4(L1, L2) case L1 + L2 + 1: launch_c2r_4step<L1, L2>(Y, bin_pitch, rows, nseg, out, out_stride, keep, out_len, scratch, tw, s); break;
+        C4(8, 7) C4(8, 8) C4(9, 8) C4(9, 9) C4(10, 9)
+#undef C4
     default: DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unsupported FFT length");
     }
 }
+
+size_t fft_scratch_elems(int nfft, size_t rows) { return nfft > 32768 ? rows * (size_t)(nfft / 2) : 0; }
 
 void launch_fdd_to_binmajor(const float2* X, size_t bin_pitch, size_t nseg, size_t nbins,
                             const int32_t* chan, const float* km, int nact, float2* Xt,

@@ -34,21 +34,26 @@ void launch_fdd_unpack(const uint8_t* in, size_t in_stride, int in_nbits, size_t
                        cudaStream_t s);
 
 // Largest real transform length handled in one CTA (shared memory).
-constexpr int kMaxSmemFft = 32768;
+constexpr int kMaxSmemFft = 32768;   // one CTA per transform up to this length
+constexpr int kMaxFft = 1 << 20;      // four-step transforms up to this length
 
 // Forward real FFT of nfft samples (power of two, 32..kMaxSmemFft) for every
 // (channel, segment): input x[c][seg*seg_stride + n], output X row
 // c*nseg + seg, bins 0..nfft/2.
+// nfft up to 32768: one CTA per transform; 65536 .. 2^20: four-step
+// (column and row passes through `scratch`, fft_scratch_elems complex values).
 void launch_fft_r2c(const float* x, size_t x_pitch, size_t nchans, size_t nseg,
                     size_t seg_stride, int nfft, float2* X, size_t bin_pitch,
-                    const TwiddleTable& tw, cudaStream_t s);
+                    const TwiddleTable& tw, float2* scratch, cudaStream_t s);
+size_t fft_scratch_elems(int nfft, size_t rows);
 
 // Inverse real FFT (normalised by 1/nfft) of every row r = dm*nseg + seg of
 // Y (bins 0..nfft/2); samples n < keep of segment seg go to
 // out[dm][seg*keep + n] when that index is < out_len.
-void launch_fft_c2r(const float2* Y, size_t bin_pitch, size_t ndm, size_t nseg, int nfft,
+// Y is overwritten (the four-step path prepares it in place).
+void launch_fft_c2r(float2* Y, size_t bin_pitch, size_t ndm, size_t nseg, int nfft,
                     float* out, size_t out_stride, size_t keep, size_t out_len,
-                    const TwiddleTable& tw, cudaStream_t s);
+                    const TwiddleTable& tw, float2* scratch, cudaStream_t s);
 
 // X -> Xt over active channels (chan[j], multiplier km[j]).
 void launch_fdd_to_binmajor(const float2* X, size_t bin_pitch, size_t nseg, size_t nbins,

@@ -213,3 +213,28 @@ def test_packed_input_widths(nbits, precision):
     rel, mx = _errs(out, ref)
     tol = (FP32_REL_L2, FP32_MAX_ABS) if precision == 0 else (1e-5, 1e-4)
     assert rel < tol[0] and mx < tol[1], (rel, mx)
+
+
+@pytest.mark.parametrize("segment_nfft,nchans,nsamps,dm_max", [
+    (65536, 64, 200000, 100.0),
+    (131072, 32, 300000, 100.0),
+    (262144, 32, 600000, 100.0),
+    (1 << 20, 32, 1100000, 50.0),
+    (0, 64, 400000, 2500.0),     # the reference rule picks 131072-point segments here
+])
+def test_four_step_fft_segments(segment_nfft, nchans, nsamps, dm_max):
+    """Segments longer than 32768 samples use the four-step FFT (column and
+    row passes through a scratch buffer)."""
+    inp, params = _input(nchans, nsamps, 17, float_input=True, f0=1400.0, df=-2.0, dt=64e-6)
+    dms = np.linspace(0, dm_max, 12, dtype=np.float32)
+    p = _plan(params, dms, segmented=1, segment_nfft=segment_nfft)
+    md = p.get_max_delay()
+    nfft, good, nchunk = po.fdd_segment_geometry(nsamps, md) if segment_nfft == 0 else (segment_nfft, segment_nfft - md, 0)
+    assert nfft > 32768
+    nout = nsamps - md
+    out = np.zeros((len(dms), nout), np.float32)
+    p.execute(nsamps, inp, 32, out, 32)
+    x = _oracle_x(inp, nsamps, params, 32)
+    ref = po.fdd_timeseries(x, _delays(params), np.ones(nchans, np.int32), dms, nout)
+    rel, mx = _errs(out, ref)
+    assert rel < FP32_REL_L2 and mx < FP32_MAX_ABS, (rel, mx)
