@@ -533,3 +533,68 @@ class StreamServer:
         return [{"beam": r.beam, "worker": r.worker, "nsamps": int(r.nsamps),
                  "t_submit": r.t_submit, "t_start": r.t_start, "t_done": r.t_done,
                  "device_ms": r.device_ms} for r in arr[:n]]
+
+
+# ---------------------------------------------------------------------------
+# SIGPROC filterbank I/O (dedisp_b200_fil_* / dedisp_b200_write_*)
+# ---------------------------------------------------------------------------
+
+class FilHeader(C.Structure):
+    _fields_ = [("tsamp", C.c_double), ("tstart", C.c_double), ("fch1", C.c_double),
+                ("foff", C.c_double), ("src_raj", C.c_double), ("src_dej", C.c_double),
+                ("az_start", C.c_double), ("za_start", C.c_double), ("nchans", C.c_int),
+                ("nifs", C.c_int), ("nbits", C.c_int), ("telescope_id", C.c_int),
+                ("machine_id", C.c_int), ("nbeams", C.c_int), ("ibeam", C.c_int),
+                ("nsamples", _sz), ("header_bytes", _sz), ("source_name", C.c_char * 80)]
+
+
+_IO_SIGS = {
+    "dedisp_b200_fil_read_header": (C.c_int, [C.c_char_p, C.POINTER(FilHeader)]),
+    "dedisp_b200_fil_read_samples": (C.c_int, [C.c_char_p, C.POINTER(FilHeader), _sz, _sz, _vp]),
+    "dedisp_b200_fil_decimate": (_sz, [_vp, _sz, _sz, _sz]),
+    "dedisp_b200_write_dat": (C.c_int, [C.c_char_p, C.c_float, _vp, _sz]),
+    "dedisp_b200_write_inf": (C.c_int, [C.c_char_p, C.c_float, C.POINTER(FilHeader), _sz]),
+}
+
+
+def _io_lib() -> C.CDLL:
+    L = lib()
+    if not getattr(L, "_io_sigs", False):
+        for name, (res, args) in _IO_SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        L._io_sigs = True
+    return L
+
+
+def fil_read_header(path: str) -> FilHeader:
+    h = FilHeader()
+    _bcheck(_io_lib().dedisp_b200_fil_read_header(path.encode(), C.byref(h)))
+    return h
+
+
+def fil_read(path: str, first: int = 0, count=None):
+    """(header, time-major packed rows as a uint8 array [count][row bytes])."""
+    h = fil_read_header(path)
+    n = h.nsamples - first if count is None else count
+    row = h.nchans * h.nifs * h.nbits // 8
+    out = np.empty((n, row), np.uint8)
+    _bcheck(_io_lib().dedisp_b200_fil_read_samples(path.encode(), C.byref(h), first, n, out.ctypes.data))
+    return h, out
+
+
+def fil_decimate(data: np.ndarray, nchans: int, factor: int) -> int:
+    """8-bit rows averaged over `factor` samples in place; returns the new count."""
+    return int(_io_lib().dedisp_b200_fil_decimate(data.ctypes.data, nchans, data.shape[0], factor))
+
+
+def write_dat_inf(prefix: str, dm: float, series: np.ndarray, header: FilHeader) -> None:
+    s = np.ascontiguousarray(series, dtype=np.float32)
+    _bcheck(_io_lib().dedisp_b200_write_dat(prefix.encode(), dm, s.ctypes.data, s.size))
+    _bcheck(_io_lib().dedisp_b200_write_inf(prefix.encode(), dm, C.byref(header), s.size))
+
+
+def fil_tool_path() -> str:
+    """The dedisp_fil command-line program built beside the library."""
+    return os.path.join(HERE, "bin", "dedisp_fil")

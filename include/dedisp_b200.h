@@ -197,6 +197,38 @@ dedisp_size dedisp_b200_server_record_count(dedisp_b200_server server);
 dedisp_error dedisp_b200_server_records(dedisp_b200_server server, dedisp_b200_gulp_record* records,
                                         dedisp_size count);
 
+/* ------------------------------------------------------------------------
+ * SIGPROC filterbank input and per-DM output, the file I/O of the
+ * reference's *_fil tools (bin/fil/fil.hpp) as library calls.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+    double tsamp, tstart, fch1, foff;
+    double src_raj, src_dej, az_start, za_start;
+    int nchans, nifs, nbits;
+    int telescope_id, machine_id, nbeams, ibeam;
+    dedisp_size nsamples;       /* from the size of the data section (fil.hpp:366-370) */
+    dedisp_size header_bytes;
+    char source_name[80];
+} dedisp_b200_fil_header;
+
+/* Parses the header (typed SIGPROC keywords; replaces read_header,
+ * fil.hpp:306-378, which stores the keyword instead of the source name). */
+dedisp_error dedisp_b200_fil_read_header(const char* path, dedisp_b200_fil_header* header);
+/* Raw time-major rows [first, first + count) (fil.hpp:210-213). */
+dedisp_error dedisp_b200_fil_read_samples(const char* path, const dedisp_b200_fil_header* header,
+                                          dedisp_size first, dedisp_size count, dedisp_byte* out);
+/* 8-bit rows averaged over `factor` samples in place, truncated to bytes
+ * (decimate_timeseries, fil.hpp:31-52; full blocks only). Returns the new
+ * sample count. */
+dedisp_size dedisp_b200_fil_decimate(dedisp_byte* data, dedisp_size nchans, dedisp_size nsamps,
+                                     dedisp_size factor);
+/* <prefix>_DM<dm, %.3f>.dat (n float32 samples) and .inf (PRESTO text,
+ * writeinf, fil.hpp:485-538). */
+dedisp_error dedisp_b200_write_dat(const char* prefix, dedisp_float dm, const dedisp_float* series,
+                                   dedisp_size n);
+dedisp_error dedisp_b200_write_inf(const char* prefix, dedisp_float dm,
+                                   const dedisp_b200_fil_header* header, dedisp_size numout);
+
 /* Floats per DM row that execute() writes for nsamps input samples. */
 dedisp_size dedisp_b200_output_row_length(dedisp_plan plan, dedisp_size nsamps);
 
