@@ -503,51 +503,32 @@ def measured_peaks():
 
 def run_ours(args):
     import torch
-    import torch.distributed as dist
     import dedisp_tests_b200 as dd
     from dedisp_tests_b200 import synthetic as sy
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    from dedisp_tests_b200.replicas import Replicas
+    reps = Replicas.from_env("nccl")
+    world, rank, local = reps.world, reps.rank, reps.local
+    barrier, max_over_ranks = reps.barrier, reps.max_over_ranks
 
     stream = torch.cuda.current_stream()
     if args.serve_only:
         res = run_serving(args, local, world)
         if rank == 0:
             print(json.dumps({"serving": res}), flush=True)
-        if world > 1:
-            dist.destroy_process_group()
+        reps.close()
         return
     if args.batched_only:
         res = run_batched(args, local, world, stream, max_over_ranks)
         if rank == 0:
             print(json.dumps({"batched": res}), flush=True)
-        if world > 1:
-            dist.destroy_process_group()
+        reps.close()
         return
     if args.fdd_only:
         fdd = run_fdd(args, local, world, stream, max_over_ranks)
         if rank == 0:
             print(json.dumps({"fdd": fdd}), flush=True)
-        if world > 1:
-            dist.destroy_process_group()
+        reps.close()
         return
 
     cfg = sy.config1(nbits=args.nbits)
@@ -752,8 +733,7 @@ def run_ours(args):
             "fdd": fdd, "batched": batched, "serving": serving,
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    reps.close()
 
 
 def run_reference(args):
