@@ -81,7 +81,8 @@ def profile_case(args):
         cfg = sy.config1(nbits=args.nbits, nsamps=1 << 17)
         p = dd.TDDPlan(cfg.nchans, cfg.dt, cfg.f_top, cfg.df)
         p.generate_dm_list(*cfg.dm_gen)
-        p.set_tile_variant(max(args.tile_variant, 0))
+        if args.tile_variant >= 0:
+            p.set_tile_variant(args.tile_variant)
         nbits = args.nbits
     else:
         cfg = sy.config2(nsamps=1 << 18)
@@ -560,7 +561,9 @@ def run_ours(args):
             plan.set_tile_variant(v)
             step(plan)
             step(plan)
-            tune[v] = plan.get_timing()["kernel_ms"]
+            t = plan.get_timing()
+            # whole device step: K1 (+ K1q for quad-strided variants) + K2
+            tune[v] = t["kernel_ms"] + t["prep_ms"]
         best = min(tune, key=tune.get)
     else:
         best = max(args.tile_variant, 0)
@@ -729,7 +732,7 @@ def run_ours(args):
                        "parallelism": f"replicas x{world}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches * world, "clocks": clocks, "variants": variants,
-            "tile_variant": {"chosen": best, "k2_ms_by_variant": tune},
+            "tile_variant": {"chosen": best, "step_ms_by_variant": tune},
             "fdd": fdd, "batched": batched, "serving": serving,
         }
         print(json.dumps(line), flush=True)

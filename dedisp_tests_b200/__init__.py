@@ -296,6 +296,12 @@ def tdd_variant_count(in_nbits: int = 8) -> int:
     return int(lib().dedisp_b200_tdd_variant_count(in_nbits))
 
 
+def batch_variant_count(in_nbits: int = 8) -> int:
+    """Number of tile-shape variants of the persistent multi-beam kernel
+    (the leading plan variants, which work on channel-major packed rows)."""
+    return int(_batch_lib().dedisp_b200_batch_variant_count(in_nbits))
+
+
 # ---------------------------------------------------------------------------
 # Batched multi-beam TDD (dedisp_b200_batch_*; device buffers only)
 # ---------------------------------------------------------------------------
@@ -314,6 +320,7 @@ _BATCH_SIGS = {
     "dedisp_b200_batch_workspace_size": (_sz, [_vp]),
     "dedisp_b200_batch_set_workspace": (C.c_int, [_vp, _vp, _sz]),
     "dedisp_b200_batch_set_shape": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "dedisp_b200_batch_variant_count": (C.c_int, [_sz]),
     "dedisp_b200_batch_autotune": (C.c_int, [_vp, _vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "dedisp_b200_batch_execute": (C.c_int, [_vp, _vp, C.c_int]),
     "dedisp_b200_batch_set_timing": (C.c_int, [_vp, C.c_int]),

@@ -164,7 +164,7 @@ void TddBatch::set_beams(std::vector<BatchBeamSpec> beams)
 
 void TddBatch::set_shape(const BatchShape& shape)
 {
-    const int nv = kern::tiled_variant_count(m_nbits);
+    const int nv = kern::tiled_batch_variant_count(m_nbits);
     if (shape.variant < 0 || shape.variant >= nv) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unknown tile-shape variant");
     if (shape.chan_per_stage < 0 || shape.chan_per_stage > kMaxStageChannels || shape.chan_per_stage % 2)
         DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "channels per stage must be even and at most 32");
@@ -258,7 +258,7 @@ TddBatch::Layout TddBatch::make_layout(const BatchShape& shape, size_t tile_limi
 size_t TddBatch::workspace_bytes() const
 {
     size_t words = 0;
-    for (int v = 0; v < kern::tiled_variant_count(m_nbits); ++v) {
+    for (int v = 0; v < kern::tiled_batch_variant_count(m_nbits); ++v) {
         BatchShape s;
         s.variant = v;
         words = std::max(words, make_layout(s, 0).ws_words);
@@ -350,7 +350,7 @@ BatchShape TddBatch::autotune(cudaStream_t stream)
     rt::DeviceGuard g(m_device);
     if (m_beams.empty()) return m_shape;
     std::vector<BatchShape> cands;
-    const int nv = m_general_mask ? 1 : kern::tiled_variant_count(m_nbits);
+    const int nv = m_general_mask ? 1 : kern::tiled_batch_variant_count(m_nbits);
     for (int v = 0; v < nv; ++v)
         for (int cs : {0, 24, 16}) {
             BatchShape s;
@@ -539,6 +539,11 @@ dedisp_size dedisp_b200_batch_workspace_size(dedisp_b200_batch batch)
 dedisp_error dedisp_b200_batch_set_workspace(dedisp_b200_batch batch, void* d_workspace, dedisp_size bytes)
 {
     return batch_call(batch, [&](dedisp::detail::TddBatch& b) { b.set_workspace(d_workspace, bytes); });
+}
+
+int dedisp_b200_batch_variant_count(dedisp_size in_nbits)
+{
+    return dedisp::kern::tiled_batch_variant_count((int)in_nbits);
 }
 
 dedisp_error dedisp_b200_batch_set_shape(dedisp_b200_batch batch, int variant, int chan_per_stage)

@@ -27,6 +27,8 @@ struct TddEngine::Setup {
     int variant = -1;
 
     bool tiled = false;
+    bool quad = false;           // 8-bit kernel on quad-strided rows
+    int period = 0;              // quad: P, words per lane set
     int nact = 0;
     int win_words = 0;
     int chan_per_stage = 0;
@@ -59,7 +61,8 @@ rt::Event& TddEngine::event(size_t i)
 void TddEngine::prepare(const TddView& v, const TddCall& c)
 {
     Setup& s = *m_setup;
-    const int eff_variant = c.in_nbits == 8 ? variant : 0;  // other widths have one shape
+    // other widths have one shape
+    const int eff_variant = c.in_nbits != 8 ? 0 : variant < 0 ? kern::tiled_default_variant(8) : variant;
     if (s.version == v.version && s.first == c.first_dm && s.count == c.dm_count &&
         s.nbits == c.in_nbits && s.kernel == kernel && s.variant == eff_variant)
         return;
@@ -123,7 +126,12 @@ void TddEngine::prepare(const TddView& v, const TddCall& c)
                 span = std::max(span, a > b ? a - b : b - a);
             }
         }
-        const size_t w = (span + 4 * (size_t)spw - 1) / spw + 32 * (size_t)J + 1;
+        // quad-strided rows: a 1-sample delay is a 1-word offset, the window
+        // is the lane set (P words) plus the span plus the 16-byte rounding
+        n.quad = kern::tiled_variant_quad(c.in_nbits, n.variant);
+        n.period = 32 * J;
+        const size_t w = n.quad ? (size_t)span + 3 + (size_t)n.period
+                                : (span + 4 * (size_t)spw - 1) / spw + 32 * (size_t)J + 1;
         n.win_words = (int)round_up(w, 4);
         const int cs = w > ((size_t)1 << 26) ? 0 : kern::tiled_stage_channels(c.in_nbits, n.win_words, n.variant);
         if (cs < 2) {
@@ -190,21 +198,28 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
     auto pitch_for = [&](size_t g) {
         return round_up((round_up(g, bt) + s.tmax + spw - 1) / spw + win + 8, 32);
     };
+    // quad-strided rows: the tile windows read up to word
+    // (tiles - 1) * bt + tmax + P + 2 of a row
+    const bool quad = s.tiled && s.quad;
+    auto qpitch_for = [&](size_t g) { return round_up(round_up(g, bt) + s.tmax + s.period + 4, 32); };
     auto bytes_for = [&](size_t g) {
         size_t b = (v.nchans + 1) * pitch_for(g) * 4;
+        if (quad) b += (v.nchans + 1) * qpitch_for(g) * 4;
         if (!dev_out) b += ndm * g * ob;
         if (!dev_in) b += 2 * std::min(kStageBytes, round_up(g + s.tmax, 128) * row_bytes);
         return b;
     };
     size_t free_b = 0, total_b = 0;
     RT_CHECK(cudaMemGetInfo(&free_b, &total_b));
-    const size_t avail = free_b + m_tr.capacity() + m_out.capacity() + m_stage[0].capacity() +
-                         m_stage[1].capacity();
+    const size_t avail = free_b + m_tr.capacity() + m_q.capacity() + m_out.capacity() +
+                         m_stage[0].capacity() + m_stage[1].capacity();
     while (G > bt && bytes_for(G) > avail / 100 * 90) G = round_up(G / 2, bt);
     if (bytes_for(G) > avail) DD_THROW(DEDISP_MEM_ALLOC_FAILED);
 
     const size_t pitch = pitch_for(G);
     m_tr.reserve((v.nchans + 1) * pitch * 4);
+    const size_t qpitch = quad ? qpitch_for(G) : 0;
+    if (quad) m_q.reserve((v.nchans + 1) * qpitch * 4);
     if (!dev_out) m_out.reserve(ndm * G * ob);
     size_t chunk_rows = 0;
     if (!dev_in) {
@@ -283,6 +298,11 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
                 stage_used[b] = true;
             }
         }
+        // K1q: quad-strided rows of every channel and the zero row
+        if (quad) {
+            kern::launch_quad_build(tr, pitch, m_q.get<uint32_t>(), qpitch, v.nchans + 1, s.period, ex);
+            ++stats.launches;
+        }
         if (t_b && g0 == 0) t_b->record(ex);
 
         // K2 per DM group.
@@ -296,8 +316,8 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
             if (s0 >= s1) continue;
             groups.emplace_back(s0, s1);
             kern::DedisperseArgs da{};
-            da.tr = tr;
-            da.tr_pitch_words = pitch;
+            da.tr = quad ? m_q.get<uint32_t>() : tr;
+            da.tr_pitch_words = quad ? qpitch : pitch;
             da.nbits = nbits;
             da.nchans = v.nchans;
             da.chan_list = m_chan.get<int32_t>();

@@ -3,8 +3,9 @@
 // One call = validate-free execution of a (sub-)range of the DM list over a
 // time series, in gulps of output samples:
 //   host rows --(H2D, pinned or pageable, chunked)--> staging --K1--> channel-
-//   major packed HBM buffer --K2 (per DM group)--> output --(D2H per DM group,
-//   overlapped with later groups)--> host rows.
+//   major packed HBM buffer [--K1q--> quad-strided rows, 8-bit quad variants]
+//   --K2 (per DM group)--> output --(D2H per DM group, overlapped with later
+//   groups)--> host rows.
 // With DEDISP_DEVICE_POINTERS the copies disappear and K1/K2 read/write the
 // caller's buffers. Derived per-plan state (active channels, sorted DMs,
 // window sizes) is cached until the DM list or killmask changes.
@@ -63,7 +64,7 @@ public:
 
     size_t gulp_size = kDefaultGulp;
     TddKernel kernel = TddKernel::Auto;
-    int variant = 0;  // tile-shape variant of the tiled kernel (8-bit input)
+    int variant = -1;  // tile-shape variant of the tiled kernel (8-bit input; -1: default)
     bool record_timing = false;
     TddStats stats;
 
@@ -73,7 +74,7 @@ private:
 
     GpuState& m_gpu;
     std::unique_ptr<Setup> m_setup;
-    rt::DeviceBuffer m_chan, m_km, m_dms, m_perm, m_tr, m_out, m_stage[2];
+    rt::DeviceBuffer m_chan, m_km, m_dms, m_perm, m_tr, m_q, m_out, m_stage[2];
     std::vector<std::unique_ptr<rt::Event>> m_events;
     rt::Event& event(size_t i);
 };

@@ -5,6 +5,8 @@
 //                              (the reference algorithm, kept as baseline)
 //   K2  dedisperse_tiled       shared-memory staged channel windows, packed
 //                              SIMD-within-a-register accumulation
+//   K1q quad_build_kernel      channel-major packed -> quad-strided rows (8-bit)
+//   K2q dedisperse_quad8       the 8-bit accumulation on quad-strided rows
 //
 // Exactness: the sums are the reference's integer sums
 // (src/tdd/dedisperse/dedisperse_kernel.cuh:145-181): every integer delay is
@@ -15,6 +17,7 @@
 #include "tdd_kernels.hpp"
 
 #include <algorithm>
+#include <utility>
 
 #include "runtime.hpp"
 
@@ -628,6 +631,256 @@ dedisperse_tiled8_batch_kernel(const DedisperseArgs* __restrict__ args,
     }
 }
 
+// ---------------------------------------------------------------------------
+// K1q + K2q: the 8-bit kernel on quad-strided rows.
+//
+// For a period of P words, word n of a quad-strided row holds samples n,
+// n + P, n + 2P, n + 3P of the channel (byte i = sample n + i*P). A block
+// tile covers output samples [t0, t0 + 4P): lane word m (0 <= m < P) of a DM
+// accumulates the row's word t0 + m + d(dm, c) for every channel, whose four
+// bytes are exactly the four samples t0 + m + i*P + d(dm, c). Every delay is
+// therefore a whole-word offset: the rows are built once per gulp in HBM
+// (four times the packed size) instead of byte-shifted copies per block and
+// stage, and a stage is one window copy and one barrier. Lane l owns words
+// l, l + 32, ..., so a warp's shared loads are 32 consecutive words.
+// ---------------------------------------------------------------------------
+constexpr int QB_THREADS = 256, QB_ITERS = 8;  // K1q: quads per block = 2048
+
+// Quad k of a row: words 4k .. 4k+3 from the packed words k + i*P/4.
+__device__ __forceinline__ uint4 quad_words(const uint32_t* __restrict__ src, size_t tr_pitch, size_t k,
+                                            size_t p4)
+{
+    // w[i] = samples 4k + i*P .. 4k + i*P + 3; zero past the row
+    uint32_t w[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const size_t idx = k + (size_t)i * p4;
+        w[i] = idx < tr_pitch ? __ldg(src + idx) : 0u;
+    }
+    // 4x4 byte transpose: output word j = byte j of w[0..3]
+    const uint32_t a_lo = __byte_perm(w[0], w[1], 0x5140), a_hi = __byte_perm(w[0], w[1], 0x7362);
+    const uint32_t b_lo = __byte_perm(w[2], w[3], 0x5140), b_hi = __byte_perm(w[2], w[3], 0x7362);
+    return make_uint4(__byte_perm(a_lo, b_lo, 0x5410), __byte_perm(a_lo, b_lo, 0x7632),
+                      __byte_perm(a_hi, b_hi, 0x5410), __byte_perm(a_hi, b_hi, 0x7632));
+}
+
+__global__ void __launch_bounds__(QB_THREADS) quad_build_kernel(const uint32_t* __restrict__ tr,
+                                                                size_t tr_pitch, uint32_t* __restrict__ q,
+                                                                size_t q_pitch, size_t nrows, size_t p4)
+{
+    constexpr size_t PER_BLOCK = (size_t)QB_THREADS * QB_ITERS;
+    const size_t nquads = q_pitch / 4;
+    for (size_t row = blockIdx.y; row < nrows; row += gridDim.y) {
+        const uint32_t* src = tr + row * tr_pitch;
+        uint4* dst = reinterpret_cast<uint4*>(q + row * q_pitch);
+        for (size_t k0 = (size_t)blockIdx.x * PER_BLOCK; k0 < nquads; k0 += (size_t)gridDim.x * PER_BLOCK) {
+            const size_t k1 = k0 + threadIdx.x;
+            if (k0 + PER_BLOCK <= nquads) {
+                uint4 v[QB_ITERS];
+#pragma unroll
+                for (int it = 0; it < QB_ITERS; ++it) v[it] = quad_words(src, tr_pitch, k1 + (size_t)it * QB_THREADS, p4);
+#pragma unroll
+                for (int it = 0; it < QB_ITERS; ++it) dst[k1 + (size_t)it * QB_THREADS] = v[it];
+            } else {
+                for (size_t k = k1; k < nquads; k += QB_THREADS) dst[k] = quad_words(src, tr_pitch, k, p4);
+            }
+        }
+    }
+}
+
+// Tile shapes of the quad-strided kernel: J words per lane (P = 32J), NW warps
+// = NW DMs per block (one DM per warp).
+struct Q8Shape { int J, NW; };
+constexpr Q8Shape Q8_SHAPES[] = {{5, 32}, {4, 32}, {6, 24}, {8, 16}};
+constexpr int Q8_NSHAPES = sizeof(Q8_SHAPES) / sizeof(Q8_SHAPES[0]);
+constexpr int Q8_MAX_STAGE = 64;
+
+// Dynamic shared memory of a quad-strided launch: the opt-in maximum less the
+// static span-reduction buffer (one word per warp).
+constexpr size_t quad_dynamic_smem_bytes(int nw) { return 227 * 1024 - 4 * (size_t)nw; }
+
+// Shared loads with 32-bit window addresses and immediate offsets. Volatile:
+// the windows change at every stage barrier.
+template <uint32_t OFF>
+__device__ __forceinline__ uint32_t lds_imm(uint32_t addr)
+{
+    uint32_t v;
+    asm volatile("ld.shared.u32 %0, [%1+%2];\n" : "=r"(v) : "r"(addr), "n"(OFF));
+    return v;
+}
+
+__device__ __forceinline__ uint4 lds128(uint32_t addr)
+{
+    uint4 v;
+    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "r"(addr));
+    return v;
+}
+
+// w[k] = word (lane + 32k) of a window row, addr = row address + 4 * lane
+template <int J, uint32_t... K>
+__device__ __forceinline__ void lds_lane_words(uint32_t addr, uint32_t (&w)[J],
+                                               std::integer_sequence<uint32_t, K...>)
+{
+    ((w[K] = lds_imm<128u * K>(addr)), ...);
+}
+
+template <int J, int NW>
+__device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size_t by, uint32_t one)
+{
+    constexpr int P = 32 * J;
+    constexpr int NT = NW * 32;
+    constexpr size_t BT = 4 * (size_t)P;
+
+    extern __shared__ __align__(16) uint32_t smem[];
+    __shared__ uint32_t s_red[NW];
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int i0 = bx * NW;
+    const size_t t0 = by * BT;
+    const int nvalid = min(NW, a.ndm - i0);
+    const float dm_first = a.dms[i0];
+    const float dm_last = a.dms[i0 + nvalid - 1];
+    const float dm_own = a.dms[i0 + min(warp, nvalid - 1)];
+    const int npad = (a.nact + 3) & ~3;  // channel list length used (padded to 4)
+
+    // This block's window W (words per row) from its own delay span: the
+    // largest (hi - lo4) over the channels, plus the P words of a lane set,
+    // rounded to 16 bytes. Then as many channels per stage (a multiple of 4,
+    // at most Q8_MAX_STAGE) as the launch's shared memory holds.
+    uint32_t vmax = 0;
+    for (int j = threadIdx.x; j < npad; j += NT) {
+        const float dl = a.delay_table[a.chan_list[j]];
+        const uint32_t d0 = delay_rn(dm_first, dl), d1 = delay_rn(dm_last, dl);
+        vmax = max(vmax, max(d0, d1) - (min(d0, d1) & ~3u));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) vmax = max(vmax, __shfl_xor_sync(0xFFFFFFFFu, vmax, o));
+    if (lane == 0) s_red[warp] = vmax;
+    __syncthreads();
+    vmax = 0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) vmax = max(vmax, s_red[w]);
+    const int W = (int)((vmax + (uint32_t)P + 3u) & ~3u);
+    const int CS = min(Q8_MAX_STAGE, (a.smem_words / (2 * W + 4 + NW)) & ~3);
+    const int nstages = (npad + CS - 1) / CS;
+    const int CSW = CS * W;
+    uint32_t* s_win = smem;                                        // [2][CS][W] row windows
+    uint32_t* s_lo = s_win + 2 * CSW;                              // [2][CS] window start - t0
+    float* s_dl = reinterpret_cast<float*>(s_lo + 2 * CS);         // [2][CS] channel delay
+    uint32_t* s_off = reinterpret_cast<uint32_t*>(s_dl + 2 * CS);  // [NW][CS] per-warp row addresses
+
+    const uint32_t win_addr = (uint32_t)__cvta_generic_to_shared(s_win);
+    uint32_t* my_off = s_off + warp * CS;
+    const uint32_t my_off_addr = (uint32_t)__cvta_generic_to_shared(my_off);
+    const uint32_t lane4 = 4u * (uint32_t)lane;
+
+    // Window of channel row j: words [t0 + lo4, t0 + lo4 + need), lo4 the
+    // block's smallest delay rounded down to 4 words (16-byte copies), need
+    // covering the largest delay plus the P words of a lane set; need <= W.
+    auto stage_size = [&](int stage) { return min(CS, npad - stage * CS); };
+    auto prep = [&](int stage, int buf) {
+        const int32_t* cl = a.chan_list + (size_t)stage * CS;
+        const int cs = stage_size(stage);
+        for (int j = warp; j < cs; j += NW) {
+            const int c = cl[j];
+            const float dl = a.delay_table[c];
+            const uint32_t d0 = delay_rn(dm_first, dl), d1 = delay_rn(dm_last, dl);
+            const uint32_t lo4 = min(d0, d1) & ~3u, hi = max(d0, d1);
+            const int need = min(W, (int)((hi - lo4 + (uint32_t)P + 3u) & ~3u));
+            const uint32_t* src = a.tr + (size_t)c * a.tr_pitch_words + t0 + lo4;
+            uint32_t* dst = s_win + buf * CSW + j * W;
+            for (int k = lane * 4; k < need; k += 128) cp_async16(dst + k, src + k);
+            if (lane == 0) {
+                s_lo[buf * CS + j] = lo4;
+                s_dl[buf * CS + j] = dl;
+            }
+        }
+    };
+
+    uint32_t acc[4 * J];
+    uint32_t sw[J], so[J];
+#pragma unroll
+    for (int k = 0; k < 4 * J; ++k) acc[k] = 0;
+#pragma unroll
+    for (int k = 0; k < J; ++k) sw[k] = so[k] = 0;
+    auto flush = [&]() {
+#pragma unroll
+        for (int k = 0; k < J; ++k) {
+            const uint32_t e = imad(so[k], 0xFFFFFF00u, sw[k]);  // S - 256*O
+            acc[4 * k + 0] += e & 0xFFFFu;
+            acc[4 * k + 2] += e >> 16;
+            acc[4 * k + 1] += so[k] & 0xFFFFu;
+            acc[4 * k + 3] += so[k] >> 16;
+            sw[k] = so[k] = 0;
+        }
+    };
+    // one channel pair: rows at a1, a2 (byte addresses including 4 * lane)
+    auto pair = [&](uint32_t a1, uint32_t a2) {
+        uint32_t w1[J], w2[J];
+        lds_lane_words<J>(a1, w1, std::make_integer_sequence<uint32_t, J>{});
+        lds_lane_words<J>(a2, w2, std::make_integer_sequence<uint32_t, J>{});
+#pragma unroll
+        for (int k = 0; k < J; ++k) {
+            sw[k] = sw[k] + w1[k] + w2[k];
+            so[k] = imad(__byte_perm(w1[k], 0u, 0x4341), one, so[k]);
+            so[k] = imad(__byte_perm(w2[k], 0u, 0x4341), one, so[k]);
+        }
+    };
+
+    prep(0, 0);
+    cp_async_commit();
+    int since_flush = 0;  // channels accumulated since the last flush
+    for (int s = 0; s < nstages; ++s) {
+        const int buf = s & 1;
+        const int cs = stage_size(s);
+        asm volatile("cp.async.wait_group 0;\n" ::);
+        __syncthreads();  // stage s landed; every warp is done with stage s - 1
+        if (s + 1 < nstages) prep(s + 1, buf ^ 1);
+        cp_async_commit();
+        // this warp's row addresses in the stage's windows
+        for (int j = lane; j < cs; j += 32) {
+            const uint32_t d = delay_rn(dm_own, s_dl[buf * CS + j]);
+            my_off[j] = win_addr + 4u * ((uint32_t)(buf * CSW + j * W) + (d - s_lo[buf * CS + j]));
+        }
+        __syncwarp();
+
+        // 16-bit lanes hold at most 256 channels of 8-bit samples
+        if (since_flush + cs > T8_FLUSH_CHANNELS) {
+            flush();
+            since_flush = 0;
+        }
+#pragma unroll 1
+        for (int j = 0; j < cs; j += 4) {
+            const uint4 f = lds128(my_off_addr + 4u * (uint32_t)j);
+            pair(f.x + lane4, f.y + lane4);
+            pair(f.z + lane4, f.w + lane4);
+        }
+        since_flush += cs;
+    }
+    flush();
+
+    if (warp < nvalid) {
+        const int row = a.perm ? a.perm[i0 + warp] : i0 + warp;
+        const size_t base = (size_t)row * a.out_stride;
+#pragma unroll
+        for (int k = 0; k < J; ++k) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const size_t t = t0 + (size_t)(lane + 32 * k) + (size_t)i * P;
+                if (t < a.nsamp_out) store_out(a.out, base + t, a.out_nbits, acc[4 * k + i], a.den, a.factor);
+            }
+        }
+    }
+}
+
+template <int J, int NW>
+__global__ void __launch_bounds__(NW * 32, 1) dedisperse_quad8_kernel(DedisperseArgs a, uint32_t one)
+{
+    quad8_tile<J, NW>(a, blockIdx.x, blockIdx.y, one);
+}
+
 // cudaFuncSetAttribute is per device context; remember what each device has
 // been given, per kernel.
 template <typename K>
@@ -659,6 +912,30 @@ void launch_tiled8_variant(const DedisperseArgs& a, cudaStream_t s)
 }
 
 template <int J, int NW>
+void launch_quad8_shape(const DedisperseArgs& a, cudaStream_t s)
+{
+    // One block per SM (registers): every block may use the whole opt-in
+    // shared memory for its windows; a block sizes its stages from its own
+    // delay span. The plan's window (the largest span) must fit 4 channels.
+    static size_t configured[64] = {};
+    const size_t smem = quad_dynamic_smem_bytes(NW);
+    if (tiled_smem_bytes(8, a.win_words, 4, a.variant) > smem)
+        DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "quad-strided window does not fit shared memory");
+    ensure_smem(dedisperse_quad8_kernel<J, NW>, smem, configured);
+    DedisperseArgs b = a;
+    b.smem_words = (int)(smem / 4);
+    dim3 grid((a.ndm + NW - 1) / NW, (unsigned)((a.nsamp_out + 128 * J - 1) / (128 * J)));
+    dedisperse_quad8_kernel<J, NW><<<grid, NW * 32, smem, s>>>(b, 1u);
+    RT_CHECK(cudaGetLastError());
+}
+
+template <int V>
+void launch_quad8_variant(const DedisperseArgs& a, cudaStream_t s)
+{
+    launch_quad8_shape<Q8_SHAPES[V].J, Q8_SHAPES[V].NW>(a, s);
+}
+
+template <int J, int NW>
 void launch_tiled8_batch_shape(const BatchLaunch& b, cudaStream_t s)
 {
     static size_t configured[64] = {};
@@ -685,13 +962,17 @@ template <int NBITS>
 void launch_tiled_n(const DedisperseArgs& a, cudaStream_t s)
 {
     if constexpr (NBITS == 8) {
-        static_assert(T8_NSHAPES == 5, "dispatch below lists every shape");
+        static_assert(T8_NSHAPES == 5 && Q8_NSHAPES == 4, "dispatch below lists every shape");
         switch (a.variant) {
         case 0: launch_tiled8_variant<0>(a, s); break;
         case 1: launch_tiled8_variant<1>(a, s); break;
         case 2: launch_tiled8_variant<2>(a, s); break;
         case 3: launch_tiled8_variant<3>(a, s); break;
         case 4: launch_tiled8_variant<4>(a, s); break;
+        case 5: launch_quad8_variant<0>(a, s); break;
+        case 6: launch_quad8_variant<1>(a, s); break;
+        case 7: launch_quad8_variant<2>(a, s); break;
+        case 8: launch_quad8_variant<3>(a, s); break;
         default: DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unknown tiled kernel variant");
         }
     } else {
@@ -727,13 +1008,23 @@ void launch_transpose_n(const TransposeArgs& a, cudaStream_t s)
 
 }  // namespace
 
-int tiled_variant_count(int nbits) { return nbits == 8 ? T8_NSHAPES : 1; }
+int tiled_variant_count(int nbits) { return nbits == 8 ? T8_NSHAPES + Q8_NSHAPES : 1; }
+int tiled_batch_variant_count(int nbits) { return nbits == 8 ? T8_NSHAPES : 1; }
+// 8-bit: the quad-strided {J = 5, 32 warps} shape, the fastest measured on
+// the 4096-channel, 3643-DM workload
+int tiled_default_variant(int nbits) { return nbits == 8 ? T8_NSHAPES : 0; }
 
 static int checked_variant(int nbits, int variant)
 {
     if (variant < 0 || variant >= tiled_variant_count(nbits))
         DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unknown tiled kernel variant");
     return variant;
+}
+
+bool tiled_variant_quad(int nbits, int variant)
+{
+    checked_variant(nbits, variant);
+    return nbits == 8 && variant >= T8_NSHAPES;
 }
 
 int tiled_block_samples(int nbits, int variant)
@@ -743,7 +1034,7 @@ int tiled_block_samples(int nbits, int variant)
     case 1: return TiledGeom<1>::BT;
     case 2: return TiledGeom<2>::BT;
     case 4: return TiledGeom<4>::BT;
-    case 8: return 128 * T8_SHAPES[variant].J;
+    case 8: return 128 * tiled_lane_words(8, variant);
     case 16: return TiledGeom<16>::BT;
     default: return TiledGeom<32>::BT;
     }
@@ -756,7 +1047,7 @@ int tiled_block_dms(int nbits, int variant)
     case 1: return TiledGeom<1>::BD;
     case 2: return TiledGeom<2>::BD;
     case 4: return TiledGeom<4>::BD;
-    case 8: return T8_SHAPES[variant].NW;
+    case 8: return variant < T8_NSHAPES ? T8_SHAPES[variant].NW : Q8_SHAPES[variant - T8_NSHAPES].NW;
     case 16: return TiledGeom<16>::BD;
     default: return TiledGeom<32>::BD;
     }
@@ -769,7 +1060,7 @@ int tiled_lane_words(int nbits, int variant)
     case 1: return TiledGeom<1>::J;
     case 2: return TiledGeom<2>::J;
     case 4: return TiledGeom<4>::J;
-    case 8: return T8_SHAPES[variant].J;
+    case 8: return variant < T8_NSHAPES ? T8_SHAPES[variant].J : Q8_SHAPES[variant - T8_NSHAPES].J;
     case 16: return TiledGeom<16>::J;
     default: return TiledGeom<32>::J;
     }
@@ -778,11 +1069,15 @@ int tiled_lane_words(int nbits, int variant)
 size_t tiled_smem_bytes(int nbits, int win_words, int chan_per_stage, int variant)
 {
     const size_t bd = (size_t)tiled_block_dms(nbits, variant);
+    const size_t cs = (size_t)chan_per_stage;
+    // quad-strided: two window buffers, window starts and delays per row,
+    // one offset per (DM, row)
+    if (tiled_variant_quad(nbits, variant)) return (2 * cs * win_words + 4 * cs + bd * cs) * 4ull;
     // 8-bit: two raw buffers plus three byte-shifted copies per stage, and
     // the per-row window lengths
     const size_t windows = nbits == 8 ? 5ull : 2ull;
-    const size_t extra = nbits == 8 ? 2ull * chan_per_stage : 0ull;
-    return (windows * chan_per_stage * win_words + 2ull * bd * chan_per_stage + extra + bd) * 4ull;
+    const size_t extra = nbits == 8 ? 2ull * cs : 0ull;
+    return (windows * cs * win_words + 2ull * bd * cs + extra + bd) * 4ull;
 }
 
 // The opt-in maximum of dynamic shared memory per block on sm_100.
@@ -790,9 +1085,27 @@ size_t tiled_max_smem_bytes() { return 227 * 1024; }
 
 int tiled_stage_channels(int nbits, int win_words, int variant)
 {
-    int cs = 32;
-    while (cs >= 2 && tiled_smem_bytes(nbits, win_words, cs, variant) > tiled_max_smem_bytes()) cs -= 2;
-    return cs >= 2 ? cs : 0;
+    // quad-strided: four channels per inner step
+    const bool quad = tiled_variant_quad(nbits, variant);
+    const int step = quad ? 4 : 2;
+    int cs = quad ? Q8_MAX_STAGE : 32;
+    const size_t cap = quad ? quad_dynamic_smem_bytes(tiled_block_dms(nbits, variant)) : tiled_max_smem_bytes();
+    while (cs >= step && tiled_smem_bytes(nbits, win_words, cs, variant) > cap) cs -= step;
+    return cs >= step ? cs : 0;
+}
+
+void launch_quad_build(const uint32_t* tr, size_t tr_pitch_words, uint32_t* q, size_t q_pitch_words,
+                       size_t nrows, int period_words, cudaStream_t s)
+{
+    if (q_pitch_words % 4 != 0 || period_words % 4 != 0 || (uintptr_t)q % 16 != 0)
+        DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "quad-strided rows need 16-byte aligned rows and a period of 4k words");
+    const size_t nquads = q_pitch_words / 4;
+    constexpr size_t per_block = (size_t)QB_THREADS * QB_ITERS;
+    dim3 grid((unsigned)std::min<size_t>((nquads + per_block - 1) / per_block, 65535),
+              (unsigned)std::min<size_t>(nrows, 65535));
+    quad_build_kernel<<<grid, QB_THREADS, 0, s>>>(tr, tr_pitch_words, q, q_pitch_words, nrows,
+                                                  (size_t)period_words / 4);
+    RT_CHECK(cudaGetLastError());
 }
 
 void launch_transpose(const TransposeArgs& a, cudaStream_t s)

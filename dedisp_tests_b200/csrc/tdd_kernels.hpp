@@ -53,11 +53,19 @@ struct DedisperseArgs {
     int win_words;              // tiled: staged window per channel (words)
     int chan_per_stage;         // tiled: channels per pipeline stage (even)
     int variant;                // tiled: tile-shape variant (8-bit input)
+    int smem_words;             // quad: dynamic shared memory of the launch (set by the launcher)
 };
 
 // Tile geometry of the tiled kernel for a given input width and tile-shape
 // variant (8-bit input has several, see tiled_variant_count; other widths 1).
+// 8-bit variants from tiled_batch_variant_count(8) on run on quad-strided
+// rows (tiled_variant_quad): word n of a row holds samples n + i*P of the
+// channel in byte i (i = 0..3, P = 32 * tiled_lane_words), built from the
+// channel-major packed rows by launch_quad_build.
 int tiled_variant_count(int nbits);
+int tiled_batch_variant_count(int nbits);  // variants of the persistent batch kernel
+int tiled_default_variant(int nbits);      // the variant a plan uses unless told otherwise
+bool tiled_variant_quad(int nbits, int variant);
 int tiled_block_samples(int nbits, int variant);  // output samples per block
 int tiled_block_dms(int nbits, int variant);      // DMs per block
 int tiled_lane_words(int nbits, int variant);     // J: words per lane
@@ -65,6 +73,12 @@ size_t tiled_smem_bytes(int nbits, int win_words, int chan_per_stage, int varian
 size_t tiled_max_smem_bytes();
 // Channels per pipeline stage for a window of win_words (0: does not fit).
 int tiled_stage_channels(int nbits, int win_words, int variant);
+
+// K1q: quad-strided rows q (q_pitch_words per row, a multiple of 4, rows
+// 16-byte aligned) from channel-major packed 8-bit rows tr, for nrows rows;
+// samples past a tr row read as zero.
+void launch_quad_build(const uint32_t* tr, size_t tr_pitch_words, uint32_t* q, size_t q_pitch_words,
+                       size_t nrows, int period_words, cudaStream_t s);
 
 void launch_dedisperse_plain(const DedisperseArgs& a, cudaStream_t s);
 void launch_dedisperse_tiled(const DedisperseArgs& a, cudaStream_t s);

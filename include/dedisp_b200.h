@@ -26,8 +26,11 @@ dedisp_error dedisp_b200_set_tdd_kernel(dedisp_plan plan, int kernel);
 
 /* Tile shape of the tiled TDD kernel (8-bit input: DMs per block, samples
  * per thread); variant in [0, dedisp_b200_tdd_variant_count(in_nbits)).
- * Every variant computes the same bit-exact sums; they differ in speed.
- * Other input widths have a single shape and ignore the setting. */
+ * 8-bit variants from dedisp_b200_batch_variant_count(8) on work on
+ * quad-strided rows built per gulp (four times the packed input size in
+ * device memory). Every variant computes the same bit-exact sums; they
+ * differ in speed. Other input widths have a single shape and ignore the
+ * setting. */
 dedisp_error dedisp_b200_set_tdd_variant(dedisp_plan plan, int variant);
 int dedisp_b200_tdd_variant_count(dedisp_size in_nbits);
 
@@ -128,8 +131,9 @@ dedisp_error dedisp_b200_batch_set_beams(dedisp_b200_batch batch, const dedisp_b
 dedisp_size dedisp_b200_batch_workspace_size(dedisp_b200_batch batch);
 dedisp_error dedisp_b200_batch_set_workspace(dedisp_b200_batch batch, void* d_workspace,
                                              dedisp_size bytes);
-/* Tile shape: variant < dedisp_b200_tdd_variant_count(in_nbits), channels
+/* Tile shape: variant < dedisp_b200_batch_variant_count(in_nbits), channels
  * per stage even and <= 32 (0: the largest that fits shared memory). */
+int dedisp_b200_batch_variant_count(dedisp_size in_nbits);
 dedisp_error dedisp_b200_batch_set_shape(dedisp_b200_batch batch, int variant, int chan_per_stage);
 /* Times every candidate shape on the leading 8192 output samples of each
  * beam (CUDA events, on `stream`, synchronous) and keeps the fastest. */

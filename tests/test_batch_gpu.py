@@ -109,7 +109,7 @@ def test_batch_oracle_one_beam_and_every_shape():
     packed, dms = host[1]
     delays = po.delay_table(PARAMS[0], np.float32(PARAMS[1]), np.float32(PARAMS[2]),
                             np.float32(PARAMS[3]))
-    for v in range(dd.tdd_variant_count(8)):
+    for v in range(dd.batch_variant_count(8)):
         for cs in (0, 8):
             got, _ = _run_batch(8, host, shape=(v, cs), reps=1)
             nout = got[1].shape[1]

@@ -180,6 +180,20 @@ def test_batch_api_argument_checks():
     assert not h.value
 
 
+def test_tile_variant_counts():
+    """8-bit input: five shapes on channel-major packed rows (also the
+    persistent batch kernel's shapes) and four on quad-strided rows; every
+    other width has one shape. Out-of-range variants are rejected."""
+    assert dd.tdd_variant_count(8) == 9 and dd.batch_variant_count(8) == 5
+    for nb in (1, 2, 4, 16, 32):
+        assert dd.tdd_variant_count(nb) == 1 and dd.batch_variant_count(nb) == 1
+    p = dd.TDDPlan(64, 1e-4, 1500.0, -1.0)
+    for bad in (-1, 9):
+        with pytest.raises(dd.DedispError):
+            p.set_tile_variant(bad)
+    p.set_tile_variant(8)
+
+
 @pytest.mark.skipif(__import__("torch").cuda.is_available(), reason="checks the no-GPU path")
 def test_batch_create_without_gpu_fails_cleanly():
     L = dd._batch_lib()

@@ -64,11 +64,12 @@ def test_all_widths_bit_exact(nbits, nchans, kernel):
         assert np.array_equal(ours.view(np.uint8), ref.view(np.uint8)), (nbits, out_nbits)
 
 
-@pytest.mark.parametrize("variant", range(5))
+@pytest.mark.parametrize("variant", range(9))
 def test_tiled8_tile_variants_bit_exact(variant):
-    """Every tile shape of the 8-bit kernel; > 256 channels so the 16-bit
-    lanes are flushed several times, with a killmask thinning the list."""
-    assert dd.tdd_variant_count(8) == 5
+    """Every tile shape of the 8-bit kernel (packed rows 0-4, quad-strided
+    rows 5-8); > 256 channels so the 16-bit lanes are flushed several times,
+    with a killmask thinning the list."""
+    assert dd.tdd_variant_count(8) == 9 and dd.batch_variant_count(8) == 5
     nchans, nsamps = 1100, 12000
     packed, dms, params = _case(8, nchans, nsamps, 75, 600.0, 900 + variant, df=-0.25)
     km = np.ones(nchans, np.int32)
@@ -83,6 +84,32 @@ def test_tiled8_tile_variants_bit_exact(variant):
     p.execute(nsamps, packed, 8, out, 32)
     ref = _oracle(packed, nsamps, 8, params, dms, km, 32, nout)
     assert np.array_equal(out.view(np.uint32), ref.view(np.uint32))
+
+
+@pytest.mark.parametrize("variant", range(5, 9))
+def test_quad_variants_gulps_unsorted_out_widths(variant):
+    """Quad-strided variants over several gulps (the rows are rebuilt per
+    gulp), an unsorted DM list with a repeat (permuted output rows), a
+    partial last DM block, and 8/16/32-bit outputs."""
+    nchans, nsamps = 320, 26000
+    packed, _, params = _case(8, nchans, nsamps, 1, 1.0, 40 + variant, df=-0.5)
+    rng = np.random.default_rng(variant)
+    dms = rng.uniform(0, 400, 77).astype(np.float32)
+    dms[5] = dms[40]
+    dms[-1] = 400.0
+    km = np.ones(nchans, np.int32)
+    for out_nbits, gulp in ((8, 3001), (16, 0), (32, 7777)):
+        p = dd.TDDPlan(*params)
+        p.set_dm_list(dms)
+        p.set_kernel(2)
+        p.set_tile_variant(variant)
+        if gulp:
+            p.set_gulp_size(gulp)
+        nout = nsamps - p.get_max_delay()
+        out = np.zeros((len(dms), nout), OUT_DTYPE[out_nbits])
+        p.execute(nsamps, packed, 8, out, out_nbits)
+        ref = _oracle(packed, nsamps, 8, params, dms, km, out_nbits, nout)
+        assert np.array_equal(out.view(np.uint8), ref.view(np.uint8)), (out_nbits, gulp)
 
 
 def test_tiled8_saturated_bytes():
