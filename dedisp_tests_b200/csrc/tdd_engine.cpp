@@ -147,10 +147,15 @@ void TddEngine::prepare(const TddView& v, const TddCall& c)
     std::vector<int32_t> chan(n.chan_list);
     if (n.tiled) chan.resize((size_t)n.nstages * n.chan_per_stage, (int32_t)v.nchans);
     if (chan.empty()) chan.push_back((int32_t)v.nchans);
+    // delay of each list entry (the padding channel's is 0)
+    std::vector<float> cdl(chan.size());
+    for (size_t j = 0; j < chan.size(); ++j) cdl[j] = chan[j] < (int32_t)v.nchans ? v.delays[chan[j]] : 0.f;
 
     cudaStream_t st = m_gpu.stream();
     m_chan.reserve(chan.size() * 4);
     RT_CHECK(cudaMemcpyAsync(m_chan.get(), chan.data(), chan.size() * 4, cudaMemcpyHostToDevice, st));
+    m_cdl.reserve(cdl.size() * 4);
+    RT_CHECK(cudaMemcpyAsync(m_cdl.get(), cdl.data(), cdl.size() * 4, cudaMemcpyHostToDevice, st));
     std::vector<uint32_t> km(n.km_vals);
     if (km.empty()) km.push_back(0);
     m_km.reserve(km.size() * 4);
@@ -325,6 +330,7 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
             da.nstages = s.nstages;
             da.km_vals = m_km.get<uint32_t>();
             da.delay_table = m_gpu.delay_table.get<float>();
+            da.chan_delay = m_cdl.get<float>();
             da.dms = m_dms.get<float>() + s0;
             da.ndm = (int)(s1 - s0);
             da.nsamp_out = gc;

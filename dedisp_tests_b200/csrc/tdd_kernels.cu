@@ -198,6 +198,11 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
 }
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
 
@@ -696,8 +701,12 @@ constexpr int Q8_NSHAPES = sizeof(Q8_SHAPES) / sizeof(Q8_SHAPES[0]);
 constexpr int Q8_MAX_STAGE = 64;
 
 // Dynamic shared memory of a quad-strided launch: the opt-in maximum less the
-// static span-reduction buffer (one word per warp).
-constexpr size_t quad_dynamic_smem_bytes(int nw) { return 227 * 1024 - 4 * (size_t)nw; }
+// static buffers (span reduction, one word per warp; channels and delays of
+// two stages).
+constexpr size_t quad_dynamic_smem_bytes(int nw)
+{
+    return 227 * 1024 - 4 * (size_t)nw - 2 * 2 * Q8_MAX_STAGE * 4;
+}
 
 // Shared loads with 32-bit window addresses and immediate offsets. Volatile:
 // the windows change at every stage barrier.
@@ -735,6 +744,8 @@ __device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size
 
     extern __shared__ __align__(16) uint32_t smem[];
     __shared__ uint32_t s_red[NW];
+    __shared__ int32_t s_cl[2][Q8_MAX_STAGE];  // channel of each row, stages fetched ahead
+    __shared__ float s_cdl[2][Q8_MAX_STAGE];   // its delay
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int i0 = bx * NW;
@@ -751,7 +762,7 @@ __device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size
     // at most Q8_MAX_STAGE) as the launch's shared memory holds.
     uint32_t vmax = 0;
     for (int j = threadIdx.x; j < npad; j += NT) {
-        const float dl = a.delay_table[a.chan_list[j]];
+        const float dl = a.chan_delay[j];
         const uint32_t d0 = delay_rn(dm_first, dl), d1 = delay_rn(dm_last, dl);
         vmax = max(vmax, max(d0, d1) - (min(d0, d1) & ~3u));
     }
@@ -780,12 +791,20 @@ __device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size
     // block's smallest delay rounded down to 4 words (16-byte copies), need
     // covering the largest delay plus the P words of a lane set; need <= W.
     auto stage_size = [&](int stage) { return min(CS, npad - stage * CS); };
+    // channels and delays of a stage's rows into s_cl/s_cdl[stage & 1]
+    auto fetch = [&](int stage) {
+        const int cs = stage_size(stage);
+        const size_t g = (size_t)stage * CS;
+        for (int j = threadIdx.x; j < cs; j += NT) {
+            cp_async4(&s_cl[stage & 1][j], a.chan_list + g + j);
+            cp_async4(&s_cdl[stage & 1][j], a.chan_delay + g + j);
+        }
+    };
     auto prep = [&](int stage, int buf) {
-        const int32_t* cl = a.chan_list + (size_t)stage * CS;
         const int cs = stage_size(stage);
         for (int j = warp; j < cs; j += NW) {
-            const int c = cl[j];
-            const float dl = a.delay_table[c];
+            const int c = s_cl[stage & 1][j];
+            const float dl = s_cdl[stage & 1][j];
             const uint32_t d0 = delay_rn(dm_first, dl), d1 = delay_rn(dm_last, dl);
             const uint32_t lo4 = min(d0, d1) & ~3u, hi = max(d0, d1);
             const int need = min(W, (int)((hi - lo4 + (uint32_t)P + 3u) & ~3u));
@@ -829,7 +848,12 @@ __device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size
         }
     };
 
-    prep(0, 0);
+    if (nstages > 0) fetch(0);
+    if (nstages > 1) fetch(1);
+    cp_async_commit();
+    asm volatile("cp.async.wait_group 0;\n" ::);
+    __syncthreads();
+    if (nstages > 0) prep(0, 0);
     cp_async_commit();
     int since_flush = 0;  // channels accumulated since the last flush
     for (int s = 0; s < nstages; ++s) {
@@ -838,6 +862,7 @@ __device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size
         asm volatile("cp.async.wait_group 0;\n" ::);
         __syncthreads();  // stage s landed; every warp is done with stage s - 1
         if (s + 1 < nstages) prep(s + 1, buf ^ 1);
+        if (s + 2 < nstages) fetch(s + 2);  // s_cl/s_cdl[s & 1]: prep(s) finished before the barrier
         cp_async_commit();
         // this warp's row addresses in the stage's windows
         for (int j = lane; j < cs; j += 32) {

@@ -41,6 +41,7 @@ struct DedisperseArgs {
     int nstages;                // tiled: padded list length / chan_per_stage
     const uint32_t* km_vals;    // plain: multiplier per active channel
     const float* delay_table;   // nchans + 1 entries, last one 0
+    const float* chan_delay;    // quad: delay_table[chan_list[j]] per list entry
     const float* dms;           // DM per slot (sorted ascending for tiled)
     const int32_t* perm;        // output row of slot i (nullptr: identity)
     int ndm;
