@@ -318,7 +318,9 @@ def run_batched(args, local, world, stream, max_over_ranks):
     torch.cuda.synchronize()
     free, _ = torch.cuda.mem_get_info(local)
     budget = free - 12e9  # output pool + transposed-input workspace
-    in_bytes = [x.numel() * 1.1 for x in d_in]
+    # workspace per beam: channel-major packed rows (1x the input) plus the
+    # quad-strided rows of the quad variants (4x), with padding
+    in_bytes = [x.numel() * 5.3 for x in d_in]
 
     def partition(cap):
         waves, cur, acc = [], [], 0.0
@@ -376,12 +378,14 @@ def run_batched(args, local, world, stream, max_over_ranks):
     torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1)) / steps
     total_units = float(sum(units))
+    # kernels per graph: K1 per beam (+ K1q per beam on quad-strided rows) + 1
+    launches_per_step = sum(b.get_timing()["launches"] for b in batches)
     res = {"workload": "96 beams x 1536 ch 8-bit, nsamp U[2^17,2^20], DM max U[500,3000], "
                        "ndm U[1024,4096] linear (seeded), f32 out",
            "units": total_units, "waves": len(waves), "beams_per_wave": [len(w) for w in waves],
            "shape": {"variant": shape[0], "chan_per_stage": shape[1]},
            "batched": {"value": total_units * world / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
-                       "launches_per_step": sum(len(w) + 1 for w in waves)}}
+                       "launches_per_step": launches_per_step}}
     for b in batches:
         b.close()
     del pool, ws, batches, spec, y

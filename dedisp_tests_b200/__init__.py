@@ -298,7 +298,7 @@ def tdd_variant_count(in_nbits: int = 8) -> int:
 
 def batch_variant_count(in_nbits: int = 8) -> int:
     """Number of tile-shape variants of the persistent multi-beam kernel
-    (the leading plan variants, which work on channel-major packed rows)."""
+    (the same shapes as the plans' tiled kernel)."""
     return int(_batch_lib().dedisp_b200_batch_variant_count(in_nbits))
 
 

@@ -36,6 +36,11 @@ struct TddBatch::Layout {
     std::vector<kern::DedisperseArgs> args;   // host copy (device pointers)
     std::vector<size_t> tr_off;               // words into the workspace
     std::vector<size_t> pitch;                // words per channel row
+    bool quad = false;                        // quad-strided rows (8-bit quad variants)
+    int period = 0;                           // quad: P words
+    std::vector<size_t> q_off;                // quad: rows' offset in the workspace (words)
+    std::vector<size_t> qpitch;               // quad: words per row
+    uint32_t* ws = nullptr;                   // workspace the args point into (upload)
     std::vector<int> nbx;
     std::vector<unsigned long long> start;    // nbeams + 1
     std::vector<size_t> units;                // DM trials x samples covered per beam
@@ -97,9 +102,13 @@ void TddBatch::set_killmask(const int32_t* killmask)
     std::vector<int32_t> padded(m_chan);
     padded.resize(round_up(std::max<size_t>(m_chan.size(), 1), kMaxStageChannels) + kMaxStageChannels,
                   (int32_t)m_nchans);
+    std::vector<float> cdl(padded.size());  // delay of each list entry
+    for (size_t j = 0; j < padded.size(); ++j) cdl[j] = m_delays[padded[j]];
     rt::DeviceGuard g(m_device);
     m_d_chan.reserve(padded.size() * 4);
     RT_CHECK(cudaMemcpy(m_d_chan.get(), padded.data(), padded.size() * 4, cudaMemcpyHostToDevice));
+    m_d_cdl.reserve(cdl.size() * 4);
+    RT_CHECK(cudaMemcpy(m_d_cdl.get(), cdl.data(), cdl.size() * 4, cudaMemcpyHostToDevice));
     m_d_kmv.reserve(std::max<size_t>(m_kmv.size(), 1) * 4);
     if (!m_kmv.empty())
         RT_CHECK(cudaMemcpy(m_d_kmv.get(), m_kmv.data(), m_kmv.size() * 4, cudaMemcpyHostToDevice));
@@ -185,10 +194,14 @@ TddBatch::Layout TddBatch::make_layout(const BatchShape& shape, size_t tile_limi
     const size_t bd = (size_t)kern::tiled_block_dms(nb, v);
     const size_t bt = (size_t)kern::tiled_block_samples(nb, v);
     const int J = kern::tiled_lane_words(nb, v);
+    const bool quad = want_tiled && kern::tiled_variant_quad(nb, v);
     const size_t nbeams = m_beams.size();
     L.args.resize(nbeams);
     L.tr_off.resize(nbeams);
     L.pitch.resize(nbeams);
+    L.q_off.assign(nbeams, 0);
+    L.qpitch.assign(nbeams, 0);
+    L.period = 32 * J;
     L.nbx.resize(nbeams);
     L.units.resize(nbeams);
     L.start.assign(nbeams + 1, 0);
@@ -206,7 +219,9 @@ TddBatch::Layout TddBatch::make_layout(const BatchShape& shape, size_t tile_limi
                 span = std::max(span, x > y ? x - y : y - x);
             }
         }
-        const size_t w = round_up((span + 4 * (size_t)spw - 1) / spw + 32 * (size_t)J + 1, 4);
+        // quad-strided rows: a 1-sample delay is a 1-word offset
+        const size_t w = quad ? round_up((size_t)span + 3 + 32 * (size_t)J, 4)
+                              : round_up((span + 4 * (size_t)spw - 1) / spw + 32 * (size_t)J + 1, 4);
         const int fit = w > ((size_t)1 << 26) ? 0 : kern::tiled_stage_channels(nb, (int)w, v);
         if (fit < 2) { tiled = false; break; }
         W[b] = (int)w;
@@ -214,6 +229,7 @@ TddBatch::Layout TddBatch::make_layout(const BatchShape& shape, size_t tile_limi
     }
     L.tiled = tiled;
     L.persistent = tiled && nb == 8;
+    L.quad = tiled && quad;
     const size_t ubt = tiled ? bt : 16, ubd = tiled ? bd : 32;
     const float in_range = (float)(nb == 32 ? 0xFFFFFFFFu : ((1u << nb) - 1u));
     size_t off = 0;
@@ -223,9 +239,15 @@ TddBatch::Layout TddBatch::make_layout(const BatchShape& shape, size_t tile_limi
         L.pitch[b] = round_up((round_up(std::max<size_t>(t.nout, 1), ubt) + t.tmax + spw - 1) / spw + win + 8, 32);
         L.tr_off[b] = off;
         off += round_up((m_nchans + 1) * L.pitch[b], 64);
+        if (L.quad) {
+            // the tile windows read up to word (tiles - 1) * bt + tmax + P + 2
+            L.qpitch[b] = round_up(round_up(std::max<size_t>(t.nout, 1), ubt) + t.tmax + L.period + 4, 32);
+            L.q_off[b] = off;
+            off += round_up((m_nchans + 1) * L.qpitch[b], 64);
+        }
         kern::DedisperseArgs& a = L.args[b];
         a = kern::DedisperseArgs{};
-        a.tr_pitch_words = L.pitch[b];
+        a.tr_pitch_words = L.quad ? L.qpitch[b] : L.pitch[b];
         a.nbits = nb;
         a.nchans = m_nchans;
         a.nact = (int)m_chan.size();
@@ -249,7 +271,7 @@ TddBatch::Layout TddBatch::make_layout(const BatchShape& shape, size_t tile_limi
         L.nbx[b] = (int)nbx;
         L.units[b] = t.sorted.size() * covered;
         L.start[b + 1] = L.start[b] + (unsigned long long)(nbx * nby);
-        if (tiled) L.smem = std::max(L.smem, kern::tiled_smem_bytes(nb, W[b], CS[b], v));
+        if (tiled) L.smem = std::max(L.smem, kern::tiled_batch_smem_bytes(nb, W[b], CS[b], v));
     }
     L.ws_words = off;
     return L;
@@ -289,8 +311,9 @@ void TddBatch::upload(Layout& L)
     for (size_t b = 0; b < m_beams.size(); ++b) {
         const BeamState& t = m_beams[b];
         kern::DedisperseArgs& a = args[b];
-        a.tr = ws + L.tr_off[b];
+        a.tr = ws + (L.quad ? L.q_off[b] : L.tr_off[b]);
         a.chan_list = m_d_chan.get<int32_t>();
+        a.chan_delay = m_d_cdl.get<float>();
         a.km_vals = m_d_kmv.get<uint32_t>();
         a.delay_table = m_d_delay.get<float>();
         a.dms = m_d_dms.get<float>() + t.dm_off;
@@ -298,6 +321,7 @@ void TddBatch::upload(Layout& L)
         a.out = t.spec.out;
     }
     L.args = args;
+    L.ws = ws;
     const size_t nb = std::max<size_t>(m_beams.size(), 1);
     m_d_args.reserve(nb * sizeof(kern::DedisperseArgs));
     m_d_start.reserve((nb + 1) * sizeof(unsigned long long));
@@ -318,14 +342,18 @@ void TddBatch::enqueue(cudaStream_t s, const Layout& L, bool timing)
     for (size_t b = 0; b < m_beams.size(); ++b) {
         const BeamState& t = m_beams[b];
         if (t.nout == 0) continue;
-        const kern::DedisperseArgs& a = L.args[b];
-        uint32_t* tr = const_cast<uint32_t*>(a.tr);
+        uint32_t* ws = L.ws;
+        uint32_t* tr = ws + L.tr_off[b];
         RT_CHECK(cudaMemsetAsync(tr + m_nchans * L.pitch[b], 0, L.pitch[b] * 4, s));
         const size_t rows = std::min(t.nout + t.tmax, t.spec.nsamps);
         kern::TransposeArgs ta{t.spec.in, t.spec.in_stride, rows, m_nchans, m_nbits, tr, L.pitch[b], 0,
                                L.pitch[b]};
         kern::launch_transpose(ta, s);
         ++launches;
+        if (L.quad) {
+            kern::launch_quad_build(tr, L.pitch[b], ws + L.q_off[b], L.qpitch[b], m_nchans + 1, L.period, s);
+            ++launches;
+        }
     }
     if (timing) m_ev[1]->record(s);
     if (L.persistent) {
@@ -353,6 +381,8 @@ BatchShape TddBatch::autotune(cudaStream_t stream)
     const int nv = m_general_mask ? 1 : kern::tiled_batch_variant_count(m_nbits);
     for (int v = 0; v < nv; ++v)
         for (int cs : {0, 24, 16}) {
+            // quad-strided blocks size their stages themselves
+            if (cs && kern::tiled_variant_quad(m_nbits, v)) continue;
             BatchShape s;
             s.variant = v;
             s.chan_per_stage = cs;

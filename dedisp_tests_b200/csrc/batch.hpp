@@ -96,7 +96,7 @@ private:
     std::unique_ptr<Layout> m_layout;  // uploaded layout for m_shape
     bool m_dirty = true;
 
-    rt::DeviceBuffer m_d_delay, m_d_chan, m_d_kmv, m_d_dms, m_d_perm, m_d_args, m_d_start, m_d_nbx;
+    rt::DeviceBuffer m_d_delay, m_d_chan, m_d_cdl, m_d_kmv, m_d_dms, m_d_perm, m_d_args, m_d_start, m_d_nbx;
     rt::DeviceBuffer m_own_ws;
     void* m_ext_ws = nullptr;
     size_t m_ext_ws_bytes = 0;

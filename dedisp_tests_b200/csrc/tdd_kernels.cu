@@ -597,12 +597,11 @@ __global__ void __launch_bounds__(NW * 32, 1) dedisperse_tiled8_kernel(Dedispers
 // b + gridDim.x, ...; item i belongs to the beam with
 // item_start[beam] <= i < item_start[beam + 1] and is tile
 // (bx, by) = (local % nbx, local / nbx) of that beam. Each beam's arguments
-// are copied to shared memory before its tiles run.
-template <int J, int NW>
-__global__ void __launch_bounds__(NW * 32, 1)
-dedisperse_tiled8_batch_kernel(const DedisperseArgs* __restrict__ args,
-                               const unsigned long long* __restrict__ item_start,
-                               const int* __restrict__ nbx, int nbeams, uint32_t one)
+// are copied to shared memory before its tiles run. TILE runs one tile.
+template <typename TILE>
+__device__ __forceinline__ void batch_items(const DedisperseArgs* __restrict__ args,
+                                            const unsigned long long* __restrict__ item_start,
+                                            const int* __restrict__ nbx, int nbeams, TILE&& tile)
 {
     __shared__ DedisperseArgs s_a;
     __shared__ int s_beam;
@@ -631,9 +630,19 @@ dedisperse_tiled8_batch_kernel(const DedisperseArgs* __restrict__ args,
         __syncthreads();
         const unsigned long long local = item - item_start[beam];
         const int n = nbx[beam];
-        tiled8_tile<J, NW>(s_a, (int)(local % (unsigned long long)n), (size_t)(local / (unsigned long long)n), one);
+        tile(s_a, (int)(local % (unsigned long long)n), (size_t)(local / (unsigned long long)n));
         __syncthreads();  // shared memory is reused by the next item
     }
+}
+
+template <int J, int NW>
+__global__ void __launch_bounds__(NW * 32, 1)
+dedisperse_tiled8_batch_kernel(const DedisperseArgs* __restrict__ args,
+                               const unsigned long long* __restrict__ item_start,
+                               const int* __restrict__ nbx, int nbeams, uint32_t one)
+{
+    batch_items(args, item_start, nbx, nbeams,
+                [&](const DedisperseArgs& a, int bx, size_t by) { tiled8_tile<J, NW>(a, bx, by, one); });
 }
 
 // ---------------------------------------------------------------------------
@@ -702,10 +711,11 @@ constexpr int Q8_MAX_STAGE = 64;
 
 // Dynamic shared memory of a quad-strided launch: the opt-in maximum less the
 // static buffers (span reduction, one word per warp; channels and delays of
-// two stages).
-constexpr size_t quad_dynamic_smem_bytes(int nw)
+// two stages; for the persistent form the beam's argument block).
+constexpr size_t kBatchStaticSmem = 256;
+constexpr size_t quad_dynamic_smem_bytes(int nw, bool batch = false)
 {
-    return 227 * 1024 - 4 * (size_t)nw - 2 * 2 * Q8_MAX_STAGE * 4;
+    return 227 * 1024 - 4 * (size_t)nw - 2 * 2 * Q8_MAX_STAGE * 4 - (batch ? kBatchStaticSmem : 0);
 }
 
 // Shared loads with 32-bit window addresses and immediate offsets. Volatile:
@@ -774,7 +784,9 @@ __device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size
 #pragma unroll
     for (int w = 0; w < NW; ++w) vmax = max(vmax, s_red[w]);
     const int W = (int)((vmax + (uint32_t)P + 3u) & ~3u);
-    const int CS = min(Q8_MAX_STAGE, (a.smem_words / (2 * W + 4 + NW)) & ~3);
+    uint32_t smem_bytes;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(smem_bytes));
+    const int CS = min(Q8_MAX_STAGE, ((int)(smem_bytes / 4) / (2 * W + 4 + NW)) & ~3);
     const int nstages = (npad + CS - 1) / CS;
     const int CSW = CS * W;
     uint32_t* s_win = smem;                                        // [2][CS][W] row windows
@@ -906,6 +918,17 @@ __global__ void __launch_bounds__(NW * 32, 1) dedisperse_quad8_kernel(Dedisperse
     quad8_tile<J, NW>(a, blockIdx.x, blockIdx.y, one);
 }
 
+template <int J, int NW>
+__global__ void __launch_bounds__(NW * 32, 1)
+dedisperse_quad8_batch_kernel(const DedisperseArgs* __restrict__ args,
+                              const unsigned long long* __restrict__ item_start,
+                              const int* __restrict__ nbx, int nbeams, uint32_t one)
+{
+    static_assert(sizeof(DedisperseArgs) + 16 <= kBatchStaticSmem, "static shared memory of the batch form");
+    batch_items(args, item_start, nbx, nbeams,
+                [&](const DedisperseArgs& a, int bx, size_t by) { quad8_tile<J, NW>(a, bx, by, one); });
+}
+
 // cudaFuncSetAttribute is per device context; remember what each device has
 // been given, per kernel.
 template <typename K>
@@ -947,10 +970,8 @@ void launch_quad8_shape(const DedisperseArgs& a, cudaStream_t s)
     if (tiled_smem_bytes(8, a.win_words, 4, a.variant) > smem)
         DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "quad-strided window does not fit shared memory");
     ensure_smem(dedisperse_quad8_kernel<J, NW>, smem, configured);
-    DedisperseArgs b = a;
-    b.smem_words = (int)(smem / 4);
     dim3 grid((a.ndm + NW - 1) / NW, (unsigned)((a.nsamp_out + 128 * J - 1) / (128 * J)));
-    dedisperse_quad8_kernel<J, NW><<<grid, NW * 32, smem, s>>>(b, 1u);
+    dedisperse_quad8_kernel<J, NW><<<grid, NW * 32, smem, s>>>(a, 1u);
     RT_CHECK(cudaGetLastError());
 }
 
@@ -981,6 +1002,32 @@ template <int V>
 void launch_tiled8_batch_variant(const BatchLaunch& b, cudaStream_t s)
 {
     launch_tiled8_batch_shape<T8_SHAPES[V].J, T8_SHAPES[V].NW>(b, s);
+}
+
+template <int J, int NW>
+void launch_quad8_batch_shape(const BatchLaunch& b, cudaStream_t s)
+{
+    static size_t configured[64] = {};
+    auto kfn = dedisperse_quad8_batch_kernel<J, NW>;
+    const size_t smem = quad_dynamic_smem_bytes(NW, true);
+    if (b.smem_bytes > smem)
+        DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "quad-strided window does not fit shared memory");
+    ensure_smem(kfn, smem, configured);
+    int dev = 0, sms = 0, per_sm = 0;
+    RT_CHECK(cudaGetDevice(&dev));
+    RT_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    RT_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, NW * 32, smem));
+    if (per_sm < 1) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "batch kernel does not fit on an SM");
+    const unsigned long long want = (unsigned long long)sms * per_sm;
+    const unsigned grid = (unsigned)std::max<unsigned long long>(1, std::min(want, b.total_items));
+    kfn<<<grid, NW * 32, smem, s>>>(b.args, b.item_start, b.nbx, b.nbeams, 1u);
+    RT_CHECK(cudaGetLastError());
+}
+
+template <int V>
+void launch_quad8_batch_variant(const BatchLaunch& b, cudaStream_t s)
+{
+    launch_quad8_batch_shape<Q8_SHAPES[V].J, Q8_SHAPES[V].NW>(b, s);
 }
 
 template <int NBITS>
@@ -1034,7 +1081,15 @@ void launch_transpose_n(const TransposeArgs& a, cudaStream_t s)
 }  // namespace
 
 int tiled_variant_count(int nbits) { return nbits == 8 ? T8_NSHAPES + Q8_NSHAPES : 1; }
-int tiled_batch_variant_count(int nbits) { return nbits == 8 ? T8_NSHAPES : 1; }
+int tiled_batch_variant_count(int nbits) { return tiled_variant_count(nbits); }
+
+size_t tiled_batch_smem_bytes(int nbits, int win_words, int chan_per_stage, int variant)
+{
+    // quad-strided: every block uses the whole dynamic budget (its stage size
+    // follows its own window)
+    if (tiled_variant_quad(nbits, variant)) return quad_dynamic_smem_bytes(tiled_block_dms(nbits, variant), true);
+    return tiled_smem_bytes(nbits, win_words, chan_per_stage, variant);
+}
 // 8-bit: the quad-strided {J = 5, 32 warps} shape, the fastest measured on
 // the 4096-channel, 3643-DM workload
 int tiled_default_variant(int nbits) { return nbits == 8 ? T8_NSHAPES : 0; }
@@ -1111,10 +1166,11 @@ size_t tiled_max_smem_bytes() { return 227 * 1024; }
 int tiled_stage_channels(int nbits, int win_words, int variant)
 {
     // quad-strided: four channels per inner step
+    // (quad: the budget of the persistent form, the smaller of the two)
     const bool quad = tiled_variant_quad(nbits, variant);
     const int step = quad ? 4 : 2;
     int cs = quad ? Q8_MAX_STAGE : 32;
-    const size_t cap = quad ? quad_dynamic_smem_bytes(tiled_block_dms(nbits, variant)) : tiled_max_smem_bytes();
+    const size_t cap = quad ? quad_dynamic_smem_bytes(tiled_block_dms(nbits, variant), true) : tiled_max_smem_bytes();
     while (cs >= step && tiled_smem_bytes(nbits, win_words, cs, variant) > cap) cs -= step;
     return cs >= step ? cs : 0;
 }
@@ -1162,13 +1218,17 @@ void launch_dedisperse_plain(const DedisperseArgs& a, cudaStream_t s)
 void launch_dedisperse_tiled8_batch(const BatchLaunch& b, int variant, cudaStream_t s)
 {
     if (b.total_items == 0) return;
-    static_assert(T8_NSHAPES == 5, "dispatch below lists every shape");
+    static_assert(T8_NSHAPES == 5 && Q8_NSHAPES == 4, "dispatch below lists every shape");
     switch (variant) {
     case 0: launch_tiled8_batch_variant<0>(b, s); break;
     case 1: launch_tiled8_batch_variant<1>(b, s); break;
     case 2: launch_tiled8_batch_variant<2>(b, s); break;
     case 3: launch_tiled8_batch_variant<3>(b, s); break;
     case 4: launch_tiled8_batch_variant<4>(b, s); break;
+    case 5: launch_quad8_batch_variant<0>(b, s); break;
+    case 6: launch_quad8_batch_variant<1>(b, s); break;
+    case 7: launch_quad8_batch_variant<2>(b, s); break;
+    case 8: launch_quad8_batch_variant<3>(b, s); break;
     default: DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unknown tiled kernel variant");
     }
 }

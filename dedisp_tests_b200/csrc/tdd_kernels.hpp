@@ -54,7 +54,6 @@ struct DedisperseArgs {
     int win_words;              // tiled: staged window per channel (words)
     int chan_per_stage;         // tiled: channels per pipeline stage (even)
     int variant;                // tiled: tile-shape variant (8-bit input)
-    int smem_words;             // quad: dynamic shared memory of the launch (set by the launcher)
 };
 
 // Tile geometry of the tiled kernel for a given input width and tile-shape
@@ -64,7 +63,7 @@ struct DedisperseArgs {
 // channel in byte i (i = 0..3, P = 32 * tiled_lane_words), built from the
 // channel-major packed rows by launch_quad_build.
 int tiled_variant_count(int nbits);
-int tiled_batch_variant_count(int nbits);  // variants of the persistent batch kernel
+int tiled_batch_variant_count(int nbits);  // variants of the persistent batch kernel (all)
 int tiled_default_variant(int nbits);      // the variant a plan uses unless told otherwise
 bool tiled_variant_quad(int nbits, int variant);
 int tiled_block_samples(int nbits, int variant);  // output samples per block
@@ -72,6 +71,8 @@ int tiled_block_dms(int nbits, int variant);      // DMs per block
 int tiled_lane_words(int nbits, int variant);     // J: words per lane
 size_t tiled_smem_bytes(int nbits, int win_words, int chan_per_stage, int variant);
 size_t tiled_max_smem_bytes();
+// Dynamic shared memory of the persistent batch launch for a beam's window.
+size_t tiled_batch_smem_bytes(int nbits, int win_words, int chan_per_stage, int variant);
 // Channels per pipeline stage for a window of win_words (0: does not fit).
 int tiled_stage_channels(int nbits, int win_words, int variant);
 
@@ -87,7 +88,8 @@ void launch_dedisperse_tiled(const DedisperseArgs& a, cudaStream_t s);
 // Persistent 8-bit tiled kernel over many series: args[beam] describes beam
 // `beam` (device array), its tiles are items item_start[beam] ..
 // item_start[beam+1]-1 (nbeams+1 entries, device), nbx[beam] DM blocks per
-// time tile (device). smem_bytes: the largest tiled_smem_bytes of the beams.
+// time tile (device). smem_bytes: the largest tiled_batch_smem_bytes of the
+// beams. Quad-strided variants read quad-strided rows (args[beam].tr).
 struct BatchLaunch {
     const DedisperseArgs* args;
     const unsigned long long* item_start;

@@ -132,7 +132,8 @@ dedisp_size dedisp_b200_batch_workspace_size(dedisp_b200_batch batch);
 dedisp_error dedisp_b200_batch_set_workspace(dedisp_b200_batch batch, void* d_workspace,
                                              dedisp_size bytes);
 /* Tile shape: variant < dedisp_b200_batch_variant_count(in_nbits), channels
- * per stage even and <= 32 (0: the largest that fits shared memory). */
+ * per stage even and <= 32 (0: the largest that fits shared memory; the
+ * quad-strided variants size their stages per block and ignore it). */
 int dedisp_b200_batch_variant_count(dedisp_size in_nbits);
 dedisp_error dedisp_b200_batch_set_shape(dedisp_b200_batch batch, int variant, int chan_per_stage);
 /* Times every candidate shape on the leading 8192 output samples of each

@@ -181,10 +181,10 @@ def test_batch_api_argument_checks():
 
 
 def test_tile_variant_counts():
-    """8-bit input: five shapes on channel-major packed rows (also the
-    persistent batch kernel's shapes) and four on quad-strided rows; every
-    other width has one shape. Out-of-range variants are rejected."""
-    assert dd.tdd_variant_count(8) == 9 and dd.batch_variant_count(8) == 5
+    """8-bit input: five shapes on channel-major packed rows and four on
+    quad-strided rows, in the plans and the persistent batch kernel alike;
+    every other width has one shape. Out-of-range variants are rejected."""
+    assert dd.tdd_variant_count(8) == 9 and dd.batch_variant_count(8) == 9
     for nb in (1, 2, 4, 16, 32):
         assert dd.tdd_variant_count(nb) == 1 and dd.batch_variant_count(nb) == 1
     p = dd.TDDPlan(64, 1e-4, 1500.0, -1.0)
