@@ -604,10 +604,20 @@ def run_ours(args):
     dd.lib().dedisp_b200_alu_probe(local, C.byref(peak))
     k2_ms = sum(kms) / len(kms)
     adds = float(units) * cfg.nchans
+    # DRAM bytes per K2 launch: ncu capture of the same kernel on the 2^17-sample
+    # case (profiles/tdd_quad8_config1_131072samples.md: 38.48 GB read + 1.41 GB
+    # written over 150 time tiles of 640 samples), scaled by the time tiles of
+    # the full launch (every tile streams its own delay band)
+    traffic, traffic_note = None, "no capture for this variant"
+    if args.nbits == 8 and best == 5 and cfg.nchans == 4096 and ndm == 3643:
+        tiles = -(-nout // 640)
+        traffic = round((38.482631e9 + 1.406025e9) / 150 * tiles)
+        traffic_note = f"ncu capture on 2^17 samples (150 tiles) scaled to {tiles} tiles"
     achieved = adds / (k2_ms * 1e-3) / 1e12
     roofline = {"bound": "int-alu", "achieved": round(achieved, 3), "peak": round(peak.value / 1e12, 3),
                 "unit": "Tadd/s", "frac": round(achieved * 1e12 / peak.value, 4),
-                "traffic": None,
+                "traffic": traffic,
+                "traffic_source": traffic_note,
                 "peak_source": "measured in this run: dedisp_b200_alu_probe (32-bit add "
                                "lane-ops/s, all SMs)",
                 "k2_ms": round(k2_ms, 3), "k1_ms": round(sum(pms) / len(pms), 3),
