@@ -60,6 +60,7 @@ TddBatch::TddBatch(size_t nchans, float dt, float f0, float df, int in_nbits, in
     if ((nchans * (size_t)in_nbits) % 32 != 0)
         DD_THROW_MSG(DEDISP_INVALID_STRIDE, "nchans * in_nbits must be a multiple of 32");
     if (nchans > 8192) DD_THROW(DEDISP_NCHANS_EXCEEDS_LIMIT);
+    m_shape.variant = kern::tiled_default_variant(in_nbits);
     m_delays.assign(nchans + 1, 0.f);
     hostmath::delay_table(nchans, dt, f0, df, m_delays.data());
     set_killmask(nullptr);
@@ -228,7 +229,7 @@ TddBatch::Layout TddBatch::make_layout(const BatchShape& shape, size_t tile_limi
         CS[b] = shape.chan_per_stage > 0 ? std::min(shape.chan_per_stage, fit) : fit;
     }
     L.tiled = tiled;
-    L.persistent = tiled && nb == 8;
+    L.persistent = tiled && (nb == 8 || quad);
     L.quad = tiled && quad;
     const size_t ubt = tiled ? bt : 16, ubd = tiled ? bd : 32;
     const float in_range = (float)(nb == 32 ? 0xFFFFFFFFu : ((1u << nb) - 1u));
@@ -351,7 +352,8 @@ void TddBatch::enqueue(cudaStream_t s, const Layout& L, bool timing)
         kern::launch_transpose(ta, s);
         ++launches;
         if (L.quad) {
-            kern::launch_quad_build(tr, L.pitch[b], ws + L.q_off[b], L.qpitch[b], m_nchans + 1, L.period, s);
+            kern::launch_quad_build(m_nbits, tr, L.pitch[b], ws + L.q_off[b], L.qpitch[b], m_nchans + 1, L.period,
+                                    s);
             ++launches;
         }
     }
@@ -359,7 +361,7 @@ void TddBatch::enqueue(cudaStream_t s, const Layout& L, bool timing)
     if (L.persistent) {
         kern::BatchLaunch bl{m_d_args.get<kern::DedisperseArgs>(), m_d_start.get<unsigned long long>(),
                              m_d_nbx.get<int>(), (int)m_beams.size(), L.start.back(), L.smem};
-        kern::launch_dedisperse_tiled8_batch(bl, L.shape.variant, s);
+        kern::launch_dedisperse_tiled_batch(bl, m_nbits, L.shape.variant, s);
         ++launches;
     } else {
         for (size_t b = 0; b < m_beams.size(); ++b) {

@@ -37,7 +37,7 @@ struct BatchBeamSpec {
 };
 
 struct BatchShape {
-    int variant = 0;         // tiled-kernel tile-shape variant (8-bit input)
+    int variant = 0;         // tiled-kernel tile-shape variant (a batch starts at its width's default)
     int chan_per_stage = 0;  // 0: the largest that fits shared memory
 };
 

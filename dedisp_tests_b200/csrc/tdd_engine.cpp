@@ -61,8 +61,11 @@ rt::Event& TddEngine::event(size_t i)
 void TddEngine::prepare(const TddView& v, const TddCall& c)
 {
     Setup& s = *m_setup;
-    // other widths have one shape
-    const int eff_variant = c.in_nbits != 8 ? 0 : variant < 0 ? kern::tiled_default_variant(8) : variant;
+    // variants are numbered per input width; one outside the width's range
+    // (or -1) selects the width's default
+    const int eff_variant = (variant >= 0 && variant < kern::tiled_variant_count(c.in_nbits))
+                                ? variant
+                                : kern::tiled_default_variant(c.in_nbits);
     if (s.version == v.version && s.first == c.first_dm && s.count == c.dm_count &&
         s.nbits == c.in_nbits && s.kernel == kernel && s.variant == eff_variant)
         return;
@@ -305,7 +308,7 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
         }
         // K1q: quad-strided rows of every channel and the zero row
         if (quad) {
-            kern::launch_quad_build(tr, pitch, m_q.get<uint32_t>(), qpitch, v.nchans + 1, s.period, ex);
+            kern::launch_quad_build(nbits, tr, pitch, m_q.get<uint32_t>(), qpitch, v.nchans + 1, s.period, ex);
             ++stats.launches;
         }
         if (t_b && g0 == 0) t_b->record(ex);

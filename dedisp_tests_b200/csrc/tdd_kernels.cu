@@ -660,27 +660,47 @@ dedisperse_tiled8_batch_kernel(const DedisperseArgs* __restrict__ args,
 // ---------------------------------------------------------------------------
 constexpr int QB_THREADS = 256, QB_ITERS = 8;  // K1q: quads per block = 2048
 
-// Quad k of a row: words 4k .. 4k+3 from the packed words k + i*P/4.
-__device__ __forceinline__ uint4 quad_words(const uint32_t* __restrict__ src, size_t tr_pitch, size_t k,
-                                            size_t p4)
+// Four NBITS-bit fields (LSB first) widened to four bytes.
+template <int NBITS>
+__device__ __forceinline__ uint32_t widen4(uint32_t x)
 {
-    // w[i] = samples 4k + i*P .. 4k + i*P + 3; zero past the row
-    uint32_t w[4];
+    if constexpr (NBITS == 8) {
+        return x;
+    } else {
+        constexpr uint32_t M = (1u << NBITS) - 1u;
+        return (x & M) | (((x >> NBITS) & M) << 8) | (((x >> (2 * NBITS)) & M) << 16) |
+               (((x >> (3 * NBITS)) & M) << 24);
+    }
+}
+
+// Quad k of a row: words 4k .. 4k+3, i.e. samples 4k + j + i*P (byte i of
+// word j), from packed NBITS-bit rows. With P and 4k multiples of 4 the four
+// samples 4k + i*P .. 4k + i*P + 3 sit in one packed word.
+template <int NBITS>
+__device__ __forceinline__ uint4 quad_words(const uint32_t* __restrict__ src, size_t tr_pitch, size_t k,
+                                            size_t period)
+{
+    constexpr int SPW = 32 / NBITS;
+    // e[i] = samples 4k + i*P .. 4k + i*P + 3 as bytes; zero past the row
+    uint32_t e[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        const size_t idx = k + (size_t)i * p4;
-        w[i] = idx < tr_pitch ? __ldg(src + idx) : 0u;
+        const size_t t = 4 * k + (size_t)i * period;
+        const size_t idx = t / SPW;
+        const uint32_t w = idx < tr_pitch ? __ldg(src + idx) : 0u;
+        e[i] = widen4<NBITS>(w >> ((t % SPW) * NBITS));
     }
-    // 4x4 byte transpose: output word j = byte j of w[0..3]
-    const uint32_t a_lo = __byte_perm(w[0], w[1], 0x5140), a_hi = __byte_perm(w[0], w[1], 0x7362);
-    const uint32_t b_lo = __byte_perm(w[2], w[3], 0x5140), b_hi = __byte_perm(w[2], w[3], 0x7362);
+    // 4x4 byte transpose: output word j = byte j of e[0..3]
+    const uint32_t a_lo = __byte_perm(e[0], e[1], 0x5140), a_hi = __byte_perm(e[0], e[1], 0x7362);
+    const uint32_t b_lo = __byte_perm(e[2], e[3], 0x5140), b_hi = __byte_perm(e[2], e[3], 0x7362);
     return make_uint4(__byte_perm(a_lo, b_lo, 0x5410), __byte_perm(a_lo, b_lo, 0x7632),
                       __byte_perm(a_hi, b_hi, 0x5410), __byte_perm(a_hi, b_hi, 0x7632));
 }
 
+template <int NBITS>
 __global__ void __launch_bounds__(QB_THREADS) quad_build_kernel(const uint32_t* __restrict__ tr,
                                                                 size_t tr_pitch, uint32_t* __restrict__ q,
-                                                                size_t q_pitch, size_t nrows, size_t p4)
+                                                                size_t q_pitch, size_t nrows, size_t period)
 {
     constexpr size_t PER_BLOCK = (size_t)QB_THREADS * QB_ITERS;
     const size_t nquads = q_pitch / 4;
@@ -692,11 +712,12 @@ __global__ void __launch_bounds__(QB_THREADS) quad_build_kernel(const uint32_t* 
             if (k0 + PER_BLOCK <= nquads) {
                 uint4 v[QB_ITERS];
 #pragma unroll
-                for (int it = 0; it < QB_ITERS; ++it) v[it] = quad_words(src, tr_pitch, k1 + (size_t)it * QB_THREADS, p4);
+                for (int it = 0; it < QB_ITERS; ++it)
+                    v[it] = quad_words<NBITS>(src, tr_pitch, k1 + (size_t)it * QB_THREADS, period);
 #pragma unroll
                 for (int it = 0; it < QB_ITERS; ++it) dst[k1 + (size_t)it * QB_THREADS] = v[it];
             } else {
-                for (size_t k = k1; k < nquads; k += QB_THREADS) dst[k] = quad_words(src, tr_pitch, k, p4);
+                for (size_t k = k1; k < nquads; k += QB_THREADS) dst[k] = quad_words<NBITS>(src, tr_pitch, k, period);
             }
         }
     }
@@ -1034,17 +1055,13 @@ template <int NBITS>
 void launch_tiled_n(const DedisperseArgs& a, cudaStream_t s)
 {
     if constexpr (NBITS == 8) {
-        static_assert(T8_NSHAPES == 5 && Q8_NSHAPES == 4, "dispatch below lists every shape");
+        static_assert(T8_NSHAPES == 5, "dispatch below lists every shape");
         switch (a.variant) {
         case 0: launch_tiled8_variant<0>(a, s); break;
         case 1: launch_tiled8_variant<1>(a, s); break;
         case 2: launch_tiled8_variant<2>(a, s); break;
         case 3: launch_tiled8_variant<3>(a, s); break;
         case 4: launch_tiled8_variant<4>(a, s); break;
-        case 5: launch_quad8_variant<0>(a, s); break;
-        case 6: launch_quad8_variant<1>(a, s); break;
-        case 7: launch_quad8_variant<2>(a, s); break;
-        case 8: launch_quad8_variant<3>(a, s); break;
         default: DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unknown tiled kernel variant");
         }
     } else {
@@ -1080,7 +1097,13 @@ void launch_transpose_n(const TransposeArgs& a, cudaStream_t s)
 
 }  // namespace
 
-int tiled_variant_count(int nbits) { return nbits == 8 ? T8_NSHAPES + Q8_NSHAPES : 1; }
+// Variants per input width: 8-bit 0-4 packed-row shapes (T8_SHAPES), 5-8
+// quad-strided shapes (Q8_SHAPES); 1/2/4-bit 0 the generic packed-row kernel,
+// 1-4 the quad-strided shapes (samples widened to bytes); 16/32-bit 0 only.
+int tiled_variant_count(int nbits)
+{
+    return nbits == 8 ? T8_NSHAPES + Q8_NSHAPES : nbits <= 4 ? 1 + Q8_NSHAPES : 1;
+}
 int tiled_batch_variant_count(int nbits) { return tiled_variant_count(nbits); }
 
 size_t tiled_batch_smem_bytes(int nbits, int win_words, int chan_per_stage, int variant)
@@ -1090,9 +1113,9 @@ size_t tiled_batch_smem_bytes(int nbits, int win_words, int chan_per_stage, int 
     if (tiled_variant_quad(nbits, variant)) return quad_dynamic_smem_bytes(tiled_block_dms(nbits, variant), true);
     return tiled_smem_bytes(nbits, win_words, chan_per_stage, variant);
 }
-// 8-bit: the quad-strided {J = 5, 32 warps} shape, the fastest measured on
-// the 4096-channel, 3643-DM workload
-int tiled_default_variant(int nbits) { return nbits == 8 ? T8_NSHAPES : 0; }
+// Widths up to 8 bits: the quad-strided {J = 5, 32 warps} shape, the fastest
+// measured on the 4096-channel, 3643-DM workload
+int tiled_default_variant(int nbits) { return nbits == 8 ? T8_NSHAPES : nbits <= 4 ? 1 : 0; }
 
 static int checked_variant(int nbits, int variant)
 {
@@ -1101,15 +1124,20 @@ static int checked_variant(int nbits, int variant)
     return variant;
 }
 
-bool tiled_variant_quad(int nbits, int variant)
+// Index into Q8_SHAPES of a quad-strided variant, -1 for the others.
+static int quad_shape(int nbits, int variant)
 {
     checked_variant(nbits, variant);
-    return nbits == 8 && variant >= T8_NSHAPES;
+    if (nbits == 8) return variant >= T8_NSHAPES ? variant - T8_NSHAPES : -1;
+    if (nbits <= 4) return variant >= 1 ? variant - 1 : -1;
+    return -1;
 }
+
+bool tiled_variant_quad(int nbits, int variant) { return quad_shape(nbits, variant) >= 0; }
 
 int tiled_block_samples(int nbits, int variant)
 {
-    checked_variant(nbits, variant);
+    if (quad_shape(nbits, variant) >= 0) return 128 * tiled_lane_words(nbits, variant);
     switch (nbits) {
     case 1: return TiledGeom<1>::BT;
     case 2: return TiledGeom<2>::BT;
@@ -1122,12 +1150,13 @@ int tiled_block_samples(int nbits, int variant)
 
 int tiled_block_dms(int nbits, int variant)
 {
-    checked_variant(nbits, variant);
+    const int q = quad_shape(nbits, variant);
+    if (q >= 0) return Q8_SHAPES[q].NW;
     switch (nbits) {
     case 1: return TiledGeom<1>::BD;
     case 2: return TiledGeom<2>::BD;
     case 4: return TiledGeom<4>::BD;
-    case 8: return variant < T8_NSHAPES ? T8_SHAPES[variant].NW : Q8_SHAPES[variant - T8_NSHAPES].NW;
+    case 8: return T8_SHAPES[variant].NW;
     case 16: return TiledGeom<16>::BD;
     default: return TiledGeom<32>::BD;
     }
@@ -1135,12 +1164,13 @@ int tiled_block_dms(int nbits, int variant)
 
 int tiled_lane_words(int nbits, int variant)
 {
-    checked_variant(nbits, variant);
+    const int q = quad_shape(nbits, variant);
+    if (q >= 0) return Q8_SHAPES[q].J;
     switch (nbits) {
     case 1: return TiledGeom<1>::J;
     case 2: return TiledGeom<2>::J;
     case 4: return TiledGeom<4>::J;
-    case 8: return variant < T8_NSHAPES ? T8_SHAPES[variant].J : Q8_SHAPES[variant - T8_NSHAPES].J;
+    case 8: return T8_SHAPES[variant].J;
     case 16: return TiledGeom<16>::J;
     default: return TiledGeom<32>::J;
     }
@@ -1175,7 +1205,7 @@ int tiled_stage_channels(int nbits, int win_words, int variant)
     return cs >= step ? cs : 0;
 }
 
-void launch_quad_build(const uint32_t* tr, size_t tr_pitch_words, uint32_t* q, size_t q_pitch_words,
+void launch_quad_build(int nbits, const uint32_t* tr, size_t tr_pitch_words, uint32_t* q, size_t q_pitch_words,
                        size_t nrows, int period_words, cudaStream_t s)
 {
     if (q_pitch_words % 4 != 0 || period_words % 4 != 0 || (uintptr_t)q % 16 != 0)
@@ -1184,8 +1214,14 @@ void launch_quad_build(const uint32_t* tr, size_t tr_pitch_words, uint32_t* q, s
     constexpr size_t per_block = (size_t)QB_THREADS * QB_ITERS;
     dim3 grid((unsigned)std::min<size_t>((nquads + per_block - 1) / per_block, 65535),
               (unsigned)std::min<size_t>(nrows, 65535));
-    quad_build_kernel<<<grid, QB_THREADS, 0, s>>>(tr, tr_pitch_words, q, q_pitch_words, nrows,
-                                                  (size_t)period_words / 4);
+    const size_t period = (size_t)period_words;
+    switch (nbits) {
+    case 1: quad_build_kernel<1><<<grid, QB_THREADS, 0, s>>>(tr, tr_pitch_words, q, q_pitch_words, nrows, period); break;
+    case 2: quad_build_kernel<2><<<grid, QB_THREADS, 0, s>>>(tr, tr_pitch_words, q, q_pitch_words, nrows, period); break;
+    case 4: quad_build_kernel<4><<<grid, QB_THREADS, 0, s>>>(tr, tr_pitch_words, q, q_pitch_words, nrows, period); break;
+    case 8: quad_build_kernel<8><<<grid, QB_THREADS, 0, s>>>(tr, tr_pitch_words, q, q_pitch_words, nrows, period); break;
+    default: DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "quad-strided rows hold samples of at most 8 bits");
+    }
     RT_CHECK(cudaGetLastError());
 }
 
@@ -1215,26 +1251,38 @@ void launch_dedisperse_plain(const DedisperseArgs& a, cudaStream_t s)
     }
 }
 
-void launch_dedisperse_tiled8_batch(const BatchLaunch& b, int variant, cudaStream_t s)
+void launch_dedisperse_tiled_batch(const BatchLaunch& b, int nbits, int variant, cudaStream_t s)
 {
     if (b.total_items == 0) return;
     static_assert(T8_NSHAPES == 5 && Q8_NSHAPES == 4, "dispatch below lists every shape");
+    switch (quad_shape(nbits, variant)) {
+    case 0: launch_quad8_batch_variant<0>(b, s); return;
+    case 1: launch_quad8_batch_variant<1>(b, s); return;
+    case 2: launch_quad8_batch_variant<2>(b, s); return;
+    case 3: launch_quad8_batch_variant<3>(b, s); return;
+    default: break;
+    }
+    if (nbits != 8) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "no persistent kernel for this width and variant");
     switch (variant) {
     case 0: launch_tiled8_batch_variant<0>(b, s); break;
     case 1: launch_tiled8_batch_variant<1>(b, s); break;
     case 2: launch_tiled8_batch_variant<2>(b, s); break;
     case 3: launch_tiled8_batch_variant<3>(b, s); break;
     case 4: launch_tiled8_batch_variant<4>(b, s); break;
-    case 5: launch_quad8_batch_variant<0>(b, s); break;
-    case 6: launch_quad8_batch_variant<1>(b, s); break;
-    case 7: launch_quad8_batch_variant<2>(b, s); break;
-    case 8: launch_quad8_batch_variant<3>(b, s); break;
     default: DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unknown tiled kernel variant");
     }
 }
 
 void launch_dedisperse_tiled(const DedisperseArgs& a, cudaStream_t s)
 {
+    // quad-strided rows hold bytes whatever the input width
+    switch (quad_shape(a.nbits, a.variant)) {
+    case 0: launch_quad8_variant<0>(a, s); return;
+    case 1: launch_quad8_variant<1>(a, s); return;
+    case 2: launch_quad8_variant<2>(a, s); return;
+    case 3: launch_quad8_variant<3>(a, s); return;
+    default: break;
+    }
     switch (a.nbits) {
     case 1: launch_tiled_n<1>(a, s); break;
     case 2: launch_tiled_n<2>(a, s); break;

@@ -57,11 +57,11 @@ struct DedisperseArgs {
 };
 
 // Tile geometry of the tiled kernel for a given input width and tile-shape
-// variant (8-bit input has several, see tiled_variant_count; other widths 1).
-// 8-bit variants from tiled_batch_variant_count(8) on run on quad-strided
-// rows (tiled_variant_quad): word n of a row holds samples n + i*P of the
-// channel in byte i (i = 0..3, P = 32 * tiled_lane_words), built from the
-// channel-major packed rows by launch_quad_build.
+// variant (tiled_variant_count per width: 8-bit 9, 1/2/4-bit 5, 16/32-bit 1).
+// Quad-strided variants (tiled_variant_quad: 8-bit 5-8, 1/2/4-bit 1-4) run
+// on quad-strided rows: word n of a row holds samples n + i*P of the channel
+// in byte i (i = 0..3, P = 32 * tiled_lane_words; narrower samples widened
+// to bytes), built from the channel-major packed rows by launch_quad_build.
 int tiled_variant_count(int nbits);
 int tiled_batch_variant_count(int nbits);  // variants of the persistent batch kernel (all)
 int tiled_default_variant(int nbits);      // the variant a plan uses unless told otherwise
@@ -77,15 +77,16 @@ size_t tiled_batch_smem_bytes(int nbits, int win_words, int chan_per_stage, int 
 int tiled_stage_channels(int nbits, int win_words, int variant);
 
 // K1q: quad-strided rows q (q_pitch_words per row, a multiple of 4, rows
-// 16-byte aligned) from channel-major packed 8-bit rows tr, for nrows rows;
-// samples past a tr row read as zero.
-void launch_quad_build(const uint32_t* tr, size_t tr_pitch_words, uint32_t* q, size_t q_pitch_words,
+// 16-byte aligned) from channel-major packed rows tr of 1/2/4/8-bit samples,
+// for nrows rows; samples past a tr row read as zero.
+void launch_quad_build(int nbits, const uint32_t* tr, size_t tr_pitch_words, uint32_t* q, size_t q_pitch_words,
                        size_t nrows, int period_words, cudaStream_t s);
 
 void launch_dedisperse_plain(const DedisperseArgs& a, cudaStream_t s);
 void launch_dedisperse_tiled(const DedisperseArgs& a, cudaStream_t s);
 
-// Persistent 8-bit tiled kernel over many series: args[beam] describes beam
+// Persistent tiled kernel over many series (8-bit packed-row variants and
+// the quad-strided variants of widths up to 8 bits): args[beam] describes beam
 // `beam` (device array), its tiles are items item_start[beam] ..
 // item_start[beam+1]-1 (nbeams+1 entries, device), nbx[beam] DM blocks per
 // time tile (device). smem_bytes: the largest tiled_batch_smem_bytes of the
@@ -98,7 +99,7 @@ struct BatchLaunch {
     unsigned long long total_items;
     size_t smem_bytes;
 };
-void launch_dedisperse_tiled8_batch(const BatchLaunch& b, int variant, cudaStream_t s);
+void launch_dedisperse_tiled_batch(const BatchLaunch& b, int nbits, int variant, cudaStream_t s);
 
 }  // namespace kern
 }  // namespace dedisp

@@ -24,13 +24,15 @@ typedef enum {
 
 dedisp_error dedisp_b200_set_tdd_kernel(dedisp_plan plan, int kernel);
 
-/* Tile shape of the tiled TDD kernel (8-bit input: DMs per block, samples
- * per thread); variant in [0, dedisp_b200_tdd_variant_count(in_nbits)).
- * 8-bit variants from dedisp_b200_batch_variant_count(8) on work on
- * quad-strided rows built per gulp (four times the packed input size in
- * device memory). Every variant computes the same bit-exact sums; they
- * differ in speed. Other input widths have a single shape and ignore the
- * setting. */
+/* Tile shape of the tiled TDD kernel (DMs per block, samples per thread).
+ * Variants are numbered per input width, [0, dedisp_b200_tdd_variant_count(
+ * in_nbits)): 8-bit 0-4 on channel-major packed rows, 5-8 on quad-strided
+ * rows; 1/2/4-bit 0 the packed-row kernel, 1-4 quad-strided rows (samples
+ * widened to bytes); 16/32-bit 0 only. Quad-strided rows are built per gulp
+ * (four bytes per sample and channel in device memory). A variant outside
+ * the executed width's range selects that width's default (quad-strided
+ * 5 words x 32 DMs for widths up to 8 bits). Every variant computes the same
+ * bit-exact sums; they differ in speed. */
 dedisp_error dedisp_b200_set_tdd_variant(dedisp_plan plan, int variant);
 int dedisp_b200_tdd_variant_count(dedisp_size in_nbits);
 

@@ -100,8 +100,9 @@ def test_batch_8bit_matches_plans_graph_and_direct():
         got, t = _run_batch(8, host, graph=graph)
         for g, w in zip(got, want):
             assert np.array_equal(g.view(np.uint32), w.view(np.uint32))
-        # transposes of the beams with output + one persistent launch
-        assert t["launches"] == sum(w.shape[1] > 0 for w in want) + 1
+        # per beam with output K1 + K1q (the default shape is quad-strided),
+        # then one persistent launch
+        assert t["launches"] == 2 * sum(w.shape[1] > 0 for w in want) + 1
 
 
 def test_batch_oracle_one_beam_and_every_shape():
@@ -130,10 +131,16 @@ def test_batch_autotune_keeps_results():
 def test_batch_other_widths(nbits):
     host = _beams(nbits, 14, _specs(6)[:3])
     want = [_plan_out(p, p.shape[0], nbits, d) for p, d in host]
+    # default: quad-strided rows (samples widened to bytes), persistent launch
     got, t = _run_batch(nbits, host)
     for g, w in zip(got, want):
         assert np.array_equal(g.view(np.uint32), w.view(np.uint32))
-    assert t["launches"] == 2 * len(host)  # one dedispersion launch per beam
+    assert t["launches"] == 2 * len(host) + 1  # K1 + K1q per beam, one persistent launch
+    # packed-row kernel: one dedispersion launch per beam
+    got, t = _run_batch(nbits, host, shape=(0, 0))
+    for g, w in zip(got, want):
+        assert np.array_equal(g.view(np.uint32), w.view(np.uint32))
+    assert t["launches"] == 2 * len(host)
 
 
 def test_batch_killmask_zero_one_and_general():

@@ -182,10 +182,13 @@ def test_batch_api_argument_checks():
 
 def test_tile_variant_counts():
     """8-bit input: five shapes on channel-major packed rows and four on
-    quad-strided rows, in the plans and the persistent batch kernel alike;
-    every other width has one shape. Out-of-range variants are rejected."""
+    quad-strided rows; 1/2/4-bit: the packed-row kernel and the four
+    quad-strided shapes; 16/32-bit one shape; the plans and the persistent
+    batch kernel alike. Out-of-range variants are rejected."""
     assert dd.tdd_variant_count(8) == 9 and dd.batch_variant_count(8) == 9
-    for nb in (1, 2, 4, 16, 32):
+    for nb in (1, 2, 4):
+        assert dd.tdd_variant_count(nb) == 5 and dd.batch_variant_count(nb) == 5
+    for nb in (16, 32):
         assert dd.tdd_variant_count(nb) == 1 and dd.batch_variant_count(nb) == 1
     p = dd.TDDPlan(64, 1e-4, 1500.0, -1.0)
     for bad in (-1, 9):

@@ -112,6 +112,34 @@ def test_quad_variants_gulps_unsorted_out_widths(variant):
         assert np.array_equal(out.view(np.uint8), ref.view(np.uint8)), (out_nbits, gulp)
 
 
+@pytest.mark.parametrize("nbits", [1, 2, 4])
+def test_narrow_widths_every_variant(nbits):
+    """1/2/4-bit input through the packed-row kernel (variant 0) and the four
+    quad-strided shapes (samples widened to bytes): random and all-maximum
+    samples over > 256 channels, a killmask, two gulps."""
+    nchans, nsamps = 1056, 9000
+    packed, dms, params = _case(nbits, nchans, nsamps, 70, 500.0, 300 + nbits, df=-0.25)
+    full = sy.pack(np.full((nsamps, nchans), (1 << nbits) - 1, np.uint32), nbits)
+    km = np.ones(nchans, np.int32)
+    km[5::37] = 0
+    assert dd.tdd_variant_count(nbits) == 5
+    for data in (packed, full):
+        ref = None
+        for variant in range(5):
+            p = dd.TDDPlan(*params)
+            p.set_dm_list(dms)
+            p.set_killmask(km)
+            p.set_kernel(2)
+            p.set_tile_variant(variant)
+            p.set_gulp_size(4000)
+            nout = nsamps - p.get_max_delay()
+            out = np.zeros((len(dms), nout), np.float32)
+            p.execute(nsamps, data, nbits, out, 32)
+            if ref is None:
+                ref = _oracle(data, nsamps, nbits, params, dms, km, 32, nout)
+            assert np.array_equal(out.view(np.uint32), ref.view(np.uint32)), (variant, data is full)
+
+
 def test_tiled8_saturated_bytes():
     """All samples 255: every 16-bit lane reaches 256 * 255 before a flush."""
     nchans, nsamps = 1024, 6000
