@@ -96,17 +96,18 @@ struct FftPlan {
 // 4-7, 8-11 and 12-15 (a bijection on [0, M), no padding), so 16 lanes that
 // access a power-of-two stride up to 2^12 elements hit 16 different 8-byte
 // bank pairs (the passes' strides and the digit-reversed final gather).
-__device__ __forceinline__ unsigned pa(unsigned a) { return a ^ (((a >> 4) ^ (a >> 8) ^ (a >> 12)) & 15u); }
+// pa is linear over XOR: pa(x ^ y) = pa(x) ^ pa(y), so the slot of an index
+// made of disjoint bit fields is the XOR of the fields' slots.
+__host__ __device__ constexpr unsigned pa(unsigned a) { return a ^ (((a >> 4) ^ (a >> 8) ^ (a >> 12)) & 15u); }
 __host__ __device__ constexpr unsigned padded_len(unsigned m) { return m; }
 
 // Smem position of frequency k after all DIF passes (mixed-radix digit
 // reversal; each pass's output digit is the next frequency digit).
 template <int LOGM>
-__device__ __forceinline__ unsigned fft_pos(unsigned k)
+__host__ __device__ constexpr unsigned fft_pos(unsigned k)
 {
     using P = FftPlan<LOGM>;
     unsigned pos = 0, rem = LOGM;
-#pragma unroll
     for (int p = 0; p < P::NP; ++p) {
         const int b = P::bits(p);
         const unsigned q = k & ((1u << b) - 1u);
@@ -123,64 +124,74 @@ __device__ __forceinline__ float2 twiddle(const float2* lo, const float2* hi, un
     return inv ? conjf2(w) : w;
 }
 
-// One DIF pass of radix R on sub-transforms of length L (in place).
-template <int R, bool INV>
-__device__ __forceinline__ void fft_pass(float2* s, unsigned M, unsigned L, int log_nl,
-                                         const float2* lo, const float2* hi)
+// One DIF pass of radix R = 2^LOG_R on sub-transforms of length
+// L = R * 2^LOG_SUB (in place) over M points. Element r of group
+// (blk, j) is index blk*L + r*SUB + j: three disjoint bit fields, so its
+// slot is pa(blk*L + j) ^ pa(r*SUB), the second term a constant.
+template <int LOG_R, int LOG_SUB, bool INV>
+__device__ __forceinline__ void fft_pass(float2* s, unsigned M, int log_nl, const float2* lo, const float2* hi)
 {
-    const unsigned sub = L / R;
-    const unsigned groups = M / R;
+    constexpr int R = 1 << LOG_R;
+    constexpr unsigned SUB = 1u << LOG_SUB;
+    const unsigned groups = M >> LOG_R;
     for (unsigned g = threadIdx.x; g < groups; g += blockDim.x) {
-        const unsigned blk = g / sub, j = g - blk * sub;
-        const unsigned base = blk * L + j;
+        const unsigned j = g & (SUB - 1u);
+        const unsigned pb = pa(((g >> LOG_SUB) << (LOG_SUB + LOG_R)) | j);
         float2 v[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = s[pa(base + r * sub)];
+        for (int r = 0; r < R; ++r) v[r] = s[pb ^ pa((unsigned)r << LOG_SUB)];
         dft_reg<R, INV>(v);
-        if (j) {
-            // W_L^{j q} = W_N^{j q N / L} (N = 2M) as powers of one looked-up
-            // W_L^j: squarings for even q, one more factor for odd q (at
-            // most 4 roundings per factor for R <= 16).
-            float2 p[R];
-            p[1] = twiddle(lo, hi, j << log_nl, INV);
+        if constexpr (SUB > 1) {
+            if (j) {
+                // W_L^{j q} = W_N^{j q N / L} (N = 2M) as powers of one looked-up
+                // W_L^j: squarings for even q, one more factor for odd q (at
+                // most 4 roundings per factor for R <= 16).
+                float2 p[R];
+                p[1] = twiddle(lo, hi, j << log_nl, INV);
 #pragma unroll
-            for (int q = 2; q < R; ++q) p[q] = (q & 1) ? cmul(p[q - 1], p[1]) : cmul(p[q / 2], p[q / 2]);
+                for (int q = 2; q < R; ++q) p[q] = (q & 1) ? cmul(p[q - 1], p[1]) : cmul(p[q / 2], p[q / 2]);
 #pragma unroll
-            for (int q = 1; q < R; ++q) v[q] = cmul(v[q], p[q]);
+                for (int q = 1; q < R; ++q) v[q] = cmul(v[q], p[q]);
+            }
         }
 #pragma unroll
-        for (int q = 0; q < R; ++q) s[pa(base + q * sub)] = v[q];
+        for (int q = 0; q < R; ++q) s[pb ^ pa((unsigned)q << LOG_SUB)] = v[q];
+    }
+}
+
+// The DIF passes of FftPlan<LOG> over M points (one transform of 2^LOG, or
+// several concatenated), pass P on, with log_nl = log2(N / L) of pass P.
+template <int LOG, int P, bool INV>
+__device__ __forceinline__ void fft_passes(float2* s, unsigned M, int log_nl, const float2* lo, const float2* hi)
+{
+    using PL = FftPlan<LOG>;
+    if constexpr (P < PL::NP) {
+        constexpr int B = PL::bits(P);
+        constexpr int LOGL = LOG - FFT_RB * P;  // every earlier pass has FFT_RB bits
+        __syncthreads();
+        fft_pass<B, LOGL - B, INV>(s, M, log_nl, lo, hi);
+        fft_passes<LOG, P + 1, INV>(s, M, log_nl + B, lo, hi);
     }
 }
 
 template <int LOGM, bool INV>
 __device__ __forceinline__ void fft_smem(float2* s, const float2* lo, const float2* hi)
 {
-    using P = FftPlan<LOGM>;
-    constexpr unsigned M = 1u << LOGM;
-    unsigned L = M;
-    int log_nl = 1;  // log2(N / L), N = 2M
-#pragma unroll
-    for (int p = 0; p < P::NP; ++p) {
-        const int b = P::bits(p);
-        __syncthreads();
-        if (b == 5) fft_pass<32, INV>(s, M, L, log_nl, lo, hi);
-        else if (b == 4) fft_pass<16, INV>(s, M, L, log_nl, lo, hi);
-        else if (b == 3) fft_pass<8, INV>(s, M, L, log_nl, lo, hi);
-        else if (b == 2) fft_pass<4, INV>(s, M, L, log_nl, lo, hi);
-        else if (b == 1) fft_pass<2, INV>(s, M, L, log_nl, lo, hi);
-        L >>= b;
-        log_nl += b;
-    }
+    fft_passes<LOGM, 0, INV>(s, 1u << LOGM, 1, lo, hi);
     __syncthreads();
 }
 
+// Slots of the transform's element n = t + i*T (t < T = threads, both powers
+// of two, so the fields are disjoint): pa(n) = pa(t) ^ pa(i*T); the final
+// order fft_pos is a permutation of bit fields, so likewise
+// pa(fft_pos(n)) = pa(fft_pos(t)) ^ pa(fft_pos(i*T)).
 template <int LOGM>
 __global__ void __launch_bounds__(FftPlan<LOGM>::threads()) fft_r2c_kernel(
     const float* x, size_t x_pitch, size_t nseg, size_t seg_stride, float2* X, size_t bin_pitch,
     TwiddleTable tw)
 {
     constexpr unsigned M = 1u << LOGM;
+    constexpr unsigned T = FftPlan<LOGM>::threads();
     extern __shared__ __align__(16) float2 s_fft[];
     float2* s = s_fft;
     float2* lo = s + padded_len(M);
@@ -192,36 +203,72 @@ __global__ void __launch_bounds__(FftPlan<LOGM>::threads()) fft_r2c_kernel(
     const size_t row = blockIdx.x;
     const size_t c = row / nseg, seg = row - c * nseg;
     const float* src = x + c * x_pitch + seg * seg_stride;
-    // Batches of loads in flight per thread (the trip count is a compile-time
-    // constant, so each batch is issued before any of its values is used).
-    constexpr unsigned T = FftPlan<LOGM>::threads();
+    const unsigned t = threadIdx.x;
+    // Batches of loads in flight per thread (compile-time trip counts, so each
+    // batch is issued before any of its values is used).
     constexpr unsigned PER = M / T, BATCH = PER < 16 ? (PER ? PER : 1) : 16;
-    for (unsigned i0 = 0; i0 < PER; i0 += BATCH) {
-        float2 v[BATCH];
+    if constexpr (M >= T) {
+        const unsigned pt = pa(t);
+        // rows (segments) that start on an 8-byte boundary load sample pairs
+        // as float2
+        const bool pairs = (reinterpret_cast<uintptr_t>(src) & 7u) == 0;
+        const float2* src2 = reinterpret_cast<const float2*>(src);
 #pragma unroll
-        for (unsigned i = 0; i < BATCH; ++i) {
-            const unsigned n = threadIdx.x + (i0 + i) * T;
-            v[i] = n < M ? make_float2(src[2 * n], src[2 * n + 1]) : make_float2(0.f, 0.f);
-        }
+        for (unsigned i0 = 0; i0 < PER; i0 += BATCH) {
+            float2 v[BATCH];
+            if (pairs) {
 #pragma unroll
-        for (unsigned i = 0; i < BATCH; ++i) {
-            const unsigned n = threadIdx.x + (i0 + i) * T;
-            if (n < M) s[pa(n)] = v[i];
+                for (unsigned i = 0; i < BATCH; ++i) v[i] = src2[t + (i0 + i) * T];
+            } else {
+#pragma unroll
+                for (unsigned i = 0; i < BATCH; ++i) {
+                    const unsigned n = t + (i0 + i) * T;
+                    v[i] = make_float2(src[2 * n], src[2 * n + 1]);
+                }
+            }
+#pragma unroll
+            for (unsigned i = 0; i < BATCH; ++i) s[pt ^ pa((i0 + i) * T)] = v[i];
         }
+    } else {
+        if (t < M) s[pa(t)] = make_float2(src[2 * t], src[2 * t + 1]);
     }
-    for (unsigned n = threadIdx.x + PER * T; n < M; n += T)  // M < T only
-        s[pa(n)] = make_float2(src[2 * n], src[2 * n + 1]);
     fft_smem<LOGM, false>(s, lo, hi);
 
+    // Bins k and M - k from the pair z_k, z_{M-k} (k = 0..M/2): with
+    // e = (z_k + conj z_{M-k}) / 2, o = (z_k - conj z_{M-k}) / (2i), w = W_2M^k,
+    // X[k] = e + w o and X[M-k] = conj(e - w o).
     float2* dst = X + row * bin_pitch;
-    for (unsigned k = threadIdx.x; k <= M; k += blockDim.x) {
-        const float2 zk = s[pa(fft_pos<LOGM>(k & (M - 1)))];
-        const float2 zm = s[pa(fft_pos<LOGM>((M - k) & (M - 1)))];
+    auto pair = [&](unsigned k, float2 zk, float2 zm) {
         const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
         const float2 d = make_float2(zk.x - zm.x, zk.y + zm.y);  // zk - conj(zm)
         const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);   // d / (2i)
-        const float2 w = (k == M) ? make_float2(-1.f, 0.f) : twiddle(lo, hi, k, false);
-        dst[k] = e + cmul(w, o);
+        const float2 wo = cmul(twiddle(lo, hi, k, false), o);
+        dst[k] = e + wo;
+        if (2 * k != M) dst[M - k] = make_float2(e.x - wo.x, wo.y - e.y);
+    };
+    if constexpr (M >= 2 * T) {
+        // k = t + i*T < M/2; M - k = (M-1) ^ (k-1) for k >= 1
+        const unsigned pk = pa(fft_pos<LOGM>(t));
+        const unsigned pm = t ? pa(M - 1u) ^ pa(fft_pos<LOGM>(t - 1)) : 0u;
+#pragma unroll 4
+        for (unsigned i = 0; i < M / (2 * T); ++i) {
+            const unsigned k = t + i * T;
+            const float2 zk = s[pk ^ pa(fft_pos<LOGM>(i * T))];
+            float2 zm;
+            if (t) zm = s[pm ^ pa(fft_pos<LOGM>(i * T))];
+            else zm = s[pa(fft_pos<LOGM>((M - k) & (M - 1u)))];
+            pair(k, zk, zm);
+        }
+        if (t == 0) {
+            const float2 z = s[pa(fft_pos<LOGM>(M / 2))];
+            pair(M / 2, z, z);
+        }
+    } else {
+        for (unsigned k = t; k <= M / 2; k += T) {
+            const float2 zk = s[pa(fft_pos<LOGM>(k & (M - 1u)))];
+            const float2 zm = s[pa(fft_pos<LOGM>((M - k) & (M - 1u)))];
+            pair(k, zk, zm);
+        }
     }
 }
 
@@ -231,6 +278,7 @@ __global__ void __launch_bounds__(FftPlan<LOGM>::threads()) fft_c2r_kernel(
     size_t out_len, TwiddleTable tw)
 {
     constexpr unsigned M = 1u << LOGM;
+    constexpr unsigned T = FftPlan<LOGM>::threads();
     extern __shared__ __align__(16) float2 s_fft[];
     float2* s = s_fft;
     float2* lo = s + padded_len(M);
@@ -243,41 +291,70 @@ __global__ void __launch_bounds__(FftPlan<LOGM>::threads()) fft_c2r_kernel(
     const size_t row = blockIdx.x;
     const size_t dm = row / nseg, seg = row - dm * nseg;
     const float2* src = Y + row * bin_pitch;
-    constexpr unsigned T = FftPlan<LOGM>::threads();
-    constexpr unsigned PER = (M + T - 1) / T, BATCH = PER < 8 ? PER : 8;
-    for (unsigned i0 = 0; i0 < PER; i0 += BATCH) {
-        float2 xk[BATCH], xm[BATCH];
-#pragma unroll
-        for (unsigned i = 0; i < BATCH; ++i) {
-            const unsigned k = threadIdx.x + (i0 + i) * T;
-            xk[i] = k < M ? src[k] : make_float2(0.f, 0.f);
-            xm[i] = k < M ? src[M - k] : make_float2(0.f, 0.f);
+    const unsigned t = threadIdx.x;
+    // z_k = E_k + i O_k and z_{M-k} from the bins a = Y[k], b = Y[M-k]
+    // (k = 0..M/2): e = (a + conj b) / 2, d = (a - conj b) / 2, o = d conj(w),
+    // w = W_2M^k; z_k = e + i o, z_{M-k} = conj(e) + i conj(o). The DC and
+    // Nyquist imaginary parts are ignored (C2R).
+    auto pair = [&](unsigned k, float2 a, float2 b, unsigned slot_k, unsigned slot_m) {
+        if (k == 0) {
+            a.y = 0.f;
+            b.y = 0.f;
         }
+        const float2 e = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
+        const float2 d = make_float2(0.5f * (a.x - b.x), 0.5f * (a.y + b.y));
+        const float2 o = cmul(d, conjf2(twiddle(lo, hi, k, false)));
+        s[slot_k] = make_float2(e.x - o.y, e.y + o.x);
+        if (k != 0 && 2 * k != M) s[slot_m] = make_float2(e.x + o.y, o.x - e.y);
+    };
+    if constexpr (M >= 2 * T) {
+        constexpr unsigned PER = M / (2 * T), BATCH = PER < 8 ? PER : 8;
+        const unsigned pt = pa(t);
+        // slot of M - k = (M-1) ^ (k-1), k >= 1
+        const unsigned pm = t ? pa(M - 1u) ^ pa(t - 1) : 0u;
 #pragma unroll
-        for (unsigned i = 0; i < BATCH; ++i) {
-            const unsigned k = threadIdx.x + (i0 + i) * T;
-            if (k >= M) continue;
-            float2 a = xk[i], b = xm[i];
-            if (k == 0) {  // the DC and Nyquist imaginary parts are ignored (C2R)
-                a.y = 0.f;
-                b.y = 0.f;
+        for (unsigned i0 = 0; i0 < PER; i0 += BATCH) {
+            float2 xa[BATCH], xb[BATCH];
+#pragma unroll
+            for (unsigned i = 0; i < BATCH; ++i) {
+                const unsigned k = t + (i0 + i) * T;
+                xa[i] = src[k];
+                xb[i] = src[M - k];
             }
-            const float2 e = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
-            const float2 d = make_float2(0.5f * (a.x - b.x), 0.5f * (a.y + b.y));
-            const float2 o = cmul(d, conjf2(twiddle(lo, hi, k, false)));
-            s[pa(k)] = make_float2(e.x - o.y, e.y + o.x);  // E + i O
+#pragma unroll
+            for (unsigned i = 0; i < BATCH; ++i) {
+                const unsigned k = t + (i0 + i) * T;
+                const unsigned sk = pt ^ pa((i0 + i) * T);
+                const unsigned sm = t ? pm ^ pa((i0 + i) * T) : pa((M - k) & (M - 1u));
+                pair(k, xa[i], xb[i], sk, sm);
+            }
         }
+        if (t == 0) {
+            const float2 y = src[M / 2];
+            pair(M / 2, y, y, pa(M / 2), pa(M / 2));
+        }
+    } else {
+        for (unsigned k = t; k <= M / 2; k += T) pair(k, src[k], src[M - k], pa(k & (M - 1u)), pa((M - k) & (M - 1u)));
     }
     fft_smem<LOGM, true>(s, lo, hi);
 
     const float scale = 1.0f / (float)M;
-    float* dst = out + dm * out_stride;
     const size_t o0 = seg * keep;
-    for (unsigned n = threadIdx.x; n < M; n += blockDim.x) {
-        const float2 z = s[pa(fft_pos<LOGM>(n))];
-        const size_t i0 = 2 * (size_t)n, i1 = i0 + 1;
-        if (i0 < keep && o0 + i0 < out_len) dst[o0 + i0] = z.x * scale;
-        if (i1 < keep && o0 + i1 < out_len) dst[o0 + i1] = z.y * scale;
+    float* dst = out + dm * out_stride + o0;
+    // samples of this segment that are kept and inside the row (<= 2M)
+    const size_t room = o0 >= out_len ? 0 : out_len - o0;
+    const unsigned lim = (unsigned)(keep < room ? keep : room);
+    auto put = [&](unsigned n, float2 z) {
+        const unsigned i0 = 2 * n;
+        if (i0 < lim) dst[i0] = z.x * scale;
+        if (i0 + 1 < lim) dst[i0 + 1] = z.y * scale;
+    };
+    if constexpr (M >= T) {
+        const unsigned pn = pa(fft_pos<LOGM>(t));
+#pragma unroll 4
+        for (unsigned i = 0; i < M / T; ++i) put(t + i * T, s[pn ^ pa(fft_pos<LOGM>(i * T))]);
+    } else {
+        if (t < M) put(t, s[pa(fft_pos<LOGM>(t))]);
     }
 }
 
@@ -299,21 +376,7 @@ template <int LOG, bool INV>
 __device__ __forceinline__ void fft_smem_multi(float2* s, unsigned nb, int log_nl0, const float2* lo,
                                                const float2* hi)
 {
-    using P = FftPlan<LOG>;
-    const unsigned M = nb << LOG;
-    unsigned L = 1u << LOG;
-    int log_nl = log_nl0;  // log2(N / L) for the twiddle table's N
-#pragma unroll
-    for (int p = 0; p < P::NP; ++p) {
-        const int b = P::bits(p);
-        __syncthreads();
-        if (b == 4) fft_pass<16, INV>(s, M, L, log_nl, lo, hi);
-        else if (b == 3) fft_pass<8, INV>(s, M, L, log_nl, lo, hi);
-        else if (b == 2) fft_pass<4, INV>(s, M, L, log_nl, lo, hi);
-        else if (b == 1) fft_pass<2, INV>(s, M, L, log_nl, lo, hi);
-        L >>= b;
-        log_nl += b;
-    }
+    fft_passes<LOG, 0, INV>(s, nb << LOG, log_nl0, lo, hi);
     __syncthreads();
 }
 
@@ -500,7 +563,7 @@ void launch_c2r_4step(float2* Y, size_t bin_pitch, size_t rows, size_t nseg, flo
 __global__ void __launch_bounds__(256) fdd_unpack_kernel(const uint8_t* in, size_t in_stride,
                                                          int in_nbits, size_t nsamps, size_t nchans,
                                                          float scale, float mid, float* x,
-                                                         size_t x_pitch, size_t x_len)
+                                                         size_t x_pitch, size_t x_len, int aligned)
 {
     __shared__ float tile[32][33];
     const size_t t0 = (size_t)blockIdx.x * 32, c0 = (size_t)blockIdx.y * 32;
@@ -513,12 +576,18 @@ __global__ void __launch_bounds__(256) fdd_unpack_kernel(const uint8_t* in, size
                 v = ((float)in[t * in_stride + c] - 127.5f) * scale;
             } else if (in_nbits == 32) {
                 const uint8_t* p = in + t * in_stride + 4 * c;
-                uint32_t u = (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) |
-                             ((uint32_t)p[3] << 24);
+                uint32_t u;
+                if (aligned) {
+                    u = __ldg(reinterpret_cast<const uint32_t*>(p));
+                } else {
+                    u = (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
+                }
                 v = __uint_as_float(u) * scale;
             } else if (in_nbits == 16) {
                 const uint8_t* p = in + t * in_stride + 2 * c;
-                v = ((float)((uint32_t)p[0] | ((uint32_t)p[1] << 8)) - mid) * scale;
+                const uint32_t u = aligned ? (uint32_t)__ldg(reinterpret_cast<const uint16_t*>(p))
+                                           : (uint32_t)p[0] | ((uint32_t)p[1] << 8);
+                v = ((float)u - mid) * scale;
             } else {
                 // 1/2/4-bit samples packed LSB-first within each byte
                 const size_t bit = c * (size_t)in_nbits;
@@ -761,8 +830,11 @@ void launch_fdd_unpack(const uint8_t* in, size_t in_stride, int in_nbits, size_t
     // (127.5 for 8-bit, as the reference's unpack_kernel.cuh:60)
     const float mid = in_nbits == 32 ? 0.f : (float)((1u << in_nbits) - 1u) * 0.5f;
     dim3 grid((unsigned)((x_len + 31) / 32), (unsigned)((nchans + 31) / 32));
+    // whole-sample loads when every sample starts on its own size
+    const size_t sb = in_nbits >= 16 ? (size_t)in_nbits / 8 : 1;
+    const int aligned = ((uintptr_t)in % sb == 0) && (in_stride % sb == 0);
     fdd_unpack_kernel<<<grid, 256, 0, s>>>(in, in_stride, in_nbits, nsamps, nchans, scale, mid, x,
-                                           x_pitch, x_len);
+                                           x_pitch, x_len, aligned);
     RT_CHECK(cudaGetLastError());
 }
 
