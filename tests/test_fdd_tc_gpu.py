@@ -105,3 +105,25 @@ def test_tc_negative_dms_use_quarter_wave_phasors():
     ref = po.fdd_spectrum(x, _delays(params), np.ones(nchans, np.int32), dms, out.shape[1])
     rel, mx = _errs(out, ref)
     assert rel < TC_REL_L2 and mx < TC_MAX_ABS, (rel, mx)
+
+
+@pytest.mark.parametrize("nsamps", [72000, 102000])
+def test_tc_many_segments(nsamps):
+    """2048-point segments: 36 segments (80 accumulator columns) and 51
+    segments (112 columns, close to the 128-column limit); killmask,
+    rounded delays."""
+    nchans = 64
+    inp, params = _input(nchans, nsamps, 11)
+    dms = np.linspace(0, 20, 37, dtype=np.float32)
+    km = np.ones(nchans, np.int32)
+    km[9::13] = 0
+    p = _plan(params, dms, km=km, segmented=1, precision=1, round_delays=True, segment_nfft=2048)
+    md = p.get_max_delay()
+    nout = nsamps - md
+    nseg = -(-nsamps // (2048 - md))  # segments of the reference rule (FDDGPUPlan.cpp:762-777)
+    assert (2 * nseg <= 80) == (nsamps == 72000)
+    out = _run(p, nsamps, inp, 8, len(dms))
+    x = _oracle_x(inp, nsamps, params, 8)
+    ref = po.fdd_timeseries(x, _delays(params), km, dms, nout, round_delays=True)
+    rel, mx = _errs(out[:, :nout], ref)
+    assert rel < TC_REL_L2 and mx < TC_MAX_ABS, (nseg, rel, mx)
