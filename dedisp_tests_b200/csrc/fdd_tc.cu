@@ -380,8 +380,8 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
             if (ok) {
                 for (int ch = 0; ch < nchunks; ++ch, ++g) {
                     const uint32_t buf = g & 1u;
-                    if (!mbar_wait_warp(&bars->a_empty[buf], ((g >> 1) & 1u) ^ 1u)) { ok = false; break; }
-                    tc_fence_after();
+                    // the phasors first: their gathers overlap the MMAs still
+                    // reading this A buffer
                     uint32_t hi[TC_PART_CH], lo[TC_PART_CH];
                     const int c0 = ch * TC_CHUNK + part * TC_PART_CH;
                     if (ptab) {
@@ -404,6 +404,8 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
                             lo[i] = __byte_perm(t.y, 0u, sy.x) ^ sy.y;
                         }
                     }
+                    if (!mbar_wait_warp(&bars->a_empty[buf], ((g >> 1) & 1u) ^ 1u)) { ok = false; break; }
+                    tc_fence_after();
                     const uint32_t acol = buf ? TM_A1 : TM_A0;
                     tmem_st16(tmem + lane_addr + acol + part * TC_PART_CH, hi);
                     tmem_st16(tmem + lane_addr + acol + 64 + part * TC_PART_CH, lo);
