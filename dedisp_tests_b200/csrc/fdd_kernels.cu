@@ -181,6 +181,15 @@ __device__ __forceinline__ void fft_smem(float2* s, const float2* lo, const floa
     __syncthreads();
 }
 
+// L2 prefetch of the bytes [p, p + n) (the 16-byte aligned part; a hint,
+// no shared memory, completes on its own).
+__device__ __forceinline__ void prefetch_l2(const void* p, size_t n)
+{
+    const uintptr_t a = ((uintptr_t)p + 15u) & ~(uintptr_t)15u;
+    const uintptr_t e = ((uintptr_t)p + n) & ~(uintptr_t)15u;
+    if (e > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((uint32_t)(e - a)) : "memory");
+}
+
 // Slots of the transform's element n = t + i*T (t < T = threads, both powers
 // of two, so the fields are disjoint): pa(n) = pa(t) ^ pa(i*T); the final
 // order fft_pos is a permutation of bit fields, so likewise
@@ -188,10 +197,16 @@ __device__ __forceinline__ void fft_smem(float2* s, const float2* lo, const floa
 template <int LOGM>
 __global__ void __launch_bounds__(FftPlan<LOGM>::threads()) fft_r2c_kernel(
     const float* x, size_t x_pitch, size_t nseg, size_t seg_stride, float2* X, size_t bin_pitch,
-    TwiddleTable tw)
+    TwiddleTable tw, size_t ahead)
 {
     constexpr unsigned M = 1u << LOGM;
     constexpr unsigned T = FftPlan<LOGM>::threads();
+    // the row that the CTA one wave later on this SM transforms: into L2 now,
+    // so that its load phase finds it there
+    if (threadIdx.x == 0 && ahead && blockIdx.x + ahead < gridDim.x) {
+        const size_t r = blockIdx.x + ahead, c = r / nseg;
+        prefetch_l2(x + c * x_pitch + (r - c * nseg) * seg_stride, (size_t)2 * M * sizeof(float));
+    }
     extern __shared__ __align__(16) float2 s_fft[];
     float2* s = s_fft;
     float2* lo = s + padded_len(M);
@@ -275,10 +290,13 @@ __global__ void __launch_bounds__(FftPlan<LOGM>::threads()) fft_r2c_kernel(
 template <int LOGM>
 __global__ void __launch_bounds__(FftPlan<LOGM>::threads()) fft_c2r_kernel(
     const float2* Y, size_t bin_pitch, size_t nseg, float* out, size_t out_stride, size_t keep,
-    size_t out_len, TwiddleTable tw)
+    size_t out_len, TwiddleTable tw, size_t ahead)
 {
     constexpr unsigned M = 1u << LOGM;
     constexpr unsigned T = FftPlan<LOGM>::threads();
+    // the row that the CTA one wave later on this SM transforms (see r2c)
+    if (threadIdx.x == 0 && ahead && blockIdx.x + ahead < gridDim.x)
+        prefetch_l2(Y + (blockIdx.x + ahead) * bin_pitch, (size_t)(M + 1) * sizeof(float2));
     extern __shared__ __align__(16) float2 s_fft[];
     float2* s = s_fft;
     float2* lo = s + padded_len(M);
@@ -784,6 +802,15 @@ __global__ void __launch_bounds__(MAC_THREADS) mac_plain_kernel(MacArgs a, int b
     }
 }
 
+// CTAs in one wave of a one-CTA-per-SM FFT launch (the L2 prefetch distance).
+size_t resident_ctas()
+{
+    int dev = 0, sms = 0;
+    RT_CHECK(cudaGetDevice(&dev));
+    RT_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    return (size_t)std::max(sms, 1);
+}
+
 template <int LOGM>
 void launch_r2c_n(const float* x, size_t x_pitch, size_t nchans, size_t nseg, size_t seg_stride,
                   float2* X, size_t bin_pitch, const TwiddleTable& tw, cudaStream_t s)
@@ -793,8 +820,8 @@ void launch_r2c_n(const float* x, size_t x_pitch, size_t nchans, size_t nseg, si
     RT_CHECK(cudaFuncSetAttribute(fft_r2c_kernel<LOGM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem));
     const unsigned threads = FftPlan<LOGM>::threads();
-    fft_r2c_kernel<LOGM><<<(unsigned)(nchans * nseg), threads, smem, s>>>(x, x_pitch, nseg,
-                                                                        seg_stride, X, bin_pitch, tw);
+    fft_r2c_kernel<LOGM><<<(unsigned)(nchans * nseg), threads, smem, s>>>(x, x_pitch, nseg, seg_stride, X,
+                                                                        bin_pitch, tw, resident_ctas());
     RT_CHECK(cudaGetLastError());
 }
 
@@ -808,8 +835,8 @@ void launch_c2r_n(const float2* Y, size_t bin_pitch, size_t ndm, size_t nseg, fl
     RT_CHECK(cudaFuncSetAttribute(fft_c2r_kernel<LOGM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem));
     const unsigned threads = FftPlan<LOGM>::threads();
-    fft_c2r_kernel<LOGM><<<(unsigned)(ndm * nseg), threads, smem, s>>>(Y, bin_pitch, nseg, out,
-                                                                      out_stride, keep, out_len, tw);
+    fft_c2r_kernel<LOGM><<<(unsigned)(ndm * nseg), threads, smem, s>>>(Y, bin_pitch, nseg, out, out_stride,
+                                                                      keep, out_len, tw, resident_ctas());
     RT_CHECK(cudaGetLastError());
 }
 
