@@ -11,7 +11,8 @@ so no flush is needed between steps.
   value  device-resident input and output (DEDISP_DEVICE_POINTERS), timed
          with CUDA events on the plan's stream: K1 transpose + K2 kernels.
   e2e    the C-ABI call dedisp_execute with pinned HOST buffers (H2D of the
-         input and D2H of the 30 GB output inside the timed region).
+         input and D2H of the 30 GB output inside the timed region), in gulps
+         of --e2e-gulp output samples (set through dedisp_set_gulp_size).
 
 N > 1 GPUs (torchrun): each rank runs its own replica of the workload (no
 collective on the data path); value = all ranks' units / max-over-ranks time.
@@ -52,6 +53,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nbits", type=int, default=8, choices=[2, 4, 8])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-gulp", type=int, default=1 << 18,
+                    help="gulp size (dedisp_set_gulp_size) of the e2e call: with several gulps the "
+                         "host copies of neighbouring gulps overlap each gulp's kernels")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fdd", action="store_true")
@@ -689,6 +693,7 @@ def run_ours(args):
                 hp = dd.TDDPlan(cfg.nchans, cfg.dt, cfg.f_top, cfg.df, local)
                 hp.generate_dm_list(*cfg.dm_gen)
                 hp.set_tile_variant(best)
+                hp.set_gulp_size(args.e2e_gulp)
                 hp.execute(cfg.nsamps, h_in, args.nbits, h_out, 32)  # warm-up
                 torch.cuda.synchronize()
                 barrier()
@@ -701,7 +706,7 @@ def run_ours(args):
                 e2e = {"value": units * world / dt_e2e, "unit": UNIT,
                        "h2d_bytes_per_step": int(h_in.numel()),
                        "d2h_bytes_per_step": int(ndm * nout * 4), "ms_per_step": dt_e2e * 1e3,
-                       "steps": ksteps}
+                       "steps": ksteps, "gulp": args.e2e_gulp}
                 del h_in, h_out, hp
         except Exception as ex:  # report, do not hide
             e2e = {"value": None, "unit": UNIT, "error": repr(ex)}

@@ -12,7 +12,6 @@ namespace dedisp {
 namespace detail {
 
 namespace {
-constexpr size_t kStageBytes = (size_t)256 << 20;  // per H2D staging buffer
 constexpr int kMaxOutGroups = 8;                   // DM groups for D2H overlap
 
 size_t round_up(size_t a, size_t b) { return (a + b - 1) / b * b; }
@@ -200,7 +199,10 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
     const size_t bt = s.tiled ? (size_t)kern::tiled_block_samples(nbits, s.variant) : 16;
     const size_t win = s.tiled ? (size_t)s.win_words : 0;
 
-    // Gulp size: the user cap, the grid limit, then device memory.
+    // Gulp size: the user cap, the grid limit, then device memory. With more
+    // than one gulp the input rows and the output rows of a gulp have two
+    // buffers each, so that gulp g+1's host-to-device copy and gulp g-1's
+    // device-to-host copy run while gulp g is dedispersed.
     size_t G = std::min(nsamp_out, gulp_size ? gulp_size : kDefaultGulp);
     G = std::min(G, (size_t)65535 * bt);
     auto pitch_for = [&](size_t g) {
@@ -210,31 +212,30 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
     // (tiles - 1) * bt + tmax + P + 2 of a row
     const bool quad = s.tiled && s.quad;
     auto qpitch_for = [&](size_t g) { return round_up(round_up(g, bt) + s.tmax + s.period + 4, 32); };
+    auto nbuf_for = [&](size_t g) -> size_t { return nsamp_out > g ? 2 : 1; };
+    auto in_bytes_for = [&](size_t g) { return round_up(g + s.tmax, 128) * row_bytes; };
     auto bytes_for = [&](size_t g) {
         size_t b = (v.nchans + 1) * pitch_for(g) * 4;
         if (quad) b += (v.nchans + 1) * qpitch_for(g) * 4;
-        if (!dev_out) b += ndm * g * ob;
-        if (!dev_in) b += 2 * std::min(kStageBytes, round_up(g + s.tmax, 128) * row_bytes);
+        if (!dev_out) b += nbuf_for(g) * ndm * g * ob;
+        if (!dev_in) b += nbuf_for(g) * in_bytes_for(g);
         return b;
     };
     size_t free_b = 0, total_b = 0;
     RT_CHECK(cudaMemGetInfo(&free_b, &total_b));
-    const size_t avail = free_b + m_tr.capacity() + m_q.capacity() + m_out.capacity() +
+    const size_t avail = free_b + m_tr.capacity() + m_q.capacity() + m_out[0].capacity() + m_out[1].capacity() +
                          m_stage[0].capacity() + m_stage[1].capacity();
     while (G > bt && bytes_for(G) > avail / 100 * 90) G = round_up(G / 2, bt);
     if (bytes_for(G) > avail) DD_THROW(DEDISP_MEM_ALLOC_FAILED);
 
+    const size_t nbuf = nbuf_for(G);
     const size_t pitch = pitch_for(G);
     m_tr.reserve((v.nchans + 1) * pitch * 4);
     const size_t qpitch = quad ? qpitch_for(G) : 0;
     if (quad) m_q.reserve((v.nchans + 1) * qpitch * 4);
-    if (!dev_out) m_out.reserve(ndm * G * ob);
-    size_t chunk_rows = 0;
-    if (!dev_in) {
-        chunk_rows = std::max<size_t>(128, kStageBytes / std::max<size_t>(row_bytes, 1) / 128 * 128);
-        chunk_rows = std::min(chunk_rows, round_up(G + s.tmax, 128));
-        m_stage[0].reserve(chunk_rows * row_bytes);
-        m_stage[1].reserve(chunk_rows * row_bytes);
+    for (size_t b = 0; b < nbuf; ++b) {
+        if (!dev_out) m_out[b].reserve(ndm * G * ob);
+        if (!dev_in) m_stage[b].reserve(in_bytes_for(G));
     }
 
     cudaStream_t ex = m_gpu.stream();
@@ -259,14 +260,13 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
     }
 
     size_t ev = 0;
-    rt::Event& ev_stage_free0 = event(ev++);
-    rt::Event& ev_stage_free1 = event(ev++);
-    rt::Event* ev_free[2] = {&ev_stage_free0, &ev_stage_free1};
-    rt::Event& ev_out_free = event(ev++);
-    bool out_free_pending = false;
-    bool stage_used[2] = {false, false};
+    rt::Event* ev_in_free[2] = {&event(ev++), &event(ev++)};   // K1 has read input buffer b
+    rt::Event* ev_out_free[2] = {&event(ev++), &event(ev++)};  // D2H has read output buffer b
+    bool in_used[2] = {false, false}, out_used[2] = {false, false};
 
-    for (size_t g0 = 0; g0 < nsamp_out; g0 += G) {
+    size_t gi = 0;
+    for (size_t g0 = 0; g0 < nsamp_out; g0 += G, ++gi) {
+        const size_t b = gi % nbuf;
         const size_t gc = std::min(G, nsamp_out - g0);
         const size_t rows_need = gc + s.tmax;
         const size_t rows_avail = std::min(rows_need, c.nsamps - g0);
@@ -276,35 +276,25 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
         RT_CHECK(cudaMemsetAsync(tr + v.nchans * pitch, 0, pitch * 4, ex));
 
         // K1: input rows -> channel-major packed, zero past the data.
-        if (dev_in) {
-            kern::TransposeArgs ta{c.in + g0 * c.in_stride, c.in_stride, rows_avail, v.nchans, nbits,
-                                   tr, pitch, 0, pitch};
-            kern::launch_transpose(ta, ex);
-            ++stats.launches;
-        } else {
-            const size_t nchunks = std::max<size_t>(1, (rows_avail + chunk_rows - 1) / chunk_rows);
-            for (size_t k = 0; k < nchunks; ++k) {
-                const size_t r = k * chunk_rows;
-                const size_t nr = rows_avail > r ? std::min(chunk_rows, rows_avail - r) : 0;
-                const int b = (int)(k & 1);
-                rt::Event& ready = event(ev++);
-                if (nr) {
-                    if (stage_used[b]) RT_CHECK(cudaStreamWaitEvent(h2d, *ev_free[b], 0));
-                    RT_CHECK(cudaMemcpy2DAsync(m_stage[b].get(), row_bytes,
-                                               c.in + (g0 + r) * c.in_stride, c.in_stride,
-                                               row_bytes, nr, cudaMemcpyHostToDevice, h2d));
-                    ready.record(h2d);
-                    RT_CHECK(cudaStreamWaitEvent(ex, ready, 0));
-                }
-                const size_t w0 = r / spw;
-                const size_t nw = (k + 1 == nchunks) ? pitch - w0 : chunk_rows / spw;
-                kern::TransposeArgs ta{m_stage[b].get<uint8_t>(), row_bytes, nr, v.nchans, nbits,
-                                       tr, pitch, w0, nw};
-                kern::launch_transpose(ta, ex);
-                ++stats.launches;
-                ev_free[b]->record(ex);
-                stage_used[b] = true;
-            }
+        const uint8_t* rows = c.in + g0 * c.in_stride;
+        size_t rows_pitch = c.in_stride;
+        if (!dev_in) {
+            // the whole gulp's rows into input buffer b, on the copy stream
+            if (in_used[b]) RT_CHECK(cudaStreamWaitEvent(h2d, *ev_in_free[b], 0));
+            RT_CHECK(cudaMemcpy2DAsync(m_stage[b].get(), row_bytes, rows, c.in_stride, row_bytes, rows_avail,
+                                       cudaMemcpyHostToDevice, h2d));
+            rt::Event& ready = event(ev++);
+            ready.record(h2d);
+            RT_CHECK(cudaStreamWaitEvent(ex, ready, 0));
+            rows = m_stage[b].get<uint8_t>();
+            rows_pitch = row_bytes;
+        }
+        kern::TransposeArgs ta{rows, rows_pitch, rows_avail, v.nchans, nbits, tr, pitch, 0, pitch};
+        kern::launch_transpose(ta, ex);
+        ++stats.launches;
+        if (!dev_in) {
+            ev_in_free[b]->record(ex);
+            in_used[b] = true;
         }
         // K1q: quad-strided rows of every channel and the zero row
         if (quad) {
@@ -314,12 +304,12 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
         if (t_b && g0 == 0) t_b->record(ex);
 
         // K2 per DM group.
-        if (out_free_pending) RT_CHECK(cudaStreamWaitEvent(ex, ev_out_free, 0));
+        if (!dev_out && out_used[b]) RT_CHECK(cudaStreamWaitEvent(ex, *ev_out_free[b], 0));
         const size_t out_elems_stride = dev_out ? c.out_stride / ob : gc;
-        uint8_t* out_base = dev_out ? c.out + g0 * ob : m_out.get<uint8_t>();
+        uint8_t* out_base = dev_out ? c.out + g0 * ob : m_out[b].get<uint8_t>();
         std::vector<std::pair<size_t, size_t>> groups;
-        for (size_t gi = 0; gi < ngroups; ++gi) {
-            const size_t t0 = ntile * gi / ngroups, t1 = ntile * (gi + 1) / ngroups;
+        for (size_t gr = 0; gr < ngroups; ++gr) {
+            const size_t t0 = ntile * gr / ngroups, t1 = ntile * (gr + 1) / ngroups;
             const size_t s0 = t0 * bd, s1 = std::min(ndm, t1 * bd);
             if (s0 >= s1) continue;
             groups.emplace_back(s0, s1);
@@ -360,18 +350,18 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
 
         // D2H per group into the caller's rows (column offset g0).
         if (!dev_out) {
-            for (size_t gi = 0; gi < groups.size(); ++gi) {
-                const size_t s0 = groups[gi].first, s1 = groups[gi].second;
+            for (size_t gr = 0; gr < groups.size(); ++gr) {
+                const size_t s0 = groups[gr].first, s1 = groups[gr].second;
                 const size_t r0 = s.identity ? s0 : 0, nrow = s.identity ? s1 - s0 : ndm;
-                RT_CHECK(cudaStreamWaitEvent(d2h, event(ev + gi), 0));
-                if (!s.identity && gi + 1 < groups.size()) continue;
+                RT_CHECK(cudaStreamWaitEvent(d2h, event(ev + gr), 0));
+                if (!s.identity && gr + 1 < groups.size()) continue;
                 RT_CHECK(cudaMemcpy2DAsync(c.out + r0 * c.out_stride + g0 * ob, c.out_stride,
-                                           m_out.get<uint8_t>() + r0 * gc * ob, gc * ob, gc * ob,
+                                           m_out[b].get<uint8_t>() + r0 * gc * ob, gc * ob, gc * ob,
                                            nrow, cudaMemcpyDeviceToHost, d2h));
             }
             ev += groups.size();
-            ev_out_free.record(d2h);
-            out_free_pending = true;
+            ev_out_free[b]->record(d2h);
+            out_used[b] = true;
         }
     }
 

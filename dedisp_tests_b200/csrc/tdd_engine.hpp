@@ -2,10 +2,11 @@
 //
 // One call = validate-free execution of a (sub-)range of the DM list over a
 // time series, in gulps of output samples:
-//   host rows --(H2D, pinned or pageable, chunked)--> staging --K1--> channel-
-//   major packed HBM buffer [--K1q--> quad-strided rows, 8-bit quad variants]
+//   host rows --(H2D, pinned or pageable)--> gulp input buffer --K1--> channel-
+//   major packed HBM buffer [--K1q--> quad-strided rows, quad variants]
 //   --K2 (per DM group)--> output --(D2H per DM group, overlapped with later
-//   groups)--> host rows.
+//   groups)--> host rows. With several gulps, input and output buffers are
+//   doubled so that the copies of neighbouring gulps overlap a gulp's kernels.
 // With DEDISP_DEVICE_POINTERS the copies disappear and K1/K2 read/write the
 // caller's buffers. Derived per-plan state (active channels, sorted DMs,
 // window sizes) is cached until the DM list or killmask changes.
@@ -74,7 +75,7 @@ private:
 
     GpuState& m_gpu;
     std::unique_ptr<Setup> m_setup;
-    rt::DeviceBuffer m_chan, m_cdl, m_km, m_dms, m_perm, m_tr, m_q, m_out, m_stage[2];
+    rt::DeviceBuffer m_chan, m_cdl, m_km, m_dms, m_perm, m_tr, m_q, m_out[2], m_stage[2];
     std::vector<std::unique_ptr<rt::Event>> m_events;
     rt::Event& event(size_t i);
 };
