@@ -203,7 +203,8 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
     // than one gulp the input rows and the output rows of a gulp have two
     // buffers each, so that gulp g+1's host-to-device copy and gulp g-1's
     // device-to-host copy run while gulp g is dedispersed.
-    size_t G = std::min(nsamp_out, gulp_size ? gulp_size : kDefaultGulp);
+    const size_t gulp_default = dev_in && dev_out ? kDefaultGulp : kHostDefaultGulp;
+    size_t G = std::min(nsamp_out, gulp_set && gulp_size ? gulp_size : gulp_default);
     G = std::min(G, (size_t)65535 * bt);
     auto pitch_for = [&](size_t g) {
         return round_up((round_up(g, bt) + s.tmax + spw - 1) / spw + win + 8, 32);

@@ -56,7 +56,11 @@ struct TddStats {
 
 class TddEngine {
 public:
+    // Gulp (output samples per pass) unless set: device-resident calls take
+    // the largest; calls with host buffers take smaller gulps so that the
+    // host copies of neighbouring gulps overlap the kernels.
     static constexpr size_t kDefaultGulp = (size_t)1 << 21;
+    static constexpr size_t kHostDefaultGulp = (size_t)1 << 18;
 
     explicit TddEngine(GpuState& gpu);
     ~TddEngine();
@@ -64,6 +68,7 @@ public:
     void execute(const TddView& v, const TddCall& c);
 
     size_t gulp_size = kDefaultGulp;
+    bool gulp_set = false;  // gulp_size was set by the caller
     TddKernel kernel = TddKernel::Auto;
     int variant = -1;  // tile-shape variant of the tiled kernel (8-bit input; -1: default)
     bool record_timing = false;

@@ -58,7 +58,11 @@ TDDPlan::TDDPlan(size_type nchans, float_type dt, float_type f0, float_type df, 
 
 TDDPlan::~TDDPlan() {}
 
-void TDDPlan::set_gulp_size(size_type gulp_size) { m_engine->gulp_size = gulp_size; }
+void TDDPlan::set_gulp_size(size_type gulp_size)
+{
+    m_engine->gulp_size = gulp_size;
+    m_engine->gulp_set = true;
+}
 dedisp_size TDDPlan::get_gulp_size() const { return m_engine->gulp_size; }
 void TDDPlan::set_kernel(TddKernel k) { m_engine->kernel = k; }
 void TDDPlan::set_tile_variant(int variant) { m_engine->variant = variant; }
@@ -128,7 +132,11 @@ DedispPlan::DedispPlan(size_type nchans, float_type dt, float_type f0, float_typ
 
 DedispPlan::~DedispPlan() {}
 
-void DedispPlan::set_gulp_size(size_type gulp_size) { m_engine->gulp_size = gulp_size; }
+void DedispPlan::set_gulp_size(size_type gulp_size)
+{
+    m_engine->gulp_size = gulp_size;
+    m_engine->gulp_set = true;
+}
 DedispPlan::size_type DedispPlan::get_gulp_size() const { return m_engine->gulp_size; }
 void DedispPlan::set_kernel(TddKernel k) { m_engine->kernel = k; }
 void DedispPlan::set_tile_variant(int variant) { m_engine->variant = variant; }
