@@ -45,6 +45,13 @@ def workload_name(nbits):
     return f"tdd 4096ch 2^21 samples {nbits}-bit, 3643 DMs (0-2000, 40us, tol 1.25), f32 out"
 
 
+def workload_config(nbits, nsamps, ndm, md, world):
+    """The `config` object of both arms' JSON lines."""
+    return {"workload": workload_name(nbits), "nchans": 4096, "nsamps": nsamps, "ndm": ndm,
+            "max_delay": md, "in_nbits": nbits, "out_nbits": 32,
+            "l2": "inputs (8.6 GB) larger than L2; no flush", "parallelism": f"replicas x{world}"}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -744,11 +751,7 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": f"u{args.nbits}->u32 sums->f32", "data": "synthetic (seeded, on device)",
-            "config": {"workload": workload_name(args.nbits), "nchans": 4096,
-                       "nsamps": cfg.nsamps, "ndm": ndm, "max_delay": md,
-                       "in_nbits": args.nbits, "out_nbits": 32,
-                       "l2": "inputs (8.6 GB) larger than L2; no flush",
-                       "parallelism": f"replicas x{world}"},
+            "config": workload_config(args.nbits, cfg.nsamps, ndm, md, world),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches * world, "clocks": clocks, "variants": variants,
             "tile_variant": {"chosen": best, "step_ms_by_variant": tune},
@@ -772,11 +775,12 @@ def run_reference(args):
                             np.float32(cfg.df))
     md = po.max_delay(dms, delays)
     cpu, t = time_cpu_oracle(cfg, dms, md, steps=args.steps, warmup=min(args.warmup, 1))
-    line = {"metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": 0,
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+    line = {"metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": f"u{args.nbits}->u32 sums->f32", "data": "synthetic (seeded)",
-            "config": {"workload": workload_name(args.nbits), "sample": cpu["sample"]},
+            "config": workload_config(args.nbits, cfg.nsamps, len(dms), md, world),
             "impl": "reference", "cpu_baseline": cpu,
             "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
