@@ -458,6 +458,8 @@ void TddBatch::execute(cudaStream_t stream, bool use_graph)
     }
     if (record_timing) {
         RT_CHECK(cudaEventSynchronize(m_ev[2]->get()));
+        if (m_layout->quad && kern::tdd_take_error(stream))
+            DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "a staged window copy did not complete");
         if (use_graph) last_k1_ms = -1.f;  // transposes are inside the graph
         else RT_CHECK(cudaEventElapsedTime(&last_k1_ms, m_ev[0]->get(), m_ev[1]->get()));
         RT_CHECK(cudaEventElapsedTime(&last_k2_ms, m_ev[1]->get(), m_ev[2]->get()));

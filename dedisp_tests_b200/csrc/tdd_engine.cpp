@@ -370,6 +370,8 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
     if (!async) {
         RT_CHECK(cudaStreamSynchronize(ex));
         if (!dev_out) RT_CHECK(cudaStreamSynchronize(d2h));
+        if (quad && kern::tdd_take_error(ex))
+            DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "a staged window copy did not complete");
     }
     if (record_timing) {
         RT_CHECK(cudaEventSynchronize(*t_c));

@@ -204,6 +204,62 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem)
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+
+// Set by a kernel whose bounded wait expired (device-wide; read and cleared
+// by tdd_take_error).
+__device__ unsigned g_tdd_error;
+
+// mbarrier + bulk asynchronous copy (global -> shared, no multicast).
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_inval(uint64_t* b)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(b)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes)
+{
+    asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(b)) : "memory");
+}
+// `bytes` (a multiple of 16) from global `src` to shared `dst` (both 16-byte
+// aligned); completion counted on mbarrier b.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* b)
+{
+    asm volatile("cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(b))
+                 : "memory");
+}
+// Wait for phase `parity` of b; false after about 2 s of global time.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, uint32_t parity)
+{
+    const uint32_t addr = smem_addr(b);
+    uint64_t t0 = 0;
+    for (uint32_t i = 0; i < (1u << 28); ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((i & 15u) == 15u) {
+            uint64_t t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            if (t0 == 0) t0 = t;
+            else if (t - t0 > 2000000000ull) return false;
+        }
+    }
+    return false;
+}
 __device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
 
 // Narrow-lane accumulation of two channels' aligned words v1, v2 for word k.
@@ -736,7 +792,8 @@ constexpr int Q8_MAX_STAGE = 64;
 constexpr size_t kBatchStaticSmem = 256;
 constexpr size_t quad_dynamic_smem_bytes(int nw, bool batch = false)
 {
-    return 227 * 1024 - 4 * (size_t)nw - 2 * 2 * Q8_MAX_STAGE * 4 - (batch ? kBatchStaticSmem : 0);
+    // (64 bytes for the two stage mbarriers and alignment)
+    return 227 * 1024 - 4 * (size_t)nw - 2 * 2 * Q8_MAX_STAGE * 4 - 64 - (batch ? kBatchStaticSmem : 0);
 }
 
 // Shared loads with 32-bit window addresses and immediate offsets. Volatile:
@@ -777,6 +834,7 @@ __device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size
     __shared__ uint32_t s_red[NW];
     __shared__ int32_t s_cl[2][Q8_MAX_STAGE];  // channel of each row, stages fetched ahead
     __shared__ float s_cdl[2][Q8_MAX_STAGE];   // its delay
+    __shared__ uint64_t s_full[2];             // window copies of stage buffer b landed
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int i0 = bx * NW;
@@ -791,6 +849,12 @@ __device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size
     // largest (hi - lo4) over the channels, plus the P words of a lane set,
     // rounded to 16 bytes. Then as many channels per stage (a multiple of 4,
     // at most Q8_MAX_STAGE) as the launch's shared memory holds.
+    // one arrival per warp and stage buffer phase (after its copies are counted)
+    if (threadIdx.x == 0) {
+        mbar_init(&s_full[0], NW);
+        mbar_init(&s_full[1], NW);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     uint32_t vmax = 0;
     for (int j = threadIdx.x; j < npad; j += NT) {
         const float dl = a.chan_delay[j];
@@ -833,7 +897,10 @@ __device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size
             cp_async4(&s_cdl[stage & 1][j], a.chan_delay + g + j);
         }
     };
+    // Lane 0 of each warp copies the warp's rows with one bulk copy each
+    // (bytes counted on s_full[buf] before the copy), then arrives.
     auto prep = [&](int stage, int buf) {
+        if (lane != 0) return;
         const int cs = stage_size(stage);
         for (int j = warp; j < cs; j += NW) {
             const int c = s_cl[stage & 1][j];
@@ -843,12 +910,12 @@ __device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size
             const int need = min(W, (int)((hi - lo4 + (uint32_t)P + 3u) & ~3u));
             const uint32_t* src = a.tr + (size_t)c * a.tr_pitch_words + t0 + lo4;
             uint32_t* dst = s_win + buf * CSW + j * W;
-            for (int k = lane * 4; k < need; k += 128) cp_async16(dst + k, src + k);
-            if (lane == 0) {
-                s_lo[buf * CS + j] = lo4;
-                s_dl[buf * CS + j] = dl;
-            }
+            mbar_expect_tx(&s_full[buf], 4u * (uint32_t)need);
+            bulk_g2s(dst, src, 4u * (uint32_t)need, &s_full[buf]);
+            s_lo[buf * CS + j] = lo4;
+            s_dl[buf * CS + j] = dl;
         }
+        mbar_arrive(&s_full[buf]);
     };
 
     uint32_t acc[4 * J];
@@ -887,13 +954,22 @@ __device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size
     asm volatile("cp.async.wait_group 0;\n" ::);
     __syncthreads();
     if (nstages > 0) prep(0, 0);
-    cp_async_commit();
     int since_flush = 0;  // channels accumulated since the last flush
+    bool failed = false;
     for (int s = 0; s < nstages; ++s) {
         const int buf = s & 1;
         const int cs = stage_size(s);
         asm volatile("cp.async.wait_group 0;\n" ::);
-        __syncthreads();  // stage s landed; every warp is done with stage s - 1
+        const bool landed = mbar_wait_bounded(&s_full[buf], ((uint32_t)s >> 1) & 1u);
+        // stage s landed; every warp is done with stage s - 1
+        if (__syncthreads_or(!landed)) {
+            // a copy did not complete: wait (bounded) for this stage's copies,
+            // the only ones in flight, record the error and leave
+            mbar_wait_bounded(&s_full[buf], ((uint32_t)s >> 1) & 1u);
+            if (threadIdx.x == 0) atomicExch(&g_tdd_error, 1u);
+            failed = true;
+            break;
+        }
         if (s + 1 < nstages) prep(s + 1, buf ^ 1);
         if (s + 2 < nstages) fetch(s + 2);  // s_cl/s_cdl[s & 1]: prep(s) finished before the barrier
         cp_async_commit();
@@ -919,7 +995,7 @@ __device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size
     }
     flush();
 
-    if (warp < nvalid) {
+    if (!failed && warp < nvalid) {
         const int row = a.perm ? a.perm[i0 + warp] : i0 + warp;
         const size_t base = (size_t)row * a.out_stride;
 #pragma unroll
@@ -930,6 +1006,12 @@ __device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size
                 if (t < a.nsamp_out) store_out(a.out, base + t, a.out_nbits, acc[4 * k + i], a.den, a.factor);
             }
         }
+    }
+    // the barriers are initialised afresh by the next tile of a persistent block
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_inval(&s_full[0]);
+        mbar_inval(&s_full[1]);
     }
 }
 
@@ -1100,6 +1182,19 @@ void launch_transpose_n(const TransposeArgs& a, cudaStream_t s)
 // Variants per input width: 8-bit 0-4 packed-row shapes (T8_SHAPES), 5-8
 // quad-strided shapes (Q8_SHAPES); 1/2/4-bit 0 the generic packed-row kernel,
 // 1-4 the quad-strided shapes (samples widened to bytes); 16/32-bit 0 only.
+bool tdd_take_error(cudaStream_t s)
+{
+    unsigned v = 0;
+    RT_CHECK(cudaMemcpyFromSymbolAsync(&v, g_tdd_error, sizeof(v), 0, cudaMemcpyDeviceToHost, s));
+    RT_CHECK(cudaStreamSynchronize(s));
+    if (v) {
+        static const unsigned zero = 0;
+        RT_CHECK(cudaMemcpyToSymbolAsync(g_tdd_error, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, s));
+        RT_CHECK(cudaStreamSynchronize(s));
+    }
+    return v != 0;
+}
+
 int tiled_variant_count(int nbits)
 {
     return nbits == 8 ? T8_NSHAPES + Q8_NSHAPES : nbits <= 4 ? 1 + Q8_NSHAPES : 1;
@@ -1113,9 +1208,9 @@ size_t tiled_batch_smem_bytes(int nbits, int win_words, int chan_per_stage, int 
     if (tiled_variant_quad(nbits, variant)) return quad_dynamic_smem_bytes(tiled_block_dms(nbits, variant), true);
     return tiled_smem_bytes(nbits, win_words, chan_per_stage, variant);
 }
-// Widths up to 8 bits: the quad-strided {J = 5, 32 warps} shape, the fastest
+// Widths up to 8 bits: the quad-strided {J = 8, 16 warps} shape, the fastest
 // measured on the 4096-channel, 3643-DM workload
-int tiled_default_variant(int nbits) { return nbits == 8 ? T8_NSHAPES : nbits <= 4 ? 1 : 0; }
+int tiled_default_variant(int nbits) { return nbits == 8 ? T8_NSHAPES + 3 : nbits <= 4 ? 1 + 3 : 0; }
 
 static int checked_variant(int nbits, int variant)
 {

@@ -82,6 +82,10 @@ int tiled_stage_channels(int nbits, int win_words, int variant);
 void launch_quad_build(int nbits, const uint32_t* tr, size_t tr_pitch_words, uint32_t* q, size_t q_pitch_words,
                        size_t nrows, int period_words, cudaStream_t s);
 
+// True if a quad-strided kernel gave up a bounded wait on its staged copies
+// since the last call (device-wide flag, cleared; synchronises s).
+bool tdd_take_error(cudaStream_t s);
+
 void launch_dedisperse_plain(const DedisperseArgs& a, cudaStream_t s);
 void launch_dedisperse_tiled(const DedisperseArgs& a, cudaStream_t s);
 
