@@ -616,15 +616,14 @@ def run_ours(args):
     k2_ms = sum(kms) / len(kms)
     adds = float(units) * cfg.nchans
     # DRAM bytes per K2 launch: ncu capture of the same kernel on the 2^17-sample
-    # case (profiles/tdd_quad8_config1_131072samples.md: 38.48 GB read + 1.41 GB
-    # written over 150 time tiles of 640 samples), scaled by the time tiles of
-    # the full launch (every tile streams its own delay band)
+    # case (profiles/tdd_quad8_config1_131072samples.md, column v5: 24.99 GB read
+    # + 1.40 GB written over 94 time tiles of 1024 samples), scaled by the time
+    # tiles of the full launch (every tile streams its own delay band)
     traffic, traffic_note = None, "no capture for this variant"
-    if args.nbits == 8 and best == 5 and cfg.nchans == 4096 and ndm == 3643:
-        tiles = -(-nout // 640)
-        traffic = round((38.482631e9 + 1.406025e9) / 150 * tiles)
-        traffic_note = f"ncu capture on 2^17 samples (150 tiles) scaled to {tiles} tiles"
-    achieved = adds / (k2_ms * 1e-3) / 1e12
+    if args.nbits == 8 and best == 8 and cfg.nchans == 4096 and ndm == 3643:
+        tiles = -(-nout // 1024)
+        traffic = round((24.988264e9 + 1.402789e9) / 94 * tiles)
+        traffic_note = f"ncu capture on 2^17 samples (94 tiles) scaled to {tiles} tiles"
     roofline = {"bound": "int-alu", "achieved": round(achieved, 3), "peak": round(peak.value / 1e12, 3),
                 "unit": "Tadd/s", "frac": round(achieved * 1e12 / peak.value, 4),
                 "traffic": traffic,
