@@ -624,6 +624,7 @@ def run_ours(args):
         tiles = -(-nout // 1024)
         traffic = round((24.988264e9 + 1.402789e9) / 94 * tiles)
         traffic_note = f"ncu capture on 2^17 samples (94 tiles) scaled to {tiles} tiles"
+    achieved = adds / (k2_ms * 1e-3) / 1e12
     roofline = {"bound": "int-alu", "achieved": round(achieved, 3), "peak": round(peak.value / 1e12, 3),
                 "unit": "Tadd/s", "frac": round(achieved * 1e12 / peak.value, 4),
                 "traffic": traffic,
