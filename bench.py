@@ -615,15 +615,19 @@ def run_ours(args):
     dd.lib().dedisp_b200_alu_probe(local, C.byref(peak))
     k2_ms = sum(kms) / len(kms)
     adds = float(units) * cfg.nchans
-    # DRAM bytes per K2 launch: ncu capture of the same kernel on the 2^17-sample
-    # case (profiles/tdd_quad8_config1_131072samples.md, column v5: 24.99 GB read
-    # + 1.40 GB written over 94 time tiles of 1024 samples), scaled by the time
-    # tiles of the full launch (every tile streams its own delay band)
+    # DRAM bytes per K2 launch: ncu captures of each quad-strided shape on the
+    # 2^17-sample case (dram__bytes_read.sum + dram__bytes_write.sum, one launch;
+    # profiles/tdd_quad8_config1_131072samples.md), scaled by the time tiles of
+    # the full launch (every tile streams its own delay band).
+    # variant: (bytes in the capture, time tiles in the capture, samples per tile)
+    captured = {5: (37970253312 + 1405260288, 150, 640), 6: (20052602880 + 1398569472, 75, 1280),
+                7: (16756359168 + 1400263424, 63, 1536), 8: (24902200832 + 1401539584, 94, 1024)}
     traffic, traffic_note = None, "no capture for this variant"
-    if args.nbits == 8 and best == 8 and cfg.nchans == 4096 and ndm == 3643:
-        tiles = -(-nout // 1024)
-        traffic = round((24.988264e9 + 1.402789e9) / 94 * tiles)
-        traffic_note = f"ncu capture on 2^17 samples (94 tiles) scaled to {tiles} tiles"
+    if args.nbits == 8 and best in captured and cfg.nchans == 4096 and ndm == 3643:
+        b, tiles_cap, bt = captured[best]
+        tiles = -(-nout // bt)
+        traffic = round(b / tiles_cap * tiles)
+        traffic_note = f"ncu capture on 2^17 samples ({tiles_cap} tiles) scaled to {tiles} tiles"
     achieved = adds / (k2_ms * 1e-3) / 1e12
     roofline = {"bound": "int-alu", "achieved": round(achieved, 3), "peak": round(peak.value / 1e12, 3),
                 "unit": "Tadd/s", "frac": round(achieved * 1e12 / peak.value, 4),
