@@ -619,9 +619,12 @@ def run_ours(args):
     # 2^17-sample case (dram__bytes_read.sum + dram__bytes_write.sum, one launch;
     # profiles/tdd_quad8_config1_131072samples.md), scaled by the time tiles of
     # the full launch (every tile streams its own delay band).
-    # variant: (bytes in the capture, time tiles in the capture, samples per tile)
-    captured = {5: (37970253312 + 1405260288, 150, 640), 6: (20052602880 + 1398569472, 75, 1280),
-                7: (16756359168 + 1400263424, 63, 1536), 8: (24902200832 + 1401539584, 94, 1024)}
+    # variant ({J, NW} of the library's quad shapes): (bytes in the capture,
+    # time tiles in the capture, samples per tile = 128 J)
+    captured = {5: (14941203968 + 1397706752, 54, 1792),   # {14, 12}
+                6: (20095108352 + 1398192896, 75, 1280),   # {10, 16}
+                7: (16810921728 + 1402316288, 63, 1536),   # {12, 12}
+                8: (24968875264 + 1401745152, 94, 1024)}   # {8, 16}
     traffic, traffic_note = None, "no capture for this variant"
     if args.nbits == 8 and best in captured and cfg.nchans == 4096 and ndm == 3643:
         b, tiles_cap, bt = captured[best]
