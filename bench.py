@@ -621,10 +621,10 @@ def run_ours(args):
     # the full launch (every tile streams its own delay band).
     # variant ({J, NW} of the library's quad shapes): (bytes in the capture,
     # time tiles in the capture, samples per tile = 128 J)
-    captured = {5: (14941203968 + 1397706752, 54, 1792),   # {14, 12}
-                6: (20095108352 + 1398192896, 75, 1280),   # {10, 16}
-                7: (16810921728 + 1402316288, 63, 1536),   # {12, 12}
-                8: (24968875264 + 1401745152, 94, 1024)}   # {8, 16}
+    captured = {5: (10798106368 + 1397426944, 38, 2560),   # {20, 12}
+                6: (9808037376 + 1385468928, 34, 2816),    # {22, 12}
+                7: (11724679936 + 1397582848, 42, 2304),   # {18, 12}
+                8: (12990360064 + 1396900352, 47, 2048)}   # {16, 12}
     traffic, traffic_note = None, "no capture for this variant"
     if args.nbits == 8 and best in captured and cfg.nchans == 4096 and ndm == 3643:
         b, tiles_cap, bt = captured[best]

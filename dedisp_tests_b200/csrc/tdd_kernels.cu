@@ -782,7 +782,7 @@ __global__ void __launch_bounds__(QB_THREADS) quad_build_kernel(const uint32_t* 
 // Tile shapes of the quad-strided kernel: J words per lane (P = 32J), NW warps
 // = NW DMs per block (one DM per warp).
 struct Q8Shape { int J, NW; };
-constexpr Q8Shape Q8_SHAPES[] = {{14, 12}, {10, 16}, {12, 12}, {8, 16}};
+constexpr Q8Shape Q8_SHAPES[] = {{20, 12}, {22, 12}, {18, 12}, {16, 12}};
 constexpr int Q8_NSHAPES = sizeof(Q8_SHAPES) / sizeof(Q8_SHAPES[0]);
 constexpr int Q8_MAX_STAGE = 64;
 
@@ -1208,7 +1208,7 @@ size_t tiled_batch_smem_bytes(int nbits, int win_words, int chan_per_stage, int 
     if (tiled_variant_quad(nbits, variant)) return quad_dynamic_smem_bytes(tiled_block_dms(nbits, variant), true);
     return tiled_smem_bytes(nbits, win_words, chan_per_stage, variant);
 }
-// Widths up to 8 bits: the quad-strided {J = 14, 12 warps} shape, the
+// Widths up to 8 bits: the quad-strided {J = 20, 12 warps} shape, the
 // fastest measured on the 4096-channel, 3643-DM workload
 int tiled_default_variant(int nbits) { return nbits == 8 ? T8_NSHAPES : nbits <= 4 ? 1 : 0; }
 

@@ -31,7 +31,7 @@ dedisp_error dedisp_b200_set_tdd_kernel(dedisp_plan plan, int kernel);
  * widened to bytes); 16/32-bit 0 only. Quad-strided rows are built per gulp
  * (four bytes per sample and channel in device memory). A variant outside
  * the executed width's range selects that width's default (quad-strided
- * 14 words x 12 DMs for widths up to 8 bits). Every variant computes the same
+ * 20 words x 12 DMs for widths up to 8 bits). Every variant computes the same
  * bit-exact sums; they differ in speed. */
 dedisp_error dedisp_b200_set_tdd_variant(dedisp_plan plan, int variant);
 int dedisp_b200_tdd_variant_count(dedisp_size in_nbits);
