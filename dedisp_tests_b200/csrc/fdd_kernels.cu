@@ -194,19 +194,21 @@ __device__ __forceinline__ void prefetch_l2(const void* p, size_t n)
 // of two, so the fields are disjoint): pa(n) = pa(t) ^ pa(i*T); the final
 // order fft_pos is a permutation of bit fields, so likewise
 // pa(fft_pos(n)) = pa(fft_pos(t)) ^ pa(fft_pos(i*T)).
+//
+// Both single-CTA transforms are persistent: CTA b takes rows b, b + G,
+// b + 2G, ... (G = gridDim.x, at most one wave). A 2^14-point transform fills
+// the shared memory of an SM, so its load, transform and store phases cannot
+// overlap with another CTA's; instead each CTA loads its next row into
+// registers while it stores the current one, and asks L2 for the row after
+// that, so that the loads of the next row find it there.
 template <int LOGM>
 __global__ void __launch_bounds__(FftPlan<LOGM>::threads()) fft_r2c_kernel(
     const float* x, size_t x_pitch, size_t nseg, size_t seg_stride, float2* X, size_t bin_pitch,
-    TwiddleTable tw, size_t ahead)
+    TwiddleTable tw, size_t rows)
 {
     constexpr unsigned M = 1u << LOGM;
     constexpr unsigned T = FftPlan<LOGM>::threads();
-    // the row that the CTA one wave later on this SM transforms: into L2 now,
-    // so that its load phase finds it there
-    if (threadIdx.x == 0 && ahead && blockIdx.x + ahead < gridDim.x) {
-        const size_t r = blockIdx.x + ahead, c = r / nseg;
-        prefetch_l2(x + c * x_pitch + (r - c * nseg) * seg_stride, (size_t)2 * M * sizeof(float));
-    }
+    constexpr unsigned PER = M >= T ? M / T : 1;  // sample pairs per thread
     extern __shared__ __align__(16) float2 s_fft[];
     float2* s = s_fft;
     float2* lo = s + padded_len(M);
@@ -215,74 +217,84 @@ __global__ void __launch_bounds__(FftPlan<LOGM>::threads()) fft_r2c_kernel(
     for (unsigned i = threadIdx.x; i < 256; i += blockDim.x) lo[i] = tw.lo[i];
     for (unsigned i = threadIdx.x; i < nhi; i += blockDim.x) hi[i] = tw.hi[i];
 
-    const size_t row = blockIdx.x;
-    const size_t c = row / nseg, seg = row - c * nseg;
-    const float* src = x + c * x_pitch + seg * seg_stride;
     const unsigned t = threadIdx.x;
-    // Batches of loads in flight per thread (compile-time trip counts, so each
-    // batch is issued before any of its values is used).
-    constexpr unsigned PER = M / T, BATCH = PER < 16 ? (PER ? PER : 1) : 16;
-    if constexpr (M >= T) {
-        const unsigned pt = pa(t);
-        // rows (segments) that start on an 8-byte boundary load sample pairs
-        // as float2
-        const bool pairs = (reinterpret_cast<uintptr_t>(src) & 7u) == 0;
-        const float2* src2 = reinterpret_cast<const float2*>(src);
-#pragma unroll
-        for (unsigned i0 = 0; i0 < PER; i0 += BATCH) {
-            float2 v[BATCH];
-            if (pairs) {
-#pragma unroll
-                for (unsigned i = 0; i < BATCH; ++i) v[i] = src2[t + (i0 + i) * T];
-            } else {
-#pragma unroll
-                for (unsigned i = 0; i < BATCH; ++i) {
-                    const unsigned n = t + (i0 + i) * T;
-                    v[i] = make_float2(src[2 * n], src[2 * n + 1]);
-                }
-            }
-#pragma unroll
-            for (unsigned i = 0; i < BATCH; ++i) s[pt ^ pa((i0 + i) * T)] = v[i];
-        }
-    } else {
-        if (t < M) s[pa(t)] = make_float2(src[2 * t], src[2 * t + 1]);
-    }
-    fft_smem<LOGM, false>(s, lo, hi);
-
-    // Bins k and M - k from the pair z_k, z_{M-k} (k = 0..M/2): with
-    // e = (z_k + conj z_{M-k}) / 2, o = (z_k - conj z_{M-k}) / (2i), w = W_2M^k,
-    // X[k] = e + w o and X[M-k] = conj(e - w o).
-    float2* dst = X + row * bin_pitch;
-    auto pair = [&](unsigned k, float2 zk, float2 zm) {
-        const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
-        const float2 d = make_float2(zk.x - zm.x, zk.y + zm.y);  // zk - conj(zm)
-        const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);   // d / (2i)
-        const float2 wo = cmul(twiddle(lo, hi, k, false), o);
-        dst[k] = e + wo;
-        if (2 * k != M) dst[M - k] = make_float2(e.x - wo.x, wo.y - e.y);
+    auto row_src = [&](size_t row) {
+        const size_t c = row / nseg;
+        return x + c * x_pitch + (row - c * nseg) * seg_stride;
     };
-    if constexpr (M >= 2 * T) {
-        // k = t + i*T < M/2; M - k = (M-1) ^ (k-1) for k >= 1
-        const unsigned pk = pa(fft_pos<LOGM>(t));
-        const unsigned pm = t ? pa(M - 1u) ^ pa(fft_pos<LOGM>(t - 1)) : 0u;
+    // pairs n = t + i*T of the row (segments that start on an 8-byte boundary
+    // load them as float2): pairs i < PF are loaded during the previous row's
+    // output phase, the rest when the row starts (register budget)
+    constexpr unsigned PF = PER > 16 ? PER / 2 : PER;
+    float2 v[PER];
+    auto fetch = [&](size_t row, bool ahead) {
+        const float* src = row_src(row);
+        if ((reinterpret_cast<uintptr_t>(src) & 7u) == 0) {
+            const float2* src2 = reinterpret_cast<const float2*>(src);
+#pragma unroll
+            for (unsigned i = 0; i < PER; ++i)
+                if ((i < PF) == ahead && (M >= T || t < M)) v[i] = src2[t + i * T];
+        } else {
+#pragma unroll
+            for (unsigned i = 0; i < PER; ++i) {
+                const unsigned n = t + i * T;
+                if ((i < PF) == ahead && (M >= T || t < M)) v[i] = make_float2(src[2 * n], src[2 * n + 1]);
+            }
+        }
+    };
+    const size_t G = gridDim.x;
+    size_t row = blockIdx.x;
+    if (row < rows) fetch(row, true);
+    if (t == 0 && row + G < rows) prefetch_l2(row_src(row + G), (size_t)2 * M * sizeof(float));
+    for (; row < rows; row += G) {
+        if (t == 0 && row + 2 * G < rows) prefetch_l2(row_src(row + 2 * G), (size_t)2 * M * sizeof(float));
+        if constexpr (PF < PER) fetch(row, false);
+        __syncthreads();  // the previous row's output phase has read s
+        if constexpr (M >= T) {
+            const unsigned pt = pa(t);
+#pragma unroll
+            for (unsigned i = 0; i < PER; ++i) s[pt ^ pa(i * T)] = v[i];
+        } else {
+            if (t < M) s[pa(t)] = v[0];
+        }
+        fft_smem<LOGM, false>(s, lo, hi);
+        if (row + G < rows) fetch(row + G, true);
+
+        // Bins k and M - k from the pair z_k, z_{M-k} (k = 0..M/2): with
+        // e = (z_k + conj z_{M-k}) / 2, o = (z_k - conj z_{M-k}) / (2i), w = W_2M^k,
+        // X[k] = e + w o and X[M-k] = conj(e - w o).
+        float2* dst = X + row * bin_pitch;
+        auto pair = [&](unsigned k, float2 zk, float2 zm) {
+            const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+            const float2 d = make_float2(zk.x - zm.x, zk.y + zm.y);  // zk - conj(zm)
+            const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);   // d / (2i)
+            const float2 wo = cmul(twiddle(lo, hi, k, false), o);
+            dst[k] = e + wo;
+            if (2 * k != M) dst[M - k] = make_float2(e.x - wo.x, wo.y - e.y);
+        };
+        if constexpr (M >= 2 * T) {
+            // k = t + i*T < M/2; M - k = (M-1) ^ (k-1) for k >= 1
+            const unsigned pk = pa(fft_pos<LOGM>(t));
+            const unsigned pm = t ? pa(M - 1u) ^ pa(fft_pos<LOGM>(t - 1)) : 0u;
 #pragma unroll 4
-        for (unsigned i = 0; i < M / (2 * T); ++i) {
-            const unsigned k = t + i * T;
-            const float2 zk = s[pk ^ pa(fft_pos<LOGM>(i * T))];
-            float2 zm;
-            if (t) zm = s[pm ^ pa(fft_pos<LOGM>(i * T))];
-            else zm = s[pa(fft_pos<LOGM>((M - k) & (M - 1u)))];
-            pair(k, zk, zm);
-        }
-        if (t == 0) {
-            const float2 z = s[pa(fft_pos<LOGM>(M / 2))];
-            pair(M / 2, z, z);
-        }
-    } else {
-        for (unsigned k = t; k <= M / 2; k += T) {
-            const float2 zk = s[pa(fft_pos<LOGM>(k & (M - 1u)))];
-            const float2 zm = s[pa(fft_pos<LOGM>((M - k) & (M - 1u)))];
-            pair(k, zk, zm);
+            for (unsigned i = 0; i < M / (2 * T); ++i) {
+                const unsigned k = t + i * T;
+                const float2 zk = s[pk ^ pa(fft_pos<LOGM>(i * T))];
+                float2 zm;
+                if (t) zm = s[pm ^ pa(fft_pos<LOGM>(i * T))];
+                else zm = s[pa(fft_pos<LOGM>((M - k) & (M - 1u)))];
+                pair(k, zk, zm);
+            }
+            if (t == 0) {
+                const float2 z = s[pa(fft_pos<LOGM>(M / 2))];
+                pair(M / 2, z, z);
+            }
+        } else {
+            for (unsigned k = t; k <= M / 2; k += T) {
+                const float2 zk = s[pa(fft_pos<LOGM>(k & (M - 1u)))];
+                const float2 zm = s[pa(fft_pos<LOGM>((M - k) & (M - 1u)))];
+                pair(k, zk, zm);
+            }
         }
     }
 }
@@ -290,13 +302,12 @@ __global__ void __launch_bounds__(FftPlan<LOGM>::threads()) fft_r2c_kernel(
 template <int LOGM>
 __global__ void __launch_bounds__(FftPlan<LOGM>::threads()) fft_c2r_kernel(
     const float2* Y, size_t bin_pitch, size_t nseg, float* out, size_t out_stride, size_t keep,
-    size_t out_len, TwiddleTable tw, size_t ahead)
+    size_t out_len, TwiddleTable tw, size_t rows)
 {
     constexpr unsigned M = 1u << LOGM;
     constexpr unsigned T = FftPlan<LOGM>::threads();
-    // the row that the CTA one wave later on this SM transforms (see r2c)
-    if (threadIdx.x == 0 && ahead && blockIdx.x + ahead < gridDim.x)
-        prefetch_l2(Y + (blockIdx.x + ahead) * bin_pitch, (size_t)(M + 1) * sizeof(float2));
+    constexpr bool WIDE = M >= 2 * T;
+    constexpr unsigned PER = WIDE ? M / (2 * T) : 1;  // bin pairs (k, M - k) per thread
     extern __shared__ __align__(16) float2 s_fft[];
     float2* s = s_fft;
     float2* lo = s + padded_len(M);
@@ -304,75 +315,87 @@ __global__ void __launch_bounds__(FftPlan<LOGM>::threads()) fft_c2r_kernel(
     const unsigned nhi = (2 * M) / 256;
     for (unsigned i = threadIdx.x; i < 256; i += blockDim.x) lo[i] = tw.lo[i];
     for (unsigned i = threadIdx.x; i < nhi; i += blockDim.x) hi[i] = tw.hi[i];
-    __syncthreads();
 
-    const size_t row = blockIdx.x;
-    const size_t dm = row / nseg, seg = row - dm * nseg;
-    const float2* src = Y + row * bin_pitch;
     const unsigned t = threadIdx.x;
-    // z_k = E_k + i O_k and z_{M-k} from the bins a = Y[k], b = Y[M-k]
-    // (k = 0..M/2): e = (a + conj b) / 2, d = (a - conj b) / 2, o = d conj(w),
-    // w = W_2M^k; z_k = e + i o, z_{M-k} = conj(e) + i conj(o). The DC and
-    // Nyquist imaginary parts are ignored (C2R).
-    auto pair = [&](unsigned k, float2 a, float2 b, unsigned slot_k, unsigned slot_m) {
-        if (k == 0) {
-            a.y = 0.f;
-            b.y = 0.f;
-        }
-        const float2 e = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
-        const float2 d = make_float2(0.5f * (a.x - b.x), 0.5f * (a.y + b.y));
-        const float2 o = cmul(d, conjf2(twiddle(lo, hi, k, false)));
-        s[slot_k] = make_float2(e.x - o.y, e.y + o.x);
-        if (k != 0 && 2 * k != M) s[slot_m] = make_float2(e.x + o.y, o.x - e.y);
-    };
-    if constexpr (M >= 2 * T) {
-        constexpr unsigned PER = M / (2 * T), BATCH = PER < 8 ? PER : 8;
-        const unsigned pt = pa(t);
-        // slot of M - k = (M-1) ^ (k-1), k >= 1
-        const unsigned pm = t ? pa(M - 1u) ^ pa(t - 1) : 0u;
+    // bins a = Y[k], b = Y[M-k] for k = t + i*T (k <= M/2), and Y[M/2] on
+    // thread 0 of the wide form
+    // (pairs i < PF loaded during the previous row's output phase, the rest
+    // when the row starts)
+    constexpr unsigned PF = PER > 8 ? PER / 2 : PER;
+    float2 xa[PER], xb[PER], ym = make_float2(0.f, 0.f);
+    auto fetch = [&](size_t row, bool ahead) {
+        const float2* src = Y + row * bin_pitch;
 #pragma unroll
-        for (unsigned i0 = 0; i0 < PER; i0 += BATCH) {
-            float2 xa[BATCH], xb[BATCH];
-#pragma unroll
-            for (unsigned i = 0; i < BATCH; ++i) {
-                const unsigned k = t + (i0 + i) * T;
+        for (unsigned i = 0; i < PER; ++i) {
+            const unsigned k = t + i * T;
+            if ((i < PF) == ahead && (WIDE || k <= M / 2)) {
                 xa[i] = src[k];
                 xb[i] = src[M - k];
             }
+        }
+        if (WIDE && ahead && t == 0) ym = src[M / 2];
+    };
+    const size_t G = gridDim.x;
+    size_t row = blockIdx.x;
+    if (row < rows) fetch(row, true);
+    if (t == 0 && row + G < rows) prefetch_l2(Y + (row + G) * bin_pitch, (size_t)(M + 1) * sizeof(float2));
+    for (; row < rows; row += G) {
+        if (t == 0 && row + 2 * G < rows)
+            prefetch_l2(Y + (row + 2 * G) * bin_pitch, (size_t)(M + 1) * sizeof(float2));
+        if constexpr (PF < PER) fetch(row, false);
+        __syncthreads();  // the previous row's output phase has read s (and lo/hi are in place)
+        // z_k = E_k + i O_k and z_{M-k} from the bins a = Y[k], b = Y[M-k]
+        // (k = 0..M/2): e = (a + conj b) / 2, d = (a - conj b) / 2, o = d conj(w),
+        // w = W_2M^k; z_k = e + i o, z_{M-k} = conj(e) + i conj(o). The DC and
+        // Nyquist imaginary parts are ignored (C2R).
+        auto pair = [&](unsigned k, float2 a, float2 b, unsigned slot_k, unsigned slot_m) {
+            if (k == 0) {
+                a.y = 0.f;
+                b.y = 0.f;
+            }
+            const float2 e = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
+            const float2 d = make_float2(0.5f * (a.x - b.x), 0.5f * (a.y + b.y));
+            const float2 o = cmul(d, conjf2(twiddle(lo, hi, k, false)));
+            s[slot_k] = make_float2(e.x - o.y, e.y + o.x);
+            if (k != 0 && 2 * k != M) s[slot_m] = make_float2(e.x + o.y, o.x - e.y);
+        };
+        if constexpr (WIDE) {
+            const unsigned pt = pa(t);
+            // slot of M - k = (M-1) ^ (k-1), k >= 1
+            const unsigned pm = t ? pa(M - 1u) ^ pa(t - 1) : 0u;
 #pragma unroll
-            for (unsigned i = 0; i < BATCH; ++i) {
-                const unsigned k = t + (i0 + i) * T;
-                const unsigned sk = pt ^ pa((i0 + i) * T);
-                const unsigned sm = t ? pm ^ pa((i0 + i) * T) : pa((M - k) & (M - 1u));
+            for (unsigned i = 0; i < PER; ++i) {
+                const unsigned k = t + i * T;
+                const unsigned sk = pt ^ pa(i * T);
+                const unsigned sm = t ? pm ^ pa(i * T) : pa((M - k) & (M - 1u));
                 pair(k, xa[i], xb[i], sk, sm);
             }
+            if (t == 0) pair(M / 2, ym, ym, pa(M / 2), pa(M / 2));
+        } else {
+            if (t <= M / 2) pair(t, xa[0], xb[0], pa(t & (M - 1u)), pa((M - t) & (M - 1u)));
         }
-        if (t == 0) {
-            const float2 y = src[M / 2];
-            pair(M / 2, y, y, pa(M / 2), pa(M / 2));
-        }
-    } else {
-        for (unsigned k = t; k <= M / 2; k += T) pair(k, src[k], src[M - k], pa(k & (M - 1u)), pa((M - k) & (M - 1u)));
-    }
-    fft_smem<LOGM, true>(s, lo, hi);
+        fft_smem<LOGM, true>(s, lo, hi);
+        if (row + G < rows) fetch(row + G, true);
 
-    const float scale = 1.0f / (float)M;
-    const size_t o0 = seg * keep;
-    float* dst = out + dm * out_stride + o0;
-    // samples of this segment that are kept and inside the row (<= 2M)
-    const size_t room = o0 >= out_len ? 0 : out_len - o0;
-    const unsigned lim = (unsigned)(keep < room ? keep : room);
-    auto put = [&](unsigned n, float2 z) {
-        const unsigned i0 = 2 * n;
-        if (i0 < lim) dst[i0] = z.x * scale;
-        if (i0 + 1 < lim) dst[i0 + 1] = z.y * scale;
-    };
-    if constexpr (M >= T) {
-        const unsigned pn = pa(fft_pos<LOGM>(t));
+        const size_t dm = row / nseg, seg = row - dm * nseg;
+        const float scale = 1.0f / (float)M;
+        const size_t o0 = seg * keep;
+        float* dst = out + dm * out_stride + o0;
+        // samples of this segment that are kept and inside the row (<= 2M)
+        const size_t room = o0 >= out_len ? 0 : out_len - o0;
+        const unsigned lim = (unsigned)(keep < room ? keep : room);
+        auto put = [&](unsigned n, float2 z) {
+            const unsigned i0 = 2 * n;
+            if (i0 < lim) dst[i0] = z.x * scale;
+            if (i0 + 1 < lim) dst[i0 + 1] = z.y * scale;
+        };
+        if constexpr (M >= T) {
+            const unsigned pn = pa(fft_pos<LOGM>(t));
 #pragma unroll 4
-        for (unsigned i = 0; i < M / T; ++i) put(t + i * T, s[pn ^ pa(fft_pos<LOGM>(i * T))]);
-    } else {
-        if (t < M) put(t, s[pa(fft_pos<LOGM>(t))]);
+            for (unsigned i = 0; i < M / T; ++i) put(t + i * T, s[pn ^ pa(fft_pos<LOGM>(i * T))]);
+        } else {
+            if (t < M) put(t, s[pa(fft_pos<LOGM>(t))]);
+        }
     }
 }
 
@@ -578,47 +601,61 @@ void launch_c2r_4step(float2* Y, size_t bin_pitch, size_t rows, size_t nseg, flo
 // ---------------------------------------------------------------------------
 // unpack / transposes
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) fdd_unpack_kernel(const uint8_t* in, size_t in_stride,
-                                                         int in_nbits, size_t nsamps, size_t nchans,
-                                                         float scale, float mid, float* x,
+// Tiles of 64 samples x 64 channels per 256 threads: each thread issues its
+// 16 loads before it uses any of them (64 KB in flight per SM at 8 blocks),
+// then writes 16 time-contiguous values per channel run.
+constexpr int UNPACK_TILE = 64;
+
+template <int NB>
+__device__ __forceinline__ float unpack_sample(const uint8_t* in, size_t in_stride, size_t t, size_t c,
+                                               float scale, float mid, int aligned)
+{
+    if constexpr (NB == 8) {
+        return ((float)__ldg(in + t * in_stride + c) - 127.5f) * scale;
+    } else if constexpr (NB == 32) {
+        const uint8_t* p = in + t * in_stride + 4 * c;
+        uint32_t u;
+        if (aligned) u = __ldg(reinterpret_cast<const uint32_t*>(p));
+        else u = (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
+        return __uint_as_float(u) * scale;
+    } else if constexpr (NB == 16) {
+        const uint8_t* p = in + t * in_stride + 2 * c;
+        const uint32_t u = aligned ? (uint32_t)__ldg(reinterpret_cast<const uint16_t*>(p))
+                                   : (uint32_t)p[0] | ((uint32_t)p[1] << 8);
+        return ((float)u - mid) * scale;
+    } else {
+        // 1/2/4-bit samples packed LSB-first within each byte
+        const size_t bit = c * (size_t)NB;
+        const uint32_t u = (__ldg(in + t * in_stride + (bit >> 3)) >> (bit & 7)) & ((1u << NB) - 1u);
+        return ((float)u - mid) * scale;
+    }
+}
+
+template <int NB>
+__global__ void __launch_bounds__(256) fdd_unpack_kernel(const uint8_t* in, size_t in_stride, size_t nsamps,
+                                                         size_t nchans, float scale, float mid, float* x,
                                                          size_t x_pitch, size_t x_len, int aligned)
 {
-    __shared__ float tile[32][33];
-    const size_t t0 = (size_t)blockIdx.x * 32, c0 = (size_t)blockIdx.y * 32;
+    constexpr int TL = UNPACK_TILE, PER = TL * TL / 256;
+    __shared__ float tile[TL][TL + 1];
+    const size_t t0 = (size_t)blockIdx.x * TL, c0 = (size_t)blockIdx.y * TL;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
-    for (int r = ty; r < 32; r += 8) {
-        const size_t t = t0 + r, c = c0 + tx;
-        float v = 0.f;
-        if (t < nsamps && c < nchans) {
-            if (in_nbits == 8) {
-                v = ((float)in[t * in_stride + c] - 127.5f) * scale;
-            } else if (in_nbits == 32) {
-                const uint8_t* p = in + t * in_stride + 4 * c;
-                uint32_t u;
-                if (aligned) {
-                    u = __ldg(reinterpret_cast<const uint32_t*>(p));
-                } else {
-                    u = (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
-                }
-                v = __uint_as_float(u) * scale;
-            } else if (in_nbits == 16) {
-                const uint8_t* p = in + t * in_stride + 2 * c;
-                const uint32_t u = aligned ? (uint32_t)__ldg(reinterpret_cast<const uint16_t*>(p))
-                                           : (uint32_t)p[0] | ((uint32_t)p[1] << 8);
-                v = ((float)u - mid) * scale;
-            } else {
-                // 1/2/4-bit samples packed LSB-first within each byte
-                const size_t bit = c * (size_t)in_nbits;
-                const uint32_t u = (in[t * in_stride + (bit >> 3)] >> (bit & 7)) & ((1u << in_nbits) - 1u);
-                v = ((float)u - mid) * scale;
-            }
-        }
-        tile[r][tx] = v;
+    float v[PER];
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        // element (sample t0 + ty + 8 (j % 8), channel c0 + tx + 32 (j / 8))
+        const size_t t = t0 + ty + 8 * (j & 7), c = c0 + tx + 32 * (j >> 3);
+        v[j] = (t < nsamps && c < nchans) ? unpack_sample<NB>(in, in_stride, t, c, scale, mid, aligned) : 0.f;
     }
+#pragma unroll
+    for (int j = 0; j < PER; ++j) tile[ty + 8 * (j & 7)][tx + 32 * (j >> 3)] = v[j];
     __syncthreads();
-    for (int r = ty; r < 32; r += 8) {
-        const size_t c = c0 + r, t = t0 + tx;
-        if (c < nchans && t < x_len) x[c * x_pitch + t] = tile[tx][r];
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        // channel c0 + ty + 8 (j % 8), sample t0 + tx + 32 (j / 8)
+        const int r = ty + 8 * (j & 7), tt = tx + 32 * (j >> 3);
+        const size_t c = c0 + r, t = t0 + tt;
+        if (c < nchans && t < x_len) x[c * x_pitch + t] = tile[tt][r];
     }
 }
 
@@ -802,13 +839,17 @@ __global__ void __launch_bounds__(MAC_THREADS) mac_plain_kernel(MacArgs a, int b
     }
 }
 
-// CTAs in one wave of a one-CTA-per-SM FFT launch (the L2 prefetch distance).
-size_t resident_ctas()
+// CTAs of one wave of a persistent kernel: resident CTAs per SM x SMs,
+// at most `rows` (at least one).
+template <typename K>
+unsigned persistent_grid(K kernel, unsigned threads, size_t smem, size_t rows)
 {
-    int dev = 0, sms = 0;
+    int dev = 0, sms = 0, per_sm = 0;
     RT_CHECK(cudaGetDevice(&dev));
     RT_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    return (size_t)std::max(sms, 1);
+    RT_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, (int)threads, smem));
+    const size_t wave = (size_t)std::max(per_sm, 1) * (size_t)std::max(sms, 1);
+    return (unsigned)std::max<size_t>(1, std::min(wave, rows));
 }
 
 template <int LOGM>
@@ -817,11 +858,13 @@ void launch_r2c_n(const float* x, size_t x_pitch, size_t nchans, size_t nseg, si
 {
     constexpr unsigned M = 1u << LOGM;
     const size_t smem = (padded_len(M) + 256 + 2 * M / 256) * sizeof(float2);
-    RT_CHECK(cudaFuncSetAttribute(fft_r2c_kernel<LOGM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
+    auto k = fft_r2c_kernel<LOGM>;
+    RT_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const unsigned threads = FftPlan<LOGM>::threads();
-    fft_r2c_kernel<LOGM><<<(unsigned)(nchans * nseg), threads, smem, s>>>(x, x_pitch, nseg, seg_stride, X,
-                                                                        bin_pitch, tw, resident_ctas());
+    const size_t rows = nchans * nseg;
+    if (rows == 0) return;
+    k<<<persistent_grid(k, threads, smem, rows), threads, smem, s>>>(x, x_pitch, nseg, seg_stride, X, bin_pitch,
+                                                                     tw, rows);
     RT_CHECK(cudaGetLastError());
 }
 
@@ -832,11 +875,13 @@ void launch_c2r_n(const float2* Y, size_t bin_pitch, size_t ndm, size_t nseg, fl
 {
     constexpr unsigned M = 1u << LOGM;
     const size_t smem = (padded_len(M) + 256 + 2 * M / 256) * sizeof(float2);
-    RT_CHECK(cudaFuncSetAttribute(fft_c2r_kernel<LOGM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
+    auto k = fft_c2r_kernel<LOGM>;
+    RT_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const unsigned threads = FftPlan<LOGM>::threads();
-    fft_c2r_kernel<LOGM><<<(unsigned)(ndm * nseg), threads, smem, s>>>(Y, bin_pitch, nseg, out, out_stride,
-                                                                      keep, out_len, tw, resident_ctas());
+    const size_t rows = ndm * nseg;
+    if (rows == 0) return;
+    k<<<persistent_grid(k, threads, smem, rows), threads, smem, s>>>(Y, bin_pitch, nseg, out, out_stride, keep,
+                                                                     out_len, tw, rows);
     RT_CHECK(cudaGetLastError());
 }
 
@@ -856,12 +901,18 @@ void launch_fdd_unpack(const uint8_t* in, size_t in_stride, int in_nbits, size_t
     // packed unsigned samples are centred at mid-scale, (2^nbits - 1) / 2
     // (127.5 for 8-bit, as the reference's unpack_kernel.cuh:60)
     const float mid = in_nbits == 32 ? 0.f : (float)((1u << in_nbits) - 1u) * 0.5f;
-    dim3 grid((unsigned)((x_len + 31) / 32), (unsigned)((nchans + 31) / 32));
+    if (x_len == 0 || nchans == 0) return;
+    dim3 grid((unsigned)((x_len + UNPACK_TILE - 1) / UNPACK_TILE),
+              (unsigned)((nchans + UNPACK_TILE - 1) / UNPACK_TILE));
     // whole-sample loads when every sample starts on its own size
     const size_t sb = in_nbits >= 16 ? (size_t)in_nbits / 8 : 1;
     const int aligned = ((uintptr_t)in % sb == 0) && (in_stride % sb == 0);
-    fdd_unpack_kernel<<<grid, 256, 0, s>>>(in, in_stride, in_nbits, nsamps, nchans, scale, mid, x,
-                                           x_pitch, x_len, aligned);
+    switch (in_nbits) {
+#define UNPACK(NB) case NB: fdd_unpack_kernel<NB><<<grid, 256, 0, s>>>(in, in_stride, nsamps, nchans, scale, mid, x, x_pitch, x_len, aligned); break;
+        UNPACK(1) UNPACK(2) UNPACK(4) UNPACK(8) UNPACK(16) UNPACK(32)
+#undef UNPACK
+    default: DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unsupported FDD input width");
+    }
     RT_CHECK(cudaGetLastError());
 }
 

@@ -206,6 +206,7 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
     const size_t gulp_default = dev_in && dev_out ? kDefaultGulp : kHostDefaultGulp;
     size_t G = std::min(nsamp_out, gulp_set && gulp_size ? gulp_size : gulp_default);
     G = std::min(G, (size_t)65535 * bt);
+    if (G < nsamp_out && G > bt) G = G / bt * bt;  // whole time tiles in every gulp but the last
     auto pitch_for = [&](size_t g) {
         return round_up((round_up(g, bt) + s.tmax + spw - 1) / spw + win + 8, 32);
     };
@@ -248,10 +249,24 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
     const float den = in_range * (float)v.nchans;
     const float factor = 3.f * 1024.f / 255.f / 16.f;
 
-    // Groups of DM slots whose output rows are contiguous (D2H overlap).
+    // The last gulp's K2 runs per group of DM slots whose output rows are
+    // contiguous, so that its device-to-host copy starts group by group
+    // (every other gulp's copy already overlaps the next gulp's kernels, and
+    // each extra launch ends with a partly filled wave).
     const size_t bd = s.tiled ? (size_t)kern::tiled_block_dms(nbits, s.variant) : 32;
     const size_t ntile = (ndm + bd - 1) / bd;
-    const size_t ngroups = (!dev_out && s.identity) ? std::min<size_t>(kMaxOutGroups, ntile) : 1;
+    const size_t ngroups_last = (!dev_out && s.identity) ? std::min<size_t>(kMaxOutGroups, ntile) : 1;
+
+    // Gulps (first output sample, samples). With host input and several
+    // gulps the first is a quarter of G: its input copy is the one that no
+    // kernel hides, and the next gulp's copy runs during its kernels.
+    std::vector<std::pair<size_t, size_t>> gulps;
+    for (size_t g0 = 0; g0 < nsamp_out;) {
+        size_t gc = std::min(G, nsamp_out - g0);
+        if (g0 == 0 && !dev_in && gc < nsamp_out && G >= 4 * bt) gc = round_up(G / 4, bt);
+        gulps.emplace_back(g0, gc);
+        g0 += gc;
+    }
 
     std::unique_ptr<rt::Event> t_a, t_b, t_c;
     if (record_timing) {
@@ -265,10 +280,11 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
     rt::Event* ev_out_free[2] = {&event(ev++), &event(ev++)};  // D2H has read output buffer b
     bool in_used[2] = {false, false}, out_used[2] = {false, false};
 
-    size_t gi = 0;
-    for (size_t g0 = 0; g0 < nsamp_out; g0 += G, ++gi) {
+    for (size_t gi = 0; gi < gulps.size(); ++gi) {
+        const size_t g0 = gulps[gi].first, gc = gulps[gi].second;
+        const bool last = gi + 1 == gulps.size();
+        const size_t ngroups = last ? ngroups_last : 1;
         const size_t b = gi % nbuf;
-        const size_t gc = std::min(G, nsamp_out - g0);
         const size_t rows_need = gc + s.tmax;
         const size_t rows_avail = std::min(rows_need, c.nsamps - g0);
 
@@ -347,7 +363,7 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
             ++stats.launches;
             if (!dev_out) event(ev + groups.size() - 1).record(ex);
         }
-        if (t_c && g0 + G >= nsamp_out) t_c->record(ex);
+        if (t_c && last) t_c->record(ex);
 
         // D2H per group into the caller's rows (column offset g0).
         if (!dev_out) {

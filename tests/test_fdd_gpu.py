@@ -194,7 +194,7 @@ def test_against_reference_fdd_outputs():
         assert our_err < FP32_REL_L2 and our_err * 5 < ref_err, (our_err, ref_err)
 
 
-@pytest.mark.parametrize("nbits,precision", [(2, 0), (4, 0), (2, 1), (16, 0)])
+@pytest.mark.parametrize("nbits,precision", [(1, 0), (2, 0), (4, 0), (2, 1), (16, 0)])
 def test_packed_input_widths(nbits, precision):
     """1/2/4/16-bit packed input (an extension; samples centred at
     (2^nbits - 1) / 2), both MAC forms."""
@@ -231,6 +231,33 @@ def test_four_step_fft_segments(segment_nfft, nchans, nsamps, dm_max):
     md = p.get_max_delay()
     nfft, good, nchunk = po.fdd_segment_geometry(nsamps, md) if segment_nfft == 0 else (segment_nfft, segment_nfft - md, 0)
     assert nfft > 32768
+    nout = nsamps - md
+    out = np.zeros((len(dms), nout), np.float32)
+    p.execute(nsamps, inp, 32, out, 32)
+    x = _oracle_x(inp, nsamps, params, 32)
+    ref = po.fdd_timeseries(x, _delays(params), np.ones(nchans, np.int32), dms, nout)
+    rel, mx = _errs(out, ref)
+    assert rel < FP32_REL_L2 and mx < FP32_MAX_ABS, (rel, mx)
+
+
+@pytest.mark.parametrize("segment_nfft,nchans,nsamps,dm_max", [
+    (512, 40, 30000, 50.0),
+    (1024, 48, 60000, 150.0),
+    (2048, 37, 60000, 300.0),
+    (4096, 33, 80000, 600.0),
+    (8192, 40, 100000, 1000.0),
+    (16384, 64, 150000, 1500.0),
+    (32768, 64, 200000, 2000.0),
+])
+def test_single_cta_fft_lengths(segment_nfft, nchans, nsamps, dm_max):
+    """Every single-CTA transform length: row counts below, at and above
+    one wave of the persistent FFT kernels, and segments that start on odd
+    sample offsets (nsamp_good odd)."""
+    inp, params = _input(nchans, nsamps, 23, float_input=True, f0=1400.0, df=-2.0, dt=64e-6)
+    dms = np.linspace(0, dm_max, 7, dtype=np.float32)
+    p = _plan(params, dms, segmented=1, segment_nfft=segment_nfft)
+    md = p.get_max_delay()
+    assert md < segment_nfft
     nout = nsamps - md
     out = np.zeros((len(dms), nout), np.float32)
     p.execute(nsamps, inp, 32, out, 32)

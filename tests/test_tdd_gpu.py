@@ -195,10 +195,34 @@ def test_strides_guru_and_gulps():
     sub = np.zeros((20, nout), np.float32)
     p.execute_guru(nsamps, packed, 8, nchans, sub, 32, nout * 4, 7, 20)
     assert np.array_equal(sub, ref[7:27])
-    # many small gulps
-    for gulp in (997, 4096):
+    # many small gulps; 12000 (whole time tiles, a quarter-size first gulp)
+    for gulp in (997, 4096, 12000):
         ours, _ = _run(dd.TDDPlan, packed, nsamps, nbits, params, dms, 32, gulp=gulp)
         assert np.array_equal(ours, ref), gulp
+
+
+@pytest.mark.parametrize("nbits", [2, 8])
+def test_host_gulp_schedule(nbits):
+    """Host buffers over several gulps: the first a quarter of the gulp
+    size, the middle ones whole time tiles, the last split into DM groups
+    for the output copies; device buffers with the same gulp size run
+    uniform gulps. Both bit-exact against the oracle."""
+    import torch
+    nchans, nsamps = 256, 70000
+    packed, dms, params = _case(nbits, nchans, nsamps, 90, 800.0, 31)
+    km = np.ones(nchans, np.int32)
+    p = dd.TDDPlan(*params)
+    p.set_dm_list(dms)
+    nout = nsamps - p.get_max_delay()
+    ref = _oracle(packed, nsamps, nbits, params, dms, km, 32, nout)
+    for gulp in (16384, 25000):
+        ours, _ = _run(dd.TDDPlan, packed, nsamps, nbits, params, dms, 32, gulp=gulp)
+        assert np.array_equal(ours, ref), gulp
+    d_in = torch.from_numpy(np.ascontiguousarray(packed)).cuda()
+    d_out = torch.zeros((len(dms), nout), dtype=torch.float32, device="cuda")
+    p.set_gulp_size(16384)
+    p.execute(nsamps, d_in, nbits, d_out, 32, dd.DEDISP_DEVICE_POINTERS)
+    assert np.array_equal(d_out.cpu().numpy(), ref)
 
 
 def test_unsorted_and_repeated_dm_list():
