@@ -606,21 +606,21 @@ void launch_c2r_4step(float2* Y, size_t bin_pitch, size_t rows, size_t nseg, flo
 // then writes 16 time-contiguous values per channel run.
 constexpr int UNPACK_TILE = 64;
 
-template <int NB>
+template <int NB, bool ALIGNED>
 __device__ __forceinline__ float unpack_sample(const uint8_t* in, size_t in_stride, size_t t, size_t c,
-                                               float scale, float mid, int aligned)
+                                               float scale, float mid)
 {
     if constexpr (NB == 8) {
         return ((float)__ldg(in + t * in_stride + c) - 127.5f) * scale;
     } else if constexpr (NB == 32) {
         const uint8_t* p = in + t * in_stride + 4 * c;
         uint32_t u;
-        if (aligned) u = __ldg(reinterpret_cast<const uint32_t*>(p));
+        if constexpr (ALIGNED) u = __ldg(reinterpret_cast<const uint32_t*>(p));
         else u = (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
         return __uint_as_float(u) * scale;
     } else if constexpr (NB == 16) {
         const uint8_t* p = in + t * in_stride + 2 * c;
-        const uint32_t u = aligned ? (uint32_t)__ldg(reinterpret_cast<const uint16_t*>(p))
+        const uint32_t u = ALIGNED ? (uint32_t)__ldg(reinterpret_cast<const uint16_t*>(p))
                                    : (uint32_t)p[0] | ((uint32_t)p[1] << 8);
         return ((float)u - mid) * scale;
     } else {
@@ -631,10 +631,11 @@ __device__ __forceinline__ float unpack_sample(const uint8_t* in, size_t in_stri
     }
 }
 
-template <int NB>
+// ALIGNED: every 16/32-bit sample starts on its own size (whole-sample loads)
+template <int NB, bool ALIGNED>
 __global__ void __launch_bounds__(256) fdd_unpack_kernel(const uint8_t* in, size_t in_stride, size_t nsamps,
                                                          size_t nchans, float scale, float mid, float* x,
-                                                         size_t x_pitch, size_t x_len, int aligned)
+                                                         size_t x_pitch, size_t x_len)
 {
     constexpr int TL = UNPACK_TILE, PER = TL * TL / 256;
     __shared__ float tile[TL][TL + 1];
@@ -645,7 +646,7 @@ __global__ void __launch_bounds__(256) fdd_unpack_kernel(const uint8_t* in, size
     for (int j = 0; j < PER; ++j) {
         // element (sample t0 + ty + 8 (j % 8), channel c0 + tx + 32 (j / 8))
         const size_t t = t0 + ty + 8 * (j & 7), c = c0 + tx + 32 * (j >> 3);
-        v[j] = (t < nsamps && c < nchans) ? unpack_sample<NB>(in, in_stride, t, c, scale, mid, aligned) : 0.f;
+        v[j] = (t < nsamps && c < nchans) ? unpack_sample<NB, ALIGNED>(in, in_stride, t, c, scale, mid) : 0.f;
     }
 #pragma unroll
     for (int j = 0; j < PER; ++j) tile[ty + 8 * (j & 7)][tx + 32 * (j >> 3)] = v[j];
@@ -660,52 +661,72 @@ __global__ void __launch_bounds__(256) fdd_unpack_kernel(const uint8_t* in, size
 }
 
 // X[c*nseg + seg][k] -> Xt[k][seg][j] for active channel j (km[j] applied).
+// Tiles of 64 bins x 32 channels per 256 threads; every thread issues its 8
+// loads before their first use.
+constexpr int BMT_BINS = 64;
 __global__ void __launch_bounds__(256) to_binmajor_kernel(const float2* X, size_t bin_pitch,
                                                           size_t nseg, size_t nbins,
                                                           const int32_t* chan, const float* km,
                                                           int nact, float2* Xt)
 {
-    __shared__ float2 tile[32][33];
-    const size_t k0 = (size_t)blockIdx.x * 32;
+    constexpr int PER = BMT_BINS / 8;
+    __shared__ float2 tile[32][BMT_BINS + 1];
+    const size_t k0 = (size_t)blockIdx.x * BMT_BINS;
     const int j0 = blockIdx.y * 32;
     const size_t seg = blockIdx.z;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    for (int r = ty; r < 32; r += 8) {
-        const int j = j0 + r;
-        const size_t k = k0 + tx;
-        float2 v = make_float2(0.f, 0.f);
-        if (j < nact && k < nbins) {
-            v = X[((size_t)chan[j] * nseg + seg) * bin_pitch + k];
-            const float m = km[j];
-            v.x *= m;
-            v.y *= m;
-        }
-        tile[r][tx] = v;
+    float2 v[PER];
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        // channel j0 + ty + 8 (i % 4), bin k0 + tx + 32 (i / 4)
+        const int j = j0 + ty + 8 * (i & 3);
+        const size_t k = k0 + tx + 32 * (i >> 2);
+        v[i] = (j < nact && k < nbins) ? X[((size_t)chan[j] * nseg + seg) * bin_pitch + k] : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        const int r = ty + 8 * (i & 3), j = j0 + r;
+        const float m = j < nact ? km[j] : 0.f;
+        tile[r][tx + 32 * (i >> 2)] = make_float2(v[i].x * m, v[i].y * m);
     }
     __syncthreads();
-    for (int r = ty; r < 32; r += 8) {
-        const size_t k = k0 + r;
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        // bin k0 + ty + 8 i, channel j0 + tx
+        const int kk = ty + 8 * i;
+        const size_t k = k0 + kk;
         const int j = j0 + tx;
-        if (k < nbins && j < nact) Xt[(k * nseg + seg) * nact + j] = tile[tx][r];
+        if (k < nbins && j < nact) Xt[(k * nseg + seg) * nact + j] = tile[tx][kk];
     }
 }
 
 // Yt[k][seg][dm] -> Y[dm*nseg + seg][k]
+// Tiles of 64 bins x 32 DMs per 256 threads; every thread issues its 8
+// loads before their first use.
+constexpr int DMT_BINS = 64;
 __global__ void __launch_bounds__(256) to_dmmajor_kernel(const float2* Yt, size_t nseg, size_t ndm,
                                                          size_t nbins, float2* Y, size_t bin_pitch)
 {
-    __shared__ float2 tile[32][33];
-    const size_t k0 = (size_t)blockIdx.x * 32, d0 = (size_t)blockIdx.y * 32;
+    constexpr int PER = DMT_BINS / 8;
+    __shared__ float2 tile[DMT_BINS][33];
+    const size_t k0 = (size_t)blockIdx.x * DMT_BINS, d0 = (size_t)blockIdx.y * 32;
     const size_t seg = blockIdx.z;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    for (int r = ty; r < 32; r += 8) {
-        const size_t k = k0 + r, d = d0 + tx;
-        tile[r][tx] = (k < nbins && d < ndm) ? Yt[(k * nseg + seg) * ndm + d] : make_float2(0.f, 0.f);
+    float2 v[PER];
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        const size_t k = k0 + ty + 8 * i, d = d0 + tx;
+        v[i] = (k < nbins && d < ndm) ? Yt[(k * nseg + seg) * ndm + d] : make_float2(0.f, 0.f);
     }
+#pragma unroll
+    for (int i = 0; i < PER; ++i) tile[ty + 8 * i][tx] = v[i];
     __syncthreads();
-    for (int r = ty; r < 32; r += 8) {
-        const size_t d = d0 + r, k = k0 + tx;
-        if (d < ndm && k < nbins) Y[(d * nseg + seg) * bin_pitch + k] = tile[tx][r];
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        // DM d0 + ty + 8 (i % 4), bin k0 + tx + 32 (i / 4)
+        const int r = ty + 8 * (i & 3), kk = tx + 32 * (i >> 2);
+        const size_t d = d0 + r, k = k0 + kk;
+        if (d < ndm && k < nbins) Y[(d * nseg + seg) * bin_pitch + k] = tile[kk][r];
     }
 }
 
@@ -906,10 +927,15 @@ void launch_fdd_unpack(const uint8_t* in, size_t in_stride, int in_nbits, size_t
               (unsigned)((nchans + UNPACK_TILE - 1) / UNPACK_TILE));
     // whole-sample loads when every sample starts on its own size
     const size_t sb = in_nbits >= 16 ? (size_t)in_nbits / 8 : 1;
-    const int aligned = ((uintptr_t)in % sb == 0) && (in_stride % sb == 0);
+    const bool aligned = ((uintptr_t)in % sb == 0) && (in_stride % sb == 0);
     switch (in_nbits) {
-#define UNPACK(NB) case NB: fdd_unpack_kernel<NB><<<grid, 256, 0, s>>>(in, in_stride, nsamps, nchans, scale, mid, x, x_pitch, x_len, aligned); break;
-        UNPACK(1) UNPACK(2) UNPACK(4) UNPACK(8) UNPACK(16) UNPACK(32)
+#define UNPACK(NB, AL) fdd_unpack_kernel<NB, AL><<<grid, 256, 0, s>>>(in, in_stride, nsamps, nchans, scale, mid, x, x_pitch, x_len)
+    case 1: UNPACK(1, true); break;
+    case 2: UNPACK(2, true); break;
+    case 4: UNPACK(4, true); break;
+    case 8: UNPACK(8, true); break;
+    case 16: if (aligned) UNPACK(16, true); else UNPACK(16, false); break;
+    case 32: if (aligned) UNPACK(32, true); else UNPACK(32, false); break;
 #undef UNPACK
     default: DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unsupported FDD input width");
     }
@@ -956,7 +982,7 @@ void launch_fdd_to_binmajor(const float2* X, size_t bin_pitch, size_t nseg, size
                             const int32_t* chan, const float* km, int nact, float2* Xt,
                             cudaStream_t s)
 {
-    dim3 grid((unsigned)((nbins + 31) / 32), (unsigned)((nact + 31) / 32), (unsigned)nseg);
+    dim3 grid((unsigned)((nbins + BMT_BINS - 1) / BMT_BINS), (unsigned)((nact + 31) / 32), (unsigned)nseg);
     to_binmajor_kernel<<<grid, 256, 0, s>>>(X, bin_pitch, nseg, nbins, chan, km, nact, Xt);
     RT_CHECK(cudaGetLastError());
 }
@@ -964,7 +990,7 @@ void launch_fdd_to_binmajor(const float2* X, size_t bin_pitch, size_t nseg, size
 void launch_fdd_to_dmmajor(const float2* Yt, size_t nseg, size_t ndm, size_t nbins, float2* Y,
                            size_t bin_pitch, cudaStream_t s)
 {
-    dim3 grid((unsigned)((nbins + 31) / 32), (unsigned)((ndm + 31) / 32), (unsigned)nseg);
+    dim3 grid((unsigned)((nbins + DMT_BINS - 1) / DMT_BINS), (unsigned)((ndm + 31) / 32), (unsigned)nseg);
     to_dmmajor_kernel<<<grid, 256, 0, s>>>(Yt, nseg, ndm, nbins, Y, bin_pitch);
     RT_CHECK(cudaGetLastError());
 }

@@ -521,19 +521,27 @@ __global__ void __launch_bounds__(256) fdd_prep_b_kernel(const float2* X, size_t
         for (int n = 2 * nseg; n < npad; ++n)
             for (int sp = 0; sp < 2; ++sp) B[((k * 2 + sp) * npad + n) * words_row + j] = 0u;
     }
+    // the next segment's loads are issued before this segment's stores
+    float2 nv[4];
+    auto load = [&](int s) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int j = j0 + ty + 8 * i;
+            const size_t k = k0 + tx;
+            nv[i] = (j < nact && k < nbins) ? X[((size_t)chan[j] * nseg + s) * bin_pitch + k]
+                                            : make_float2(0.f, 0.f);
+        }
+    };
+    load(0);
     for (int s = 0; s < nseg; ++s) {
         __syncthreads();
-        for (int r = ty; r < 32; r += 8) {
-            const int j = j0 + r;
-            const size_t k = k0 + tx;
-            float2 v = make_float2(0.f, 0.f);
-            if (j < nact && k < nbins) {
-                v = X[((size_t)chan[j] * nseg + s) * bin_pitch + k];
-                v.x *= km[j];
-                v.y *= km[j];
-            }
-            tile[r][tx] = v;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int j = j0 + ty + 8 * i;
+            const float w = j < nact ? km[j] : 0.f;
+            tile[ty + 8 * i][tx] = make_float2(nv[i].x * w, nv[i].y * w);
         }
+        if (s + 1 < nseg) load(s + 1);
         __syncthreads();
         for (int r = ty; r < 32; r += 8) {
             const size_t k = k0 + r;
