@@ -389,7 +389,7 @@ def run_batched(args, local, world, stream, max_over_ranks):
     torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1)) / steps
     total_units = float(sum(units))
-    # kernels per graph: K1 per beam (+ K1q per beam on quad-strided rows) + 1
+    # kernels per graph: K1d (quad-strided rows) or K1 per beam + 1
     launches_per_step = sum(b.get_timing()["launches"] for b in batches)
     res = {"workload": "96 beams x 1536 ch 8-bit, nsamp U[2^17,2^20], DM max U[500,3000], "
                        "ndm U[1024,4096] linear (seeded), f32 out",
@@ -577,7 +577,7 @@ def run_ours(args):
             step(plan)
             step(plan)
             t = plan.get_timing()
-            # whole device step: K1 (+ K1q for quad-strided variants) + K2
+            # whole device step: K1d (quad-strided variants) or K1, then K2
             tune[v] = t["kernel_ms"] + t["prep_ms"]
         best = min(tune, key=tune.get)
     else:

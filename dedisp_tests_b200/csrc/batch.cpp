@@ -238,8 +238,10 @@ TddBatch::Layout TddBatch::make_layout(const BatchShape& shape, size_t tile_limi
         const BeamState& t = m_beams[b];
         const size_t win = tiled ? (size_t)W[b] : 0;
         L.pitch[b] = round_up((round_up(std::max<size_t>(t.nout, 1), ubt) + t.tmax + spw - 1) / spw + win + 8, 32);
+        // quad-strided rows are built straight from the input (K1d); the
+        // channel-major packed copy exists only for the other forms
         L.tr_off[b] = off;
-        off += round_up((m_nchans + 1) * L.pitch[b], 64);
+        if (!L.quad) off += round_up((m_nchans + 1) * L.pitch[b], 64);
         if (L.quad) {
             // the tile windows read up to word (tiles - 1) * bt + tmax + P + 2
             L.qpitch[b] = round_up(round_up(std::max<size_t>(t.nout, 1), ubt) + t.tmax + L.period + 4, 32);
@@ -344,18 +346,22 @@ void TddBatch::enqueue(cudaStream_t s, const Layout& L, bool timing)
         const BeamState& t = m_beams[b];
         if (t.nout == 0) continue;
         uint32_t* ws = L.ws;
-        uint32_t* tr = ws + L.tr_off[b];
-        RT_CHECK(cudaMemsetAsync(tr + m_nchans * L.pitch[b], 0, L.pitch[b] * 4, s));
         const size_t rows = std::min(t.nout + t.tmax, t.spec.nsamps);
-        kern::TransposeArgs ta{t.spec.in, t.spec.in_stride, rows, m_nchans, m_nbits, tr, L.pitch[b], 0,
-                               L.pitch[b]};
-        kern::launch_transpose(ta, s);
-        ++launches;
         if (L.quad) {
-            kern::launch_quad_build(m_nbits, tr, L.pitch[b], ws + L.q_off[b], L.qpitch[b], m_nchans + 1, L.period,
-                                    s);
-            ++launches;
+            // K1d: quad-strided rows and the zero padding row
+            uint32_t* q = ws + L.q_off[b];
+            RT_CHECK(cudaMemsetAsync(q + m_nchans * L.qpitch[b], 0, L.qpitch[b] * 4, s));
+            kern::QuadDirectArgs qa{t.spec.in, t.spec.in_stride, rows, m_nchans, m_nbits, q, L.qpitch[b],
+                                    L.period};
+            kern::launch_quad_direct(qa, s);
+        } else {
+            uint32_t* tr = ws + L.tr_off[b];
+            RT_CHECK(cudaMemsetAsync(tr + m_nchans * L.pitch[b], 0, L.pitch[b] * 4, s));
+            kern::TransposeArgs ta{t.spec.in, t.spec.in_stride, rows, m_nchans, m_nbits, tr, L.pitch[b], 0,
+                                   L.pitch[b]};
+            kern::launch_transpose(ta, s);
         }
+        ++launches;
     }
     if (timing) m_ev[1]->record(s);
     if (L.persistent) {

@@ -216,9 +216,10 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
     auto qpitch_for = [&](size_t g) { return round_up(round_up(g, bt) + s.tmax + s.period + 4, 32); };
     auto nbuf_for = [&](size_t g) -> size_t { return nsamp_out > g ? 2 : 1; };
     auto in_bytes_for = [&](size_t g) { return round_up(g + s.tmax, 128) * row_bytes; };
+    // quad-strided rows are built straight from the input rows (K1d); the
+    // channel-major packed copy exists only for the other forms
     auto bytes_for = [&](size_t g) {
-        size_t b = (v.nchans + 1) * pitch_for(g) * 4;
-        if (quad) b += (v.nchans + 1) * qpitch_for(g) * 4;
+        size_t b = quad ? (v.nchans + 1) * qpitch_for(g) * 4 : (v.nchans + 1) * pitch_for(g) * 4;
         if (!dev_out) b += nbuf_for(g) * ndm * g * ob;
         if (!dev_in) b += nbuf_for(g) * in_bytes_for(g);
         return b;
@@ -232,7 +233,7 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
 
     const size_t nbuf = nbuf_for(G);
     const size_t pitch = pitch_for(G);
-    m_tr.reserve((v.nchans + 1) * pitch * 4);
+    if (!quad) m_tr.reserve((v.nchans + 1) * pitch * 4);
     const size_t qpitch = quad ? qpitch_for(G) : 0;
     if (quad) m_q.reserve((v.nchans + 1) * qpitch * 4);
     for (size_t b = 0; b < nbuf; ++b) {
@@ -290,9 +291,11 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
 
         if (t_a && g0 == 0) t_a->record(ex);
         // Padding channel row (all zero).
-        RT_CHECK(cudaMemsetAsync(tr + v.nchans * pitch, 0, pitch * 4, ex));
+        if (quad) RT_CHECK(cudaMemsetAsync(m_q.get<uint32_t>() + v.nchans * qpitch, 0, qpitch * 4, ex));
+        else RT_CHECK(cudaMemsetAsync(tr + v.nchans * pitch, 0, pitch * 4, ex));
 
-        // K1: input rows -> channel-major packed, zero past the data.
+        // K1 (channel-major packed) or K1d (quad-strided rows) from the
+        // gulp's input rows, zero past the data.
         const uint8_t* rows = c.in + g0 * c.in_stride;
         size_t rows_pitch = c.in_stride;
         if (!dev_in) {
@@ -306,17 +309,18 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
             rows = m_stage[b].get<uint8_t>();
             rows_pitch = row_bytes;
         }
-        kern::TransposeArgs ta{rows, rows_pitch, rows_avail, v.nchans, nbits, tr, pitch, 0, pitch};
-        kern::launch_transpose(ta, ex);
+        if (quad) {
+            kern::QuadDirectArgs qa{rows, rows_pitch, rows_avail, v.nchans, nbits, m_q.get<uint32_t>(), qpitch,
+                                    s.period};
+            kern::launch_quad_direct(qa, ex);
+        } else {
+            kern::TransposeArgs ta{rows, rows_pitch, rows_avail, v.nchans, nbits, tr, pitch, 0, pitch};
+            kern::launch_transpose(ta, ex);
+        }
         ++stats.launches;
         if (!dev_in) {
             ev_in_free[b]->record(ex);
             in_used[b] = true;
-        }
-        // K1q: quad-strided rows of every channel and the zero row
-        if (quad) {
-            kern::launch_quad_build(nbits, tr, pitch, m_q.get<uint32_t>(), qpitch, v.nchans + 1, s.period, ex);
-            ++stats.launches;
         }
         if (t_b && g0 == 0) t_b->record(ex);
 

@@ -2,13 +2,13 @@
 //
 // One call = validate-free execution of a (sub-)range of the DM list over a
 // time series, in gulps of output samples:
-//   host rows --(H2D, pinned or pageable)--> gulp input buffer --K1--> channel-
-//   major packed HBM buffer [--K1q--> quad-strided rows, quad variants]
-//   --K2 (per DM group)--> output --(D2H per DM group, overlapped with later
-//   groups)--> host rows. With several gulps, input and output buffers are
-//   doubled so that the copies of neighbouring gulps overlap a gulp's kernels.
-// With DEDISP_DEVICE_POINTERS the copies disappear and K1/K2 read/write the
-// caller's buffers. Derived per-plan state (active channels, sorted DMs,
+//   host rows --(H2D, pinned or pageable)--> gulp input buffer --K1d-->
+//   quad-strided rows (quad variants; K1: channel-major packed rows for the
+//   others) --K2--> output --(D2H)--> host rows. With several gulps, input and
+//   output buffers are doubled so that the copies of neighbouring gulps
+//   overlap a gulp's kernels; the last gulp's K2 and D2H run per DM group.
+// With DEDISP_DEVICE_POINTERS the copies disappear and K1d/K1/K2 read/write
+// the caller's buffers. Derived per-plan state (active channels, sorted DMs,
 // window sizes) is cached until the DM list or killmask changes.
 #pragma once
 

@@ -5,8 +5,9 @@
 //                              (the reference algorithm, kept as baseline)
 //   K2  dedisperse_tiled       shared-memory staged channel windows, packed
 //                              SIMD-within-a-register accumulation
-//   K1q quad_build_kernel      channel-major packed -> quad-strided rows (8-bit)
-//   K2q dedisperse_quad8       the 8-bit accumulation on quad-strided rows
+//   K1d quad_direct_kernel     time-major packed -> quad-strided rows (samples
+//                              of up to 8 bits widened to bytes)
+//   K2q dedisperse_quad8       the byte accumulation on quad-strided rows
 //
 // Exactness: the sums are the reference's integer sums
 // (src/tdd/dedisperse/dedisperse_kernel.cuh:145-181): every integer delay is
@@ -702,7 +703,7 @@ dedisperse_tiled8_batch_kernel(const DedisperseArgs* __restrict__ args,
 }
 
 // ---------------------------------------------------------------------------
-// K1q + K2q: the 8-bit kernel on quad-strided rows.
+// K1d + K2q: the byte kernel on quad-strided rows.
 //
 // For a period of P words, word n of a quad-strided row holds samples n,
 // n + P, n + 2P, n + 3P of the channel (byte i = sample n + i*P). A block
@@ -714,8 +715,6 @@ dedisperse_tiled8_batch_kernel(const DedisperseArgs* __restrict__ args,
 // stage, and a stage is one window copy and one barrier. Lane l owns words
 // l, l + 32, ..., so a warp's shared loads are 32 consecutive words.
 // ---------------------------------------------------------------------------
-constexpr int QB_THREADS = 256, QB_ITERS = 8;  // K1q: quads per block = 2048
-
 // Four NBITS-bit fields (LSB first) widened to four bytes.
 template <int NBITS>
 __device__ __forceinline__ uint32_t widen4(uint32_t x)
@@ -729,53 +728,67 @@ __device__ __forceinline__ uint32_t widen4(uint32_t x)
     }
 }
 
-// Quad k of a row: words 4k .. 4k+3, i.e. samples 4k + j + i*P (byte i of
-// word j), from packed NBITS-bit rows. With P and 4k multiples of 4 the four
-// samples 4k + i*P .. 4k + i*P + 3 sit in one packed word.
-template <int NBITS>
-__device__ __forceinline__ uint4 quad_words(const uint32_t* __restrict__ src, size_t tr_pitch, size_t k,
-                                            size_t period)
-{
-    constexpr int SPW = 32 / NBITS;
-    // e[i] = samples 4k + i*P .. 4k + i*P + 3 as bytes; zero past the row
-    uint32_t e[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const size_t t = 4 * k + (size_t)i * period;
-        const size_t idx = t / SPW;
-        const uint32_t w = idx < tr_pitch ? __ldg(src + idx) : 0u;
-        e[i] = widen4<NBITS>(w >> ((t % SPW) * NBITS));
-    }
-    // 4x4 byte transpose: output word j = byte j of e[0..3]
-    const uint32_t a_lo = __byte_perm(e[0], e[1], 0x5140), a_hi = __byte_perm(e[0], e[1], 0x7362);
-    const uint32_t b_lo = __byte_perm(e[2], e[3], 0x5140), b_hi = __byte_perm(e[2], e[3], 0x7362);
-    return make_uint4(__byte_perm(a_lo, b_lo, 0x5410), __byte_perm(a_lo, b_lo, 0x7632),
-                      __byte_perm(a_hi, b_hi, 0x5410), __byte_perm(a_hi, b_hi, 0x7632));
-}
+// K1d: quad-strided rows built straight from the time-major input. A block
+// takes QD_WORDS input words of every row (QD_WORDS * 32 / NBITS channels)
+// and QD_N output words n0 .. n0 + QD_N - 1: it stages the four row windows
+// n0 + i*P .. n0 + i*P + QD_N - 1 (i = 0..3) in shared memory, then each
+// thread turns one staged word of each window (the same 32 / NBITS channels,
+// rows n + i*P) into output word n of four channels at a time (widen to
+// bytes, 4x4 byte transpose). Lanes take consecutive n, so the shared reads
+// (row stride QD_WORDS + 1) are conflict-free and each store is a 128-byte
+// run of one channel's row. An input row is read by the four blocks whose
+// windows contain it, close together in launch order (L2 hits).
+constexpr int QD_WORDS = 16, QD_N = 128, QD_THREADS = 256;
 
 template <int NBITS>
-__global__ void __launch_bounds__(QB_THREADS) quad_build_kernel(const uint32_t* __restrict__ tr,
-                                                                size_t tr_pitch, uint32_t* __restrict__ q,
-                                                                size_t q_pitch, size_t nrows, size_t period)
+__global__ void __launch_bounds__(QD_THREADS) quad_direct_kernel(QuadDirectArgs a, int aligned)
 {
-    constexpr size_t PER_BLOCK = (size_t)QB_THREADS * QB_ITERS;
-    const size_t nquads = q_pitch / 4;
-    for (size_t row = blockIdx.y; row < nrows; row += gridDim.y) {
-        const uint32_t* src = tr + row * tr_pitch;
-        uint4* dst = reinterpret_cast<uint4*>(q + row * q_pitch);
-        for (size_t k0 = (size_t)blockIdx.x * PER_BLOCK; k0 < nquads; k0 += (size_t)gridDim.x * PER_BLOCK) {
-            const size_t k1 = k0 + threadIdx.x;
-            if (k0 + PER_BLOCK <= nquads) {
-                uint4 v[QB_ITERS];
+    constexpr int CH = QD_WORDS * 32 / NBITS;  // channels per block
+    constexpr int LOADS = 4 * QD_N * QD_WORDS / QD_THREADS;
+    __shared__ uint32_t tile[4][QD_N][QD_WORDS + 1];
+    const size_t n0 = (size_t)blockIdx.x * QD_N;
+    const size_t w0 = (size_t)blockIdx.y * QD_WORDS;
+    const size_t row_words = a.nchans * NBITS / 32;
+    const size_t P = (size_t)a.period_words;
+
+    uint32_t v[LOADS];
 #pragma unroll
-                for (int it = 0; it < QB_ITERS; ++it)
-                    v[it] = quad_words<NBITS>(src, tr_pitch, k1 + (size_t)it * QB_THREADS, period);
-#pragma unroll
-                for (int it = 0; it < QB_ITERS; ++it) dst[k1 + (size_t)it * QB_THREADS] = v[it];
-            } else {
-                for (size_t k = k1; k < nquads; k += QB_THREADS) dst[k] = quad_words<NBITS>(src, tr_pitch, k, period);
-            }
+    for (int it = 0; it < LOADS; ++it) {
+        const int idx = threadIdx.x + it * QD_THREADS;
+        const int k = idx % QD_WORDS, r = (idx / QD_WORDS) % QD_N, i = idx / (QD_WORDS * QD_N);
+        const size_t row = n0 + r + (size_t)i * P, wi = w0 + k;
+        v[it] = 0u;
+        if (row < a.rows_valid && wi < row_words) {
+            const uint8_t* p = a.in + row * a.in_pitch + wi * 4;
+            v[it] = aligned ? __ldg(reinterpret_cast<const uint32_t*>(p))
+                            : (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) |
+                                  ((uint32_t)p[3] << 24);
         }
+    }
+#pragma unroll
+    for (int it = 0; it < LOADS; ++it) {
+        const int idx = threadIdx.x + it * QD_THREADS;
+        tile[idx / (QD_WORDS * QD_N)][(idx / QD_WORDS) % QD_N][idx % QD_WORDS] = v[it];
+    }
+    __syncthreads();
+
+    const size_t c0 = w0 * 32 / NBITS;
+    for (int item = threadIdx.x; item < (CH / 4) * QD_N; item += QD_THREADS) {
+        const int r = item % QD_N, g = item / QD_N;  // output word n0 + r, channels c0 + 4g ..
+        const size_t n = n0 + r, c = c0 + 4 * (size_t)g;
+        if (n >= a.q_pitch_words || c >= a.nchans) continue;
+        const int bit = 4 * g * NBITS, kw = bit >> 5, sh = bit & 31;
+        uint32_t e[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) e[i] = widen4<NBITS>(tile[i][r][kw] >> sh);
+        // word j (channel c + j) = byte j of e[0..3]
+        const uint32_t a_lo = __byte_perm(e[0], e[1], 0x5140), a_hi = __byte_perm(e[0], e[1], 0x7362);
+        const uint32_t b_lo = __byte_perm(e[2], e[3], 0x5140), b_hi = __byte_perm(e[2], e[3], 0x7362);
+        uint32_t* dst = a.q + c * a.q_pitch_words + n;
+        dst[0] = __byte_perm(a_lo, b_lo, 0x5410);
+        dst[a.q_pitch_words] = __byte_perm(a_lo, b_lo, 0x7632);
+        dst[2 * a.q_pitch_words] = __byte_perm(a_hi, b_hi, 0x5410);
+        dst[3 * a.q_pitch_words] = __byte_perm(a_hi, b_hi, 0x7632);
     }
 }
 
@@ -1300,21 +1313,21 @@ int tiled_stage_channels(int nbits, int win_words, int variant)
     return cs >= step ? cs : 0;
 }
 
-void launch_quad_build(int nbits, const uint32_t* tr, size_t tr_pitch_words, uint32_t* q, size_t q_pitch_words,
-                       size_t nrows, int period_words, cudaStream_t s)
+void launch_quad_direct(const QuadDirectArgs& a, cudaStream_t s)
 {
-    if (q_pitch_words % 4 != 0 || period_words % 4 != 0 || (uintptr_t)q % 16 != 0)
-        DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "quad-strided rows need 16-byte aligned rows and a period of 4k words");
-    const size_t nquads = q_pitch_words / 4;
-    constexpr size_t per_block = (size_t)QB_THREADS * QB_ITERS;
-    dim3 grid((unsigned)std::min<size_t>((nquads + per_block - 1) / per_block, 65535),
-              (unsigned)std::min<size_t>(nrows, 65535));
-    const size_t period = (size_t)period_words;
-    switch (nbits) {
-    case 1: quad_build_kernel<1><<<grid, QB_THREADS, 0, s>>>(tr, tr_pitch_words, q, q_pitch_words, nrows, period); break;
-    case 2: quad_build_kernel<2><<<grid, QB_THREADS, 0, s>>>(tr, tr_pitch_words, q, q_pitch_words, nrows, period); break;
-    case 4: quad_build_kernel<4><<<grid, QB_THREADS, 0, s>>>(tr, tr_pitch_words, q, q_pitch_words, nrows, period); break;
-    case 8: quad_build_kernel<8><<<grid, QB_THREADS, 0, s>>>(tr, tr_pitch_words, q, q_pitch_words, nrows, period); break;
+    if (a.q_pitch_words % 4 != 0 || a.period_words % 4 != 0 || a.period_words <= 0)
+        DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "quad-strided rows need a period of 4k words");
+    if (a.nchans == 0 || a.q_pitch_words == 0) return;
+    const size_t row_words = a.nchans * (size_t)a.nbits / 32;
+    const dim3 grid((unsigned)((a.q_pitch_words + QD_N - 1) / QD_N), (unsigned)((row_words + QD_WORDS - 1) / QD_WORDS));
+    if ((a.q_pitch_words + QD_N - 1) / QD_N > 0x7FFFFFFFu || grid.y > 65535u)
+        DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "quad-strided rows too long for one launch");
+    const int aligned = ((uintptr_t)a.in % 4 == 0) && (a.in_pitch % 4 == 0);
+    switch (a.nbits) {
+    case 1: quad_direct_kernel<1><<<grid, QD_THREADS, 0, s>>>(a, aligned); break;
+    case 2: quad_direct_kernel<2><<<grid, QD_THREADS, 0, s>>>(a, aligned); break;
+    case 4: quad_direct_kernel<4><<<grid, QD_THREADS, 0, s>>>(a, aligned); break;
+    case 8: quad_direct_kernel<8><<<grid, QD_THREADS, 0, s>>>(a, aligned); break;
     default: DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "quad-strided rows hold samples of at most 8 bits");
     }
     RT_CHECK(cudaGetLastError());

@@ -61,7 +61,7 @@ struct DedisperseArgs {
 // Quad-strided variants (tiled_variant_quad: 8-bit 5-8, 1/2/4-bit 1-4) run
 // on quad-strided rows: word n of a row holds samples n + i*P of the channel
 // in byte i (i = 0..3, P = 32 * tiled_lane_words; narrower samples widened
-// to bytes), built from the channel-major packed rows by launch_quad_build.
+// to bytes), built from the input rows by launch_quad_direct.
 int tiled_variant_count(int nbits);
 int tiled_batch_variant_count(int nbits);  // variants of the persistent batch kernel (all)
 int tiled_default_variant(int nbits);      // the variant a plan uses unless told otherwise
@@ -76,11 +76,21 @@ size_t tiled_batch_smem_bytes(int nbits, int win_words, int chan_per_stage, int 
 // Channels per pipeline stage for a window of win_words (0: does not fit).
 int tiled_stage_channels(int nbits, int win_words, int variant);
 
-// K1q: quad-strided rows q (q_pitch_words per row, a multiple of 4, rows
-// 16-byte aligned) from channel-major packed rows tr of 1/2/4/8-bit samples,
-// for nrows rows; samples past a tr row read as zero.
-void launch_quad_build(int nbits, const uint32_t* tr, size_t tr_pitch_words, uint32_t* q, size_t q_pitch_words,
-                       size_t nrows, int period_words, cudaStream_t s);
+// K1d: quad-strided rows straight from time-major packed 1/2/4/8-bit input:
+// rows 0..nchans-1 of q, word n of channel c holding samples n + i*P
+// (i = 0..3) of the channel as bytes, zero at or past rows_valid. The
+// all-zero padding row is the caller's.
+struct QuadDirectArgs {
+    const uint8_t* in;    // input row t at in + t * in_pitch
+    size_t in_pitch;      // bytes
+    size_t rows_valid;    // rows present in `in`
+    size_t nchans;
+    int nbits;            // 1, 2, 4 or 8
+    uint32_t* q;          // quad-strided rows, q_pitch_words apart
+    size_t q_pitch_words; // words per row (a multiple of 4), all written
+    int period_words;     // P, a multiple of 4
+};
+void launch_quad_direct(const QuadDirectArgs& a, cudaStream_t s);
 
 // True if a quad-strided kernel gave up a bounded wait on its staged copies
 // since the last call (device-wide flag, cleared; synchronises s).
