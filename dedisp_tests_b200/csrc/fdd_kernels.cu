@@ -567,8 +567,8 @@ void launch_r2c_4step(const float* x, size_t x_pitch, size_t rows, size_t nseg, 
     const size_t sa = FT_TILE * M1 * sizeof(float2) + tws, sb = FT_TILE * M2 * sizeof(float2) + tws;
     auto ka = fft4_cols_kernel<L1, L2, true, false>;
     auto kb = fft4_rows_kernel<L1, L2, false, false>;
-    RT_CHECK(cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sa));
-    RT_CHECK(cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb));
+    rt::raise_smem_limit(ka, sa);
+    rt::raise_smem_limit(kb, sb);
     ka<<<dim3(M2 / FT_TILE, (unsigned)rows), FT_THREADS, sa, s>>>(x, x_pitch, nseg, seg_stride, nullptr, 0,
                                                                 Z1, tw);
     RT_CHECK(cudaGetLastError());
@@ -589,8 +589,8 @@ void launch_c2r_4step(float2* Y, size_t bin_pitch, size_t rows, size_t nseg, flo
     RT_CHECK(cudaGetLastError());
     auto ka = fft4_cols_kernel<L1, L2, false, true>;
     auto kb = fft4_rows_kernel<L1, L2, true, true>;
-    RT_CHECK(cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sa));
-    RT_CHECK(cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb));
+    rt::raise_smem_limit(ka, sa);
+    rt::raise_smem_limit(kb, sb);
     ka<<<dim3(M2 / FT_TILE, (unsigned)rows), FT_THREADS, sa, s>>>(nullptr, 0, 1, 0, Y, bin_pitch, Z1, tw);
     RT_CHECK(cudaGetLastError());
     kb<<<dim3(M1 / FT_TILE, (unsigned)rows), FT_THREADS, sb, s>>>(Z1, nullptr, 0, out, out_stride, nseg, keep,
@@ -880,7 +880,7 @@ void launch_r2c_n(const float* x, size_t x_pitch, size_t nchans, size_t nseg, si
     constexpr unsigned M = 1u << LOGM;
     const size_t smem = (padded_len(M) + 256 + 2 * M / 256) * sizeof(float2);
     auto k = fft_r2c_kernel<LOGM>;
-    RT_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    rt::raise_smem_limit(k, smem);
     const unsigned threads = FftPlan<LOGM>::threads();
     const size_t rows = nchans * nseg;
     if (rows == 0) return;
@@ -897,7 +897,7 @@ void launch_c2r_n(const float2* Y, size_t bin_pitch, size_t ndm, size_t nseg, fl
     constexpr unsigned M = 1u << LOGM;
     const size_t smem = (padded_len(M) + 256 + 2 * M / 256) * sizeof(float2);
     auto k = fft_c2r_kernel<LOGM>;
-    RT_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    rt::raise_smem_limit(k, smem);
     const unsigned threads = FftPlan<LOGM>::threads();
     const size_t rows = ndm * nseg;
     if (rows == 0) return;
@@ -1007,8 +1007,7 @@ void launch_fdd_mac_plain(const MacArgs& a, cudaStream_t s)
 {
     const size_t smem = (MAC_BK * MAC_BM + MAC_BK * MAC_BN + 256 + a.nfft / 256) * sizeof(float2);
     if (smem > 200 * 1024) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "FFT length too large for the MAC table");
-    RT_CHECK(cudaFuncSetAttribute(mac_plain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
+    rt::raise_smem_limit(mac_plain_kernel, smem);
     const unsigned dm_tiles = (unsigned)((a.ndm + MAC_BM - 1) / MAC_BM);
     // enough blocks to fill the GPU several times over
     const size_t want_blocks = 148 * 8;

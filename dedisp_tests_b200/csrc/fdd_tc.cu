@@ -674,8 +674,7 @@ void launch_fdd_mac_tc(const TcMacArgs& a, const void* B, cudaStream_t s)
     if (r != CUDA_SUCCESS) DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "cuTensorMapEncodeTiled failed");
     if (a.stages < 2 || a.stages > TC_MAX_STAGES) DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "bad stage count");
     const size_t smem = tc_smem_bytes(a.nfft, a.nact_pad, a.npad, a.dmax, a.stages);
-    RT_CHECK(cudaFuncSetAttribute(fdd_mac_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
+    rt::raise_smem_limit(fdd_mac_tc_kernel, smem);
     int sms = 148;
     int dev = 0;
     RT_CHECK(cudaGetDevice(&dev));

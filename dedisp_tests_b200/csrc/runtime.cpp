@@ -2,6 +2,8 @@
 #include "runtime.hpp"
 
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <sstream>
 
 namespace dedisp {
@@ -120,6 +122,19 @@ bool is_pinned_host(const void* p)
         return false;
     }
     return a.type == cudaMemoryTypeHost;
+}
+
+void raise_smem_limit(const void* kfn, size_t bytes)
+{
+    static std::mutex m;
+    static std::map<std::pair<const void*, int>, size_t> set;
+    int dev = 0;
+    RT_CHECK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(m);
+    size_t& have = set[{kfn, dev}];
+    if (bytes <= have) return;
+    RT_CHECK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    have = bytes;
 }
 
 }  // namespace rt

@@ -105,5 +105,16 @@ private:
 // registered), so copies can be asynchronous without staging.
 bool is_pinned_host(const void* p);
 
+// Raise kernel `kfn`'s dynamic shared-memory limit on the current device to
+// at least `bytes`. The limit only grows: each (kernel, device) keeps the
+// largest value set so far, under one lock, so that a thread launching with
+// a larger limit never has it lowered by another thread in between.
+void raise_smem_limit(const void* kfn, size_t bytes);
+template <typename K>
+void raise_smem_limit(K* kfn, size_t bytes)
+{
+    raise_smem_limit(reinterpret_cast<const void*>(kfn), bytes);
+}
+
 }  // namespace rt
 }  // namespace dedisp

@@ -1045,25 +1045,11 @@ dedisperse_quad8_batch_kernel(const DedisperseArgs* __restrict__ args,
                 [&](const DedisperseArgs& a, int bx, size_t by) { quad8_tile<J, NW>(a, bx, by, one); });
 }
 
-// cudaFuncSetAttribute is per device context; remember what each device has
-// been given, per kernel.
-template <typename K>
-void ensure_smem(K kfn, size_t smem, size_t (&configured)[64])
-{
-    int dev = 0;
-    RT_CHECK(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64 || smem > configured[dev]) {
-        RT_CHECK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        if (dev >= 0 && dev < 64) configured[dev] = smem;
-    }
-}
-
 template <int J, int NW>
 void launch_tiled8_shape(const DedisperseArgs& a, cudaStream_t s)
 {
-    static size_t configured[64] = {};
     const size_t smem = tiled_smem_bytes(8, a.win_words, a.chan_per_stage, a.variant);
-    ensure_smem(dedisperse_tiled8_kernel<J, NW>, smem, configured);
+    rt::raise_smem_limit(dedisperse_tiled8_kernel<J, NW>, smem);
     dim3 grid((a.ndm + NW - 1) / NW, (unsigned)((a.nsamp_out + 128 * J - 1) / (128 * J)));
     dedisperse_tiled8_kernel<J, NW><<<grid, NW * 32, smem, s>>>(a, 1u);
     RT_CHECK(cudaGetLastError());
@@ -1081,11 +1067,10 @@ void launch_quad8_shape(const DedisperseArgs& a, cudaStream_t s)
     // One block per SM (registers): every block may use the whole opt-in
     // shared memory for its windows; a block sizes its stages from its own
     // delay span. The plan's window (the largest span) must fit 4 channels.
-    static size_t configured[64] = {};
     const size_t smem = quad_dynamic_smem_bytes(NW);
     if (tiled_smem_bytes(8, a.win_words, 4, a.variant) > smem)
         DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "quad-strided window does not fit shared memory");
-    ensure_smem(dedisperse_quad8_kernel<J, NW>, smem, configured);
+    rt::raise_smem_limit(dedisperse_quad8_kernel<J, NW>, smem);
     dim3 grid((a.ndm + NW - 1) / NW, (unsigned)((a.nsamp_out + 128 * J - 1) / (128 * J)));
     dedisperse_quad8_kernel<J, NW><<<grid, NW * 32, smem, s>>>(a, 1u);
     RT_CHECK(cudaGetLastError());
@@ -1100,9 +1085,8 @@ void launch_quad8_variant(const DedisperseArgs& a, cudaStream_t s)
 template <int J, int NW>
 void launch_tiled8_batch_shape(const BatchLaunch& b, cudaStream_t s)
 {
-    static size_t configured[64] = {};
     auto kfn = dedisperse_tiled8_batch_kernel<J, NW>;
-    ensure_smem(kfn, b.smem_bytes, configured);
+    rt::raise_smem_limit(kfn, b.smem_bytes);
     int dev = 0, sms = 0, per_sm = 0;
     RT_CHECK(cudaGetDevice(&dev));
     RT_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -1123,12 +1107,11 @@ void launch_tiled8_batch_variant(const BatchLaunch& b, cudaStream_t s)
 template <int J, int NW>
 void launch_quad8_batch_shape(const BatchLaunch& b, cudaStream_t s)
 {
-    static size_t configured[64] = {};
     auto kfn = dedisperse_quad8_batch_kernel<J, NW>;
     const size_t smem = quad_dynamic_smem_bytes(NW, true);
     if (b.smem_bytes > smem)
         DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "quad-strided window does not fit shared memory");
-    ensure_smem(kfn, smem, configured);
+    rt::raise_smem_limit(kfn, smem);
     int dev = 0, sms = 0, per_sm = 0;
     RT_CHECK(cudaGetDevice(&dev));
     RT_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -1161,9 +1144,8 @@ void launch_tiled_n(const DedisperseArgs& a, cudaStream_t s)
         }
     } else {
         using G = TiledGeom<NBITS>;
-        static size_t configured[64] = {};
-        const size_t smem = tiled_smem_bytes(NBITS, a.win_words, a.chan_per_stage, 0);
-        ensure_smem(dedisperse_tiled_kernel<NBITS>, smem, configured);
+            const size_t smem = tiled_smem_bytes(NBITS, a.win_words, a.chan_per_stage, 0);
+        rt::raise_smem_limit(dedisperse_tiled_kernel<NBITS>, smem);
         dim3 grid((a.ndm + G::BD - 1) / G::BD, (unsigned)((a.nsamp_out + G::BT - 1) / G::BT));
         dedisperse_tiled_kernel<NBITS><<<grid, G::NT, smem, s>>>(a);
         RT_CHECK(cudaGetLastError());
