@@ -566,15 +566,16 @@ __global__ void __launch_bounds__(256) fdd_prep_b_kernel(const float2* X, size_t
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
+    // initialised once, thread-safely (a failed lookup throws and is retried
+    // by the next call)
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
         void* p = nullptr;
         cudaDriverEntryPointQueryResult q;
         RT_CHECK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
         if (!p || q != cudaDriverEntryPointSuccess)
             DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "cuTensorMapEncodeTiled unavailable");
-        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
     return fn;
 }
 
