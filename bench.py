@@ -693,9 +693,13 @@ def run_ours(args):
     if not args.no_e2e:
         try:
             import psutil
-            need = d_in.numel() + ndm * nout * 4
+            # every rank on this node pins its own buffers, so the node must
+            # hold them all; the ranks take the same branch (their barriers
+            # and reductions below must match)
+            local_world = int(os.environ.get("LOCAL_WORLD_SIZE", "1"))
+            need = (d_in.numel() + ndm * nout * 4) * local_world
             avail = psutil.virtual_memory().available
-            if avail < need * 1.25:
+            if max_over_ranks(0.0 if avail >= need * 1.25 else 1.0) > 0.0:
                 e2e = {"value": None, "unit": UNIT, "skipped": f"host RAM {avail/1e9:.0f} GB < "
                                                                f"{need*1.25/1e9:.0f} GB needed"}
             else:
