@@ -1,7 +1,8 @@
 """Programs written against the reference interfaces build unchanged against
 include/ and link to libdedisp.so: a C program on the C API
 (src/clib/dedisp.h; its use mirrors bin/test/ctestdedisp.c:286-345) and a
-C++ program on dedisp::TDDPlan (src/tdd/TDDPlan.hpp:17-57). Both stop at
+C++ program on the plan classes (src/tdd/TDDPlan.hpp:17-57,
+src/dedisp/DedispPlan.hpp:21-66, src/fdd/FDDGPUPlan.hpp:18-35). Both stop at
 plan setup, which needs no GPU: the DM list, delays and getters."""
 import os
 import shutil
@@ -40,6 +41,8 @@ int main(void)
 CXX_PROGRAM = r"""
 #include <cstdio>
 #include <vector>
+#include <dedisp/DedispPlan.hpp>
+#include <fdd/FDDGPUPlan.hpp>
 #include <tdd/TDDPlan.hpp>
 
 int main()
@@ -51,6 +54,12 @@ int main()
     plan.set_gulp_size(65536);
     std::printf("%lu %lu %lu\n", (unsigned long)plan.get_dm_count(),
                 (unsigned long)plan.get_max_delay(), (unsigned long)plan.get_gulp_size());
+    dedisp::DedispPlan legacy(4096, 64e-6f, 1500.0f, -0.078125f);
+    legacy.generate_dm_list(0.f, 2000.f, 40.f, 1.25f);
+    dedisp::FDDGPUPlan fdd(1024, 250e-6f, 1581.8f, -0.390625f);
+    fdd.set_dm_list(dms.data(), dms.size());
+    std::printf("%lu %lu %lu\n", (unsigned long)legacy.get_dm_count(), (unsigned long)legacy.get_max_delay(),
+                (unsigned long)fdd.get_max_delay());
     return 0;
 }
 """
@@ -77,6 +86,7 @@ def test_c_program_on_the_reference_c_api(tmp_path):
 
 
 @pytest.mark.skipif(shutil.which("g++") is None, reason="no C++ compiler")
-def test_cxx_program_on_the_reference_tddplan(tmp_path):
+def test_cxx_program_on_the_reference_plan_classes(tmp_path):
     out = _build_and_run(tmp_path, "g++", CXX_PROGRAM, "app.cpp", ["-std=c++17"])
     assert out[0] == "512 2622 65536"
+    assert out[1] == "3643 35500 2622"
