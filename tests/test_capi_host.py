@@ -222,3 +222,37 @@ def test_server_api_host_checks():
     assert L.dedisp_b200_server_create(C.byref(h), 256, 64e-6, 1500.0, -0.25, 3, 0, 0, 4096, 1, 0, 1, 0, 0) == 10
     assert L.dedisp_b200_server_create(C.byref(h), 256, 64e-6, 1500.0, -0.25, 8, 0, 0, 4096, 0, 0, 1, 0, 0) != 0
     assert L.dedisp_b200_server_drain(None) == 4
+
+
+def _prototypes():
+    """name -> (returns void, parameter count) for every function declared in
+    include/dedisp.h and include/dedisp_b200.h."""
+    protos = {}
+    for header in ("dedisp.h", "dedisp_b200.h"):
+        text = open(os.path.join(ROOT, "include", header)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        text = re.sub(r"//[^\n]*", "", text)
+        for ret, name, params in re.findall(r"([A-Za-z_][\w\s\*]*?)\b(dedisp_\w+)\s*\(([^;{}]*?)\)\s*;", text):
+            params = " ".join(params.split())
+            n = 0 if params in ("", "void") else params.count(",") + 1
+            protos[name] = (ret.split()[-1] == "void" and "*" not in ret, n)
+    return protos
+
+
+def test_python_binding_matches_the_headers():
+    """Every function the ctypes binding declares has the header's parameter
+    count and void/non-void return."""
+    protos = _prototypes()
+    L = dd.lib()
+    dd._batch_lib()
+    dd._server_lib()
+    dd._io_lib()
+    checked = 0
+    for name, (void, nparams) in protos.items():
+        fn = getattr(L, name)
+        if fn.argtypes is None:
+            continue
+        assert len(fn.argtypes) == nparams, name
+        assert (fn.restype is None) == void, name
+        checked += 1
+    assert checked >= 50, checked
