@@ -612,13 +612,18 @@ def run_ours(args):
     # --- roofline of the dominant kernel (K2) --------------------------------
     import ctypes as C
     peak = C.c_double()
-    dd.lib().dedisp_b200_alu_probe(local, C.byref(peak))
+    probe = C.CDLL(os.path.join(os.path.dirname(dd.LIB_PATH), "libdedisp_probe.so"))
+    probe.dedisp_probe_alu.restype = C.c_int
+    probe.dedisp_probe_alu.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    if probe.dedisp_probe_alu(local, C.byref(peak)) != 0:
+        raise RuntimeError("integer-pipe probe failed")
     k2_ms = sum(kms) / len(kms)
     adds = float(units) * cfg.nchans
-    # DRAM bytes per K2 launch: ncu captures of each quad-strided shape on the
-    # 2^17-sample case (dram__bytes_read.sum + dram__bytes_write.sum, one launch;
-    # profiles/tdd_quad8_config1_131072samples.md), scaled by the time tiles of
-    # the full launch (every tile streams its own delay band).
+    # DRAM bytes per K2 launch: ncu captures (2026-12-03, --clock-control none)
+    # of each quad-strided shape on the same workload cut to 2^17 samples
+    # (dram__bytes_read.sum + dram__bytes_write.sum of one launch), scaled by
+    # the time tiles of the full launch (every tile streams its own delay
+    # band, so the traffic grows with the tiles).
     # variant ({J, NW} of the library's quad shapes): (bytes in the capture,
     # time tiles in the capture, samples per tile = 128 J)
     captured = {5: (10798106368 + 1397426944, 38, 2560),   # {20, 12}
@@ -630,13 +635,15 @@ def run_ours(args):
         b, tiles_cap, bt = captured[best]
         tiles = -(-nout // bt)
         traffic = round(b / tiles_cap * tiles)
-        traffic_note = f"ncu capture on 2^17 samples ({tiles_cap} tiles) scaled to {tiles} tiles"
+        traffic_note = (f"ncu capture 2026-12-03 of variant {best} on the workload cut to 2^17 samples "
+                        f"({tiles_cap} tiles), scaled to this launch's {tiles} tiles; not measured "
+                        f"in this run")
     achieved = adds / (k2_ms * 1e-3) / 1e12
     roofline = {"bound": "int-alu", "achieved": round(achieved, 3), "peak": round(peak.value / 1e12, 3),
                 "unit": "Tadd/s", "frac": round(achieved * 1e12 / peak.value, 4),
                 "traffic": traffic,
                 "traffic_source": traffic_note,
-                "peak_source": "measured in this run: dedisp_b200_alu_probe (32-bit add "
+                "peak_source": "measured in this run: dedisp_probe_alu (lib/libdedisp_probe.so; 32-bit add "
                                "lane-ops/s, all SMs)",
                 "k2_ms": round(k2_ms, 3), "k1_ms": round(sum(pms) / len(pms), 3),
                 "algorithmic": "nchan=4096 integer adds per DM-trial x sample; "

@@ -118,6 +118,9 @@ def lib() -> C.CDLL:
         "dedisp_b200_last_error": (err, [C.c_char_p, _sz]),
         "dedisp_b200_set_fdd_options": (err, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _sz]),
         "dedisp_b200_output_row_length": (_sz, [_vp, _sz]),
+        "dedisp_b200_set_wait_limit_ns": (err, [C.c_ulonglong]),
+        "dedisp_b200_get_wait_limit_ns": (C.c_ulonglong, []),
+        "dedisp_b200_set_wait_expiry_test": (err, [C.c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -291,6 +294,22 @@ class FDDGPUPlan(Plan):
                                                  precision, int(round_delays), segment_nfft))
 
 
+def set_wait_limit_ns(ns: int) -> None:
+    """Limit of the kernels' bounded waits on their own copies and MMAs
+    (nanoseconds of GPU global time; 0 restores the default, 2 s)."""
+    _check(lib().dedisp_b200_set_wait_limit_ns(int(ns)))
+
+
+def get_wait_limit_ns() -> int:
+    return int(lib().dedisp_b200_get_wait_limit_ns())
+
+
+def set_wait_expiry_test(enable: bool) -> None:
+    """Expiry test: each kernel with bounded waits also waits on a barrier
+    that nothing arrives on, so its error path runs (for tests)."""
+    _check(lib().dedisp_b200_set_wait_expiry_test(1 if enable else 0))
+
+
 def tdd_variant_count(in_nbits: int = 8) -> int:
     """Number of tile-shape variants of the tiled TDD kernel for in_nbits."""
     return int(lib().dedisp_b200_tdd_variant_count(in_nbits))
@@ -323,6 +342,7 @@ _BATCH_SIGS = {
     "dedisp_b200_batch_variant_count": (C.c_int, [_sz]),
     "dedisp_b200_batch_autotune": (C.c_int, [_vp, _vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "dedisp_b200_batch_execute": (C.c_int, [_vp, _vp, C.c_int]),
+    "dedisp_b200_batch_sync": (C.c_int, [_vp, _vp]),
     "dedisp_b200_batch_set_timing": (C.c_int, [_vp, C.c_int]),
     "dedisp_b200_batch_get_timing": (C.c_int, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                                C.POINTER(C.c_int)]),
@@ -410,6 +430,11 @@ class Batch:
 
     def execute(self, stream: int = 0, use_graph: bool = True) -> None:
         _bcheck(_batch_lib().dedisp_b200_batch_execute(self._h, stream, int(use_graph)))
+
+    def sync(self, stream: int = 0) -> None:
+        """Waits for the batch's work on `stream`; raises if a bounded wait
+        of the last execute expired."""
+        _bcheck(_batch_lib().dedisp_b200_batch_sync(self._h, stream))
 
     def set_timing(self, enable: bool = True) -> None:
         _bcheck(_batch_lib().dedisp_b200_batch_set_timing(self._h, int(enable)))

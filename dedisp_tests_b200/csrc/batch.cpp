@@ -67,6 +67,8 @@ TddBatch::TddBatch(size_t nchans, float dt, float f0, float df, int in_nbits, in
     rt::DeviceGuard g(m_device);
     for (auto& e : m_ev) e.reset(new rt::Event(true));
     m_d_delay.reserve(m_delays.size() * 4);
+    m_d_err.reserve(sizeof(unsigned));
+    RT_CHECK(cudaMemset(m_d_err.get(), 0, sizeof(unsigned)));
     RT_CHECK(cudaMemcpy(m_d_delay.get(), m_delays.data(), m_delays.size() * 4, cudaMemcpyHostToDevice));
 }
 
@@ -322,6 +324,7 @@ void TddBatch::upload(Layout& L)
         a.dms = m_d_dms.get<float>() + t.dm_off;
         a.perm = t.perm.empty() ? nullptr : m_d_perm.get<int32_t>() + t.dm_off;
         a.out = t.spec.out;
+        a.err = m_d_err.get<unsigned>();
     }
     L.args = args;
     L.ws = ws;
@@ -342,6 +345,7 @@ void TddBatch::enqueue(cudaStream_t s, const Layout& L, bool timing)
 {
     int launches = 0;
     if (timing) m_ev[0]->record(s);  // never inside a stream capture (see execute)
+    if (L.quad) RT_CHECK(cudaMemsetAsync(m_d_err.get(), 0, sizeof(unsigned), s));
     for (size_t b = 0; b < m_beams.size(); ++b) {
         const BeamState& t = m_beams[b];
         if (t.nout == 0) continue;
@@ -379,6 +383,14 @@ void TddBatch::enqueue(cudaStream_t s, const Layout& L, bool timing)
     }
     if (timing) m_ev[2]->record(s);
     last_launches = launches;
+}
+
+void TddBatch::sync(cudaStream_t stream)
+{
+    rt::DeviceGuard g(m_device);
+    RT_CHECK(cudaStreamSynchronize(stream));
+    if (kern::read_error_word(m_d_err.get<unsigned>(), stream))
+        DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "a staged window copy did not complete");
 }
 
 BatchShape TddBatch::autotune(cudaStream_t stream)
@@ -464,7 +476,7 @@ void TddBatch::execute(cudaStream_t stream, bool use_graph)
     }
     if (record_timing) {
         RT_CHECK(cudaEventSynchronize(m_ev[2]->get()));
-        if (m_layout->quad && kern::tdd_take_error(stream))
+        if (m_layout->quad && kern::read_error_word(m_d_err.get<unsigned>(), stream))
             DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "a staged window copy did not complete");
         if (use_graph) last_k1_ms = -1.f;  // transposes are inside the graph
         else RT_CHECK(cudaEventElapsedTime(&last_k1_ms, m_ev[0]->get(), m_ev[1]->get()));
@@ -611,6 +623,11 @@ dedisp_error dedisp_b200_batch_execute(dedisp_b200_batch batch, void* stream, in
     return batch_call(batch, [&](dedisp::detail::TddBatch& b) {
         b.execute(static_cast<cudaStream_t>(stream), use_graph != 0);
     });
+}
+
+dedisp_error dedisp_b200_batch_sync(dedisp_b200_batch batch, void* stream)
+{
+    return batch_call(batch, [&](dedisp::detail::TddBatch& b) { b.sync(static_cast<cudaStream_t>(stream)); });
 }
 
 dedisp_error dedisp_b200_batch_set_timing(dedisp_b200_batch batch, int enable)

@@ -62,6 +62,9 @@ public:
 
     // Enqueues the whole batch on `stream` (graph: captured once, replayed).
     void execute(cudaStream_t stream, bool use_graph);
+    // Waits for `stream` and throws DEDISP_INTERNAL_GPU_ERROR if a bounded
+    // wait of the last execute's dedispersion expired.
+    void sync(cudaStream_t stream);
 
     size_t beam_count() const { return m_beams.size(); }
     size_t max_delay(size_t beam) const;
@@ -97,6 +100,7 @@ private:
     bool m_dirty = true;
 
     rt::DeviceBuffer m_d_delay, m_d_chan, m_d_cdl, m_d_kmv, m_d_dms, m_d_perm, m_d_args, m_d_start, m_d_nbx;
+    rt::DeviceBuffer m_d_err;  // set by a quad-strided kernel whose bounded wait expired
     rt::DeviceBuffer m_own_ws;
     void* m_ext_ws = nullptr;
     size_t m_ext_ws_bytes = 0;

@@ -359,6 +359,20 @@ dedisp_error dedisp_b200_set_fdd_options(dedisp_plan plan, int segmented, int ti
     });
 }
 
+dedisp_error dedisp_b200_set_wait_limit_ns(unsigned long long ns)
+{
+    dedisp::rt::set_wait_limit_ns(ns);
+    return DEDISP_NO_ERROR;
+}
+
+unsigned long long dedisp_b200_get_wait_limit_ns(void) { return dedisp::rt::wait_limit_ns(); }
+
+dedisp_error dedisp_b200_set_wait_expiry_test(int enable)
+{
+    dedisp::rt::set_wait_expiry_test(enable != 0);
+    return DEDISP_NO_ERROR;
+}
+
 dedisp_size dedisp_b200_output_row_length(dedisp_plan plan, dedisp_size nsamps)
 {
     if (!plan || plan->ptr->get_dm_count() == 0) return 0;

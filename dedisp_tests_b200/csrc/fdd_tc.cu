@@ -45,9 +45,8 @@ constexpr int TC_PRODUCER_WARPS = 16;  // 4 per TMEM lane quadrant
 constexpr int TC_PARTS = TC_PRODUCER_WARPS / 4;  // producers sharing one DM row
 constexpr int TC_PART_CH = 64 / TC_PARTS;        // channels per producer per chunk
 constexpr int TC_THREADS = (TC_PRODUCER_WARPS + 2) * 32;
-// Bounded mbarrier waits: give up after TC_WAIT_NS of global time (checked
+// Bounded mbarrier waits: give up after a.wait_ns of global time (checked
 // every 16 polls) or TC_WAIT_POLLS polls, whichever comes first.
-constexpr uint64_t TC_WAIT_NS = 2000000000ull;
 constexpr uint32_t TC_WAIT_POLLS = 1u << 28;
 // Dynamic shared memory requested per CTA is at least this much so that only
 // one CTA fits on an SM (each CTA allocates all 512 tensor-memory columns).
@@ -66,9 +65,11 @@ struct alignas(8) SmemBarriers {
     uint64_t c_full[2];
     uint64_t c_empty[2];
     uint64_t drain;
+    uint64_t never;       // expiry test: nothing arrives on it
     uint32_t tmem_base;
     uint32_t abort_flag;  // a producer gave up a bounded wait (delay-table mode)
 };
+static_assert(sizeof(SmemBarriers) <= 256, "barriers precede the phasor table at +256 bytes");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
@@ -100,7 +101,7 @@ __device__ __forceinline__ uint64_t global_ns()
 }
 
 // Bounded wait for phase `parity` of barrier b; false if the limit expired.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity)
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, uint64_t limit_ns)
 {
     const uint32_t addr = smem_u32(b);
     uint64_t t0 = 0;
@@ -117,7 +118,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity)
         if ((i & 15u) == 15u) {
             const uint64_t t = global_ns();
             if (t0 == 0) t0 = t;
-            else if (t - t0 > TC_WAIT_NS) return false;
+            else if (t - t0 > limit_ns) return false;
         }
     }
     return false;
@@ -125,9 +126,9 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity)
 
 // The same wait for a whole warp, with one outcome for all its lanes (the
 // tensor-memory loads and stores that follow are warp-collective).
-__device__ __forceinline__ bool mbar_wait_warp(uint64_t* b, uint32_t parity)
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* b, uint32_t parity, uint64_t limit_ns)
 {
-    const bool done = mbar_wait(b, parity);
+    const bool done = mbar_wait(b, parity, limit_ns);
     return __all_sync(0xFFFFFFFFu, done);
 }
 
@@ -293,6 +294,7 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
             mbar_init(&bars->c_empty[i], TC_PRODUCER_WARPS);
         }
         mbar_init(&bars->drain, 1);
+        mbar_init(&bars->never, 1);
         bars->abort_flag = 0u;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -324,7 +326,7 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
 
         auto epilogue = [&](int it, size_t kk) -> bool {
             const uint32_t cb = (uint32_t)it & 1u;
-            if (!mbar_wait_warp(&bars->c_full[cb], ((uint32_t)it >> 1) & 1u)) return false;
+            if (!mbar_wait_warp(&bars->c_full[cb], ((uint32_t)it >> 1) & 1u, a.wait_ns)) return false;
             tc_fence_after();
             const uint32_t ccol = cb ? TM_C1 : TM_C0;
             const int sh = (a.nseg + TC_PARTS - 1) / TC_PARTS;
@@ -404,7 +406,7 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
                             lo[i] = __byte_perm(t.y, 0u, sy.x) ^ sy.y;
                         }
                     }
-                    if (!mbar_wait_warp(&bars->a_empty[buf], ((g >> 1) & 1u) ^ 1u)) { ok = false; break; }
+                    if (!mbar_wait_warp(&bars->a_empty[buf], ((g >> 1) & 1u) ^ 1u, a.wait_ns)) { ok = false; break; }
                     tc_fence_after();
                     const uint32_t acol = buf ? TM_A1 : TM_A0;
                     tmem_st16(tmem + lane_addr + acol + part * TC_PART_CH, hi);
@@ -427,7 +429,7 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
             for (size_t k = k_begin; k < k_end && ok; ++k) {
                 for (int ch = 0; ch < nchunks; ++ch, ++g) {
                     const uint32_t st = g % (uint32_t)nst;
-                    if (!mbar_wait(&bars->b_empty[st], ((g / nst) & 1u) ^ 1u)) { ok = false; break; }
+                    if (!mbar_wait(&bars->b_empty[st], ((g / nst) & 1u) ^ 1u, a.wait_ns)) { ok = false; break; }
                     mbar_expect_tx(&bars->b_full[st], stage_bytes);
                     uint8_t* dst = s_b + st * stage_bytes;
                     // coordinates: (kk, n, split, bin)
@@ -440,7 +442,7 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
             // do not leave while loads are in flight: wait for the last stages
             const uint32_t issued = g;
             for (uint32_t j = (issued > (uint32_t)nst ? issued - nst : 0); j < issued; ++j)
-                mbar_wait(&bars->b_full[j % nst], (j / nst) & 1u);
+                mbar_wait(&bars->b_full[j % nst], (j / nst) & 1u, a.wait_ns);
         }
     } else {
         // --- MMA issuer ----------------------------------------------------------
@@ -451,13 +453,15 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
             int bin_iter = 0;
             for (size_t k = k_begin; k < k_end && ok; ++k, ++bin_iter) {
                 const uint32_t cb = (uint32_t)bin_iter & 1u;
-                if (!mbar_wait(&bars->c_empty[cb], (((uint32_t)bin_iter >> 1) & 1u) ^ 1u)) { ok = false; break; }
+                if (!mbar_wait(&bars->c_empty[cb], (((uint32_t)bin_iter >> 1) & 1u) ^ 1u, a.wait_ns)) { ok = false; break; }
                 tc_fence_after();
                 const uint32_t dcol = tmem + (cb ? TM_C1 : TM_C0);
                 for (int ch = 0; ch < nchunks; ++ch, ++g) {
                     const uint32_t buf = g & 1u, st = g % (uint32_t)nst;
-                    if (!mbar_wait(&bars->a_full[buf], (g >> 1) & 1u)) { ok = false; break; }
-                    if (!mbar_wait(&bars->b_full[st], (g / nst) & 1u)) { ok = false; break; }
+                    if (!mbar_wait(&bars->a_full[buf], (g >> 1) & 1u, a.wait_ns)) { ok = false; break; }
+                    if (!mbar_wait(&bars->b_full[st], (g / nst) & 1u, a.wait_ns)) { ok = false; break; }
+                    // expiry test: one more wait, on a barrier nothing arrives on
+                    if (a.wait_test && g == 0 && !mbar_wait(&bars->never, 0u, a.wait_ns)) { ok = false; break; }
                     tc_fence_after();
                     const uint32_t acol = tmem + (buf ? TM_A1 : TM_A0);
                     const uint32_t bbase = smem_u32(s_b + st * stage_bytes);
@@ -480,7 +484,7 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
             }
             // all issued MMAs complete before the accumulator memory goes away
             mma_commit(&bars->drain);
-            mbar_wait(&bars->drain, 0);
+            mbar_wait(&bars->drain, 0, a.wait_ns);
         }
     }
     if (!ok) atomicExch(a.err, 1u);
@@ -683,7 +687,10 @@ void launch_fdd_mac_tc(const TcMacArgs& a, const void* B, cudaStream_t s)
     const int ntiles = (a.ndm + TC_M - 1) / TC_M;
     int ngroups = std::max(1, sms / ntiles);
     ngroups = (int)std::min<size_t>((size_t)ngroups, a.nbins);
-    fdd_mac_tc_kernel<<<ntiles * ngroups, TC_THREADS, smem, s>>>(map, a);
+    TcMacArgs ka = a;
+    ka.wait_ns = rt::wait_limit_ns();
+    ka.wait_test = rt::wait_expiry_test() ? 1 : 0;
+    fdd_mac_tc_kernel<<<ntiles * ngroups, TC_THREADS, smem, s>>>(map, ka);
     RT_CHECK(cudaGetLastError());
 }
 

@@ -32,6 +32,8 @@ struct TcMacArgs {
     int round_delays;
     int dmax;                  // >= 0: delay-table mode, every delay in 0..dmax; -1: quarter-wave mode
     int stages;                // B pipeline depth (tc_stages)
+    unsigned long long wait_ns = 2000000000ull;  // bounded-wait limit (rt::wait_limit_ns)
+    int wait_test = 0;         // expiry test (rt::wait_expiry_test)
 };
 
 // Shapes the tensor-core MAC handles: 2*nseg <= 128 output columns, a

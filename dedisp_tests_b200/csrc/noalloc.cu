@@ -47,7 +47,6 @@ static __device__ __align__(256) float g_noalloc_dms[kMaxDms];
 static __device__ __align__(256) int32_t g_noalloc_perm[kMaxDms];
 static __device__ __align__(256) float g_noalloc_delays[kMaxChans + 1];
 static __device__ __align__(256) int32_t g_noalloc_chan[kMaxChans + kListPad];
-static __device__ __align__(256) uint32_t g_noalloc_km[kMaxChans + kListPad];
 
 namespace {
 
@@ -58,7 +57,6 @@ struct DeviceSymbols {
     int32_t* perm = nullptr;
     float* delays = nullptr;
     int32_t* chan = nullptr;
-    uint32_t* km = nullptr;
 };
 
 constexpr int kMaxDevices = 64;
@@ -73,12 +71,22 @@ dedisp_error fail(dedisp_error code, const char* msg)
     return code;
 }
 
-// Resolves the device addresses of the arrays for the current device.
-dedisp_error symbols_for_current_device(DeviceSymbols** out)
+// Resolves the device addresses of the arrays for the current device, which
+// must be the device of `stream` (the arrays' addresses differ per device).
+dedisp_error symbols_for_current_device(cudaStream_t stream, DeviceSymbols** out)
 {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
         return fail(DEDISP_INVALID_DEVICE_INDEX, "no usable current CUDA device");
+    if (stream) {
+        int sdev = -1;
+        if (cudaStreamGetDevice(stream, &sdev) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(DEDISP_INVALID_DEVICE_INDEX, "cannot query the stream's device");
+        }
+        if (sdev != dev)
+            return fail(DEDISP_INVALID_DEVICE_INDEX, "the stream belongs to another device than the current one");
+    }
     std::lock_guard<std::mutex> lock(g_symbols_mutex);
     DeviceSymbols& s = g_symbols[dev];
     if (!s.ready) {
@@ -86,8 +94,7 @@ dedisp_error symbols_for_current_device(DeviceSymbols** out)
             cudaGetSymbolAddress((void**)&s.dms, g_noalloc_dms) != cudaSuccess ||
             cudaGetSymbolAddress((void**)&s.perm, g_noalloc_perm) != cudaSuccess ||
             cudaGetSymbolAddress((void**)&s.delays, g_noalloc_delays) != cudaSuccess ||
-            cudaGetSymbolAddress((void**)&s.chan, g_noalloc_chan) != cudaSuccess ||
-            cudaGetSymbolAddress((void**)&s.km, g_noalloc_km) != cudaSuccess) {
+            cudaGetSymbolAddress((void**)&s.chan, g_noalloc_chan) != cudaSuccess) {
             cudaGetLastError();
             return fail(DEDISP_INTERNAL_GPU_ERROR, "cudaGetSymbolAddress failed");
         }
@@ -110,6 +117,7 @@ extern "C" dedisp_error dedisp_b200_tdd_execute_noalloc(
     dedisp_byte* d_out, dedisp_size out_nbits, dedisp_size out_stride, void* stream)
 {
     using namespace dedisp;
+    t_noalloc_msg.clear();  // the message describes this call's failure only
     if (!dm_list || !d_in || !d_out) return fail(DEDISP_INVALID_POINTER, "NULL pointer");
     if (dm_count == 0) return fail(DEDISP_NO_DM_LIST_SET, "empty DM list");
     if (!valid_nbits(in_nbits) || (nchans * in_nbits) % 32 != 0)
@@ -174,6 +182,7 @@ extern "C" dedisp_error dedisp_b200_tdd_execute_noalloc(
         }
     }
     const size_t win = round_up((span + 4 * spw - 1) / spw + 32 * J + 1, 4);
+    if (win > ((size_t)1 << 26)) return fail(DEDISP_UNKNOWN_ERROR, "DM spacing too wide for the tiled kernel");
     const int cs = kern::tiled_stage_channels(nbits, (int)win, 0);
     if (cs < 2) return fail(DEDISP_UNKNOWN_ERROR, "DM spacing too wide for the tiled kernel");
     const int nstages = std::max(1, (nact + cs - 1) / cs);
@@ -188,7 +197,7 @@ extern "C" dedisp_error dedisp_b200_tdd_execute_noalloc(
                     "(nsamps - max_delay + max delay) samples must fit");
 
     DeviceSymbols* sym = nullptr;
-    const dedisp_error se = symbols_for_current_device(&sym);
+    const dedisp_error se = symbols_for_current_device(static_cast<cudaStream_t>(stream), &sym);
     if (se != DEDISP_NO_ERROR) return se;
 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -215,7 +224,7 @@ extern "C" dedisp_error dedisp_b200_tdd_execute_noalloc(
         da.chan_list = sym->chan;
         da.nact = nact;
         da.nstages = nstages;
-        da.km_vals = sym->km;
+        da.km_vals = nullptr;  // the tiled kernel reads no per-channel multipliers (0/1 mask)
         da.delay_table = sym->delays;
         da.dms = sym->dms;
         da.perm = sym->perm;

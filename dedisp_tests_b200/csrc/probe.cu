@@ -1,6 +1,7 @@
-// Integer-pipe throughput probe (extension, used by the benchmark to state
-// the roofline of the TDD kernel, which is bound by 32-bit integer
-// instruction issue rather than by HBM or tensor cores).
+// Integer-pipe throughput probe: a measurement tool of the benchmark, built
+// into its own library (lib/libdedisp_probe.so), not into libdedisp.so. It
+// states the roofline of the TDD kernel, which is bound by 32-bit integer
+// instruction issue rather than by HBM or tensor cores.
 //
 // Each thread runs 8 independent chains of 32-bit adds; the result is the
 // measured rate of 32-bit integer add lane-operations per second on the
@@ -9,8 +10,7 @@
 
 #include <cstdint>
 
-#include "dedisp_b200.h"
-#include "runtime.hpp"
+#include "dedisp.h"
 
 namespace {
 
@@ -36,34 +36,45 @@ __global__ void __launch_bounds__(512) alu_probe_kernel(uint32_t* sink, int iter
 
 }  // namespace
 
-extern "C" dedisp_error dedisp_b200_alu_probe(int device, double* lane_adds_per_s)
+// 32-bit integer add lane-operations per second on `device` (the caller's
+// current device is restored).
+extern "C" dedisp_error dedisp_probe_alu(int device, double* lane_adds_per_s)
 {
-    try {
-        dedisp::rt::DeviceGuard guard(device);
-        cudaDeviceProp prop;
-        RT_CHECK(cudaGetDeviceProperties(&prop, device));
-        const int blocks = prop.multiProcessorCount * 4;
-        const int threads = 512;
-        const int iters = 4096;
-        uint32_t* sink = nullptr;
-        RT_CHECK(cudaMalloc(&sink, blocks * sizeof(uint32_t)));
-        cudaEvent_t e0, e1;
-        RT_CHECK(cudaEventCreate(&e0));
-        RT_CHECK(cudaEventCreate(&e1));
+    if (!lane_adds_per_s) return DEDISP_INVALID_POINTER;
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return DEDISP_INVALID_DEVICE_INDEX;
+    }
+    cudaDeviceProp prop;
+    uint32_t* sink = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    float ms = 0.f;
+    const int threads = 512, iters = 4096;
+    int blocks = 0;
+    bool ok = cudaGetDeviceProperties(&prop, device) == cudaSuccess;
+    if (ok) {
+        blocks = prop.multiProcessorCount * 4;
+        ok = cudaMalloc(&sink, blocks * sizeof(uint32_t)) == cudaSuccess &&
+             cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess;
+    }
+    if (ok) {
         alu_probe_kernel<<<blocks, threads>>>(sink, 64, 7u);  // warm-up
-        RT_CHECK(cudaEventRecord(e0));
+        cudaEventRecord(e0);
         for (int r = 0; r < 5; ++r) alu_probe_kernel<<<blocks, threads>>>(sink, iters, 7u + r);
-        RT_CHECK(cudaEventRecord(e1));
-        RT_CHECK(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        RT_CHECK(cudaEventElapsedTime(&ms, e0, e1));
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        cudaFree(sink);
-        const double ops = 5.0 * blocks * threads * (double)iters * 16.0;
-        *lane_adds_per_s = ops / (ms * 1e-3);
-        return DEDISP_NO_ERROR;
-    } catch (...) {
+        cudaEventRecord(e1);
+        ok = cudaGetLastError() == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
+             cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && ms > 0.f;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (sink) cudaFree(sink);
+    cudaSetDevice(prev);
+    if (!ok) {
+        cudaGetLastError();
         return DEDISP_INTERNAL_GPU_ERROR;
     }
+    const double ops = 5.0 * blocks * threads * (double)iters * 16.0;
+    *lane_adds_per_s = ops / (ms * 1e-3);
+    return DEDISP_NO_ERROR;
 }

@@ -1,6 +1,8 @@
 // CUDA runtime RAII helpers (see runtime.hpp) and the error helpers.
 #include "runtime.hpp"
 
+#include <atomic>
+
 #include <cstdio>
 #include <map>
 #include <mutex>
@@ -136,6 +138,16 @@ void raise_smem_limit(const void* kfn, size_t bytes)
     RT_CHECK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     have = bytes;
 }
+
+namespace {
+std::atomic<unsigned long long> g_wait_limit_ns{kDefaultWaitLimitNs};
+std::atomic<bool> g_wait_expiry_test{false};
+}  // namespace
+
+unsigned long long wait_limit_ns() { return g_wait_limit_ns.load(); }
+void set_wait_limit_ns(unsigned long long ns) { g_wait_limit_ns.store(ns ? ns : kDefaultWaitLimitNs); }
+bool wait_expiry_test() { return g_wait_expiry_test.load(); }
+void set_wait_expiry_test(bool on) { g_wait_expiry_test.store(on); }
 
 }  // namespace rt
 }  // namespace dedisp

@@ -116,5 +116,19 @@ void raise_smem_limit(K* kfn, size_t bytes)
     raise_smem_limit(reinterpret_cast<const void*>(kfn), bytes);
 }
 
+// Kernels that poll an mbarrier for their own asynchronous copies or
+// tensor-core work (the quad-strided TDD kernels, the tensor-core FDD MAC)
+// give up after this many nanoseconds of global time, record an error that
+// the plan reports as DEDISP_INTERNAL_GPU_ERROR, wait (again bounded) for
+// their own work in flight and return. Process-wide; read at each launch.
+constexpr unsigned long long kDefaultWaitLimitNs = 2000000000ull;
+unsigned long long wait_limit_ns();
+void set_wait_limit_ns(unsigned long long ns);  // 0 restores the default (2 s)
+// Expiry test: each such kernel additionally waits (bounded by the limit)
+// on an mbarrier that nothing arrives on, at the first wait of its
+// pipeline, so the expiry path runs deterministically.
+bool wait_expiry_test();
+void set_wait_expiry_test(bool on);
+
 }  // namespace rt
 }  // namespace dedisp

@@ -245,6 +245,10 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
     cudaStream_t h2d = m_gpu.h2d->get();
     cudaStream_t d2h = m_gpu.d2h->get();
     uint32_t* tr = m_tr.get<uint32_t>();
+    if (quad) {
+        m_err.reserve(sizeof(unsigned));
+        RT_CHECK(cudaMemsetAsync(m_err.get(), 0, sizeof(unsigned), ex));
+    }
 
     const float in_range = (float)(nbits == 32 ? 0xFFFFFFFFu : ((1u << nbits) - 1u));
     const float den = in_range * (float)v.nchans;
@@ -355,6 +359,7 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
             da.win_words = s.win_words;
             da.chan_per_stage = s.chan_per_stage;
             da.variant = s.variant;
+            da.err = m_err.get<unsigned>();
             if (s.identity) {
                 da.perm = nullptr;
                 da.out = out_base + s0 * out_elems_stride * ob;
@@ -390,7 +395,7 @@ void TddEngine::execute(const TddView& v, const TddCall& c)
     if (!async) {
         RT_CHECK(cudaStreamSynchronize(ex));
         if (!dev_out) RT_CHECK(cudaStreamSynchronize(d2h));
-        if (quad && kern::tdd_take_error(ex))
+        if (quad && kern::read_error_word(m_err.get<unsigned>(), ex))
             DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "a staged window copy did not complete");
     }
     if (record_timing) {

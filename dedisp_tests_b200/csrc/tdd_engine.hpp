@@ -81,6 +81,7 @@ private:
     GpuState& m_gpu;
     std::unique_ptr<Setup> m_setup;
     rt::DeviceBuffer m_chan, m_cdl, m_km, m_dms, m_perm, m_tr, m_q, m_out[2], m_stage[2];
+    rt::DeviceBuffer m_err;  // set by a quad-strided kernel whose bounded wait expired
     std::vector<std::unique_ptr<rt::Event>> m_events;
     rt::Event& event(size_t i);
 };

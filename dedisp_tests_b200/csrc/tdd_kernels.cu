@@ -208,7 +208,6 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 
 // Set by a kernel whose bounded wait expired (device-wide; read and cleared
 // by tdd_take_error).
-__device__ unsigned g_tdd_error;
 
 // mbarrier + bulk asynchronous copy (global -> shared, no multicast).
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -237,8 +236,18 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                  "l"(src), "r"(bytes), "r"(smem_addr(b))
                  : "memory");
 }
-// Wait for phase `parity` of b; false after about 2 s of global time.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, uint32_t parity)
+// Limit of the bounded mbarrier waits (nanoseconds of global time) and the
+// expiry test switch (rt::wait_limit_ns, rt::wait_expiry_test), passed to
+// the kernels by value.
+struct WaitCfg {
+    unsigned long long ns;
+    int expiry_test;
+};
+WaitCfg wait_cfg() { return WaitCfg{rt::wait_limit_ns(), rt::wait_expiry_test() ? 1 : 0}; }
+
+// Wait for phase `parity` of b; false after limit_ns of global time (checked
+// every 16 polls) or 2^28 polls.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, uint32_t parity, unsigned long long limit_ns)
 {
     const uint32_t addr = smem_addr(b);
     uint64_t t0 = 0;
@@ -256,7 +265,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, uint32_t parity)
             uint64_t t;
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
             if (t0 == 0) t0 = t;
-            else if (t - t0 > 2000000000ull) return false;
+            else if (t - t0 > limit_ns) return false;
         }
     }
     return false;
@@ -837,7 +846,7 @@ __device__ __forceinline__ void lds_lane_words(uint32_t addr, uint32_t (&w)[J],
 }
 
 template <int J, int NW>
-__device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size_t by, uint32_t one)
+__device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size_t by, uint32_t one, WaitCfg wc)
 {
     constexpr int P = 32 * J;
     constexpr int NT = NW * 32;
@@ -848,6 +857,7 @@ __device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size
     __shared__ int32_t s_cl[2][Q8_MAX_STAGE];  // channel of each row, stages fetched ahead
     __shared__ float s_cdl[2][Q8_MAX_STAGE];   // its delay
     __shared__ uint64_t s_full[2];             // window copies of stage buffer b landed
+    __shared__ uint64_t s_never;               // expiry test: nothing arrives on it
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int i0 = bx * NW;
@@ -866,6 +876,7 @@ __device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size
     if (threadIdx.x == 0) {
         mbar_init(&s_full[0], NW);
         mbar_init(&s_full[1], NW);
+        mbar_init(&s_never, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     uint32_t vmax = 0;
@@ -973,13 +984,15 @@ __device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size
         const int buf = s & 1;
         const int cs = stage_size(s);
         asm volatile("cp.async.wait_group 0;\n" ::);
-        const bool landed = mbar_wait_bounded(&s_full[buf], ((uint32_t)s >> 1) & 1u);
+        bool landed = mbar_wait_bounded(&s_full[buf], ((uint32_t)s >> 1) & 1u, wc.ns);
+        // expiry test: one more wait, on a barrier nothing arrives on
+        if (wc.expiry_test && s == 0) landed = landed && mbar_wait_bounded(&s_never, 0u, wc.ns);
         // stage s landed; every warp is done with stage s - 1
         if (__syncthreads_or(!landed)) {
             // a copy did not complete: wait (bounded) for this stage's copies,
             // the only ones in flight, record the error and leave
-            mbar_wait_bounded(&s_full[buf], ((uint32_t)s >> 1) & 1u);
-            if (threadIdx.x == 0) atomicExch(&g_tdd_error, 1u);
+            mbar_wait_bounded(&s_full[buf], ((uint32_t)s >> 1) & 1u, wc.ns);
+            if (threadIdx.x == 0) atomicExch(a.err, 1u);
             failed = true;
             break;
         }
@@ -1025,24 +1038,25 @@ __device__ __forceinline__ void quad8_tile(const DedisperseArgs& a, int bx, size
     if (threadIdx.x == 0) {
         mbar_inval(&s_full[0]);
         mbar_inval(&s_full[1]);
+        mbar_inval(&s_never);
     }
 }
 
 template <int J, int NW>
-__global__ void __launch_bounds__(NW * 32, 1) dedisperse_quad8_kernel(DedisperseArgs a, uint32_t one)
+__global__ void __launch_bounds__(NW * 32, 1) dedisperse_quad8_kernel(DedisperseArgs a, uint32_t one, WaitCfg wc)
 {
-    quad8_tile<J, NW>(a, blockIdx.x, blockIdx.y, one);
+    quad8_tile<J, NW>(a, blockIdx.x, blockIdx.y, one, wc);
 }
 
 template <int J, int NW>
 __global__ void __launch_bounds__(NW * 32, 1)
 dedisperse_quad8_batch_kernel(const DedisperseArgs* __restrict__ args,
                               const unsigned long long* __restrict__ item_start,
-                              const int* __restrict__ nbx, int nbeams, uint32_t one)
+                              const int* __restrict__ nbx, int nbeams, uint32_t one, WaitCfg wc)
 {
     static_assert(sizeof(DedisperseArgs) + 16 <= kBatchStaticSmem, "static shared memory of the batch form");
     batch_items(args, item_start, nbx, nbeams,
-                [&](const DedisperseArgs& a, int bx, size_t by) { quad8_tile<J, NW>(a, bx, by, one); });
+                [&](const DedisperseArgs& a, int bx, size_t by) { quad8_tile<J, NW>(a, bx, by, one, wc); });
 }
 
 template <int J, int NW>
@@ -1072,7 +1086,7 @@ void launch_quad8_shape(const DedisperseArgs& a, cudaStream_t s)
         DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "quad-strided window does not fit shared memory");
     rt::raise_smem_limit(dedisperse_quad8_kernel<J, NW>, smem);
     dim3 grid((a.ndm + NW - 1) / NW, (unsigned)((a.nsamp_out + 128 * J - 1) / (128 * J)));
-    dedisperse_quad8_kernel<J, NW><<<grid, NW * 32, smem, s>>>(a, 1u);
+    dedisperse_quad8_kernel<J, NW><<<grid, NW * 32, smem, s>>>(a, 1u, wait_cfg());
     RT_CHECK(cudaGetLastError());
 }
 
@@ -1119,7 +1133,7 @@ void launch_quad8_batch_shape(const BatchLaunch& b, cudaStream_t s)
     if (per_sm < 1) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "batch kernel does not fit on an SM");
     const unsigned long long want = (unsigned long long)sms * per_sm;
     const unsigned grid = (unsigned)std::max<unsigned long long>(1, std::min(want, b.total_items));
-    kfn<<<grid, NW * 32, smem, s>>>(b.args, b.item_start, b.nbx, b.nbeams, 1u);
+    kfn<<<grid, NW * 32, smem, s>>>(b.args, b.item_start, b.nbx, b.nbeams, 1u, wait_cfg());
     RT_CHECK(cudaGetLastError());
 }
 
@@ -1177,17 +1191,12 @@ void launch_transpose_n(const TransposeArgs& a, cudaStream_t s)
 // Variants per input width: 8-bit 0-4 packed-row shapes (T8_SHAPES), 5-8
 // quad-strided shapes (Q8_SHAPES); 1/2/4-bit 0 the generic packed-row kernel,
 // 1-4 the quad-strided shapes (samples widened to bytes); 16/32-bit 0 only.
-bool tdd_take_error(cudaStream_t s)
+unsigned read_error_word(const unsigned* d_err, cudaStream_t s)
 {
     unsigned v = 0;
-    RT_CHECK(cudaMemcpyFromSymbolAsync(&v, g_tdd_error, sizeof(v), 0, cudaMemcpyDeviceToHost, s));
+    RT_CHECK(cudaMemcpyAsync(&v, d_err, sizeof(v), cudaMemcpyDeviceToHost, s));
     RT_CHECK(cudaStreamSynchronize(s));
-    if (v) {
-        static const unsigned zero = 0;
-        RT_CHECK(cudaMemcpyToSymbolAsync(g_tdd_error, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, s));
-        RT_CHECK(cudaStreamSynchronize(s));
-    }
-    return v != 0;
+    return v;
 }
 
 int tiled_variant_count(int nbits)
@@ -1366,7 +1375,10 @@ void launch_dedisperse_tiled_batch(const BatchLaunch& b, int nbits, int variant,
 void launch_dedisperse_tiled(const DedisperseArgs& a, cudaStream_t s)
 {
     // quad-strided rows hold bytes whatever the input width
-    switch (quad_shape(a.nbits, a.variant)) {
+    const int qs = quad_shape(a.nbits, a.variant);
+    if (qs >= 0 && a.err == nullptr)
+        DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "quad-strided launch without an error word");
+    switch (qs) {
     case 0: launch_quad8_variant<0>(a, s); return;
     case 1: launch_quad8_variant<1>(a, s); return;
     case 2: launch_quad8_variant<2>(a, s); return;

@@ -54,6 +54,8 @@ struct DedisperseArgs {
     int win_words;              // tiled: staged window per channel (words)
     int chan_per_stage;         // tiled: channels per pipeline stage (even)
     int variant;                // tiled: tile-shape variant (8-bit input)
+    unsigned* err;              // quad-strided: device word set to 1 when a bounded
+                                // wait on the staged copies expired (required)
 };
 
 // Tile geometry of the tiled kernel for a given input width and tile-shape
@@ -92,9 +94,8 @@ struct QuadDirectArgs {
 };
 void launch_quad_direct(const QuadDirectArgs& a, cudaStream_t s);
 
-// True if a quad-strided kernel gave up a bounded wait on its staged copies
-// since the last call (device-wide flag, cleared; synchronises s).
-bool tdd_take_error(cudaStream_t s);
+// Value of a kernel error word (synchronises s first).
+unsigned read_error_word(const unsigned* d_err, cudaStream_t s);
 
 void launch_dedisperse_plain(const DedisperseArgs& a, cudaStream_t s);
 void launch_dedisperse_tiled(const DedisperseArgs& a, cudaStream_t s);

@@ -63,10 +63,21 @@ dedisp_error dedisp_b200_set_fdd_options(dedisp_plan plan, int segmented, int ti
                                          int precision, int round_delays,
                                          dedisp_size segment_nfft);
 
-/* Measures the device's 32-bit integer add throughput (lane-adds per
- * second) with a kernel of independent add chains on every SM. Used to
- * state the roofline of the integer-bound TDD kernel. */
-dedisp_error dedisp_b200_alu_probe(int device, double* lane_adds_per_s);
+/* Bounded device waits. No counterpart in the reference (its kernels do not
+ * wait on asynchronous copies). The quad-strided TDD kernels and the
+ * tensor-core FDD MAC poll mbarriers for their own bulk copies and MMAs; a
+ * poll that has not seen its phase complete after `ns` nanoseconds of GPU
+ * global time gives up: the kernel waits (bounded again) for its own work
+ * still in flight, frees its tensor memory and returns, and the plan's
+ * execute fails with DEDISP_INTERNAL_GPU_ERROR (dedisp_b200_last_error); the
+ * plan stays usable. Process-wide, read at each launch (a captured CUDA graph
+ * keeps the values of its capture). ns = 0 restores the default, 2 s.
+ * With the expiry test enabled, each of those kernels additionally waits, at
+ * the first wait of its pipeline, on an mbarrier that nothing arrives on, so
+ * that the limit expires and the error path runs; for tests only. */
+dedisp_error dedisp_b200_set_wait_limit_ns(unsigned long long ns);
+unsigned long long dedisp_b200_get_wait_limit_ns(void);
+dedisp_error dedisp_b200_set_wait_expiry_test(int enable);
 
 /* Allocation-free time-domain dedispersion. No counterpart in the reference.
  *
@@ -86,9 +97,12 @@ dedisp_error dedisp_b200_alu_probe(int device, double* lane_adds_per_s);
  * channel-major copy, (nchans + 1) x (nsamps rounded up + padding) samples,
  * does not fit are rejected with DEDISP_MEM_ALLOC_FAILED. The first call on
  * a device looks up the arrays' device addresses (cudaGetSymbolAddress) and
- * should therefore come before any stream capture on that device. All calls
- * share the scratch: calls that overlap on the GPU race. On failure,
- * dedisp_b200_noalloc_last_message() describes the reason. */
+ * should therefore come before any stream capture on that device; `stream`
+ * (NULL: the legacy default stream) must belong to the current device
+ * (DEDISP_INVALID_DEVICE_INDEX otherwise). All calls share the scratch:
+ * calls that overlap on the GPU race. On failure,
+ * dedisp_b200_noalloc_last_message() describes the reason; after a
+ * successful call it is empty. */
 dedisp_error dedisp_b200_tdd_execute_noalloc(
     dedisp_size nchans, dedisp_float dt, dedisp_float f0, dedisp_float df,
     const dedisp_float* dm_list, dedisp_size dm_count, const dedisp_bool* killmask,
@@ -143,6 +157,10 @@ dedisp_error dedisp_b200_batch_set_shape(dedisp_b200_batch batch, int variant, i
 dedisp_error dedisp_b200_batch_autotune(dedisp_b200_batch batch, void* stream, int* variant,
                                         int* chan_per_stage);
 dedisp_error dedisp_b200_batch_execute(dedisp_b200_batch batch, void* stream, int use_graph);
+/* Waits for the batch's work on `stream`; DEDISP_INTERNAL_GPU_ERROR if a
+ * bounded wait of the last execute expired (dedisp_b200_set_wait_limit_ns).
+ * With timing enabled execute performs this check itself. */
+dedisp_error dedisp_b200_batch_sync(dedisp_b200_batch batch, void* stream);
 /* Device time of the last execute's transposes and dedispersion (with
  * timing enabled; execute then waits for its work). With use_graph the
  * transposes are inside the graph: transpose_ms is -1 and dedisperse_ms is

@@ -14,7 +14,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
-REFERENCE_ROOT = "/root/reference"
+# Root of the reference source tree (read only; present where the oracle is
+# pinned, absent on machines that only run the prebuilt pieces). Override
+# with DEDISP_REFERENCE_ROOT, as REF overrides it in oracle/ref/Makefile.
+REFERENCE_ROOT = os.environ.get("DEDISP_REFERENCE_ROOT", "/root/reference")
 
 _u8p = C.POINTER(C.c_uint8)
 _f32p = C.POINTER(C.c_float)

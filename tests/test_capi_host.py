@@ -256,3 +256,15 @@ def test_python_binding_matches_the_headers():
         assert (fn.restype is None) == void, name
         checked += 1
     assert checked >= 50, checked
+
+
+def test_wait_limit_setting_round_trip():
+    """The bounded-wait limit is process-wide; 0 restores the 2 s default."""
+    try:
+        dd.set_wait_limit_ns(12345)
+        assert dd.get_wait_limit_ns() == 12345
+        dd.set_wait_expiry_test(True)
+        dd.set_wait_expiry_test(False)
+    finally:
+        dd.set_wait_limit_ns(0)
+    assert dd.get_wait_limit_ns() == 2_000_000_000

@@ -141,6 +141,31 @@ def test_device_pointers():
     assert rel < FP32_REL_L2 and mx < FP32_MAX_ABS
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_spectrum_output_on_device_pointers(precision):
+    """The whole-series spectrum (the fork's default output,
+    src/fdd/FDDGPUPlan.hpp:6) kept on the device: device input and output
+    rows, both MAC forms, against the FP64 spectrum."""
+    import torch
+    nchans, nsamps = 128, 30000
+    inp, params = _input(nchans, nsamps, 17)
+    dms = np.linspace(0, 90, 40, dtype=np.float32)
+    p = _plan(params, dms, segmented=0, precision=precision)
+    p.set_timing(True)
+    row = p.output_row_length(nsamps)
+    assert row == po.fdd_nfft_spectrum(nsamps, p.get_max_delay())
+    d_in = torch.from_numpy(inp).cuda()
+    d_out = torch.full((len(dms), row), 3.0, dtype=torch.float32, device="cuda")
+    p.execute(nsamps, d_in, 8, d_out, 32, dd.DEDISP_DEVICE_POINTERS)
+    torch.cuda.synchronize()
+    assert p.get_timing()["variant"] == precision
+    x = _oracle_x(inp, nsamps, params, 8)
+    ref = po.fdd_spectrum(x, _delays(params), np.ones(nchans, np.int32), dms, row)
+    rel, mx = _errs(d_out.cpu().numpy(), ref)
+    lim = (FP32_REL_L2, FP32_MAX_ABS) if precision == 0 else (1e-5, 1e-4)
+    assert rel < lim[0] and mx < lim[1], (precision, rel, mx)
+
+
 def test_use_segmented_environment(monkeypatch):
     nchans, nsamps = 64, 40000
     inp, params = _input(nchans, nsamps, 13)

@@ -57,6 +57,7 @@ def _case(nchans, nbits, nsamps, dms, km, seed, out_nbits):
             d_in.data_ptr(), nbits, packed.shape[1], got.data_ptr(), out_nbits,
             nout * out_nbits // 8, stream)
     assert rc == 0, msg()
+    assert msg() == b"", "the message must be empty after a successful call"
     torch.cuda.synchronize()
     return got, expect
 
@@ -77,6 +78,25 @@ def test_noalloc_matches_plan_on_two_consecutive_calls():
     assert torch.equal(got, expect)
 
 
+@pytest.mark.parametrize("in_nbits", [1, 4, 16, 32])
+def test_noalloc_other_widths_8bit_output(in_nbits):
+    """Input widths whose tiled-kernel instances the calls above do not reach,
+    with 8-bit (clipped) output, two calls in a row."""
+    import torch
+    for seed in (11, 12):
+        got, expect = _case(256, in_nbits, 12000 + 1000 * seed,
+                            np.linspace(0, 150 + seed, 21, dtype=np.float32), None, seed, 8)
+        assert torch.equal(got, expect), (in_nbits, seed)
+
+
+def test_noalloc_all_channels_killed():
+    """An all-zero killmask (no active channel) gives the plan's output."""
+    import torch
+    km = np.zeros(256, np.int32)
+    got, expect = _case(256, 8, 15000, np.linspace(0, 100, 17, dtype=np.float32), km, 21, 32)
+    assert torch.equal(got.view(torch.int32), expect.view(torch.int32))
+
+
 def test_noalloc_rejects_oversized_request():
     import torch
     fn, msg = _noalloc_fn()
@@ -88,3 +108,6 @@ def test_noalloc_rejects_oversized_request():
             4, None, nsamps, d_in.data_ptr(), 8, nchans, d_out.data_ptr(), 32, nsamps * 4, None)
     assert rc == 1  # DEDISP_MEM_ALLOC_FAILED
     assert b"64 MiB" in msg()
+    # the next successful call clears the message
+    got, expect = _case(64, 8, 6000, np.linspace(0, 50, 9, dtype=np.float32), None, 31, 32)
+    assert torch.equal(got.view(torch.int32), expect.view(torch.int32))
