@@ -24,6 +24,8 @@ struct FddEngine::Impl {
     // tensor-core form
     rt::DeviceBuffer B, delay_pad, qtable, err;
     rt::DeviceBuffer fft_tmp;  // four-step FFT scratch (nfft > 32768)
+    rt::DeviceBuffer twp_lo, twp_hi, wq;  // transforms of 16384 Q points: 16384-point table, W_Q
+    unsigned wq_n = 0;
     unsigned qtable_n = 0;
     int delay_pad_n = -1;
     unsigned tw_n = 0;
@@ -53,9 +55,15 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
     stats = ExecTiming();
 
     const FddGeometry g = fdd_geometry(opt, c.nsamps, v.max_delay);
-    if (g.nfft > (size_t)kern::kMaxFft || g.nfft < 512 || (g.nfft & (g.nfft - 1)) != 0)
+    // Power-of-two lengths up to 2^20: one-CTA or four-step transforms;
+    // other multiples of 16384 (the whole-series rule) and longer lengths:
+    // the 16384 Q-point transforms (spectra in the BinMap order).
+    const bool pow2 = (g.nfft & (g.nfft - 1)) == 0;
+    const bool qpath = !(pow2 && g.nfft >= 512 && g.nfft <= (size_t)kern::kMaxFft);
+    if (qpath && !kern::fftq_length(g.nfft))
         DD_THROW_MSG(DEDISP_UNKNOWN_ERROR,
-                     "FDD transform length must be a power of two in 512..2^20");
+                     "FDD transform length must be a power of two in 512..2^20 or a multiple of 16384");
+    const kern::BinMap bmap = qpath ? kern::fdd_binmap(g.nfft) : kern::BinMap{8192u, 1u, g.nfft / 2};
     const bool dev = (c.flags & DEDISP_DEVICE_POINTERS) != 0;
     cudaStream_t st = m_gpu.stream();
     const size_t nchans = v.nchans, ndm = v.ndm, nseg = g.nchunk;
@@ -91,8 +99,7 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
         m.delays_active.assign(dl.begin(), dl.begin() + m.nact);
         m.version = v.version;
     }
-    const bool use_tc = opt.precision == FddPrecision::BF16x3 &&
-                        kern::tc_supported((int)nseg, (unsigned)g.nfft, m.nact);
+    const bool use_tc = opt.precision == FddPrecision::BF16x3 && m.nact > 0;
     // Twiddles W_N^t = exp(-2 pi i t / N) as hi[t >> 8] * lo[t & 255].
     if (m.tw_n != g.nfft) {
         const unsigned n = (unsigned)g.nfft;
@@ -113,6 +120,31 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
         m.tw_n = n;
     }
     kern::TwiddleTable tw{m.tw_lo.get<float2>(), m.tw_hi.get<float2>(), (unsigned)g.nfft};
+    kern::TwiddleTable twp{nullptr, nullptr, 16384};
+    if (qpath) {
+        if (!m.twp_lo.get()) {
+            std::vector<float2> lo(256), hi(16384 / 256);
+            for (unsigned l = 0; l < 256; ++l) {
+                const double a = -2.0 * 3.14159265358979323846 * (double)l / 16384.0;
+                lo[l] = make_float2((float)std::cos(a), (float)std::sin(a));
+            }
+            for (unsigned h = 0; h < hi.size(); ++h) {
+                const double a = -2.0 * 3.14159265358979323846 * (double)h * 256.0 / 16384.0;
+                hi[h] = make_float2((float)std::cos(a), (float)std::sin(a));
+            }
+            m.twp_lo.reserve(lo.size() * sizeof(float2));
+            m.twp_hi.reserve(hi.size() * sizeof(float2));
+            RT_CHECK(cudaMemcpy(m.twp_lo.get(), lo.data(), lo.size() * sizeof(float2), cudaMemcpyHostToDevice));
+            RT_CHECK(cudaMemcpy(m.twp_hi.get(), hi.data(), hi.size() * sizeof(float2), cudaMemcpyHostToDevice));
+        }
+        twp = kern::TwiddleTable{m.twp_lo.get<float2>(), m.twp_hi.get<float2>(), 16384};
+        if (m.wq_n != bmap.Q) {
+            const std::vector<float2> w = kern::fftq_wq_table(bmap.Q);
+            m.wq.reserve(w.size() * sizeof(float2));
+            RT_CHECK(cudaMemcpy(m.wq.get(), w.data(), w.size() * sizeof(float2), cudaMemcpyHostToDevice));
+            m.wq_n = bmap.Q;
+        }
+    }
 
     // Buffers.
     const uint8_t* d_in = c.in;
@@ -122,10 +154,12 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
     }
     m.x.reserve(nchans * x_len * sizeof(float));
     m.X.reserve(nchans * nseg * bin_pitch * sizeof(float2));
-    int nact_pad = 0, npad = 0;
+    int nact_pad = 0, npad = 0, tc_dmax = -1;
+    bool tc_direct = false;
+    const int seg_group = (int)std::min<size_t>(nseg, (size_t)kern::kTcMaxSeg);
     if (use_tc) {
         nact_pad = kern::tc_pad_channels(m.nact);
-        npad = kern::tc_pad_n((int)nseg);
+        npad = kern::tc_pad_n(seg_group);
         m.B.reserve(kern::tc_b_bytes(nbins, nact_pad, npad));
         if (m.pad_version != v.version || m.delay_pad_n != nact_pad) {
             std::vector<float> dp(m.delays_active);
@@ -135,6 +169,35 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
             m.pad_version = v.version;
             m.delay_pad_n = nact_pad;
         }
+        // Largest delay index over all DMs and active channels (same float
+        // operations as the kernel); the kernel builds a per-bin phasor table
+        // over 0..dmax when it fits shared memory, else it indexes the
+        // quarter-wave table (power-of-two lengths whose table fits).
+        const int rnd = opt.round_delays ? 1 : 0;
+        if (m.dmax_version != v.version || m.dmax_round != rnd) {
+            long dmax = 0;
+            bool ok = true;
+            for (size_t i = 0; i < ndm && ok; ++i) {
+                const float d = v.dms[i];
+                if (!(d >= 0.f)) { ok = false; break; }
+                for (float dl : m.delays_active) {
+                    const long x = rnd ? (long)hostmath::delay_rn(d, dl) : (long)hostmath::delay_trunc(d, dl);
+                    dmax = std::max(dmax, x);
+                }
+            }
+            m.dmax = (ok && dmax < (1l << 30)) ? (int)dmax : -1;
+            m.dmax_version = v.version;
+            m.dmax_round = rnd;
+        }
+        // Phasor source, in order of preference: the per-bin delay table,
+        // the quarter-wave table (power-of-two lengths), or each phasor from
+        // the two-level twiddle tables (any length whose tables fit).
+        tc_dmax = kern::tc_table_mode_dmax(m.dmax, (unsigned)g.nfft, nact_pad, npad);
+        tc_direct = tc_dmax < 0 && !kern::tc_quarter_mode_fits((unsigned)g.nfft, nact_pad, npad);
+        if (tc_direct && !kern::tc_direct_mode_fits((unsigned)g.nfft, nact_pad, npad))
+            DD_THROW_MSG(DEDISP_UNKNOWN_ERROR,
+                         "tensor-core MAC: transform length too large for its twiddle tables in shared "
+                         "memory; use precision 0");
         if (m.qtable_n != g.nfft) {
             const std::vector<uint2> t = kern::tc_quarter_table((unsigned)g.nfft);
             m.qtable.reserve(t.size() * sizeof(uint2));
@@ -173,16 +236,18 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
     const float scale = (float)(1.0 / (double)nchans);
     kern::launch_fdd_unpack(d_in, in_stride, c.in_nbits, c.nsamps, nchans, scale, m.x.get<float>(),
                             x_len, x_len, st);
-    const size_t tmp_elems = kern::fft_scratch_elems((int)g.nfft, std::max(nchans, ndm) * nseg);
+    const size_t tmp_elems = qpath ? std::max(nchans, ndm) * nseg * (g.nfft / 2)
+                                   : kern::fft_scratch_elems((int)g.nfft, std::max(nchans, ndm) * nseg);
     if (tmp_elems) m.fft_tmp.reserve(tmp_elems * sizeof(float2));
-    kern::launch_fft_r2c(m.x.get<float>(), x_len, nchans, nseg, seg_stride, (int)g.nfft,
-                         m.X.get<float2>(), bin_pitch, tw, m.fft_tmp.get<float2>(), st);
-    if (use_tc)
-        kern::launch_fdd_prep_b(m.X.get<float2>(), bin_pitch, (int)nseg, nbins, m.chan.get<int32_t>(),
-                                m.km.get<float>(), m.nact, nact_pad, npad, m.B.get(), st);
-    else if (m.nact > 0)
+    if (qpath)
+        kern::launch_fft_r2c_q(m.x.get<float>(), x_len, nchans, nseg, seg_stride, g.nfft, m.X.get<float2>(),
+                               bin_pitch, tw, twp, m.wq.get<float2>(), m.fft_tmp.get<float2>(), st);
+    else
+        kern::launch_fft_r2c(m.x.get<float>(), x_len, nchans, nseg, seg_stride, (int)g.nfft,
+                             m.X.get<float2>(), bin_pitch, tw, m.fft_tmp.get<float2>(), st);
+    if (!use_tc && m.nact > 0)
         kern::launch_fdd_to_binmajor(m.X.get<float2>(), bin_pitch, nseg, nbins, m.chan.get<int32_t>(),
-                                     m.km.get<float>(), m.nact, m.Xt.get<float2>(), st);
+                                     m.km.get<float>(), m.nact, m.Xt.get<float2>(), bmap, st);
     if (e1) e1->record(st);
 
     if (use_tc) {
@@ -199,34 +264,27 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
         ta.err = m.err.get<unsigned>();
         ta.nact_pad = nact_pad;
         ta.ndm = (int)ndm;
-        ta.nseg = (int)nseg;
+        ta.nseg_total = (int)nseg;
         ta.npad = npad;
         ta.nbins = nbins;
         ta.nfft = (unsigned)g.nfft;
         ta.round_delays = opt.round_delays ? 1 : 0;
-        // Largest delay index over all DMs and active channels (same float
-        // operations as the kernel); the kernel then builds a per-bin
-        // phasor table over 0..dmax when it fits shared memory.
-        if (m.dmax_version != v.version || m.dmax_round != ta.round_delays) {
-            long dmax = 0;
-            bool ok = true;
-            for (size_t i = 0; i < ndm && ok; ++i) {
-                const float d = v.dms[i];
-                if (!(d >= 0.f)) { ok = false; break; }
-                for (float dl : m.delays_active) {
-                    const long x = ta.round_delays ? (long)hostmath::delay_rn(d, dl)
-                                                   : (long)hostmath::delay_trunc(d, dl);
-                    dmax = std::max(dmax, x);
-                }
-            }
-            m.dmax = (ok && dmax < (1l << 30)) ? (int)dmax : -1;
-            m.dmax_version = v.version;
-            m.dmax_round = ta.round_delays;
+        ta.dmax = tc_dmax;
+        ta.direct = tc_direct ? 1 : 0;
+        ta.stages = kern::tc_stages(ta.nfft, nact_pad, npad, ta.dmax, tc_direct);
+        // Segment groups of at most kTcMaxSeg (the accumulator's 128
+        // columns): B operand and one MAC launch per group.
+        stats.launches = 0;
+        for (size_t s0 = 0; s0 < nseg; s0 += (size_t)seg_group) {
+            const int ns = (int)std::min(nseg - s0, (size_t)seg_group);
+            kern::launch_fdd_prep_b(m.X.get<float2>(), bin_pitch, ns, nbins, m.chan.get<int32_t>(),
+                                    m.km.get<float>(), m.nact, nact_pad, npad, m.B.get(), bmap, (int)s0,
+                                    (int)nseg, st);
+            ta.nseg = ns;
+            ta.seg0 = (int)s0;
+            kern::launch_fdd_mac_tc(ta, m.B.get(), st);
+            ++stats.launches;
         }
-        ta.dmax = kern::tc_table_mode_dmax(m.dmax, ta.nfft, nact_pad, npad);
-        ta.stages = kern::tc_stages(ta.nfft, nact_pad, npad, ta.dmax);
-        kern::launch_fdd_mac_tc(ta, m.B.get(), st);
-        stats.launches = 1;
     } else if (m.nact > 0) {
         kern::MacArgs a;
         a.Xt = m.Xt.get<float2>();
@@ -253,10 +311,14 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
     } else {
         if (!direct_y)
             kern::launch_fdd_to_dmmajor(m.Yt.get<float2>(), nseg, ndm, nbins, m.Y.get<float2>(),
-                                        bin_pitch, st);
+                                        bin_pitch, bmap, st);
         const size_t keep = g.segmented ? g.nsamp_good : g.nfft;
-        kern::launch_fft_c2r(m.Y.get<float2>(), bin_pitch, ndm, nseg, (int)g.nfft, d_out, g.row_len,
-                             keep, g.row_len, tw, m.fft_tmp.get<float2>(), st);
+        if (qpath)
+            kern::launch_fft_c2r_q(m.Y.get<float2>(), bin_pitch, ndm, nseg, g.nfft, d_out, g.row_len, keep,
+                                   g.row_len, tw, twp, m.wq.get<float2>(), m.fft_tmp.get<float2>(), st);
+        else
+            kern::launch_fft_c2r(m.Y.get<float2>(), bin_pitch, ndm, nseg, (int)g.nfft, d_out, g.row_len,
+                                 keep, g.row_len, tw, m.fft_tmp.get<float2>(), st);
     }
     if (e3) e3->record(st);
     if (!dev)

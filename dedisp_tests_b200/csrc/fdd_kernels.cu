@@ -18,6 +18,8 @@
 // (fdd_kernel.cuh:262-273).
 #include "fdd_kernels.hpp"
 
+#include <cmath>
+
 #include "runtime.hpp"
 
 namespace dedisp {
@@ -31,6 +33,12 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b)
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 __device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
+
+// Bin at row position p of the BinMap order.
+__device__ __forceinline__ size_t qbin(size_t p, const BinMap& m)
+{
+    return (m.Q <= 1 || p >= m.M) ? p : (size_t)m.Q * (p & (m.P - 1)) + p / m.P;
+}
 
 // exp(-2 pi i t / 32), t = 0..15 (forward); conjugated for the inverse.
 __device__ __forceinline__ float2 w32(int t, bool inv)
@@ -599,6 +607,288 @@ void launch_c2r_4step(float2* Y, size_t bin_pitch, size_t rows, size_t nseg, flo
 }
 
 // ---------------------------------------------------------------------------
+// Transforms of N = 16384 Q real points for any Q >= 1 (the whole-series
+// length rule round_up(nsamp + max_delay, 16384), FDDGPUPlan.cpp:85-93, is
+// rarely a power of two): M = N / 2 = P Q complex points, P = 8192. With
+// n = n1 + P n2 and k = Q k1 + k2,
+//   Z[Q k1 + k2] = sum_n1 W_P^{n1 k1} W_M^{n1 k2} sum_n2 z[n1 + P n2] W_Q^{n2 k2}:
+// (1) Q-point DFTs over n2 for tiles of T consecutive n1 (mixed-radix
+//     Stockham passes in shared memory; radices 4, 2, 3, 5, 7 in registers,
+//     larger prime radices as direct sums), times W_M^{n1 k2}, stored as rows
+//     k2 of P points in scratch;
+// (2) P-point transforms of those rows (the shared-memory radix-16 kernel).
+// The spectrum stays in this transposed order: bin k < M of a row at position
+// (k mod Q) P + k / Q, bin M at position M (BinMap); the layout kernels read
+// and write it in that order, the MAC sees true bins. The inverse runs the
+// steps backwards. The Stockham formulation (autosort, decimation in time)
+// follows Govindaraju et al., "High performance discrete Fourier transforms
+// on graphics processors", SC 2008.
+// ---------------------------------------------------------------------------
+constexpr int FQ_LOGP = 13;
+constexpr unsigned FQ_P = 1u << FQ_LOGP;
+constexpr int FQ_THREADS = 256;
+
+// One radix-r pass over T columns of Q points ([T][Q] in shared memory,
+// from `in` to `out`); Ns = product of the earlier passes' radices;
+// wq[x] = W_Q^x (conjugated for the inverse).
+template <bool INV>
+__device__ __forceinline__ void stockham_pass(const float2* __restrict__ in, float2* __restrict__ out, int Q,
+                                              int T, int r, int Ns, const float2* __restrict__ wq)
+{
+    const int R = Q / r;
+    const int ws = Q / (Ns * r);  // W_{Ns r}^x = W_Q^{x ws}
+    const int wr = R;             // W_r^x = W_Q^{x Q / r}
+    auto W = [&](int x) {
+        const float2 w = wq[x];
+        return INV ? conjf2(w) : w;
+    };
+    if (r <= 8) {
+        for (int g = threadIdx.x; g < T * R; g += blockDim.x) {
+            const int col = g / R, j = g - col * R;
+            const int k = j % Ns;
+            const float2* src = in + col * Q + j;
+            float2 v[8];
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                if (t < r) {
+                    float2 a = src[t * R];
+                    if (t > 0 && k > 0) a = cmul(a, W(t * k * ws));
+                    v[t] = a;
+                }
+            }
+            float2* dst = out + col * Q + (j / Ns) * Ns * r + k;
+            if (r == 2) {
+                dst[0] = v[0] + v[1];
+                dst[Ns] = v[0] - v[1];
+            } else if (r == 4) {
+                const float2 s02 = v[0] + v[2], d02 = v[0] - v[2], s13 = v[1] + v[3], d13 = v[1] - v[3];
+                // W_4 = -i (forward) or +i (inverse) times d13
+                const float2 rot = INV ? make_float2(-d13.y, d13.x) : make_float2(d13.y, -d13.x);
+                dst[0] = s02 + s13;
+                dst[Ns] = d02 + rot;
+                dst[2 * Ns] = s02 - s13;
+                dst[3 * Ns] = d02 - rot;
+            } else {
+                for (int u = 0; u < r; ++u) {
+                    float2 acc = v[0];
+#pragma unroll
+                    for (int t = 1; t < 8; ++t)
+                        if (t < r) acc = acc + cmul(v[t], W(((t * u) % r) * wr));
+                    dst[u * Ns] = acc;
+                }
+            }
+        }
+    } else {
+        // one output (butterfly j, output u) per work item
+        for (int g = threadIdx.x; g < T * Q; g += blockDim.x) {
+            const int col = g / Q, rem = g - col * Q;
+            const int j = rem % R, u = rem / R;
+            const int k = j % Ns;
+            const float2* src = in + col * Q + j;
+            float2 acc = src[0];
+            for (int t = 1; t < r; ++t) {
+                const int x = (t * k * ws + ((t * u) % r) * wr) % Q;
+                acc = acc + cmul(src[t * R], W(x));
+            }
+            out[col * Q + (j / Ns) * Ns * r + k + u * Ns] = acc;
+        }
+    }
+}
+
+// All passes; returns the buffer holding the natural-order result.
+template <bool INV>
+__device__ __forceinline__ float2* stockham_all(float2* b0, float2* b1, int Q, int T, const QRadices& rad,
+                                                const float2* wq)
+{
+    float2* cur = b0;
+    float2* nxt = b1;
+    int Ns = 1;
+    for (int p = 0; p < rad.n; ++p) {
+        stockham_pass<INV>(cur, nxt, Q, T, rad.r[p], Ns, wq);
+        __syncthreads();
+        float2* t = cur;
+        cur = nxt;
+        nxt = t;
+        Ns *= rad.r[p];
+    }
+    return cur;
+}
+
+// W_N^t from the two-level table in global memory (L1/L2 resident).
+__device__ __forceinline__ float2 twiddle_g(const TwiddleTable& tw, size_t t, bool inv)
+{
+    const float2 w = cmul(__ldg(tw.hi + (t >> 8)), __ldg(tw.lo + (t & 255)));
+    return inv ? conjf2(w) : w;
+}
+
+// Step (1), forward: row `row` = (c, seg) of real samples, columns
+// n1 in [blockIdx.x T, +T): Z1[row][k2 P + n1] = W_M^{n1 k2} DFT_Q(z[n1 + P n2]).
+__global__ void __launch_bounds__(FQ_THREADS) fftq_cols_fwd_kernel(
+    const float* x, size_t x_pitch, size_t nseg, size_t seg_stride, float2* Z1, int Q, int T, QRadices rad,
+    const float2* wq_g, TwiddleTable tw)
+{
+    extern __shared__ __align__(16) float2 s_q[];
+    float2* b0 = s_q;
+    float2* b1 = b0 + T * Q;
+    float2* wq = b1 + T * Q;
+    for (int i = threadIdx.x; i < Q; i += blockDim.x) wq[i] = wq_g[i];
+    const size_t row = blockIdx.y;
+    const unsigned n1_0 = blockIdx.x * (unsigned)T;
+    const size_t c = row / nseg, seg = row - c * nseg;
+    const float* xr = x + c * x_pitch + seg * seg_stride;
+    for (int idx = threadIdx.x; idx < T * Q; idx += blockDim.x) {
+        const int col = idx % T, n2 = idx / T;
+        const size_t n = (size_t)n1_0 + col + (size_t)FQ_P * n2;
+        b0[col * Q + n2] = make_float2(xr[2 * n], xr[2 * n + 1]);
+    }
+    __syncthreads();
+    const float2* res = stockham_all<false>(b0, b1, Q, T, rad, wq);
+    const size_t M = (size_t)FQ_P * Q;
+    float2* zo = Z1 + row * M;
+    for (int idx = threadIdx.x; idx < T * Q; idx += blockDim.x) {
+        const int col = idx % T, k2 = idx / T;
+        const size_t n1 = (size_t)n1_0 + col;
+        // W_M^{n1 k2} = W_N^{2 n1 k2}, 2 n1 k2 < 2M = N
+        zo[(size_t)k2 * FQ_P + n1] = cmul(res[col * Q + k2], twiddle_g(tw, 2 * n1 * (size_t)k2, false));
+    }
+}
+
+// Step (1) backwards: u rows k2 (Z1[row][k2 P + n1]) times W_M^{-n1 k2},
+// inverse Q-point DFTs over k2, then z[n1 + P n2] / M as real samples
+// 2n, 2n + 1 of segment `seg` (the first `keep`, at most out_len).
+__global__ void __launch_bounds__(FQ_THREADS) fftq_cols_inv_kernel(
+    const float2* Z1, float* out, size_t out_stride, size_t nseg, size_t keep, size_t out_len, int Q, int T,
+    QRadices rad, const float2* wq_g, TwiddleTable tw)
+{
+    extern __shared__ __align__(16) float2 s_q[];
+    float2* b0 = s_q;
+    float2* b1 = b0 + T * Q;
+    float2* wq = b1 + T * Q;
+    for (int i = threadIdx.x; i < Q; i += blockDim.x) wq[i] = wq_g[i];
+    const size_t row = blockIdx.y;
+    const unsigned n1_0 = blockIdx.x * (unsigned)T;
+    const size_t M = (size_t)FQ_P * Q;
+    const float2* zr = Z1 + row * M;
+    for (int idx = threadIdx.x; idx < T * Q; idx += blockDim.x) {
+        const int col = idx % T, k2 = idx / T;
+        const size_t n1 = (size_t)n1_0 + col;
+        b0[col * Q + k2] = cmul(zr[(size_t)k2 * FQ_P + n1], twiddle_g(tw, 2 * n1 * (size_t)k2, true));
+    }
+    __syncthreads();
+    const float2* res = stockham_all<true>(b0, b1, Q, T, rad, wq);
+    const float scale = 1.0f / (float)M;
+    const size_t dm = row / nseg, seg = row - dm * nseg;
+    float* dst = out + dm * out_stride;
+    const size_t o0 = seg * keep;
+    for (int idx = threadIdx.x; idx < T * Q; idx += blockDim.x) {
+        const int col = idx % T, n2 = idx / T;
+        const float2 z = res[col * Q + n2];
+        const size_t n = (size_t)n1_0 + col + (size_t)FQ_P * n2;
+        const size_t i0 = 2 * n, i1 = i0 + 1;
+        if (i0 < keep && o0 + i0 < out_len) dst[o0 + i0] = z.x * scale;
+        if (i1 < keep && o0 + i1 < out_len) dst[o0 + i1] = z.y * scale;
+    }
+}
+
+// Step (2): P-point complex transforms of contiguous rows; row g = o Q + k2
+// at src + o src_pitch + k2 P, natural-order result to the same place in dst.
+// twp: twiddle table for 2P.
+template <int LOGP, bool INV>
+__global__ void __launch_bounds__(FftPlan<LOGP>::threads()) fft_c2c_rows_kernel(
+    const float2* src, size_t src_pitch, float2* dst, size_t dst_pitch, unsigned Q, TwiddleTable twp, size_t rows)
+{
+    constexpr unsigned P = 1u << LOGP;
+    constexpr unsigned T = FftPlan<LOGP>::threads();
+    constexpr unsigned PER = P / T;
+    extern __shared__ __align__(16) float2 s_fft[];
+    float2* s = s_fft;
+    float2* lo = s + P;
+    float2* hi = lo + 256;
+    for (unsigned i = threadIdx.x; i < 256; i += blockDim.x) lo[i] = twp.lo[i];
+    for (unsigned i = threadIdx.x; i < 2 * P / 256; i += blockDim.x) hi[i] = twp.hi[i];
+    const unsigned t = threadIdx.x;
+    const unsigned pt = pa(t);
+    for (size_t g = blockIdx.x; g < rows; g += gridDim.x) {
+        const size_t o = g / Q, k2 = g - o * Q;
+        const float2* in = src + o * src_pitch + k2 * P;
+        float2 v[PER];
+#pragma unroll
+        for (unsigned i = 0; i < PER; ++i) v[i] = in[t + i * T];
+        __syncthreads();  // the previous row's output phase has read s
+#pragma unroll
+        for (unsigned i = 0; i < PER; ++i) s[pt ^ pa(i * T)] = v[i];
+        fft_smem<LOGP, INV>(s, lo, hi);
+        float2* outp = dst + o * dst_pitch + k2 * P;
+        const unsigned pk = pa(fft_pos<LOGP>(t));
+#pragma unroll 4
+        for (unsigned i = 0; i < PER; ++i) outp[t + i * T] = s[pk ^ pa(fft_pos<LOGP>(i * T))];
+    }
+}
+
+__device__ __forceinline__ size_t qpos(size_t k, const BinMap& m)
+{
+    return (m.Q <= 1 || k >= m.M) ? k : (k % m.Q) * m.P + k / m.Q;
+}
+
+// Real-FFT post step in place over rows in the transposed order: bins k and
+// M - k (k = 0..M/2) from z at the positions of k and M - k (formula of
+// fft_r2c_kernel; bin M at position M).
+__global__ void __launch_bounds__(256) r2c_post_q_kernel(float2* X, size_t x_pitch, BinMap map, TwiddleTable tw)
+{
+    const size_t M = map.M;
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > M / 2) return;
+    float2* r = X + (size_t)blockIdx.y * x_pitch;
+    const size_t pk = qpos(k, map), pm = qpos(k ? M - k : 0, map);
+    const float2 a = r[pk], b = r[pm];
+    auto bin = [&](float2 zk, float2 zm, size_t kk) {
+        const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+        const float2 d = make_float2(zk.x - zm.x, zk.y + zm.y);
+        const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
+        const float2 w = (kk == M) ? make_float2(-1.f, 0.f) : twiddle_g(tw, kk, false);
+        return e + cmul(w, o);
+    };
+    const float2 xk = bin(a, b, k);
+    const float2 xm = bin(b, a, M - k);
+    r[pk] = xk;
+    if (M - k != k) r[qpos(M - k, map)] = xm;
+}
+
+// Inverse real-FFT pre step in place over transposed rows (formula of
+// fft_c2r_kernel): bins k and M - k -> z at the positions of k and M - k.
+__global__ void __launch_bounds__(256) c2r_pre_q_kernel(float2* Y, size_t y_pitch, BinMap map, TwiddleTable tw)
+{
+    const size_t M = map.M;
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > M / 2) return;
+    float2* r = Y + (size_t)blockIdx.y * y_pitch;
+    const size_t pk = qpos(k, map), pm = qpos(M - k, map);
+    float2 a = r[pk], b = r[pm];
+    if (k == 0) {  // the DC and Nyquist imaginary parts are ignored (C2R)
+        a.y = 0.f;
+        b.y = 0.f;
+    }
+    auto pre = [&](float2 xk, float2 xm, size_t kk) {
+        const float2 e = make_float2(0.5f * (xk.x + xm.x), 0.5f * (xk.y - xm.y));
+        const float2 d = make_float2(0.5f * (xk.x - xm.x), 0.5f * (xk.y + xm.y));
+        const float2 o = cmul(d, conjf2(twiddle_g(tw, kk, false)));
+        return make_float2(e.x - o.y, e.y + o.x);
+    };
+    const float2 zk = pre(a, b, k);
+    if (k != 0 && M - k != k) r[pm] = pre(b, a, M - k);
+    r[pk] = zk;
+}
+
+// Columns per CTA of step (1): the largest of 16, 8, 4 whose two [T][Q]
+// buffers and the W_Q table fit in shared memory (0: none fits).
+int fftq_tile(unsigned Q)
+{
+    for (int T : {16, 8, 4})
+        if ((2 * (size_t)T * Q + Q) * sizeof(float2) <= kFqMaxSmem) return T;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
 // unpack / transposes
 // ---------------------------------------------------------------------------
 // Tiles of 64 samples x 64 channels per 256 threads: each thread issues its
@@ -667,8 +957,10 @@ constexpr int BMT_BINS = 64;
 __global__ void __launch_bounds__(256) to_binmajor_kernel(const float2* X, size_t bin_pitch,
                                                           size_t nseg, size_t nbins,
                                                           const int32_t* chan, const float* km,
-                                                          int nact, float2* Xt)
+                                                          int nact, float2* Xt, BinMap map)
 {
+    // tiles run over row positions (contiguous reads); each position's bin
+    // is qbin(position)
     constexpr int PER = BMT_BINS / 8;
     __shared__ float2 tile[32][BMT_BINS + 1];
     const size_t k0 = (size_t)blockIdx.x * BMT_BINS;
@@ -692,11 +984,11 @@ __global__ void __launch_bounds__(256) to_binmajor_kernel(const float2* X, size_
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < PER; ++i) {
-        // bin k0 + ty + 8 i, channel j0 + tx
+        // position k0 + ty + 8 i, channel j0 + tx
         const int kk = ty + 8 * i;
-        const size_t k = k0 + kk;
+        const size_t p = k0 + kk;
         const int j = j0 + tx;
-        if (k < nbins && j < nact) Xt[(k * nseg + seg) * nact + j] = tile[tx][kk];
+        if (p < nbins && j < nact) Xt[(qbin(p, map) * nseg + seg) * nact + j] = tile[tx][kk];
     }
 }
 
@@ -705,8 +997,10 @@ __global__ void __launch_bounds__(256) to_binmajor_kernel(const float2* X, size_
 // loads before their first use.
 constexpr int DMT_BINS = 64;
 __global__ void __launch_bounds__(256) to_dmmajor_kernel(const float2* Yt, size_t nseg, size_t ndm,
-                                                         size_t nbins, float2* Y, size_t bin_pitch)
+                                                         size_t nbins, float2* Y, size_t bin_pitch,
+                                                         BinMap map)
 {
+    // tiles run over row positions of Y (contiguous writes)
     constexpr int PER = DMT_BINS / 8;
     __shared__ float2 tile[DMT_BINS][33];
     const size_t k0 = (size_t)blockIdx.x * DMT_BINS, d0 = (size_t)blockIdx.y * 32;
@@ -715,8 +1009,8 @@ __global__ void __launch_bounds__(256) to_dmmajor_kernel(const float2* Yt, size_
     float2 v[PER];
 #pragma unroll
     for (int i = 0; i < PER; ++i) {
-        const size_t k = k0 + ty + 8 * i, d = d0 + tx;
-        v[i] = (k < nbins && d < ndm) ? Yt[(k * nseg + seg) * ndm + d] : make_float2(0.f, 0.f);
+        const size_t p = k0 + ty + 8 * i, d = d0 + tx;
+        v[i] = (p < nbins && d < ndm) ? Yt[(qbin(p, map) * nseg + seg) * ndm + d] : make_float2(0.f, 0.f);
     }
 #pragma unroll
     for (int i = 0; i < PER; ++i) tile[ty + 8 * i][tx] = v[i];
@@ -978,20 +1272,120 @@ void launch_fft_c2r(float2* Y, size_t bin_pitch, size_t ndm, size_t nseg, int nf
 
 size_t fft_scratch_elems(int nfft, size_t rows) { return nfft > 32768 ? rows * (size_t)(nfft / 2) : 0; }
 
+bool fftq_length(size_t nfft)
+{
+    return nfft >= 16384 && nfft % 16384 == 0 && fftq_tile((unsigned)(nfft / 16384)) > 0 &&
+           nfft / 2 <= ((size_t)1 << 31);
+}
+
+BinMap fdd_binmap(size_t nfft)
+{
+    BinMap m;
+    m.M = nfft / 2;
+    const bool pow2 = (nfft & (nfft - 1)) == 0;
+    m.Q = (!pow2 || nfft > (size_t)kMaxFft) ? (unsigned)(nfft / 16384) : 1u;
+    m.P = FQ_P;
+    return m;
+}
+
+QRadices fftq_radices(unsigned Q)
+{
+    QRadices r;
+    unsigned q = Q;
+    auto push = [&](unsigned f) {
+        if (r.n >= 24) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "too many FFT radices");
+        r.r[r.n++] = (int)f;
+        q /= f;
+    };
+    for (unsigned f : {4u, 2u, 3u, 5u, 7u})
+        while (q % f == 0) push(f);
+    for (unsigned f = 11; q > 1; f += 2)
+        while (q % f == 0) push(f);
+    return r;
+}
+
+std::vector<float2> fftq_wq_table(unsigned Q)
+{
+    std::vector<float2> w(Q);
+    for (unsigned x = 0; x < Q; ++x) {
+        const double a = -2.0 * 3.14159265358979323846 * (double)x / (double)Q;
+        w[x] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    return w;
+}
+
+void launch_fft_r2c_q(const float* x, size_t x_pitch, size_t nchans, size_t nseg, size_t seg_stride,
+                      size_t nfft, float2* X, size_t bin_pitch, const TwiddleTable& tw,
+                      const TwiddleTable& twp, const float2* wq, float2* scratch, cudaStream_t s)
+{
+    if (!fftq_length(nfft)) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unsupported FFT length");
+    const unsigned Q = (unsigned)(nfft / 16384);
+    const size_t rows = nchans * nseg;
+    if (rows == 0) return;
+    if (rows > 65535) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "too many FFT rows");
+    const int T = fftq_tile(Q);
+    const QRadices rad = fftq_radices(Q);
+    const BinMap map = fdd_binmap(nfft);
+    const size_t sq = (2 * (size_t)T * Q + Q) * sizeof(float2);
+    rt::raise_smem_limit(fftq_cols_fwd_kernel, sq);
+    fftq_cols_fwd_kernel<<<dim3(FQ_P / T, (unsigned)rows), FQ_THREADS, sq, s>>>(x, x_pitch, nseg, seg_stride,
+                                                                              scratch, (int)Q, T, rad, wq, tw);
+    RT_CHECK(cudaGetLastError());
+    auto kr = fft_c2c_rows_kernel<FQ_LOGP, false>;
+    const size_t sr = (FQ_P + 256 + 2 * FQ_P / 256) * sizeof(float2);
+    rt::raise_smem_limit(kr, sr);
+    const size_t nrows = rows * Q;
+    kr<<<persistent_grid(kr, FftPlan<FQ_LOGP>::threads(), sr, nrows), FftPlan<FQ_LOGP>::threads(), sr, s>>>(
+        scratch, map.M, X, bin_pitch, Q, twp, nrows);
+    RT_CHECK(cudaGetLastError());
+    r2c_post_q_kernel<<<dim3((unsigned)((map.M / 2 + 256) / 256), (unsigned)rows), 256, 0, s>>>(X, bin_pitch, map,
+                                                                                              tw);
+    RT_CHECK(cudaGetLastError());
+}
+
+void launch_fft_c2r_q(float2* Y, size_t bin_pitch, size_t ndm, size_t nseg, size_t nfft, float* out,
+                      size_t out_stride, size_t keep, size_t out_len, const TwiddleTable& tw,
+                      const TwiddleTable& twp, const float2* wq, float2* scratch, cudaStream_t s)
+{
+    if (!fftq_length(nfft)) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unsupported FFT length");
+    const unsigned Q = (unsigned)(nfft / 16384);
+    const size_t rows = ndm * nseg;
+    if (rows == 0) return;
+    if (rows > 65535) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "too many FFT rows");
+    const int T = fftq_tile(Q);
+    const QRadices rad = fftq_radices(Q);
+    const BinMap map = fdd_binmap(nfft);
+    c2r_pre_q_kernel<<<dim3((unsigned)((map.M / 2 + 256) / 256), (unsigned)rows), 256, 0, s>>>(Y, bin_pitch, map,
+                                                                                             tw);
+    RT_CHECK(cudaGetLastError());
+    auto kr = fft_c2c_rows_kernel<FQ_LOGP, true>;
+    const size_t sr = (FQ_P + 256 + 2 * FQ_P / 256) * sizeof(float2);
+    rt::raise_smem_limit(kr, sr);
+    const size_t nrows = rows * Q;
+    kr<<<persistent_grid(kr, FftPlan<FQ_LOGP>::threads(), sr, nrows), FftPlan<FQ_LOGP>::threads(), sr, s>>>(
+        Y, bin_pitch, scratch, map.M, Q, twp, nrows);
+    RT_CHECK(cudaGetLastError());
+    const size_t sq = (2 * (size_t)T * Q + Q) * sizeof(float2);
+    rt::raise_smem_limit(fftq_cols_inv_kernel, sq);
+    fftq_cols_inv_kernel<<<dim3(FQ_P / T, (unsigned)rows), FQ_THREADS, sq, s>>>(scratch, out, out_stride, nseg, keep,
+                                                                              out_len, (int)Q, T, rad, wq, tw);
+    RT_CHECK(cudaGetLastError());
+}
+
 void launch_fdd_to_binmajor(const float2* X, size_t bin_pitch, size_t nseg, size_t nbins,
                             const int32_t* chan, const float* km, int nact, float2* Xt,
-                            cudaStream_t s)
+                            const BinMap& map, cudaStream_t s)
 {
     dim3 grid((unsigned)((nbins + BMT_BINS - 1) / BMT_BINS), (unsigned)((nact + 31) / 32), (unsigned)nseg);
-    to_binmajor_kernel<<<grid, 256, 0, s>>>(X, bin_pitch, nseg, nbins, chan, km, nact, Xt);
+    to_binmajor_kernel<<<grid, 256, 0, s>>>(X, bin_pitch, nseg, nbins, chan, km, nact, Xt, map);
     RT_CHECK(cudaGetLastError());
 }
 
 void launch_fdd_to_dmmajor(const float2* Yt, size_t nseg, size_t ndm, size_t nbins, float2* Y,
-                           size_t bin_pitch, cudaStream_t s)
+                           size_t bin_pitch, const BinMap& map, cudaStream_t s)
 {
     dim3 grid((unsigned)((nbins + DMT_BINS - 1) / DMT_BINS), (unsigned)((ndm + 31) / 32), (unsigned)nseg);
-    to_dmmajor_kernel<<<grid, 256, 0, s>>>(Yt, nseg, ndm, nbins, Y, bin_pitch);
+    to_dmmajor_kernel<<<grid, 256, 0, s>>>(Yt, nseg, ndm, nbins, Y, bin_pitch, map);
     RT_CHECK(cudaGetLastError());
 }
 

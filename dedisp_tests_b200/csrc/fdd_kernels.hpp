@@ -15,6 +15,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 namespace dedisp {
 namespace kern {
@@ -26,6 +27,23 @@ struct TwiddleTable {
     const float2* hi;  // N / 256 entries
     unsigned n;
 };
+
+// Bin order of a spectrum row. Q <= 1: natural (bin k at position k).
+// Q > 1 (transforms of N = 16384 Q points, M = N / 2 = P Q, P = 8192): bin
+// k < M at position (k mod Q) P + k / Q, bin M at position M.
+struct BinMap {
+    unsigned P = 8192;
+    unsigned Q = 1;
+    size_t M = 0;
+};
+
+// Radices of the Q-point passes (product Q), from fftq_radices.
+struct QRadices {
+    int n = 0;
+    int r[24] = {};
+};
+QRadices fftq_radices(unsigned Q);
+constexpr size_t kFqMaxSmem = 200 * 1024;
 
 // 8-bit or float32 time-major input -> x rows, scaled (FDDGPUPlan.cpp:472,
 // unpack_kernel.cuh:60): 8-bit ((float)v - 127.5f) * scale, float v * scale.
@@ -55,15 +73,31 @@ void launch_fft_c2r(float2* Y, size_t bin_pitch, size_t ndm, size_t nseg, int nf
                     float* out, size_t out_stride, size_t keep, size_t out_len,
                     const TwiddleTable& tw, float2* scratch, cudaStream_t s);
 
-// X -> Xt over active channels (chan[j], multiplier km[j]).
+// Transforms of N = 16384 Q real points for any Q (not a power-of-two
+// length, or above 2^20): X rows (bins 0..N/2) in the BinMap order of
+// fdd_binmap(N). tw: table for N; twp: table for 16384; wq: W_Q^x, x < Q
+// (fftq_wq_table); scratch: fft_scratch_elems complex values.
+bool fftq_length(size_t nfft);  // handled by this path (N = 16384 Q, Q >= 1)
+BinMap fdd_binmap(size_t nfft); // the order launch_fft_r2c / _q leaves X in
+std::vector<float2> fftq_wq_table(unsigned Q);
+void launch_fft_r2c_q(const float* x, size_t x_pitch, size_t nchans, size_t nseg, size_t seg_stride,
+                      size_t nfft, float2* X, size_t bin_pitch, const TwiddleTable& tw,
+                      const TwiddleTable& twp, const float2* wq, float2* scratch, cudaStream_t s);
+// Y rows in the BinMap order (overwritten).
+void launch_fft_c2r_q(float2* Y, size_t bin_pitch, size_t ndm, size_t nseg, size_t nfft, float* out,
+                      size_t out_stride, size_t keep, size_t out_len, const TwiddleTable& tw,
+                      const TwiddleTable& twp, const float2* wq, float2* scratch, cudaStream_t s);
+
+// X -> Xt over active channels (chan[j], multiplier km[j]); X rows in the
+// order `map`.
 void launch_fdd_to_binmajor(const float2* X, size_t bin_pitch, size_t nseg, size_t nbins,
                             const int32_t* chan, const float* km, int nact, float2* Xt,
-                            cudaStream_t s);
+                            const BinMap& map, cudaStream_t s);
 
 // Yt -> Y (DM-major spectra); with spectrum_out, writes the first nspec bins
 // straight into output rows instead: out[dm][2k], out[dm][2k+1].
 void launch_fdd_to_dmmajor(const float2* Yt, size_t nseg, size_t ndm, size_t nbins,
-                           float2* Y, size_t bin_pitch, cudaStream_t s);
+                           float2* Y, size_t bin_pitch, const BinMap& map, cudaStream_t s);
 void launch_fdd_spectrum_out(const float2* Yt, size_t ndm, size_t nspec, float* out,
                              size_t out_stride, cudaStream_t s);
 

@@ -249,12 +249,14 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
     uint2* s_table = reinterpret_cast<uint2*>(reinterpret_cast<uint8_t*>(bars) + 256);
     const uint32_t qn = a.nfft / 4;                    // quarter-wave entries (+1)
     const bool ptab = a.dmax >= 0;
-    const uint32_t tab_n = ptab ? (uint32_t)a.dmax + 1u : qn + 1u;
+    const bool direct = !ptab && a.direct;  // phasors from the two-level twiddles
+    const bool twl = ptab || direct;        // the twiddle tables are in shared memory
+    const uint32_t tab_n = ptab ? (uint32_t)a.dmax + 1u : direct ? 0u : qn + 1u;
     // table mode: exp(-2 pi i t / N) = tw_hi[t >> 8] * tw_lo[t & 255] (FP32)
     const uint32_t nhi = a.nfft / 256;
     float2* s_tw_lo = reinterpret_cast<float2*>(s_table + tab_n);
-    float2* s_tw_hi = s_tw_lo + (ptab ? 256 : 0);
-    float* s_delay = reinterpret_cast<float*>(s_tw_hi + (ptab ? nhi : 0));
+    float2* s_tw_hi = s_tw_lo + (twl ? 256 : 0);
+    float* s_delay = reinterpret_cast<float*>(s_tw_hi + (twl ? nhi : 0));
     uint2* s_sym = reinterpret_cast<uint2*>(s_delay + a.nact_pad);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -267,7 +269,7 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
     const int nchunks = a.nact_pad / TC_CHUNK;
 
     // --- set-up -------------------------------------------------------------
-    if (!ptab) {
+    if (!twl) {
         for (uint32_t i = tid; i <= qn; i += blockDim.x) s_table[i] = a.table[i];
     } else {
         for (uint32_t i = tid; i < 256; i += blockDim.x) s_tw_lo[i] = a.tw_lo[i];
@@ -319,6 +321,7 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
         const float dm = a.dms[min(m, a.ndm - 1)];
         const uint32_t lane_addr = (uint32_t)(quad * 32) << 16;
         const uint32_t nmask = a.nfft - 1u, qshift = (uint32_t)(31 - __clz((int)qn));
+        const bool pow2n = (a.nfft & nmask) == 0u;
         const int ptid = warp * 32 + lane;                      // 0..255
         volatile uint32_t* abort_flag = &bars->abort_flag;
         uint32_t g = 0;  // global chunk counter
@@ -349,8 +352,8 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
                             // DM-major rows for the inverse FFT (successive bins of
                             // this CTA fill the same L2 sectors), else bin-major
                             const float2 y = make_float2(yr[i], yi[i]);
-                            if (a.Y) a.Y[((size_t)m * a.nseg + sb + i) * a.y_pitch + kk] = y;
-                            else a.Yt[(kk * a.nseg + sb + i) * a.ndm + m] = y;
+                            if (a.Y) a.Y[((size_t)m * a.nseg_total + a.seg0 + sb + i) * a.y_pitch + kk] = y;
+                            else a.Yt[(kk * a.nseg_total + a.seg0 + sb + i) * a.ndm + m] = y;
                         }
                 }
             }
@@ -367,9 +370,13 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
                 // every abort raised before this point is visible to all.
                 asm volatile("bar.sync 1, %0;" ::"n"(TC_PRODUCER_WARPS * 32) : "memory");
                 if (*abort_flag) { aborted = true; break; }
-                for (int d = ptid; d <= a.dmax; d += TC_PRODUCER_WARPS * 32) {
+                // idx = (k d) mod N for d = ptid, ptid + S, ... (S = 512 threads),
+                // stepped by (k S) mod N: exact for any N (N < 2^31)
+                constexpr uint32_t S = TC_PRODUCER_WARPS * 32;
+                uint32_t idx = (uint32_t)(((uint64_t)k * (uint64_t)ptid) % a.nfft);
+                const uint32_t step = (uint32_t)(((uint64_t)k * S) % a.nfft);
+                for (int d = ptid; d <= a.dmax; d += S, idx = (idx + step >= a.nfft) ? idx + step - a.nfft : idx + step) {
                     // exp(+2 pi i idx / N) = conj(tw_hi[idx >> 8] * tw_lo[idx & 255])
-                    const uint32_t idx = ((uint32_t)k * (uint32_t)d) & nmask;
                     const float2 h = s_tw_hi[idx >> 8], l = s_tw_lo[idx & 255u];
                     const float c = __fsub_rn(__fmul_rn(h.x, l.x), __fmul_rn(h.y, l.y));
                     const float sn = -__fadd_rn(__fmul_rn(h.x, l.y), __fmul_rn(h.y, l.x));
@@ -391,6 +398,30 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
                         for (int i = 0; i < TC_PART_CH; ++i) {
                             const int d = min(max(tc_delay_small(dm, s_delay[c0 + i], a.round_delays), 0), a.dmax);
                             const uint2 v = s_table[d];
+                            hi[i] = v.x;
+                            lo[i] = v.y;
+                        }
+                    } else if (direct) {
+#pragma unroll
+                        for (int i = 0; i < TC_PART_CH; ++i) {
+                            const int d = tc_delay(dm, s_delay[c0 + i], a.round_delays);
+                            uint32_t idx;
+                            if (pow2n) {
+                                idx = ((uint32_t)k * (uint32_t)d) & nmask;
+                            } else {
+                                // (k d) mod N by Barrett reduction, d taken mod N first
+                                const uint32_t dn = d >= 0 ? (uint32_t)d % a.nfft
+                                                           : a.nfft - 1u - (uint32_t)(-(d + 1)) % a.nfft;
+                                const uint64_t p = (uint64_t)k * dn;
+                                uint64_t r = p - __umul64hi(p, a.nmagic) * (uint64_t)a.nfft;
+                                while (r >= a.nfft) r -= a.nfft;
+                                idx = (uint32_t)r;
+                            }
+                            // exp(+2 pi i idx / N) = conj(tw_hi[idx >> 8] * tw_lo[idx & 255])
+                            const float2 h = s_tw_hi[idx >> 8], l = s_tw_lo[idx & 255u];
+                            const float c = __fsub_rn(__fmul_rn(h.x, l.x), __fmul_rn(h.y, l.y));
+                            const float sn = -__fadd_rn(__fmul_rn(h.x, l.y), __fmul_rn(h.y, l.x));
+                            const uint2 v = split_bf16x2(c, sn);
                             hi[i] = v.x;
                             lo[i] = v.y;
                         }
@@ -509,9 +540,15 @@ __device__ __forceinline__ uint32_t bf16x2_bits(float lo_half, float hi_half)
 __global__ void __launch_bounds__(256) fdd_prep_b_kernel(const float2* X, size_t bin_pitch, int nseg,
                                                          size_t nbins, const int32_t* chan,
                                                          const float* km, int nact, int nact_pad,
-                                                         int npad, uint32_t* B)
+                                                         int npad, uint32_t* B, BinMap map, int seg0,
+                                                         int nseg_total)
 {
-    // one block per (bin tile of 32, channel tile of 32), looping over n
+    // segments seg0 .. seg0 + nseg - 1 of X rows c * nseg_total + s
+    // one block per (tile of 32 row positions of X, channel tile of 32),
+    // looping over n; position p holds bin pbin(p) (BinMap order)
+    auto pbin = [&](size_t p) -> size_t {
+        return (map.Q <= 1 || p >= map.M) ? p : (size_t)map.Q * (p & (map.P - 1)) + p / map.P;
+    };
     __shared__ float2 tile[32][33];
     const size_t k0 = (size_t)blockIdx.x * 32;
     const int j0 = blockIdx.y * 32;
@@ -519,9 +556,9 @@ __global__ void __launch_bounds__(256) fdd_prep_b_kernel(const float2* X, size_t
     const size_t words_row = (size_t)nact_pad;  // 2*nact_pad bf16 per row
     // padding rows n in [2*nseg, npad) are zero
     for (int r = ty; r < 32; r += 8) {
-        const size_t k = k0 + r;
+        if (k0 + r >= nbins || j0 + tx >= nact_pad) continue;
+        const size_t k = pbin(k0 + r);
         const int j = j0 + tx;
-        if (k >= nbins || j >= nact_pad) continue;
         for (int n = 2 * nseg; n < npad; ++n)
             for (int sp = 0; sp < 2; ++sp) B[((k * 2 + sp) * npad + n) * words_row + j] = 0u;
     }
@@ -532,7 +569,7 @@ __global__ void __launch_bounds__(256) fdd_prep_b_kernel(const float2* X, size_t
         for (int i = 0; i < 4; ++i) {
             const int j = j0 + ty + 8 * i;
             const size_t k = k0 + tx;
-            nv[i] = (j < nact && k < nbins) ? X[((size_t)chan[j] * nseg + s) * bin_pitch + k]
+            nv[i] = (j < nact && k < nbins) ? X[((size_t)chan[j] * nseg_total + seg0 + s) * bin_pitch + k]
                                             : make_float2(0.f, 0.f);
         }
     };
@@ -548,9 +585,9 @@ __global__ void __launch_bounds__(256) fdd_prep_b_kernel(const float2* X, size_t
         if (s + 1 < nseg) load(s + 1);
         __syncthreads();
         for (int r = ty; r < 32; r += 8) {
-            const size_t k = k0 + r;
+            if (k0 + r >= nbins || j0 + tx >= nact_pad) continue;
+            const size_t k = pbin(k0 + r);
             const int j = j0 + tx;
-            if (k >= nbins || j >= nact_pad) continue;
             const float2 v = tile[tx][r];
             // real-output column s: (Xr, -Xi); imaginary-output column
             // nseg + s: (Xi, Xr); element 2j in the low half, 2j+1 high
@@ -592,20 +629,20 @@ size_t tc_b_bytes(size_t nbins, int nact_pad, int npad)
 
 int tc_pad_channels(int nact) { return ((nact + TC_CHUNK - 1) / TC_CHUNK) * TC_CHUNK; }
 int tc_pad_n(int nseg) { return ((2 * nseg + 15) / 16) * 16; }
-bool tc_supported(int nseg, unsigned nfft, int nact)
+bool tc_quarter_mode_fits(unsigned nfft, int nact_pad, int npad)
 {
-    if (2 * nseg > 128 || nfft < 256 || (nfft & (nfft - 1)) != 0 || nact <= 0) return false;
-    return tc_smem_bytes(nfft, tc_pad_channels(nact), tc_pad_n(nseg), -1, 2) <= TC_MAX_SMEM;
+    if (nfft < 256 || (nfft & (nfft - 1)) != 0) return false;  // quarter-wave indexing needs a power of two
+    return tc_smem_bytes(nfft, nact_pad, npad, -1, 2, false) <= TC_MAX_SMEM;
 }
 
 void launch_fdd_prep_b(const float2* X, size_t bin_pitch, int nseg, size_t nbins,
                        const int32_t* chan, const float* km, int nact, int nact_pad, int npad,
-                       void* B, cudaStream_t s)
+                       void* B, const BinMap& map, int seg0, int nseg_total, cudaStream_t s)
 {
     // every word of B is written (zeros for padding rows and channels)
     dim3 grid((unsigned)((nbins + 31) / 32), (unsigned)((nact_pad + 31) / 32));
     fdd_prep_b_kernel<<<grid, 256, 0, s>>>(X, bin_pitch, nseg, nbins, chan, km, nact, nact_pad, npad,
-                                           static_cast<uint32_t*>(B));
+                                           static_cast<uint32_t*>(B), map, seg0, nseg_total);
     RT_CHECK(cudaGetLastError());
 }
 
@@ -638,11 +675,13 @@ std::vector<uint2> tc_quarter_table(unsigned nfft)
     return t;
 }
 
-size_t tc_smem_bytes(unsigned nfft, int nact_pad, int npad, int dmax, int stages)
+size_t tc_smem_bytes(unsigned nfft, int nact_pad, int npad, int dmax, int stages, bool direct)
 {
     const size_t stage = 4ull * (size_t)npad * 128ull;
-    // table mode: dmax + 1 phasors + the two twiddle tables (256 + nfft/256 float2)
-    const size_t table = dmax >= 0 ? (size_t)dmax + 1 + 256 + nfft / 256 : (size_t)nfft / 4 + 1;
+    // table mode: dmax + 1 phasors + the two twiddle tables (256 + nfft/256 float2);
+    // direct mode: the twiddle tables; quarter-wave mode: nfft/4 + 1 phasors
+    const size_t table = dmax >= 0 ? (size_t)dmax + 1 + 256 + nfft / 256
+                                   : direct ? 256 + (size_t)nfft / 256 : (size_t)nfft / 4 + 1;
     const size_t need = 1024 /* base alignment */ + (size_t)stages * stage + 256 + table * 8 +
                         (size_t)nact_pad * 4 + 4 * 8;
     return std::max(need, TC_MIN_SMEM);
@@ -651,14 +690,19 @@ size_t tc_smem_bytes(unsigned nfft, int nact_pad, int npad, int dmax, int stages
 int tc_table_mode_dmax(int dmax, unsigned nfft, int nact_pad, int npad)
 {
     if (dmax < 0) return -1;
-    return tc_smem_bytes(nfft, nact_pad, npad, dmax, 2) <= TC_MAX_SMEM ? dmax : -1;
+    return tc_smem_bytes(nfft, nact_pad, npad, dmax, 2, false) <= TC_MAX_SMEM ? dmax : -1;
 }
 
-int tc_stages(unsigned nfft, int nact_pad, int npad, int dmax)
+int tc_stages(unsigned nfft, int nact_pad, int npad, int dmax, bool direct)
 {
     int st = TC_MAX_STAGES;
-    while (st > 2 && tc_smem_bytes(nfft, nact_pad, npad, dmax, st) > TC_MAX_SMEM) --st;
+    while (st > 2 && tc_smem_bytes(nfft, nact_pad, npad, dmax, st, direct) > TC_MAX_SMEM) --st;
     return st;
+}
+
+bool tc_direct_mode_fits(unsigned nfft, int nact_pad, int npad)
+{
+    return nfft % 256 == 0 && tc_smem_bytes(nfft, nact_pad, npad, -1, 2, true) <= TC_MAX_SMEM;
 }
 
 void launch_fdd_mac_tc(const TcMacArgs& a, const void* B, cudaStream_t s)
@@ -678,7 +722,7 @@ void launch_fdd_mac_tc(const TcMacArgs& a, const void* B, cudaStream_t s)
                                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "cuTensorMapEncodeTiled failed");
     if (a.stages < 2 || a.stages > TC_MAX_STAGES) DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "bad stage count");
-    const size_t smem = tc_smem_bytes(a.nfft, a.nact_pad, a.npad, a.dmax, a.stages);
+    const size_t smem = tc_smem_bytes(a.nfft, a.nact_pad, a.npad, a.dmax, a.stages, a.direct != 0);
     rt::raise_smem_limit(fdd_mac_tc_kernel, smem);
     int sms = 148;
     int dev = 0;
@@ -688,6 +732,11 @@ void launch_fdd_mac_tc(const TcMacArgs& a, const void* B, cudaStream_t s)
     int ngroups = std::max(1, sms / ntiles);
     ngroups = (int)std::min<size_t>((size_t)ngroups, a.nbins);
     TcMacArgs ka = a;
+    if (ka.nseg_total <= 0) ka.nseg_total = ka.nseg;
+    // Barrett constant floor((2^64 - 1) / N) for (k d) mod N in direct mode
+    ka.nmagic = ~0ull / (unsigned long long)ka.nfft;
+    if (ka.nseg > kTcMaxSeg || ka.seg0 + ka.nseg > ka.nseg_total)
+        DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "tensor-core MAC: bad segment group");
     ka.wait_ns = rt::wait_limit_ns();
     ka.wait_test = rt::wait_expiry_test() ? 1 : 0;
     fdd_mac_tc_kernel<<<ntiles * ngroups, TC_THREADS, smem, s>>>(map, ka);

@@ -10,6 +10,8 @@
 
 #include <cuda_bf16.h>
 
+#include "fdd_kernels.hpp"
+
 namespace dedisp {
 namespace kern {
 
@@ -25,26 +27,37 @@ struct TcMacArgs {
     unsigned* err;             // set to 1 if a bounded wait expired
     int nact_pad;              // channels, multiple of 64
     int ndm;
-    int nseg;
+    int nseg;                  // segments of this launch (2*nseg <= 128)
+    int seg0 = 0;              // first segment of this launch in Yt / Y
+    int nseg_total = 0;        // segments per bin in Yt / Y
     int npad;                  // 2*nseg rounded up to 16
     size_t nbins;
-    unsigned nfft;             // power of two
+    unsigned nfft;             // transform length (multiple of 256; quarter-wave mode: a power of two)
     int round_delays;
     int dmax;                  // >= 0: delay-table mode, every delay in 0..dmax; -1: quarter-wave mode
     int stages;                // B pipeline depth (tc_stages)
+    int direct = 0;            // dmax < 0: 1 phasors from the two-level twiddles, 0 quarter-wave table
+    unsigned long long nmagic = 0;  // set by the launcher
     unsigned long long wait_ns = 2000000000ull;  // bounded-wait limit (rt::wait_limit_ns)
     int wait_test = 0;         // expiry test (rt::wait_expiry_test)
 };
 
-// Shapes the tensor-core MAC handles: 2*nseg <= 128 output columns, a
-// power-of-two nfft >= 256, and its shared-memory footprint within a CTA.
-bool tc_supported(int nseg, unsigned nfft, int nact);
+// One launch covers at most kTcMaxSeg segments (2 x segments <= 128
+// accumulator columns); the engine runs segment groups.
+constexpr int kTcMaxSeg = 64;
+// Quarter-wave mode (the phasor table of exp(2 pi i r / N), r <= N/4) fits
+// shared memory and N is a power of two; otherwise the per-bin delay table
+// (tc_table_mode_dmax) must fit.
+bool tc_quarter_mode_fits(unsigned nfft, int nact_pad, int npad);
 int tc_pad_channels(int nact);
 int tc_pad_n(int nseg);
 size_t tc_b_bytes(size_t nbins, int nact_pad, int npad);
-size_t tc_smem_bytes(unsigned nfft, int nact_pad, int npad, int dmax, int stages);
+size_t tc_smem_bytes(unsigned nfft, int nact_pad, int npad, int dmax, int stages, bool direct);
 // Deepest B pipeline (2..6 stages) that fits shared memory.
-int tc_stages(unsigned nfft, int nact_pad, int npad, int dmax);
+int tc_stages(unsigned nfft, int nact_pad, int npad, int dmax, bool direct);
+// Direct mode (every phasor from the two-level twiddle tables, any length
+// that is a multiple of 256) fits shared memory.
+bool tc_direct_mode_fits(unsigned nfft, int nact_pad, int npad);
 // dmax if the per-bin delay table (dmax + 1 phasors) fits shared memory,
 // else -1 (the kernel then indexes the quarter-wave table per phasor).
 int tc_table_mode_dmax(int dmax, unsigned nfft, int nact_pad, int npad);
@@ -52,9 +65,11 @@ std::vector<uint2> tc_quarter_table(unsigned nfft);
 
 // X [nchans*nseg][bin_pitch] complex spectra -> B operand
 // Bsplit[bin][hi|lo][n < npad][kk < 2*nact_pad] (bf16).
+// X rows in the order `map` (fdd_kernels.hpp).
+// Segments seg0 .. seg0 + nseg - 1 of X rows c * nseg_total + s.
 void launch_fdd_prep_b(const float2* X, size_t bin_pitch, int nseg, size_t nbins,
                        const int32_t* chan, const float* km, int nact, int nact_pad, int npad,
-                       void* B, cudaStream_t s);
+                       void* B, const BinMap& map, int seg0, int nseg_total, cudaStream_t s);
 
 void launch_fdd_mac_tc(const TcMacArgs& a, const void* B, cudaStream_t s);
 
