@@ -22,7 +22,7 @@ import numpy as np
 __all__ = [
     "DedispError", "lib", "build", "Plan", "DedispPlan", "TDDPlan", "FDDGPUPlan",
     "DEDISP_USE_DEFAULT", "DEDISP_HOST_POINTERS", "DEDISP_DEVICE_POINTERS",
-    "DEDISP_WAIT", "DEDISP_ASYNC", "DEDISP_DEDISP", "DEDISP_TDD", "DEDISP_FDD",
+    "DEDISP_WAIT", "DEDISP_ASYNC", "DEDISP_DEDISP", "DEDISP_TDD", "DEDISP_FDD", "Batch", "FddBatch",
     "ERROR_NAMES",
 ]
 
@@ -347,6 +347,19 @@ _BATCH_SIGS = {
     "dedisp_b200_batch_get_timing": (C.c_int, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                                C.POINTER(C.c_int)]),
     "dedisp_b200_batch_max_delay": (_sz, [_vp, _sz]),
+    "dedisp_b200_fdd_batch_create": (C.c_int, [C.POINTER(_vp), _sz, C.c_float, C.c_float, C.c_float,
+                                               _sz, C.c_int]),
+    "dedisp_b200_fdd_batch_destroy": (None, [_vp]),
+    "dedisp_b200_fdd_batch_set_killmask": (C.c_int, [_vp, _vp]),
+    "dedisp_b200_fdd_batch_set_beams": (C.c_int, [_vp, C.POINTER(_Beam), _sz]),
+    "dedisp_b200_fdd_batch_workspace_size": (_sz, [_vp]),
+    "dedisp_b200_fdd_batch_set_workspace": (C.c_int, [_vp, _vp, _sz]),
+    "dedisp_b200_fdd_batch_execute": (C.c_int, [_vp, _vp, C.c_int]),
+    "dedisp_b200_fdd_batch_sync": (C.c_int, [_vp, _vp]),
+    "dedisp_b200_fdd_batch_set_timing": (C.c_int, [_vp, C.c_int]),
+    "dedisp_b200_fdd_batch_get_timing": (C.c_int, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                                   C.POINTER(C.c_float), C.POINTER(C.c_int)]),
+    "dedisp_b200_fdd_batch_max_delay": (_sz, [_vp, _sz]),
 }
 
 
@@ -452,6 +465,77 @@ class Batch:
 # ---------------------------------------------------------------------------
 # Streaming server (dedisp_b200_server_*)
 # ---------------------------------------------------------------------------
+
+class FddBatch:
+    """Many beams with one channel setup, dedispersed in the Fourier domain
+    (segmented time series, 3xBF16 tensor-core MAC) with ONE persistent MAC
+    launch over all of them, the whole sequence graph-captured. Beams are
+    (device input, in_stride, nsamps, DM list, device output, out_stride);
+    output rows hold nsamps - max_delay floats."""
+
+    def __init__(self, nchans: int, dt: float, f0: float, df: float, in_nbits: int = 8,
+                 device: int = 0):
+        self._h = _vp()
+        _bcheck(_batch_lib().dedisp_b200_fdd_batch_create(C.byref(self._h), nchans, dt, f0, df,
+                                                          in_nbits, device))
+        self._keep = []
+        self._ws = None
+
+    def close(self) -> None:
+        if self._h:
+            _batch_lib().dedisp_b200_fdd_batch_destroy(self._h)
+            self._h = _vp()
+        self._keep = []
+        self._ws = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_killmask(self, killmask=None) -> None:
+        if killmask is None:
+            _bcheck(_batch_lib().dedisp_b200_fdd_batch_set_killmask(self._h, None))
+            return
+        km = np.ascontiguousarray(killmask, dtype=np.int32)
+        _bcheck(_batch_lib().dedisp_b200_fdd_batch_set_killmask(self._h, km.ctypes.data))
+
+    def set_beams(self, beams) -> None:
+        """beams: sequence of (d_in, in_stride, nsamps, dm_list, d_out, out_stride)."""
+        arr = (_Beam * max(len(beams), 1))()
+        for i, (d_in, in_stride, nsamps, dms, d_out, out_stride) in enumerate(beams):
+            dm = np.ascontiguousarray(dms, dtype=np.float32)
+            arr[i] = _Beam(_addr(d_in), in_stride, nsamps, dm.ctypes.data, len(dm), _addr(d_out),
+                           out_stride)
+        _bcheck(_batch_lib().dedisp_b200_fdd_batch_set_beams(self._h, arr, len(beams)))
+        self._keep = [b[0] for b in beams] + [b[4] for b in beams]
+
+    def workspace_size(self) -> int:
+        return int(_batch_lib().dedisp_b200_fdd_batch_workspace_size(self._h))
+
+    def set_workspace(self, buf, nbytes: int) -> None:
+        _bcheck(_batch_lib().dedisp_b200_fdd_batch_set_workspace(self._h, _addr(buf), nbytes))
+        self._ws = buf
+
+    def execute(self, stream: int = 0, use_graph: bool = True) -> None:
+        _bcheck(_batch_lib().dedisp_b200_fdd_batch_execute(self._h, stream, int(use_graph)))
+
+    def sync(self, stream: int = 0) -> None:
+        _bcheck(_batch_lib().dedisp_b200_fdd_batch_sync(self._h, stream))
+
+    def set_timing(self, enable: bool = True) -> None:
+        _bcheck(_batch_lib().dedisp_b200_fdd_batch_set_timing(self._h, int(enable)))
+
+    def get_timing(self) -> dict:
+        p, m, q, n = C.c_float(), C.c_float(), C.c_float(), C.c_int()
+        _bcheck(_batch_lib().dedisp_b200_fdd_batch_get_timing(self._h, C.byref(p), C.byref(m),
+                                                              C.byref(q), C.byref(n)))
+        return {"prep_ms": p.value, "mac_ms": m.value, "post_ms": q.value, "launches": n.value}
+
+    def max_delay(self, beam: int) -> int:
+        return int(_batch_lib().dedisp_b200_fdd_batch_max_delay(self._h, beam))
+
 
 class _GulpRecord(C.Structure):
     _fields_ = [("beam", C.c_int), ("worker", C.c_int), ("nsamps", _sz), ("t_submit", C.c_double),

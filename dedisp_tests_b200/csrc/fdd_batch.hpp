@@ -1,0 +1,102 @@
+// Batched multi-beam Fourier-domain dedispersion (no counterpart in the
+// reference, whose FDDGPUPlan dedisperses one series per execute call,
+// src/fdd/FDDGPUPlan.cpp:429-546 and :725-1271).
+//
+// Beams share the channel setup (nchans, dt, f0, df, killmask, input width)
+// and each has its own device input, sample count, DM list and device output
+// (dm_count rows of nsamps - max_delay floats: the segmented overlap-save
+// time series, segment length from the reference doubling rule). One
+// execute() enqueues, per beam, the unpack, the forward real FFTs and the
+// split B operand of each segment group, then ONE persistent tensor-core
+// (3xBF16) MAC launch over a work list of (beam segment group, DM tile, bin
+// range) items of all beams, then per beam the DM-major transpose and the
+// inverse FFTs straight into the caller's rows. The sequence is captured once
+// into a CUDA graph and replayed. Results equal those of an FDDGPUPlan per
+// beam (segmented, tensor-core precision), which is what the tests check.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include "fdd_engine.hpp"
+#include "fdd_kernels.hpp"
+#include "fdd_tc.hpp"
+#include "runtime.hpp"
+#include "tdd_kernels.hpp"
+
+namespace dedisp {
+namespace detail {
+
+struct FddBeamSpec {
+    const uint8_t* in;    // device, time-major rows
+    size_t in_stride;     // bytes per input row
+    size_t nsamps;
+    std::vector<float> dms;
+    uint8_t* out;         // device, dm_count rows of nsamps - max_delay floats
+    size_t out_stride;    // bytes per output row
+};
+
+class FddBatch {
+public:
+    FddBatch(size_t nchans, float dt, float f0, float df, int in_nbits, int device);
+    ~FddBatch();
+
+    void set_killmask(const int32_t* killmask);  // nullptr: all channels
+    void set_beams(std::vector<FddBeamSpec> beams);
+    size_t beam_count() const { return m_beams.size(); }
+    size_t max_delay(size_t beam) const;
+    size_t nsamp_out(size_t beam) const;
+
+    // Device bytes of scratch and per-beam operands the batch needs.
+    size_t workspace_bytes() const;
+    // Caller-owned scratch (device, >= workspace_bytes()); nullptr: own.
+    void set_workspace(void* ptr, size_t bytes);
+
+    // Enqueues the whole batch on `stream` (graph: captured once, replayed).
+    void execute(cudaStream_t stream, bool use_graph);
+    // Waits for `stream`; DEDISP_INTERNAL_GPU_ERROR if a bounded wait of the
+    // last execute's MAC expired.
+    void sync(cudaStream_t stream);
+
+    // With timing on, execute waits for its work and reports the device time
+    // of the preparation (unpack, FFT, B operand), of the MAC launch and of the
+    // inverse side (in graph mode: the whole graph as mac_ms, the others -1).
+    bool record_timing = false;
+    float last_prep_ms = 0.f, last_mac_ms = 0.f, last_post_ms = 0.f;
+    int last_launches = 0;
+
+private:
+    struct Beam;
+    void plan();                       // geometry, modes, workspace offsets
+    void upload();                     // per-beam tables, work list
+    void enqueue(cudaStream_t s, bool timing);
+    void drop_graph();
+    uint8_t* workspace_base();
+
+    size_t m_nchans;
+    int m_nbits, m_device;
+    float m_dt;
+    std::vector<float> m_delays;       // nchans
+    std::vector<int32_t> m_km;
+    std::vector<std::unique_ptr<Beam>> m_beams;
+    bool m_dirty = true;
+    int m_nact = 0, m_nact_pad = 0;
+    size_t m_ws_bytes = 0, m_shared_bytes = 0, m_scratch_off = 0, m_scratch_bytes = 0;
+
+    rt::DeviceBuffer m_chan, m_kmv, m_delay_pad, m_err, m_items, m_twp_lo, m_twp_hi;
+    rt::DeviceBuffer m_own_ws;
+    void* m_ext_ws = nullptr;
+    size_t m_ext_ws_bytes = 0;
+    std::unique_ptr<kern::TcParams> m_params;
+    cudaGraph_t m_graph = nullptr;
+    cudaGraphExec_t m_exec = nullptr;
+    int m_graph_launches = 0;
+    std::unique_ptr<rt::Event> m_ev[4];
+};
+
+}  // namespace detail
+}  // namespace dedisp

@@ -22,7 +22,7 @@ size_t round_up(size_t a, size_t b) { return (a + b - 1) / b * b; }
 struct FddEngine::Impl {
     rt::DeviceBuffer in, x, X, Xt, Yt, Y, out, tw_lo, tw_hi, dms, chan, km, delay_act;
     // tensor-core form
-    rt::DeviceBuffer B, delay_pad, qtable, err;
+    rt::DeviceBuffer B, delay_pad, qtable, err, tcwork;
     rt::DeviceBuffer fft_tmp;  // four-step FFT scratch (nfft > 32768)
     rt::DeviceBuffer twp_lo, twp_hi, wq;  // transforms of 16384 Q points: 16384-point table, W_Q
     unsigned wq_n = 0;
@@ -271,7 +271,8 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
         ta.round_delays = opt.round_delays ? 1 : 0;
         ta.dmax = tc_dmax;
         ta.direct = tc_direct ? 1 : 0;
-        ta.stages = kern::tc_stages(ta.nfft, nact_pad, npad, ta.dmax, tc_direct);
+        const size_t wb = kern::tc_work_bytes((size_t)kern::tc_sm_count() + 64);
+        m.tcwork.reserve(wb);
         // Segment groups of at most kTcMaxSeg (the accumulator's 128
         // columns): B operand and one MAC launch per group.
         stats.launches = 0;
@@ -282,7 +283,7 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
                                     (int)nseg, st);
             ta.nseg = ns;
             ta.seg0 = (int)s0;
-            kern::launch_fdd_mac_tc(ta, m.B.get(), st);
+            kern::launch_fdd_mac_tc(ta, m.B.get(), m.tcwork.get(), wb, st);
             ++stats.launches;
         }
     } else if (m.nact > 0) {

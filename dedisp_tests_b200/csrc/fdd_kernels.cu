@@ -1272,6 +1272,20 @@ void launch_fft_c2r(float2* Y, size_t bin_pitch, size_t ndm, size_t nseg, int nf
 
 size_t fft_scratch_elems(int nfft, size_t rows) { return nfft > 32768 ? rows * (size_t)(nfft / 2) : 0; }
 
+void make_twiddle_tables(size_t n, std::vector<float2>& lo, std::vector<float2>& hi)
+{
+    lo.resize(256);
+    hi.resize(n / 256);
+    for (unsigned l = 0; l < 256; ++l) {
+        const double a = -2.0 * 3.14159265358979323846 * (double)l / (double)n;
+        lo[l] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    for (size_t h = 0; h < hi.size(); ++h) {
+        const double a = -2.0 * 3.14159265358979323846 * (double)h * 256.0 / (double)n;
+        hi[h] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+}
+
 bool fftq_length(size_t nfft)
 {
     return nfft >= 16384 && nfft % 16384 == 0 && fftq_tile((unsigned)(nfft / 16384)) > 0 &&

@@ -28,6 +28,10 @@ struct TwiddleTable {
     unsigned n;
 };
 
+// Host tables of W_N^t (two-level, FP64-computed): lo[t] t < 256,
+// hi[h] = W_N^{256 h}, h < N / 256.
+void make_twiddle_tables(size_t n, std::vector<float2>& lo, std::vector<float2>& hi);
+
 // Bin order of a spectrum row. Q <= 1: natural (bin k at position k).
 // Q > 1 (transforms of N = 16384 Q points, M = N / 2 = P Q, P = 8192): bin
 // k < M at position (k mod Q) P + k / Q, bin M at position M.

@@ -29,6 +29,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <memory>
+#include <type_traits>
 #include <vector>
 
 #include "fdd_tc.hpp"
@@ -231,51 +233,43 @@ __device__ __forceinline__ uint2 split_bf16x2(float re, float im)
     return make_uint2(*reinterpret_cast<const uint32_t*>(&hi), *reinterpret_cast<const uint32_t*>(&lo));
 }
 
-__global__ void __launch_bounds__(TC_THREADS, 1)
-fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
+// The MAC over a work list: item i = bins [k_begin, k_end) of DM tile `tile`
+// of descriptor `desc` (its own DM list, length, B operand and tensor map,
+// output and segment group); CTA b takes items b, b + G, b + 2G, ... The
+// pipeline counters run on across items, so the hand-offs of consecutive
+// items overlap; each item's last accumulator is read out before the next
+// item starts. One plan's launch is the one-descriptor case.
+__global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_constant__ TcParams P)
 {
+    // descriptors and tensor maps live in the parameter bank (constant
+    // operands, no registers); the items in global memory
+    const TcMacArgs* descs = P.descs;
+    const CUtensorMap* maps = P.maps;
+    const TcWork* items = P.items;
+    const int nitems = P.nitems;
+    const TcLayout& L = P.layout;
     extern __shared__ __align__(1024) uint8_t smem_dyn[];
     // layout (from a 1024-byte aligned base, as the 128-byte swizzle needs):
-    // [B stages][barriers][phasor table][delays][sym]; the phasor table is
-    // the quarter-wave table (nfft/4 + 1 entries) or, in delay-table mode
-    // (a.dmax >= 0), the phasors of the current bin for every delay 0..dmax
+    // [B stages][barriers][phasor table][twiddles lo, hi][delays][sym]; the
+    // phasor table is the quarter-wave table (nfft/4 + 1 entries) or, in
+    // delay-table mode (dmax >= 0), the phasors of the current bin for every
+    // delay 0..dmax; each region is sized for the largest descriptor
     uint8_t* smem_raw = smem_dyn + ((1024u - (smem_u32(smem_dyn) & 1023u)) & 1023u);
-    const uint32_t npad = (uint32_t)a.npad;
-    const uint32_t atom_bytes = npad * 128u;           // one 64-kk atom of one split
-    const uint32_t stage_bytes = 4u * atom_bytes;      // hi/lo x 2 atoms
     uint8_t* s_b = smem_raw;
-    const int nst = a.stages;
-    SmemBarriers* bars = reinterpret_cast<SmemBarriers*>(smem_raw + nst * stage_bytes);
+    const int nst = L.stages;
+    SmemBarriers* bars = reinterpret_cast<SmemBarriers*>(smem_raw + nst * L.stage_bytes);
     uint2* s_table = reinterpret_cast<uint2*>(reinterpret_cast<uint8_t*>(bars) + 256);
-    const uint32_t qn = a.nfft / 4;                    // quarter-wave entries (+1)
-    const bool ptab = a.dmax >= 0;
-    const bool direct = !ptab && a.direct;  // phasors from the two-level twiddles
-    const bool twl = ptab || direct;        // the twiddle tables are in shared memory
-    const uint32_t tab_n = ptab ? (uint32_t)a.dmax + 1u : direct ? 0u : qn + 1u;
-    // table mode: exp(-2 pi i t / N) = tw_hi[t >> 8] * tw_lo[t & 255] (FP32)
-    const uint32_t nhi = a.nfft / 256;
-    float2* s_tw_lo = reinterpret_cast<float2*>(s_table + tab_n);
-    float2* s_tw_hi = s_tw_lo + (twl ? 256 : 0);
-    float* s_delay = reinterpret_cast<float*>(s_tw_hi + (twl ? nhi : 0));
-    uint2* s_sym = reinterpret_cast<uint2*>(s_delay + a.nact_pad);
+    float2* s_tw_lo = reinterpret_cast<float2*>(s_table + L.table_entries);
+    float2* s_tw_hi = s_tw_lo + 256;
+    float* s_delay = reinterpret_cast<float*>(s_tw_hi + L.tw_hi_entries);
+    uint2* s_sym = reinterpret_cast<uint2*>(s_delay + L.nact_pad);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int ntiles = (a.ndm + TC_M - 1) / TC_M;
-    const int tile = blockIdx.x % ntiles, group = blockIdx.x / ntiles;
-    const int ngroups = gridDim.x / ntiles;
-    if (group >= ngroups) return;  // whole CTA leaves before touching barriers
-    const size_t k_begin = a.nbins * (size_t)group / ngroups;
-    const size_t k_end = a.nbins * (size_t)(group + 1) / ngroups;
-    const int nchunks = a.nact_pad / TC_CHUNK;
+    if ((int)blockIdx.x >= nitems) return;  // whole CTA leaves before touching barriers
+    const int nchunks = L.nact_pad / TC_CHUNK;
 
     // --- set-up -------------------------------------------------------------
-    if (!twl) {
-        for (uint32_t i = tid; i <= qn; i += blockDim.x) s_table[i] = a.table[i];
-    } else {
-        for (uint32_t i = tid; i < 256; i += blockDim.x) s_tw_lo[i] = a.tw_lo[i];
-        for (uint32_t i = tid; i < nhi; i += blockDim.x) s_tw_hi[i] = a.tw_hi[i];
-    }
-    for (int i = tid; i < a.nact_pad; i += blockDim.x) s_delay[i] = a.delay_act[i];
+    for (int i = tid; i < L.nact_pad; i += blockDim.x) s_delay[i] = descs[0].delay_act[i];
     if (tid < 4) {
         // quadrant q of exp(+i theta): (re, im) = R^q (c, s); in packed
         // bf16x2 (re low half, im high half): selector swaps halves,
@@ -315,210 +309,255 @@ fdd_mac_tc_kernel(const __grid_constant__ CUtensorMap bmap, TcMacArgs a)
         // --- phasor producers + epilogue ------------------------------------
         // Order per bin k: (delay-table mode: rebuild the table for k), store
         // the A chunks of k, then read out the accumulator of bin k-1 while
-        // the tensor cores work on k.
+        // the tensor cores work on k. Every producer warp passes the same
+        // named barriers (bar 1) in the same order, on failure too: a warp
+        // that gives up sets abort_flag and goes on to the next barrier,
+        // where all of them see the flag and stop together.
         const int quad = warp & 3, part = warp >> 2;
-        const int m = tile * TC_M + quad * 32 + lane;          // this thread's DM row
-        const float dm = a.dms[min(m, a.ndm - 1)];
         const uint32_t lane_addr = (uint32_t)(quad * 32) << 16;
-        const uint32_t nmask = a.nfft - 1u, qshift = (uint32_t)(31 - __clz((int)qn));
-        const bool pow2n = (a.nfft & nmask) == 0u;
-        const int ptid = warp * 32 + lane;                      // 0..255
+        const int ptid = warp * 32 + lane;                      // 0..511
         volatile uint32_t* abort_flag = &bars->abort_flag;
-        uint32_t g = 0;  // global chunk counter
-        int bin_iter = 0;
-
-        auto epilogue = [&](int it, size_t kk) -> bool {
-            const uint32_t cb = (uint32_t)it & 1u;
-            if (!mbar_wait_warp(&bars->c_full[cb], ((uint32_t)it >> 1) & 1u, a.wait_ns)) return false;
-            tc_fence_after();
-            const uint32_t ccol = cb ? TM_C1 : TM_C0;
-            const int sh = (a.nseg + TC_PARTS - 1) / TC_PARTS;
-            const int s0 = min(a.nseg, part * sh), s1 = min(a.nseg, s0 + sh);
-            for (int sb = s0; sb < s1; sb += 8) {
-                const int cnt = min(8, s1 - sb);  // the same for the whole warp
-                float yr[8], yi[8];
-#pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    if (i < cnt) {
-                        yr[i] = tmem_ld1(tmem + lane_addr + ccol + sb + i);
-                        yi[i] = tmem_ld1(tmem + lane_addr + ccol + a.nseg + sb + i);
-                    }
+        uint32_t g = 0;    // chunk counter (A buffers)
+        int bin_iter = 0;  // bin counter (accumulators)
+        int cur_desc = -1; // descriptor whose tables are in shared memory
+        for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+            asm volatile("bar.sync 1, %0;" ::"n"(TC_PRODUCER_WARPS * 32) : "memory");
+            if (*abort_flag) { ok = false; break; }
+            const TcWork w = items[it];
+            const TcMacArgs& a = descs[w.desc];  // read-only descriptor (L1)
+            const uint32_t nfft = a.nfft, qn = nfft / 4;
+            const bool ptab = a.dmax >= 0;
+            const bool direct = !ptab && a.direct;
+            const bool twl = ptab || direct;
+            if (w.desc != cur_desc) {
+                // this descriptor's tables (all producers are past the last
+                // item's reads: barrier above)
+                if (!twl) {
+                    for (uint32_t i = ptid; i <= qn; i += TC_PRODUCER_WARPS * 32) s_table[i] = a.table[i];
+                } else {
+                    for (uint32_t i = ptid; i < 256; i += TC_PRODUCER_WARPS * 32) s_tw_lo[i] = a.tw_lo[i];
+                    for (uint32_t i = ptid; i < nfft / 256; i += TC_PRODUCER_WARPS * 32) s_tw_hi[i] = a.tw_hi[i];
                 }
-                tmem_wait_ld();
-                if (m < a.ndm) {
+                cur_desc = w.desc;
+            }
+            asm volatile("bar.sync 1, %0;" ::"n"(TC_PRODUCER_WARPS * 32) : "memory");
+            const int m = w.tile * TC_M + quad * 32 + lane;          // this thread's DM row
+            const float dm = a.dms[min(m, a.ndm - 1)];
+            const int first_iter = bin_iter;
+
+            auto epilogue = [&](int itr, size_t kk) -> bool {
+                const uint32_t cb = (uint32_t)itr & 1u;
+                if (!mbar_wait_warp(&bars->c_full[cb], ((uint32_t)itr >> 1) & 1u, L.wait_ns)) return false;
+                tc_fence_after();
+                const uint32_t ccol = cb ? TM_C1 : TM_C0;
+                const int sh = (a.nseg + TC_PARTS - 1) / TC_PARTS;
+                const int s0 = min(a.nseg, part * sh), s1 = min(a.nseg, s0 + sh);
+                // the row's output element offsets: Y (DM-major) or Yt (bin-major)
+                float2* const yrow = a.Y ? a.Y + ((size_t)m * a.nseg_total + a.seg0) * a.y_pitch + kk
+                                         : a.Yt + (kk * a.nseg_total + a.seg0) * a.ndm + m;
+                const size_t ystep = a.Y ? a.y_pitch : (size_t)a.ndm;
+                const bool mine = m < a.ndm;
+                for (int sb = s0; sb < s1; sb += 4) {
+                    const int cnt = min(4, s1 - sb);  // the same for the whole warp
+                    float yr[4], yi[4];
 #pragma unroll
-                    for (int i = 0; i < 8; ++i)
+                    for (int i = 0; i < 4; ++i) {
                         if (i < cnt) {
-                            // DM-major rows for the inverse FFT (successive bins of
-                            // this CTA fill the same L2 sectors), else bin-major
-                            const float2 y = make_float2(yr[i], yi[i]);
-                            if (a.Y) a.Y[((size_t)m * a.nseg_total + a.seg0 + sb + i) * a.y_pitch + kk] = y;
-                            else a.Yt[(kk * a.nseg_total + a.seg0 + sb + i) * a.ndm + m] = y;
-                        }
-                }
-            }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&bars->c_empty[cb]);
-            return true;
-        };
-
-        bool aborted = false;
-        for (size_t k = k_begin; k < k_end; ++k, ++bin_iter) {
-            if (ptab) {
-                // All producers are done with the previous bin's table, and
-                // every abort raised before this point is visible to all.
-                asm volatile("bar.sync 1, %0;" ::"n"(TC_PRODUCER_WARPS * 32) : "memory");
-                if (*abort_flag) { aborted = true; break; }
-                // idx = (k d) mod N for d = ptid, ptid + S, ... (S = 512 threads),
-                // stepped by (k S) mod N: exact for any N (N < 2^31)
-                constexpr uint32_t S = TC_PRODUCER_WARPS * 32;
-                uint32_t idx = (uint32_t)(((uint64_t)k * (uint64_t)ptid) % a.nfft);
-                const uint32_t step = (uint32_t)(((uint64_t)k * S) % a.nfft);
-                for (int d = ptid; d <= a.dmax; d += S, idx = (idx + step >= a.nfft) ? idx + step - a.nfft : idx + step) {
-                    // exp(+2 pi i idx / N) = conj(tw_hi[idx >> 8] * tw_lo[idx & 255])
-                    const float2 h = s_tw_hi[idx >> 8], l = s_tw_lo[idx & 255u];
-                    const float c = __fsub_rn(__fmul_rn(h.x, l.x), __fmul_rn(h.y, l.y));
-                    const float sn = -__fadd_rn(__fmul_rn(h.x, l.y), __fmul_rn(h.y, l.x));
-                    s_table[d] = split_bf16x2(c, sn);
-                }
-                asm volatile("bar.sync 1, %0;" ::"n"(TC_PRODUCER_WARPS * 32) : "memory");
-            } else if (!ok) {
-                break;
-            }
-            if (ok) {
-                for (int ch = 0; ch < nchunks; ++ch, ++g) {
-                    const uint32_t buf = g & 1u;
-                    // the phasors first: their gathers overlap the MMAs still
-                    // reading this A buffer
-                    uint32_t hi[TC_PART_CH], lo[TC_PART_CH];
-                    const int c0 = ch * TC_CHUNK + part * TC_PART_CH;
-                    if (ptab) {
-#pragma unroll
-                        for (int i = 0; i < TC_PART_CH; ++i) {
-                            const int d = min(max(tc_delay_small(dm, s_delay[c0 + i], a.round_delays), 0), a.dmax);
-                            const uint2 v = s_table[d];
-                            hi[i] = v.x;
-                            lo[i] = v.y;
-                        }
-                    } else if (direct) {
-#pragma unroll
-                        for (int i = 0; i < TC_PART_CH; ++i) {
-                            const int d = tc_delay(dm, s_delay[c0 + i], a.round_delays);
-                            uint32_t idx;
-                            if (pow2n) {
-                                idx = ((uint32_t)k * (uint32_t)d) & nmask;
-                            } else {
-                                // (k d) mod N by Barrett reduction, d taken mod N first
-                                const uint32_t dn = d >= 0 ? (uint32_t)d % a.nfft
-                                                           : a.nfft - 1u - (uint32_t)(-(d + 1)) % a.nfft;
-                                const uint64_t p = (uint64_t)k * dn;
-                                uint64_t r = p - __umul64hi(p, a.nmagic) * (uint64_t)a.nfft;
-                                while (r >= a.nfft) r -= a.nfft;
-                                idx = (uint32_t)r;
-                            }
-                            // exp(+2 pi i idx / N) = conj(tw_hi[idx >> 8] * tw_lo[idx & 255])
-                            const float2 h = s_tw_hi[idx >> 8], l = s_tw_lo[idx & 255u];
-                            const float c = __fsub_rn(__fmul_rn(h.x, l.x), __fmul_rn(h.y, l.y));
-                            const float sn = -__fadd_rn(__fmul_rn(h.x, l.y), __fmul_rn(h.y, l.x));
-                            const uint2 v = split_bf16x2(c, sn);
-                            hi[i] = v.x;
-                            lo[i] = v.y;
-                        }
-                    } else {
-#pragma unroll
-                        for (int i = 0; i < TC_PART_CH; ++i) {
-                            const int d = tc_delay(dm, s_delay[c0 + i], a.round_delays);
-                            const uint32_t idx = ((uint32_t)k * (uint32_t)d) & nmask;
-                            const uint32_t q = idx >> qshift, r = idx & (qn - 1u);
-                            const uint2 t = s_table[r];
-                            const uint2 sy = s_sym[q];
-                            hi[i] = __byte_perm(t.x, 0u, sy.x) ^ sy.y;
-                            lo[i] = __byte_perm(t.y, 0u, sy.x) ^ sy.y;
+                            yr[i] = tmem_ld1(tmem + lane_addr + ccol + sb + i);
+                            yi[i] = tmem_ld1(tmem + lane_addr + ccol + a.nseg + sb + i);
                         }
                     }
-                    if (!mbar_wait_warp(&bars->a_empty[buf], ((g >> 1) & 1u) ^ 1u, a.wait_ns)) { ok = false; break; }
-                    tc_fence_after();
-                    const uint32_t acol = buf ? TM_A1 : TM_A0;
-                    tmem_st16(tmem + lane_addr + acol + part * TC_PART_CH, hi);
-                    tmem_st16(tmem + lane_addr + acol + 64 + part * TC_PART_CH, lo);
-                    tmem_wait_st();
-                    tc_fence_before();
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(&bars->a_full[buf]);
+                    tmem_wait_ld();
+                    if (mine) {
+#pragma unroll
+                        for (int i = 0; i < 4; ++i)
+                            if (i < cnt) yrow[(size_t)(sb + i) * ystep] = make_float2(yr[i], yi[i]);
+                    }
                 }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bars->c_empty[cb]);
+                return true;
+            };
+
+            const uint32_t nmask = nfft - 1u, qshift = (uint32_t)(31 - __clz((int)max(qn, 1u)));
+            const bool pow2n = (nfft & nmask) == 0u;
+            bool aborted = false;
+            // k == k_end: only the read-out of the item's last bin (one call
+            // site of the epilogue keeps it inlined once)
+            for (size_t k = w.k_begin; k <= w.k_end; ++k) {
+                const bool tail = k == w.k_end;
+                if (tail) {
+                    if (ok && bin_iter > first_iter) ok = epilogue(bin_iter - 1, k - 1);
+                    if (!ok) *abort_flag = 1u;
+                    break;
+                }
+                if (ptab) {
+                    // All producers are done with the previous bin's table, and
+                    // every abort raised before this point is visible to all.
+                    asm volatile("bar.sync 1, %0;" ::"n"(TC_PRODUCER_WARPS * 32) : "memory");
+                    if (*abort_flag) { aborted = true; break; }
+                    // idx = (k d) mod N for d = ptid, ptid + S, ... (S = 512 threads),
+                    // stepped by (k S) mod N: exact for any N (N < 2^31)
+                    constexpr uint32_t S = TC_PRODUCER_WARPS * 32;
+                    uint32_t idx = (uint32_t)(((uint64_t)k * (uint64_t)ptid) % nfft);
+                    const uint32_t step = (uint32_t)(((uint64_t)k * S) % nfft);
+                    for (int d = ptid; d <= a.dmax; d += S, idx = (idx + step >= nfft) ? idx + step - nfft : idx + step) {
+                        // exp(+2 pi i idx / N) = conj(tw_hi[idx >> 8] * tw_lo[idx & 255])
+                        const float2 h = s_tw_hi[idx >> 8], l = s_tw_lo[idx & 255u];
+                        const float c = __fsub_rn(__fmul_rn(h.x, l.x), __fmul_rn(h.y, l.y));
+                        const float sn = -__fadd_rn(__fmul_rn(h.x, l.y), __fmul_rn(h.y, l.x));
+                        s_table[d] = split_bf16x2(c, sn);
+                    }
+                    asm volatile("bar.sync 1, %0;" ::"n"(TC_PRODUCER_WARPS * 32) : "memory");
+                } else if (!ok) {
+                    break;
+                }
+                if (ok) {
+                    for (int ch = 0; ch < nchunks; ++ch, ++g) {
+                        const uint32_t buf = g & 1u;
+                        // the phasors first: their gathers overlap the MMAs still
+                        // reading this A buffer
+                        uint32_t hi[TC_PART_CH], lo[TC_PART_CH];
+                        const int c0 = ch * TC_CHUNK + part * TC_PART_CH;
+                        if (ptab) {
+#pragma unroll
+                            for (int i = 0; i < TC_PART_CH; ++i) {
+                                const int d = min(max(tc_delay_small(dm, s_delay[c0 + i], a.round_delays), 0), a.dmax);
+                                const uint2 v = s_table[d];
+                                hi[i] = v.x;
+                                lo[i] = v.y;
+                            }
+                        } else if (direct) {
+#pragma unroll
+                            for (int i = 0; i < TC_PART_CH; ++i) {
+                                const int d = tc_delay(dm, s_delay[c0 + i], a.round_delays);
+                                uint32_t idx;
+                                if (pow2n) {
+                                    idx = ((uint32_t)k * (uint32_t)d) & nmask;
+                                } else {
+                                    // (k d) mod N by Barrett reduction, d taken mod N first
+                                    const uint32_t dn = d >= 0 ? (uint32_t)d % nfft
+                                                               : nfft - 1u - (uint32_t)(-(d + 1)) % nfft;
+                                    const uint64_t p = (uint64_t)k * dn;
+                                    uint64_t r = p - __umul64hi(p, a.nmagic) * (uint64_t)nfft;
+                                    while (r >= nfft) r -= nfft;
+                                    idx = (uint32_t)r;
+                                }
+                                // exp(+2 pi i idx / N) = conj(tw_hi[idx >> 8] * tw_lo[idx & 255])
+                                const float2 h = s_tw_hi[idx >> 8], l = s_tw_lo[idx & 255u];
+                                const float c = __fsub_rn(__fmul_rn(h.x, l.x), __fmul_rn(h.y, l.y));
+                                const float sn = -__fadd_rn(__fmul_rn(h.x, l.y), __fmul_rn(h.y, l.x));
+                                const uint2 v = split_bf16x2(c, sn);
+                                hi[i] = v.x;
+                                lo[i] = v.y;
+                            }
+                        } else {
+#pragma unroll
+                            for (int i = 0; i < TC_PART_CH; ++i) {
+                                const int d = tc_delay(dm, s_delay[c0 + i], a.round_delays);
+                                const uint32_t idx = ((uint32_t)k * (uint32_t)d) & nmask;
+                                const uint32_t q = idx >> qshift, r = idx & (qn - 1u);
+                                const uint2 t = s_table[r];
+                                const uint2 sy = s_sym[q];
+                                hi[i] = __byte_perm(t.x, 0u, sy.x) ^ sy.y;
+                                lo[i] = __byte_perm(t.y, 0u, sy.x) ^ sy.y;
+                            }
+                        }
+                        if (!mbar_wait_warp(&bars->a_empty[buf], ((g >> 1) & 1u) ^ 1u, L.wait_ns)) { ok = false; break; }
+                        tc_fence_after();
+                        const uint32_t acol = buf ? TM_A1 : TM_A0;
+                        tmem_st16(tmem + lane_addr + acol + part * TC_PART_CH, hi);
+                        tmem_st16(tmem + lane_addr + acol + 64 + part * TC_PART_CH, lo);
+                        tmem_wait_st();
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(&bars->a_full[buf]);
+                    }
+                }
+                if (ok && bin_iter > first_iter) ok = epilogue(bin_iter - 1, k - 1);
+                if (!ok) *abort_flag = 1u;  // the others stop at the next barrier
+                ++bin_iter;
             }
-            if (ok && bin_iter > 0) ok = epilogue(bin_iter - 1, k - 1);
-            if (!ok && ptab) *abort_flag = 1u;  // the others stop at the next barrier
+            if (aborted) ok = false;
+            if (!ok) *abort_flag = 1u;
         }
-        if (ok && !aborted && bin_iter > 0) ok = epilogue(bin_iter - 1, k_end - 1);
-        if (aborted) ok = false;
     } else if (warp == TC_PRODUCER_WARPS) {
         // --- TMA producer ------------------------------------------------------
         if (lane == 0) {
             uint32_t g = 0;
-            for (size_t k = k_begin; k < k_end && ok; ++k) {
-                for (int ch = 0; ch < nchunks; ++ch, ++g) {
-                    const uint32_t st = g % (uint32_t)nst;
-                    if (!mbar_wait(&bars->b_empty[st], ((g / nst) & 1u) ^ 1u, a.wait_ns)) { ok = false; break; }
-                    mbar_expect_tx(&bars->b_full[st], stage_bytes);
-                    uint8_t* dst = s_b + st * stage_bytes;
-                    // coordinates: (kk, n, split, bin)
-                    for (int sp = 0; sp < 2; ++sp)
-                        for (int at = 0; at < 2; ++at)
-                            tma_load_4d(dst + (sp * 2 + at) * atom_bytes, &bmap, &bars->b_full[st],
-                                        ch * 128 + at * 64, 0, sp, (int)k);
+            for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+                const TcWork w = items[it];
+                const CUtensorMap* bmap = maps + w.desc;
+                const uint32_t atom_bytes = (uint32_t)descs[w.desc].npad * 128u;  // one 64-kk atom of one split
+                for (size_t k = w.k_begin; k < w.k_end && ok; ++k) {
+                    for (int ch = 0; ch < nchunks; ++ch, ++g) {
+                        const uint32_t st = g % (uint32_t)nst;
+                        if (!mbar_wait(&bars->b_empty[st], ((g / nst) & 1u) ^ 1u, L.wait_ns)) { ok = false; break; }
+                        mbar_expect_tx(&bars->b_full[st], 4u * atom_bytes);
+                        uint8_t* dst = s_b + st * L.stage_bytes;
+                        // coordinates: (kk, n, split, bin)
+                        for (int sp = 0; sp < 2; ++sp)
+                            for (int at = 0; at < 2; ++at)
+                                tma_load_4d(dst + (sp * 2 + at) * atom_bytes, bmap, &bars->b_full[st],
+                                            ch * 128 + at * 64, 0, sp, (int)k);
+                    }
                 }
             }
             // do not leave while loads are in flight: wait for the last stages
             const uint32_t issued = g;
             for (uint32_t j = (issued > (uint32_t)nst ? issued - nst : 0); j < issued; ++j)
-                mbar_wait(&bars->b_full[j % nst], (j / nst) & 1u, a.wait_ns);
+                mbar_wait(&bars->b_full[j % nst], (j / nst) & 1u, L.wait_ns);
         }
     } else {
         // --- MMA issuer ----------------------------------------------------------
         if (lane == 0) {
-            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((npad >> 3) << 17) |
-                                   ((uint32_t)(TC_M >> 4) << 24);
             uint32_t g = 0;
             int bin_iter = 0;
-            for (size_t k = k_begin; k < k_end && ok; ++k, ++bin_iter) {
-                const uint32_t cb = (uint32_t)bin_iter & 1u;
-                if (!mbar_wait(&bars->c_empty[cb], (((uint32_t)bin_iter >> 1) & 1u) ^ 1u, a.wait_ns)) { ok = false; break; }
-                tc_fence_after();
-                const uint32_t dcol = tmem + (cb ? TM_C1 : TM_C0);
-                for (int ch = 0; ch < nchunks; ++ch, ++g) {
-                    const uint32_t buf = g & 1u, st = g % (uint32_t)nst;
-                    if (!mbar_wait(&bars->a_full[buf], (g >> 1) & 1u, a.wait_ns)) { ok = false; break; }
-                    if (!mbar_wait(&bars->b_full[st], (g / nst) & 1u, a.wait_ns)) { ok = false; break; }
-                    // expiry test: one more wait, on a barrier nothing arrives on
-                    if (a.wait_test && g == 0 && !mbar_wait(&bars->never, 0u, a.wait_ns)) { ok = false; break; }
+            for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+                const TcWork w = items[it];
+                const uint32_t npad = (uint32_t)descs[w.desc].npad;
+                const uint32_t atom_bytes = npad * 128u;
+                const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((npad >> 3) << 17) |
+                                       ((uint32_t)(TC_M >> 4) << 24);
+                for (size_t k = w.k_begin; k < w.k_end && ok; ++k, ++bin_iter) {
+                    const uint32_t cb = (uint32_t)bin_iter & 1u;
+                    if (!mbar_wait(&bars->c_empty[cb], (((uint32_t)bin_iter >> 1) & 1u) ^ 1u, L.wait_ns)) { ok = false; break; }
                     tc_fence_after();
-                    const uint32_t acol = tmem + (buf ? TM_A1 : TM_A0);
-                    const uint32_t bbase = smem_u32(s_b + st * stage_bytes);
+                    const uint32_t dcol = tmem + (cb ? TM_C1 : TM_C0);
+                    for (int ch = 0; ch < nchunks; ++ch, ++g) {
+                        const uint32_t buf = g & 1u, st = g % (uint32_t)nst;
+                        if (!mbar_wait(&bars->a_full[buf], (g >> 1) & 1u, L.wait_ns)) { ok = false; break; }
+                        if (!mbar_wait(&bars->b_full[st], (g / nst) & 1u, L.wait_ns)) { ok = false; break; }
+                        // expiry test: one more wait, on a barrier nothing arrives on
+                        if (L.wait_test && g == 0 && !mbar_wait(&bars->never, 0u, L.wait_ns)) { ok = false; break; }
+                        tc_fence_after();
+                        const uint32_t acol = tmem + (buf ? TM_A1 : TM_A0);
+                        const uint32_t bbase = smem_u32(s_b + st * L.stage_bytes);
 #pragma unroll
-                    for (int s = 0; s < 8; ++s) {
-                        const uint32_t at = (uint32_t)s >> 2, sub = (uint32_t)s & 3u;
-                        const uint64_t bh = sw128_desc(bbase + (0 * 2 + at) * atom_bytes + sub * 32);
-                        const uint64_t bl = sw128_desc(bbase + (1 * 2 + at) * atom_bytes + sub * 32);
-                        const uint32_t ah = acol + s * 8, al = acol + 64 + s * 8;
-                        const uint32_t first = (ch == 0 && s == 0) ? 0u : 1u;
-                        mma_ts(dcol, ah, bh, idesc, first);
-                        mma_ts(dcol, ah, bl, idesc, 1u);
-                        mma_ts(dcol, al, bh, idesc, 1u);
+                        for (int s = 0; s < 8; ++s) {
+                            const uint32_t at = (uint32_t)s >> 2, sub = (uint32_t)s & 3u;
+                            const uint64_t bh = sw128_desc(bbase + (0 * 2 + at) * atom_bytes + sub * 32);
+                            const uint64_t bl = sw128_desc(bbase + (1 * 2 + at) * atom_bytes + sub * 32);
+                            const uint32_t ah = acol + s * 8, al = acol + 64 + s * 8;
+                            const uint32_t first = (ch == 0 && s == 0) ? 0u : 1u;
+                            mma_ts(dcol, ah, bh, idesc, first);
+                            mma_ts(dcol, ah, bl, idesc, 1u);
+                            mma_ts(dcol, al, bh, idesc, 1u);
+                        }
+                        mma_commit(&bars->a_empty[buf]);
+                        mma_commit(&bars->b_empty[st]);
                     }
-                    mma_commit(&bars->a_empty[buf]);
-                    mma_commit(&bars->b_empty[st]);
+                    if (!ok) break;
+                    mma_commit(&bars->c_full[cb]);
                 }
-                if (!ok) break;
-                mma_commit(&bars->c_full[cb]);
             }
             // all issued MMAs complete before the accumulator memory goes away
             mma_commit(&bars->drain);
-            mbar_wait(&bars->drain, 0, a.wait_ns);
+            mbar_wait(&bars->drain, 0, L.wait_ns);
         }
     }
-    if (!ok) atomicExch(a.err, 1u);
+    if (!ok) atomicExch(L.err, 1u);
 
     tc_fence_before();
     __syncthreads();
@@ -677,12 +716,14 @@ std::vector<uint2> tc_quarter_table(unsigned nfft)
 
 size_t tc_smem_bytes(unsigned nfft, int nact_pad, int npad, int dmax, int stages, bool direct)
 {
+    // the layout of fdd_mac_tc_kernel (tc_layout) for one descriptor:
+    // table mode: dmax + 1 phasors and the twiddle tables; direct mode: the
+    // twiddle tables; quarter-wave mode: nfft/4 + 1 phasors
     const size_t stage = 4ull * (size_t)npad * 128ull;
-    // table mode: dmax + 1 phasors + the two twiddle tables (256 + nfft/256 float2);
-    // direct mode: the twiddle tables; quarter-wave mode: nfft/4 + 1 phasors
-    const size_t table = dmax >= 0 ? (size_t)dmax + 1 + 256 + nfft / 256
-                                   : direct ? 256 + (size_t)nfft / 256 : (size_t)nfft / 4 + 1;
-    const size_t need = 1024 /* base alignment */ + (size_t)stages * stage + 256 + table * 8 +
+    const size_t table = dmax >= 0 ? (size_t)dmax + 1 : direct ? 0 : (size_t)nfft / 4 + 1;
+    const size_t hi = (dmax >= 0 || direct) ? (size_t)nfft / 256 : 0;
+    const size_t need = 1024 /* base alignment */ + (size_t)stages * stage + 256 +
+                        (((table + 1) & ~(size_t)1) + 256 + ((hi + 1) & ~(size_t)1)) * 8 +
                         (size_t)nact_pad * 4 + 4 * 8;
     return std::max(need, TC_MIN_SMEM);
 }
@@ -705,10 +746,10 @@ bool tc_direct_mode_fits(unsigned nfft, int nact_pad, int npad)
     return nfft % 256 == 0 && tc_smem_bytes(nfft, nact_pad, npad, -1, 2, true) <= TC_MAX_SMEM;
 }
 
-void launch_fdd_mac_tc(const TcMacArgs& a, const void* B, cudaStream_t s)
+void tc_encode_map(void* map_out, const TcMacArgs& a, const void* B)
 {
     // Tensor map over Bsplit[bin][split][n][kk]: dims (kk, n, split, bin).
-    CUtensorMap map;
+    CUtensorMap* map = static_cast<CUtensorMap*>(map_out);
     const cuuint64_t dims[4] = {(cuuint64_t)(2 * a.nact_pad), (cuuint64_t)a.npad, 2,
                                 (cuuint64_t)a.nbins};
     const cuuint64_t strides[3] = {(cuuint64_t)(2 * a.nact_pad) * 2,
@@ -716,31 +757,136 @@ void launch_fdd_mac_tc(const TcMacArgs& a, const void* B, cudaStream_t s)
                                    (cuuint64_t)(2 * a.nact_pad) * 2 * a.npad * 2};
     const cuuint32_t box[4] = {64, (cuuint32_t)a.npad, 1, 1};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
-    const CUresult r = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(B),
+    const CUresult r = encode_fn()(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(B),
                                    dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                                    CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "cuTensorMapEncodeTiled failed");
-    if (a.stages < 2 || a.stages > TC_MAX_STAGES) DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "bad stage count");
-    const size_t smem = tc_smem_bytes(a.nfft, a.nact_pad, a.npad, a.dmax, a.stages, a.direct != 0);
-    rt::raise_smem_limit(fdd_mac_tc_kernel, smem);
-    int sms = 148;
-    int dev = 0;
-    RT_CHECK(cudaGetDevice(&dev));
-    RT_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const int ntiles = (a.ndm + TC_M - 1) / TC_M;
-    int ngroups = std::max(1, sms / ntiles);
-    ngroups = (int)std::min<size_t>((size_t)ngroups, a.nbins);
+}
+
+TcMacArgs tc_finish_args(const TcMacArgs& a)
+{
     TcMacArgs ka = a;
     if (ka.nseg_total <= 0) ka.nseg_total = ka.nseg;
+    if (ka.nseg > kTcMaxSeg || ka.seg0 + ka.nseg > ka.nseg_total || ka.npad < 2 * ka.nseg ||
+        ka.npad % 16 != 0 || ka.npad > 128 || ka.nact_pad % TC_CHUNK != 0 || ka.nfft % 256 != 0)
+        DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "tensor-core MAC: bad shape");
     // Barrett constant floor((2^64 - 1) / N) for (k d) mod N in direct mode
     ka.nmagic = ~0ull / (unsigned long long)ka.nfft;
-    if (ka.nseg > kTcMaxSeg || ka.seg0 + ka.nseg > ka.nseg_total)
-        DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "tensor-core MAC: bad segment group");
-    ka.wait_ns = rt::wait_limit_ns();
-    ka.wait_test = rt::wait_expiry_test() ? 1 : 0;
-    fdd_mac_tc_kernel<<<ntiles * ngroups, TC_THREADS, smem, s>>>(map, ka);
+    return ka;
+}
+
+TcLayout tc_layout(const std::vector<TcMacArgs>& descs, unsigned* err)
+{
+    if (descs.empty()) DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "tensor-core MAC: no descriptors");
+    TcLayout L{};
+    int npad = 16;
+    size_t table = 0, hi = 0;
+    for (const TcMacArgs& a : descs) {
+        npad = std::max(npad, a.npad);
+        const size_t t = a.dmax >= 0 ? (size_t)a.dmax + 1 : a.direct ? 0 : (size_t)a.nfft / 4 + 1;
+        table = std::max(table, t);
+        if (a.dmax >= 0 || a.direct) hi = std::max(hi, (size_t)a.nfft / 256);
+        if (a.nact_pad != descs[0].nact_pad)
+            DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "tensor-core MAC: descriptors differ in channels");
+    }
+    L.stage_bytes = 4u * (uint32_t)npad * 128u;
+    L.table_entries = (uint32_t)((table + 1) & ~(size_t)1);  // keep the float2 tables 16-byte aligned
+    L.tw_hi_entries = (uint32_t)((hi + 1) & ~(size_t)1);
+    L.nact_pad = descs[0].nact_pad;
+    auto bytes = [&](int st) {
+        return std::max(TC_MIN_SMEM, (size_t)1024 + (size_t)st * L.stage_bytes + 256 +
+                                         ((size_t)L.table_entries + 256 + L.tw_hi_entries) * 8 +
+                                         (size_t)L.nact_pad * 4 + 4 * 8);
+    };
+    int st = TC_MAX_STAGES;
+    while (st > 2 && bytes(st) > TC_MAX_SMEM) --st;
+    if (bytes(st) > TC_MAX_SMEM)
+        DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "tensor-core MAC: tables do not fit shared memory");
+    L.stages = st;
+    L.smem_bytes = bytes(st);
+    L.wait_ns = rt::wait_limit_ns();
+    L.wait_test = rt::wait_expiry_test() ? 1 : 0;
+    L.err = err;
+    return L;
+}
+
+std::vector<TcWork> tc_work_items(const std::vector<TcMacArgs>& descs, int ctas)
+{
+    // Every (descriptor, DM tile) pair split into bin ranges so that the work
+    // list holds about `ctas` equal parts per wave of CTAs: the cost of a bin
+    // is taken as its chunks (phasor generation and MMAs scale with them).
+    double total = 0;
+    for (const TcMacArgs& a : descs) total += (double)((a.ndm + TC_M - 1) / TC_M) * (double)a.nbins;
+    const double per = std::max(1.0, total / (double)std::max(ctas, 1));
+    std::vector<TcWork> items;
+    for (size_t d = 0; d < descs.size(); ++d) {
+        const TcMacArgs& a = descs[d];
+        const int ntiles = (a.ndm + TC_M - 1) / TC_M;
+        // floor: one descriptor gives at most `ctas` items (one wave)
+        const size_t parts = std::max<size_t>(1, (size_t)std::floor((double)a.nbins / per + 1e-9));
+        for (size_t p = 0; p < parts; ++p) {
+            const size_t k0 = a.nbins * p / parts, k1 = a.nbins * (p + 1) / parts;
+            if (k0 == k1) continue;
+            for (int t = 0; t < ntiles; ++t) items.push_back(TcWork{(int)d, t, (unsigned)k0, (unsigned)k1});
+        }
+    }
+    return items;
+}
+
+size_t tc_work_bytes(size_t nitems) { return nitems * sizeof(TcWork) + 256; }
+
+int tc_sm_count()
+{
+    int dev = 0, sms = 148;
+    RT_CHECK(cudaGetDevice(&dev));
+    RT_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    return sms;
+}
+
+void tc_prepare_list(TcParams& P, const std::vector<TcMacArgs>& descs_in, const std::vector<const void*>& Bs,
+                     const std::vector<TcWork>& items, unsigned* err, void* d_items, size_t items_bytes,
+                     cudaStream_t s)
+{
+    if (descs_in.empty() || descs_in.size() != Bs.size() || descs_in.size() > (size_t)kTcMaxDesc)
+        DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "tensor-core MAC: 1 to 48 descriptors per launch");
+    std::vector<TcMacArgs> descs;
+    for (size_t d = 0; d < descs_in.size(); ++d) {
+        descs.push_back(tc_finish_args(descs_in[d]));
+        P.descs[d] = descs.back();
+        tc_encode_map(&P.maps[d], descs.back(), Bs[d]);
+    }
+    P.ndesc = (int)descs.size();
+    if (tc_work_bytes(items.size()) > items_bytes)
+        DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "tensor-core MAC: work buffer too small");
+    for (const TcWork& w : items)
+        if (w.desc < 0 || w.desc >= P.ndesc || w.k_end > descs[w.desc].nbins || w.k_begin >= w.k_end ||
+            w.tile < 0 || w.tile * 128 >= descs[w.desc].ndm)
+            DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "tensor-core MAC: bad work item");
+    // pageable source: the call returns once the bytes are staged
+    if (!items.empty())
+        RT_CHECK(cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(TcWork), cudaMemcpyHostToDevice, s));
+    P.items = static_cast<const TcWork*>(d_items);
+    P.nitems = (int)items.size();
+    P.layout = tc_layout(descs, err);
+}
+
+void launch_fdd_mac_tc_list(const TcParams& P, cudaStream_t s)
+{
+    if (P.nitems <= 0) return;
+    rt::raise_smem_limit(fdd_mac_tc_kernel, P.layout.smem_bytes);
+    const int grid = std::min(P.nitems, tc_sm_count());
+    fdd_mac_tc_kernel<<<grid, TC_THREADS, P.layout.smem_bytes, s>>>(P);
     RT_CHECK(cudaGetLastError());
+}
+
+void launch_fdd_mac_tc(const TcMacArgs& a, const void* B, void* d_items, size_t items_bytes, cudaStream_t s)
+{
+    const std::vector<TcMacArgs> descs{tc_finish_args(a)};
+    const std::vector<TcWork> items = tc_work_items(descs, tc_sm_count());
+    std::unique_ptr<TcParams> P(new TcParams());
+    tc_prepare_list(*P, descs, {B}, items, a.err, d_items, items_bytes, s);
+    launch_fdd_mac_tc_list(*P, s);
 }
 
 }  // namespace kern

@@ -1,6 +1,7 @@
 // Launch interface of the tensor-core (tcgen05, 3xBF16) FDD phasor MAC.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -24,7 +25,7 @@ struct TcMacArgs {
     const uint2* table;        // quarter-wave table, nfft/4 + 1 entries
     const float2* tw_lo;       // exp(-2 pi i t / nfft), t < 256
     const float2* tw_hi;       // exp(-2 pi i 256 h / nfft), h < nfft / 256
-    unsigned* err;             // set to 1 if a bounded wait expired
+    unsigned* err;             // set to 1 if a bounded wait expired (single launches)
     int nact_pad;              // channels, multiple of 64
     int ndm;
     int nseg;                  // segments of this launch (2*nseg <= 128)
@@ -35,11 +36,43 @@ struct TcMacArgs {
     unsigned nfft;             // transform length (multiple of 256; quarter-wave mode: a power of two)
     int round_delays;
     int dmax;                  // >= 0: delay-table mode, every delay in 0..dmax; -1: quarter-wave mode
-    int stages;                // B pipeline depth (tc_stages)
     int direct = 0;            // dmax < 0: 1 phasors from the two-level twiddles, 0 quarter-wave table
     unsigned long long nmagic = 0;  // set by the launcher
-    unsigned long long wait_ns = 2000000000ull;  // bounded-wait limit (rt::wait_limit_ns)
-    int wait_test = 0;         // expiry test (rt::wait_expiry_test)
+};
+
+// One item of a MAC launch: bins [k_begin, k_end) of DM tile `tile` (128
+// DMs) of descriptor `desc`.
+struct TcWork {
+    int desc;
+    int tile;
+    unsigned k_begin;
+    unsigned k_end;
+};
+
+// Shared-memory layout and wait settings of a launch (the largest over its
+// descriptors, which share the channel set).
+struct TcLayout {
+    int stages;                // B pipeline depth
+    uint32_t stage_bytes;      // per stage (largest npad)
+    uint32_t table_entries;    // phasor table (largest)
+    uint32_t tw_hi_entries;    // two-level twiddle table, hi part (largest nfft / 256)
+    int nact_pad;
+    size_t smem_bytes;
+    unsigned long long wait_ns;  // bounded-wait limit (rt::wait_limit_ns)
+    int wait_test;               // expiry test (rt::wait_expiry_test)
+    unsigned* err;               // set to 1 if a bounded wait expired
+};
+
+// Parameters of a MAC launch: descriptors and their tensor maps (kernel
+// parameter bank), work items (device memory).
+constexpr int kTcMaxDesc = 48;
+struct alignas(64) TcParams {
+    CUtensorMap maps[kTcMaxDesc];
+    TcMacArgs descs[kTcMaxDesc];
+    int ndesc;
+    const TcWork* items;
+    int nitems;
+    TcLayout layout;
 };
 
 // One launch covers at most kTcMaxSeg segments (2 x segments <= 128
@@ -71,7 +104,21 @@ void launch_fdd_prep_b(const float2* X, size_t bin_pitch, int nseg, size_t nbins
                        const int32_t* chan, const float* km, int nact, int nact_pad, int npad,
                        void* B, const BinMap& map, int seg0, int nseg_total, cudaStream_t s);
 
-void launch_fdd_mac_tc(const TcMacArgs& a, const void* B, cudaStream_t s);
+// One plan's MAC (one descriptor). d_items: device scratch of at least
+// tc_work_bytes(SMs) bytes for its work items.
+void launch_fdd_mac_tc(const TcMacArgs& a, const void* B, void* d_items, size_t items_bytes, cudaStream_t s);
+
+// Up to kTcMaxDesc descriptors in one persistent launch: work items over all
+// of them (tc_work_items, about `ctas` equal parts), tensor maps encoded (B
+// operand per descriptor) into P, items copied to d_items; then launched
+// (possibly later, or inside a graph: P is copied into the launch).
+size_t tc_work_bytes(size_t nitems);
+std::vector<TcWork> tc_work_items(const std::vector<TcMacArgs>& descs, int ctas);
+void tc_prepare_list(TcParams& P, const std::vector<TcMacArgs>& descs, const std::vector<const void*>& Bs,
+                     const std::vector<TcWork>& items, unsigned* err, void* d_items, size_t items_bytes,
+                     cudaStream_t s);
+void launch_fdd_mac_tc_list(const TcParams& P, cudaStream_t s);
+int tc_sm_count();
 
 }  // namespace kern
 }  // namespace dedisp

@@ -173,6 +173,49 @@ dedisp_size dedisp_b200_batch_max_delay(dedisp_b200_batch batch, dedisp_size bea
  * last failure on the calling thread is available from dedisp_b200_last_error. */
 
 /* ------------------------------------------------------------------------
+ * Batched multi-beam FDD. No counterpart in the reference (its FDDGPUPlan
+ * takes one series per execute call, src/fdd/FDDGPUPlan.cpp:429-546).
+ * Beams share the channel setup and input width; each has its own DEVICE
+ * input (time-major rows, in_stride bytes apart), sample count, DM list and
+ * DEVICE output: dm_count rows of nsamps - max_delay floats, out_stride bytes
+ * apart (max_delay: last DM of the list x delay of the last channel). Every
+ * beam is dedispersed in the segmented (overlap-save) form with the
+ * reference's segment-length rule and the 3xBF16 tensor-core MAC, as an
+ * FDD plan with segmented = 1, precision = 1 computes it. One execute
+ * enqueues each beam's unpack, forward FFTs and split operand, ONE
+ * persistent MAC launch over all beams (at most 48 segment groups of 64
+ * segments per batch), then each beam's inverse FFTs; captured once into a
+ * CUDA graph when use_graph != 0 and replayed. Inputs, outputs and the
+ * workspace must stay valid while a captured graph may run.
+ * ---------------------------------------------------------------------- */
+typedef struct dedisp_b200_fdd_batch_struct* dedisp_b200_fdd_batch;
+
+dedisp_error dedisp_b200_fdd_batch_create(dedisp_b200_fdd_batch* batch, dedisp_size nchans,
+                                          dedisp_float dt, dedisp_float f0, dedisp_float df,
+                                          dedisp_size in_nbits, int device);
+void dedisp_b200_fdd_batch_destroy(dedisp_b200_fdd_batch batch);
+dedisp_error dedisp_b200_fdd_batch_set_killmask(dedisp_b200_fdd_batch batch, const dedisp_bool* killmask);
+dedisp_error dedisp_b200_fdd_batch_set_beams(dedisp_b200_fdd_batch batch, const dedisp_b200_beam* beams,
+                                             dedisp_size nbeams);
+/* Device bytes of scratch and per-beam operands (spectra split into BF16
+ * parts and dedispersed spectra of every beam); a caller may hand in its own
+ * buffer, else the batch allocates it at the first execute. */
+dedisp_size dedisp_b200_fdd_batch_workspace_size(dedisp_b200_fdd_batch batch);
+dedisp_error dedisp_b200_fdd_batch_set_workspace(dedisp_b200_fdd_batch batch, void* d_workspace,
+                                                 dedisp_size bytes);
+dedisp_error dedisp_b200_fdd_batch_execute(dedisp_b200_fdd_batch batch, void* stream, int use_graph);
+/* Waits for the batch's work on `stream`; DEDISP_INTERNAL_GPU_ERROR if a
+ * bounded wait of the last execute's MAC expired. */
+dedisp_error dedisp_b200_fdd_batch_sync(dedisp_b200_fdd_batch batch, void* stream);
+/* With timing enabled execute waits for its work and reports the device time
+ * of the preparation, of the MAC launch and of the inverse side (graph mode:
+ * the whole graph as mac_ms, the others -1). */
+dedisp_error dedisp_b200_fdd_batch_set_timing(dedisp_b200_fdd_batch batch, int enable);
+dedisp_error dedisp_b200_fdd_batch_get_timing(dedisp_b200_fdd_batch batch, float* prep_ms, float* mac_ms,
+                                              float* post_ms, int* launches);
+dedisp_size dedisp_b200_fdd_batch_max_delay(dedisp_b200_fdd_batch batch, dedisp_size beam);
+
+/* ------------------------------------------------------------------------
  * Streaming server. No counterpart in the reference. Beams deliver host
  * gulps of any length (<= max_gulp); the server keeps each beam's last
  * max_delay input rows on the device, so a gulp of n rows yields n output
