@@ -118,6 +118,7 @@ def lib() -> C.CDLL:
         "dedisp_b200_last_error": (err, [C.c_char_p, _sz]),
         "dedisp_b200_set_fdd_options": (err, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _sz]),
         "dedisp_b200_output_row_length": (_sz, [_vp, _sz]),
+        "dedisp_b200_get_stage_times": (err, [_vp, C.POINTER(C.c_float), C.c_int]),
         "dedisp_b200_set_wait_limit_ns": (err, [C.c_ulonglong]),
         "dedisp_b200_get_wait_limit_ns": (C.c_ulonglong, []),
         "dedisp_b200_set_wait_expiry_test": (err, [C.c_int]),
@@ -264,6 +265,14 @@ class Plan:
                                             C.byref(v)))
         return {"kernel_ms": k.value, "prep_ms": p.value, "launches": n.value,
                 "variant": v.value}
+
+    STAGES = ("unpack", "fft_fwd", "layout", "mac", "transpose", "fft_inv")
+
+    def get_stage_times(self) -> dict:
+        """FDD plans: device ms of each stage of the last timed execute."""
+        v = (C.c_float * 6)()
+        _check(lib().dedisp_b200_get_stage_times(self._h, v, 6))
+        return dict(zip(self.STAGES, [float(x) for x in v]))
 
 
 class DedispPlan(Plan):

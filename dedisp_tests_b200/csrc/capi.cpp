@@ -332,6 +332,17 @@ dedisp_error dedisp_b200_get_timing(dedisp_plan plan, float* kernel_ms, float* p
     return DEDISP_NO_ERROR;
 }
 
+dedisp_error dedisp_b200_get_stage_times(dedisp_plan plan, float* stage_ms, int count)
+{
+    if (!plan) return DEDISP_INVALID_PLAN;
+    auto* g = dynamic_cast<dedisp::GPUPlan*>(plan->ptr.get());
+    if (!g) return DEDISP_INVALID_PLAN;
+    if (!stage_ms && count > 0) return DEDISP_INVALID_POINTER;
+    const dedisp::ExecTiming t = g->last_timing();
+    for (int i = 0; i < count; ++i) stage_ms[i] = i < 6 ? t.stage_ms[i] : 0.f;
+    return DEDISP_NO_ERROR;
+}
+
 dedisp_error dedisp_b200_last_error(char* msg, dedisp_size len)
 {
     if (msg && len) {

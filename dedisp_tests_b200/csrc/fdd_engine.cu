@@ -222,20 +222,23 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
         d_out = m.out.get<float>();
     }
 
-    std::unique_ptr<rt::Event> e0, e1, e2, e3;
-    if (record_timing) {
-        e0.reset(new rt::Event(true));
-        e1.reset(new rt::Event(true));
-        e2.reset(new rt::Event(true));
-        e3.reset(new rt::Event(true));
-    }
+    // stage boundaries: ev[0] start, ev[1] unpacked, ev[2] forward FFT,
+    // ev[3] operand layout (= e1), ev[4] MAC (= e2), ev[5] transpose / spectrum
+    // output, ev[6] inverse FFT (= e3)
+    std::unique_ptr<rt::Event> ev[7];
+    if (record_timing)
+        for (auto& e : ev) e.reset(new rt::Event(true));
+    auto mark = [&](int i) {
+        if (ev[i]) ev[i]->record(st);
+    };
     if (!dev)
         RT_CHECK(cudaMemcpyAsync(m.in.get(), c.in, c.nsamps * in_stride, cudaMemcpyHostToDevice, st));
-    if (e0) e0->record(st);
+    mark(0);
 
     const float scale = (float)(1.0 / (double)nchans);
     kern::launch_fdd_unpack(d_in, in_stride, c.in_nbits, c.nsamps, nchans, scale, m.x.get<float>(),
                             x_len, x_len, st);
+    mark(1);
     const size_t tmp_elems = qpath ? std::max(nchans, ndm) * nseg * (g.nfft / 2)
                                    : kern::fft_scratch_elems((int)g.nfft, std::max(nchans, ndm) * nseg);
     if (tmp_elems) m.fft_tmp.reserve(tmp_elems * sizeof(float2));
@@ -245,10 +248,17 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
     else
         kern::launch_fft_r2c(m.x.get<float>(), x_len, nchans, nseg, seg_stride, (int)g.nfft,
                              m.X.get<float2>(), bin_pitch, tw, m.fft_tmp.get<float2>(), st);
+    mark(2);
     if (!use_tc && m.nact > 0)
         kern::launch_fdd_to_binmajor(m.X.get<float2>(), bin_pitch, nseg, nbins, m.chan.get<int32_t>(),
                                      m.km.get<float>(), m.nact, m.Xt.get<float2>(), bmap, st);
-    if (e1) e1->record(st);
+    // one segment group: its B operand is built here (operand stage); with
+    // several, each group's B is built right before its MAC launch
+    const bool one_group = nseg <= (size_t)seg_group;
+    if (use_tc && one_group)
+        kern::launch_fdd_prep_b(m.X.get<float2>(), bin_pitch, (int)nseg, nbins, m.chan.get<int32_t>(),
+                                m.km.get<float>(), m.nact, nact_pad, npad, m.B.get(), bmap, 0, (int)nseg, st);
+    mark(3);
 
     if (use_tc) {
         RT_CHECK(cudaMemsetAsync(m.err.get(), 0, sizeof(unsigned), st));
@@ -278,9 +288,10 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
         stats.launches = 0;
         for (size_t s0 = 0; s0 < nseg; s0 += (size_t)seg_group) {
             const int ns = (int)std::min(nseg - s0, (size_t)seg_group);
-            kern::launch_fdd_prep_b(m.X.get<float2>(), bin_pitch, ns, nbins, m.chan.get<int32_t>(),
-                                    m.km.get<float>(), m.nact, nact_pad, npad, m.B.get(), bmap, (int)s0,
-                                    (int)nseg, st);
+            if (!one_group)
+                kern::launch_fdd_prep_b(m.X.get<float2>(), bin_pitch, ns, nbins, m.chan.get<int32_t>(),
+                                        m.km.get<float>(), m.nact, nact_pad, npad, m.B.get(), bmap, (int)s0,
+                                        (int)nseg, st);
             ta.nseg = ns;
             ta.seg0 = (int)s0;
             kern::launch_fdd_mac_tc(ta, m.B.get(), m.tcwork.get(), wb, st);
@@ -304,7 +315,7 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
     } else {
         RT_CHECK(cudaMemsetAsync(m.Yt.get(), 0, nbins * nseg * ndm * sizeof(float2), st));
     }
-    if (e2) e2->record(st);
+    mark(4);
 
     if (!inverse) {
         // spectrum: first nfft/2 bins of each DM row, interleaved re/im
@@ -313,6 +324,7 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
         if (!direct_y)
             kern::launch_fdd_to_dmmajor(m.Yt.get<float2>(), nseg, ndm, nbins, m.Y.get<float2>(),
                                         bin_pitch, bmap, st);
+        mark(5);
         const size_t keep = g.segmented ? g.nsamp_good : g.nfft;
         if (qpath)
             kern::launch_fft_c2r_q(m.Y.get<float2>(), bin_pitch, ndm, nseg, g.nfft, d_out, g.row_len, keep,
@@ -321,7 +333,8 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
             kern::launch_fft_c2r(m.Y.get<float2>(), bin_pitch, ndm, nseg, (int)g.nfft, d_out, g.row_len,
                                  keep, g.row_len, tw, m.fft_tmp.get<float2>(), st);
     }
-    if (e3) e3->record(st);
+    if (!inverse) mark(5);
+    mark(6);
     if (!dev)
         RT_CHECK(cudaMemcpyAsync(c.out, d_out, ndm * g.row_len * sizeof(float),
                                  cudaMemcpyDeviceToHost, st));
@@ -333,13 +346,12 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
         if (err) DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "tensor-core MAC pipeline wait expired");
     }
     if (record_timing) {
-        RT_CHECK(cudaEventSynchronize(*e3));
-        float pre = 0.f, mac = 0.f, post = 0.f;
-        RT_CHECK(cudaEventElapsedTime(&pre, *e0, *e1));
-        RT_CHECK(cudaEventElapsedTime(&mac, *e1, *e2));
-        RT_CHECK(cudaEventElapsedTime(&post, *e2, *e3));
-        stats.prep_ms = pre + post;
-        stats.kernel_ms = mac;
+        RT_CHECK(cudaEventSynchronize(*ev[6]));
+        for (int i = 0; i < 6; ++i) RT_CHECK(cudaEventElapsedTime(&stats.stage_ms[i], *ev[i], *ev[i + 1]));
+        // prep: unpack, forward FFT, operand layout; post: transpose, inverse FFT
+        stats.prep_ms = stats.stage_ms[0] + stats.stage_ms[1] + stats.stage_ms[2] + stats.stage_ms[4] +
+                        stats.stage_ms[5];
+        stats.kernel_ms = stats.stage_ms[3];
         stats.variant = use_tc ? 1 : 0;
     }
 }

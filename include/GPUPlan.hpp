@@ -23,6 +23,10 @@ struct ExecTiming {
     float prep_ms = 0.f;     /* transpose / unpack + forward FFT */
     int launches = 0;        /* dedispersion kernel launches */
     int variant = 0;         /* kernel form actually used (plan specific) */
+    /* FDD plans: device time of each stage (ms), in pipeline order: unpack,
+     * forward FFT, operand layout (B split or bin-major), MAC, DM-major
+     * transpose or spectrum output, inverse FFT (0 when a stage did not run) */
+    float stage_ms[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 };
 
 class GPUPlan : public Plan {

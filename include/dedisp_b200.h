@@ -47,6 +47,12 @@ dedisp_error dedisp_b200_set_timing(dedisp_plan plan, int enable);
 dedisp_error dedisp_b200_get_timing(dedisp_plan plan, float* kernel_ms, float* prep_ms,
                                     int* launches, int* variant);
 
+/* FDD plans, with timing enabled: device time (ms) of each stage of the last
+ * execute, in order: unpack, forward FFT, operand layout (split B or
+ * bin-major), MAC, DM-major transpose (or spectrum output), inverse FFT.
+ * Writes `count` values (at most 6 meaningful; the rest 0). */
+dedisp_error dedisp_b200_get_stage_times(dedisp_plan plan, float* stage_ms, int count);
+
 /* The C functions of dedisp.h report every failure inside the plan classes
  * as DEDISP_UNKNOWN_ERROR, like the reference (src/clib/dedisp.cpp:520-523).
  * This returns the specific code of the most recent such failure in the
