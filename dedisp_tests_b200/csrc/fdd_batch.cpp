@@ -144,7 +144,8 @@ void FddBatch::plan()
         b.direct = b.tc_dmax < 0 && !kern::tc_quarter_mode_fits((unsigned)nfft, m_nact_pad, b.npad);
         if (b.direct && !kern::tc_direct_mode_fits((unsigned)nfft, m_nact_pad, b.npad))
             DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "tensor-core MAC: transform length too large");
-        b.b_bytes = round_up(kern::tc_b_bytes(nbins, m_nact_pad, b.npad), kAlign);
+        b.b_bytes = round_up(kern::tc_b_bytes(nbins, m_nact_pad, (int)std::min<size_t>(nseg, kern::kTcMaxSeg)),
+                             kAlign);
         const size_t yt = round_up(nbins * nseg * ndm * sizeof(float2), kAlign);
         b.off_b = per_beam;
         b.off_yt = per_beam + (size_t)b.ngroups * b.b_bytes;

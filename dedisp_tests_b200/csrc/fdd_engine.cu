@@ -160,7 +160,7 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
     if (use_tc) {
         nact_pad = kern::tc_pad_channels(m.nact);
         npad = kern::tc_pad_n(seg_group);
-        m.B.reserve(kern::tc_b_bytes(nbins, nact_pad, npad));
+        m.B.reserve(kern::tc_b_bytes(nbins, nact_pad, seg_group));
         if (m.pad_version != v.version || m.delay_pad_n != nact_pad) {
             std::vector<float> dp(m.delays_active);
             dp.resize(nact_pad, 0.f);

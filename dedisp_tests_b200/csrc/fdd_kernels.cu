@@ -1050,8 +1050,11 @@ __global__ void __launch_bounds__(256) spectrum_out_kernel(const float2* Yt, siz
 // Plain FP32 phasor MAC: a complex GEMM per bin on CUDA cores.
 // Block tile: 64 DMs x 40 segments (thread tile 4 x 5), channel chunk 32.
 // ---------------------------------------------------------------------------
-constexpr int MAC_BM = 64, MAC_BN = 40, MAC_BK = 32, MAC_TM = 4, MAC_TN = 5;
-constexpr int MAC_THREADS = (MAC_BM / MAC_TM) * (MAC_BN / MAC_TN);  // 128
+// Segment tiles: 40 (thread tile 4 x 5) for many segments, 8 (4 x 1) for
+// few (whole-series and short segmented inputs, where a 40-wide tile would
+// multiply padding); 16 x 8 threads either way.
+constexpr int MAC_BM = 64, MAC_BK = 32, MAC_TM = 4;
+constexpr int MAC_THREADS = 128;
 
 __device__ __forceinline__ int fdd_delay(float dm, float delay, int round_delays)
 {
@@ -1073,8 +1076,10 @@ __device__ __forceinline__ unsigned phase_index(size_t k, int d, unsigned nfft, 
     return (unsigned)p;
 }
 
+template <int MAC_BN, int MAC_TN>
 __global__ void __launch_bounds__(MAC_THREADS) mac_plain_kernel(MacArgs a, int bins_per_block)
 {
+    static_assert((MAC_BM / MAC_TM) * (MAC_BN / MAC_TN) == MAC_THREADS, "thread tile");
     extern __shared__ __align__(16) float2 s_mac[];
     float2* As = s_mac;                        // [BK][BM]
     float2* Bs = As + MAC_BK * MAC_BM;         // [BK][BN]
@@ -1413,9 +1418,12 @@ void launch_fdd_spectrum_out(const float2* Yt, size_t ndm, size_t nspec, float* 
 
 void launch_fdd_mac_plain(const MacArgs& a, cudaStream_t s)
 {
-    const size_t smem = (MAC_BK * MAC_BM + MAC_BK * MAC_BN + 256 + a.nfft / 256) * sizeof(float2);
+    const bool narrow = a.nseg <= 8;
+    const int bn = narrow ? 8 : 40;
+    const size_t smem = (MAC_BK * MAC_BM + MAC_BK * (size_t)bn + 256 + a.nfft / 256) * sizeof(float2);
     if (smem > 200 * 1024) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "FFT length too large for the MAC table");
-    rt::raise_smem_limit(mac_plain_kernel, smem);
+    auto kern = narrow ? mac_plain_kernel<8, 1> : mac_plain_kernel<40, 5>;
+    rt::raise_smem_limit(kern, smem);
     const unsigned dm_tiles = (unsigned)((a.ndm + MAC_BM - 1) / MAC_BM);
     // enough blocks to fill the GPU several times over
     const size_t want_blocks = 148 * 8;
@@ -1424,7 +1432,7 @@ void launch_fdd_mac_plain(const MacArgs& a, cudaStream_t s)
     const int per = (int)((a.nbins + bin_blocks - 1) / bin_blocks);
     bin_blocks = (a.nbins + per - 1) / per;
     dim3 grid(dm_tiles, (unsigned)bin_blocks);
-    mac_plain_kernel<<<grid, MAC_THREADS, smem, s>>>(a, per);
+    kern<<<grid, MAC_THREADS, smem, s>>>(a, per);
     RT_CHECK(cudaGetLastError());
 }
 

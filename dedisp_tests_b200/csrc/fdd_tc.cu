@@ -573,7 +573,7 @@ __device__ __forceinline__ uint32_t bf16x2_bits(float lo_half, float hi_half)
     return *reinterpret_cast<const uint32_t*>(&v);
 }
 
-// B operand from the spectra: Bsplit[k][split][n][kk] bf16, n < npad,
+// B operand from the spectra: Bsplit[k][split][n][kk] bf16, n < 2 nseg,
 // kk < 2*nact_pad (hi = bf16(v), lo = bf16(v - hi)); killmask applied.
 // Element pairs (kk = 2j, 2j+1) are written as one 32-bit word.
 __global__ void __launch_bounds__(256) fdd_prep_b_kernel(const float2* X, size_t bin_pitch, int nseg,
@@ -593,14 +593,9 @@ __global__ void __launch_bounds__(256) fdd_prep_b_kernel(const float2* X, size_t
     const int j0 = blockIdx.y * 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const size_t words_row = (size_t)nact_pad;  // 2*nact_pad bf16 per row
-    // padding rows n in [2*nseg, npad) are zero
-    for (int r = ty; r < 32; r += 8) {
-        if (k0 + r >= nbins || j0 + tx >= nact_pad) continue;
-        const size_t k = pbin(k0 + r);
-        const int j = j0 + tx;
-        for (int n = 2 * nseg; n < npad; ++n)
-            for (int sp = 0; sp < 2; ++sp) B[((k * 2 + sp) * npad + n) * words_row + j] = 0u;
-    }
+    // B holds the 2*nseg real rows of each bin; the MMA's rows up to npad are
+    // zeros that the tensor-map load fills in (out-of-bounds fill)
+    const size_t nrow = 2 * (size_t)nseg;
     // the next segment's loads are issued before this segment's stores
     float2 nv[4];
     auto load = [&](int s) {
@@ -637,8 +632,8 @@ __global__ void __launch_bounds__(256) fdd_prep_b_kernel(const float2* X, size_t
                 const float a0 = vals[part][0], a1 = vals[part][1];
                 const float h0 = __bfloat162float(__float2bfloat16_rn(a0));
                 const float h1 = __bfloat162float(__float2bfloat16_rn(a1));
-                B[((k * 2 + 0) * npad + n) * words_row + j] = bf16x2_bits(h0, h1);
-                B[((k * 2 + 1) * npad + n) * words_row + j] = bf16x2_bits(a0 - h0, a1 - h1);
+                B[((k * 2 + 0) * nrow + n) * words_row + j] = bf16x2_bits(h0, h1);
+                B[((k * 2 + 1) * nrow + n) * words_row + j] = bf16x2_bits(a0 - h0, a1 - h1);
             }
         }
     }
@@ -661,9 +656,9 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 
 }  // namespace
 
-size_t tc_b_bytes(size_t nbins, int nact_pad, int npad)
+size_t tc_b_bytes(size_t nbins, int nact_pad, int nseg)
 {
-    return nbins * 2 * (size_t)npad * 2 * (size_t)nact_pad * sizeof(__nv_bfloat16);
+    return nbins * 2 * (2 * (size_t)nseg) * 2 * (size_t)nact_pad * sizeof(__nv_bfloat16);
 }
 
 int tc_pad_channels(int nact) { return ((nact + TC_CHUNK - 1) / TC_CHUNK) * TC_CHUNK; }
@@ -750,11 +745,12 @@ void tc_encode_map(void* map_out, const TcMacArgs& a, const void* B)
 {
     // Tensor map over Bsplit[bin][split][n][kk]: dims (kk, n, split, bin).
     CUtensorMap* map = static_cast<CUtensorMap*>(map_out);
-    const cuuint64_t dims[4] = {(cuuint64_t)(2 * a.nact_pad), (cuuint64_t)a.npad, 2,
-                                (cuuint64_t)a.nbins};
-    const cuuint64_t strides[3] = {(cuuint64_t)(2 * a.nact_pad) * 2,
-                                   (cuuint64_t)(2 * a.nact_pad) * 2 * a.npad,
-                                   (cuuint64_t)(2 * a.nact_pad) * 2 * a.npad * 2};
+    // (kk, n < 2 nseg stored rows, split, bin); the box's npad rows past the
+    // stored ones read as zero (out-of-bounds fill), the count is the full box
+    const cuuint64_t nrow = 2 * (cuuint64_t)a.nseg;
+    const cuuint64_t dims[4] = {(cuuint64_t)(2 * a.nact_pad), nrow, 2, (cuuint64_t)a.nbins};
+    const cuuint64_t strides[3] = {(cuuint64_t)(2 * a.nact_pad) * 2, (cuuint64_t)(2 * a.nact_pad) * 2 * nrow,
+                                   (cuuint64_t)(2 * a.nact_pad) * 2 * nrow * 2};
     const cuuint32_t box[4] = {64, (cuuint32_t)a.npad, 1, 1};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     const CUresult r = encode_fn()(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(B),

@@ -84,7 +84,9 @@ constexpr int kTcMaxSeg = 64;
 bool tc_quarter_mode_fits(unsigned nfft, int nact_pad, int npad);
 int tc_pad_channels(int nact);
 int tc_pad_n(int nseg);
-size_t tc_b_bytes(size_t nbins, int nact_pad, int npad);
+// Bytes of the split B operand of one segment group (2 nseg stored rows per
+// bin and split; the MMA's padding rows are not stored).
+size_t tc_b_bytes(size_t nbins, int nact_pad, int nseg);
 size_t tc_smem_bytes(unsigned nfft, int nact_pad, int npad, int dmax, int stages, bool direct);
 // Deepest B pipeline (2..6 stages) that fits shared memory.
 int tc_stages(unsigned nfft, int nact_pad, int npad, int dmax, bool direct);
@@ -97,7 +99,7 @@ int tc_table_mode_dmax(int dmax, unsigned nfft, int nact_pad, int npad);
 std::vector<uint2> tc_quarter_table(unsigned nfft);
 
 // X [nchans*nseg][bin_pitch] complex spectra -> B operand
-// Bsplit[bin][hi|lo][n < npad][kk < 2*nact_pad] (bf16).
+// Bsplit[bin][hi|lo][n < 2 nseg][kk < 2*nact_pad] (bf16).
 // X rows in the order `map` (fdd_kernels.hpp).
 // Segments seg0 .. seg0 + nseg - 1 of X rows c * nseg_total + s.
 void launch_fdd_prep_b(const float2* X, size_t bin_pitch, int nseg, size_t nbins,
