@@ -74,11 +74,15 @@ def parse():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-only", action="store_true",
                     help="run only the streaming server (config 4) and print its JSON object")
+    ap.add_argument("--batched-fdd-only", action="store_true",
+                    help="run only the batched multi-beam FDD (config 3) and print its JSON object")
     ap.add_argument("--batched-only", action="store_true",
                     help="run only the batched multi-beam TDD (config 3) and print its JSON object")
     ap.add_argument("--profile-case", default="",
                     help="run one small case for ncu and exit: tdd (the TDD workload with "
-                         "2^17 samples) or fdd (config-2 geometry with 2^18 samples)")
+                         "2^17 samples), fdd / fdd-tc (config-2 geometry with 2^18 samples, FP32 "
+                         "or tensor-core MAC), fdd-tc-n80 (the tensor-core MAC's config-2 shape "
+                         "per bin, 80 columns, on a few GB)")
     return ap.parse_args()
 
 
@@ -95,6 +99,17 @@ def profile_case(args):
         if args.tile_variant >= 0:
             p.set_tile_variant(args.tile_variant)
         nbits = args.nbits
+    elif args.profile_case == "fdd-tc-n80":
+        # the MAC's per-bin shape at config 2 (1024 channels = 16 chunks,
+        # 2048 DMs = 16 tiles, 39 segments = 80 columns) on a few GB: DMs
+        # 0-250 (max delay 1311), 8192-point segments, 39 x 6881 samples
+        import dataclasses
+        cfg = dataclasses.replace(sy.config2(), nsamps=39 * 6881,
+                                  dm_list=(250.0 * np.arange(2048) / 2047.0).astype(np.float32))
+        p = dd.FDDGPUPlan(cfg.nchans, cfg.dt, cfg.f_top, cfg.df)
+        p.set_dm_list(cfg.dm_list)
+        p.set_options(segmented=1, precision=1, segment_nfft=8192)
+        nbits = 32
     else:
         cfg = sy.config2(nsamps=1 << 18)
         p = dd.FDDGPUPlan(cfg.nchans, cfg.dt, cfg.f_top, cfg.df)
@@ -592,7 +607,7 @@ def run_batched_fdd(args, local, world, stream, max_over_ranks, nbeams=12, nplai
         return (d_in[i], c.nchans, c.nsamps, c.dm_list, y, nouts[i] * 4)
 
     # waves: add beams while workspace + outputs fit the budget
-    probe = torch.empty(0, dtype=torch.uint8, device=dev)
+    probe = torch.empty(16, dtype=torch.uint8, device=dev)  # stand-in output (sizing only)
     waves, cur = [], []
     for i in range(nbeams):
         trial = cur + [i]
@@ -642,9 +657,10 @@ def run_batched_fdd(args, local, world, stream, max_over_ranks, nbeams=12, nplai
            "units": total, "waves": len(waves), "beams_per_wave": [len(w) for w in waves],
            "batched_bf16x3_tc": {"value": total * world / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
                                  "mac_launches_per_step": len(waves)}}
-    # error of beam 0 (first wave) against float64 on two DMs x 2^16 samples
-    y0 = pool[:out_bytes[waves[0][0]]].view(torch.float32).view(len(beams[waves[0][0]].dm_list), -1)
-    bi = waves[0][0]
+    # error of the last wave's first beam (the pool holds the last wave's
+    # rows) against float64 on two DMs x 2^16 samples
+    bi = waves[-1][0]
+    y0 = pool[:out_bytes[bi]].view(torch.float32).view(len(beams[bi].dm_list), -1)
     c = beams[bi]
     nchk = min(1 << 16, nouts[bi])
     h = d_in[bi][:nchk + mds[bi]].cpu().numpy()
@@ -697,10 +713,11 @@ def run_serving(args, local, world):
     """Config 4: 32 beams of 4096 ch 2-bit (f_top 1500 MHz, df -0.078125 MHz,
     dt 64 us), 2048 DM trials over 0-1500, through the streaming server: 28
     TDD beams (gulps of 16384, 65536 or 262144 samples) and 4 FDD beams (3xBF16
-    tensor-core MAC, gulps of 16384 or 65536). FDD segments are 65536 points:
-    with the 26616-sample overlap tail a gulp then costs one or two segments,
-    2-4x its new samples (32768-point segments cost 5-6x, the long-series
-    rule's 262144 up to 8x). Gulps arrive as a Poisson process at 1x, 2x, 4x
+    tensor-core MAC, gulps of 16384 or 65536). FDD segments are 32768 points,
+    the shortest above the 26616-sample overlap tail: the MAC's cost is set by
+    its phasors, one per (DM, channel, bin) and shared by all segments, so it
+    grows with the bins of a segment (nfft / 2), not with the segment count
+    (65536-point segments measured 2x slower per gulp). Gulps arrive as a Poisson process at 1x, 2x, 4x
     and 8x the aggregate real-time sample rate (32 x 15625 samples/s) for a
     fixed window each (20 s: at least 100 gulps per rate, so p99 is not the
     maximum); outputs stay on the device (a GPU consumer reads each worker's
@@ -716,7 +733,7 @@ def run_serving(args, local, world):
     sizes_tdd, sizes_fdd = [16384, 65536, 262144], [16384, 65536]
     srv = dd.StreamServer(nch, dt, f0, df, in_nbits=nbits, device=local, hbm_budget=int(120e9),
                           max_gulp=max(sizes_tdd), tdd_workers=4, fdd_workers=1, fdd_precision=1,
-                          fdd_segment=65536, fdd_max_gulp=max(sizes_fdd))
+                          fdd_segment=32768, fdd_max_gulp=max(sizes_fdd))
     kinds = [0] * (nbeams - n_fdd) + [1] * n_fdd
     for k in kinds:
         srv.add_beam(dms, k)
@@ -771,6 +788,11 @@ def run_serving(args, local, world):
     return out
 
 
+def _log(msg):
+    """Progress on stderr (the JSON line is the only stdout)."""
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -798,6 +820,12 @@ def run_ours(args):
         res = run_serving(args, local, world)
         if rank == 0:
             print(json.dumps({"serving": res}), flush=True)
+        reps.close()
+        return
+    if args.batched_fdd_only:
+        resf = run_batched_fdd(args, local, world, stream, max_over_ranks)
+        if rank == 0:
+            print(json.dumps({"batched_fdd": resf}), flush=True)
         reps.close()
         return
     if args.batched_only:
@@ -1010,11 +1038,13 @@ def run_ours(args):
 
     # --- FDD forms (config 2) -------------------------------------------------------
     fdd = None
+    _log("tdd sections done")
     if not args.no_fdd:
         del plan, d_in
         d_out = None
         torch.cuda.empty_cache()
         fdd = run_fdd(args, local, world, stream, max_over_ranks)
+        _log("fdd done")
 
     # --- batched multi-beam TDD (config 3) ----------------------------------------
     batched = None
@@ -1024,16 +1054,19 @@ def run_ours(args):
             d_out = None
             torch.cuda.empty_cache()
         batched = run_batched(args, local, world, stream, max_over_ranks)
+        _log("batched tdd done")
 
     # --- batched multi-beam FDD (config 3) -----------------------------------------
     batched_fdd = None
     if not args.no_batched:
         batched_fdd = run_batched_fdd(args, local, world, stream, max_over_ranks)
+        _log("batched fdd done")
 
     # --- streaming server (config 4) -----------------------------------------------
     serving = None
     if not args.no_serve:
         serving = run_serving(args, local, world)
+        _log("serving done")
 
     if rank == 0:
         line = {

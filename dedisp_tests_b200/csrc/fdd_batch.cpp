@@ -301,7 +301,7 @@ void FddBatch::upload()
         DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "a batch holds at most 48 beam segment groups");
     m_params.reset(new kern::TcParams());
     if (!descs.empty()) {
-        const std::vector<kern::TcWork> items = kern::tc_work_items(descs, 4 * kern::tc_sm_count());
+        const std::vector<kern::TcWork> items = kern::tc_work_items(descs, kern::tc_sm_count());
         const size_t ib = kern::tc_work_bytes(items.size());
         m_items.reserve(ib);
         kern::tc_prepare_list(*m_params, descs, Bs, items, m_err.get<unsigned>(), m_items.get(), ib, nullptr);

@@ -832,11 +832,15 @@ __device__ __forceinline__ size_t qpos(size_t k, const BinMap& m)
 
 // Real-FFT post step in place over rows in the transposed order: bins k and
 // M - k (k = 0..M/2) from z at the positions of k and M - k (formula of
-// fft_r2c_kernel; bin M at position M).
+// fft_r2c_kernel; bin M at position M). Threads run over consecutive
+// positions p (bin k = qbin(p)); the thread whose bin is the smaller of the
+// pair does the work, so both the bin and its partner are contiguous runs.
 __global__ void __launch_bounds__(256) r2c_post_q_kernel(float2* X, size_t x_pitch, BinMap map, TwiddleTable tw)
 {
     const size_t M = map.M;
-    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= M) return;
+    const size_t k = qbin(p, map);
     if (k > M / 2) return;
     float2* r = X + (size_t)blockIdx.y * x_pitch;
     const size_t pk = qpos(k, map), pm = qpos(k ? M - k : 0, map);
@@ -856,10 +860,13 @@ __global__ void __launch_bounds__(256) r2c_post_q_kernel(float2* X, size_t x_pit
 
 // Inverse real-FFT pre step in place over transposed rows (formula of
 // fft_c2r_kernel): bins k and M - k -> z at the positions of k and M - k.
+// Threads run over consecutive positions, as in r2c_post_q_kernel.
 __global__ void __launch_bounds__(256) c2r_pre_q_kernel(float2* Y, size_t y_pitch, BinMap map, TwiddleTable tw)
 {
     const size_t M = map.M;
-    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= M) return;
+    const size_t k = qbin(p, map);
     if (k > M / 2) return;
     float2* r = Y + (size_t)blockIdx.y * y_pitch;
     const size_t pk = qpos(k, map), pm = qpos(M - k, map);
@@ -1357,8 +1364,7 @@ void launch_fft_r2c_q(const float* x, size_t x_pitch, size_t nchans, size_t nseg
     kr<<<persistent_grid(kr, FftPlan<FQ_LOGP>::threads(), sr, nrows), FftPlan<FQ_LOGP>::threads(), sr, s>>>(
         scratch, map.M, X, bin_pitch, Q, twp, nrows);
     RT_CHECK(cudaGetLastError());
-    r2c_post_q_kernel<<<dim3((unsigned)((map.M / 2 + 256) / 256), (unsigned)rows), 256, 0, s>>>(X, bin_pitch, map,
-                                                                                              tw);
+    r2c_post_q_kernel<<<dim3((unsigned)((map.M + 255) / 256), (unsigned)rows), 256, 0, s>>>(X, bin_pitch, map, tw);
     RT_CHECK(cudaGetLastError());
 }
 
@@ -1374,8 +1380,7 @@ void launch_fft_c2r_q(float2* Y, size_t bin_pitch, size_t ndm, size_t nseg, size
     const int T = fftq_tile(Q);
     const QRadices rad = fftq_radices(Q);
     const BinMap map = fdd_binmap(nfft);
-    c2r_pre_q_kernel<<<dim3((unsigned)((map.M / 2 + 256) / 256), (unsigned)rows), 256, 0, s>>>(Y, bin_pitch, map,
-                                                                                             tw);
+    c2r_pre_q_kernel<<<dim3((unsigned)((map.M + 255) / 256), (unsigned)rows), 256, 0, s>>>(Y, bin_pitch, map, tw);
     RT_CHECK(cudaGetLastError());
     auto kr = fft_c2c_rows_kernel<FQ_LOGP, true>;
     const size_t sr = (FQ_P + 256 + 2 * FQ_P / 256) * sizeof(float2);

@@ -29,6 +29,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <memory>
 #include <type_traits>
 #include <vector>
@@ -41,7 +42,7 @@ namespace kern {
 namespace {
 
 constexpr int TC_M = 128;              // DMs per CTA (accumulator lanes)
-constexpr int TC_CHUNK = 64;           // channels per K chunk (K = 128 reals)
+constexpr int TC_CHUNK = 64;           // channel padding (a multiple of both forms' A chunks)
 constexpr int TC_MAX_STAGES = 6;       // B pipeline depth: as many as shared memory allows, 2..6
 constexpr int TC_PRODUCER_WARPS = 16;  // 4 per TMEM lane quadrant
 constexpr int TC_PARTS = TC_PRODUCER_WARPS / 4;  // producers sharing one DM row
@@ -55,15 +56,33 @@ constexpr uint32_t TC_WAIT_POLLS = 1u << 28;
 constexpr size_t TC_MIN_SMEM = 120 * 1024;
 constexpr size_t TC_MAX_SMEM = 227 * 1024;
 
-// TMEM column map (512 allocated): A buffers (hi 64 + lo 64 columns) x 2,
-// accumulators x 2.
-constexpr uint32_t TM_A0 = 0, TM_A1 = 128, TM_C0 = 256, TM_C1 = 384;
+// Two MMA forms. Per K step of 16 reals:
+//   plain (any npad <= 128): Ah Bh, Ah Bl, Al Bh as three N = npad MMAs into
+//     one accumulator; 64-channel A chunks, 2 A buffers (hi 64 + lo 64
+//     columns each), accumulators of 128 columns at 256 and 384;
+//   fused (npad <= 80): Ah [Bh | Bl] as one N = 2 npad MMA (B hi and lo atoms
+//     adjacent in shared memory), then Al Bh (N = npad) into its first npad
+//     columns; the epilogue adds the two halves. Accumulators of 160 columns at
+//     0 and 160, 32-channel A chunks in 3 buffers of 64 columns at 320, 384, 448.
+template <bool FUSED>
+struct TcForm {
+    static constexpr int CH = FUSED ? 32 : 64;            // channels per A chunk
+    static constexpr int PART_CH = CH / TC_PARTS;         // per producer thread
+    static constexpr int NBUF = FUSED ? 3 : 2;            // A buffers
+    static constexpr uint32_t A_COLS = 2 * CH;            // hi CH + lo CH columns
+    static constexpr uint32_t A_BASE = FUSED ? 320 : 0;
+    static constexpr uint32_t C0 = FUSED ? 0 : 256, C1 = FUSED ? 160 : 384;
+    static constexpr int KSTEPS = CH / 8;                 // K16 steps per chunk
+    static constexpr int ATOMS = CH / 32;                 // 64-kk TMA atoms per split
+};
+constexpr int TC_FUSED_MAX_NPAD = 80;
+constexpr int TC_MAX_ABUF = 3;
 
 struct alignas(8) SmemBarriers {
     uint64_t b_full[TC_MAX_STAGES];
     uint64_t b_empty[TC_MAX_STAGES];
-    uint64_t a_full[2];
-    uint64_t a_empty[2];
+    uint64_t a_full[TC_MAX_ABUF];
+    uint64_t a_empty[TC_MAX_ABUF];
     uint64_t c_full[2];
     uint64_t c_empty[2];
     uint64_t drain;
@@ -166,6 +185,12 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar)
 
 // 32 consecutive 32-bit columns of this thread's lane.
 // 16 consecutive 32-bit columns of this thread's lane.
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&v)[8])
+{
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr),
+                 "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]));
+}
+
 __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&v)[16])
 {
     asm volatile(
@@ -239,8 +264,10 @@ __device__ __forceinline__ uint2 split_bf16x2(float re, float im)
 // pipeline counters run on across items, so the hand-offs of consecutive
 // items overlap; each item's last accumulator is read out before the next
 // item starts. One plan's launch is the one-descriptor case.
+template <bool FUSED>
 __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_constant__ TcParams P)
 {
+    using F = TcForm<FUSED>;
     // descriptors and tensor maps live in the parameter bank (constant
     // operands, no registers); the items in global memory
     const TcMacArgs* descs = P.descs;
@@ -266,7 +293,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if ((int)blockIdx.x >= nitems) return;  // whole CTA leaves before touching barriers
-    const int nchunks = L.nact_pad / TC_CHUNK;
+    const int nchunks = L.nact_pad / F::CH;
 
     // --- set-up -------------------------------------------------------------
     for (int i = tid; i < L.nact_pad; i += blockDim.x) s_delay[i] = descs[0].delay_act[i];
@@ -283,9 +310,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
             mbar_init(&bars->b_full[i], 1);
             mbar_init(&bars->b_empty[i], 1);
         }
-        for (int i = 0; i < 2; ++i) {
+        for (int i = 0; i < F::NBUF; ++i) {
             mbar_init(&bars->a_full[i], TC_PRODUCER_WARPS);   // one arrive per producer warp
             mbar_init(&bars->a_empty[i], 1);
+        }
+        for (int i = 0; i < 2; ++i) {
             mbar_init(&bars->c_full[i], 1);
             mbar_init(&bars->c_empty[i], TC_PRODUCER_WARPS);
         }
@@ -341,15 +370,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                 cur_desc = w.desc;
             }
             asm volatile("bar.sync 1, %0;" ::"n"(TC_PRODUCER_WARPS * 32) : "memory");
-            const int m = w.tile * TC_M + quad * 32 + lane;          // this thread's DM row
-            const float dm = a.dms[min(m, a.ndm - 1)];
+            const int row = quad * 32 + lane;  // this thread's DM row within a tile
             const int first_iter = bin_iter;
+            int prev_m = 0;                    // DM row of the previous (bin, tile) pair
 
-            auto epilogue = [&](int itr, size_t kk) -> bool {
+            auto epilogue = [&](int itr, size_t kk, int m) -> bool {
                 const uint32_t cb = (uint32_t)itr & 1u;
                 if (!mbar_wait_warp(&bars->c_full[cb], ((uint32_t)itr >> 1) & 1u, L.wait_ns)) return false;
                 tc_fence_after();
-                const uint32_t ccol = cb ? TM_C1 : TM_C0;
+                const uint32_t ccol = cb ? F::C1 : F::C0;
+                const uint32_t half = FUSED ? (uint32_t)a.npad : 0u;  // fused: Ah Bl columns
                 const int sh = (a.nseg + TC_PARTS - 1) / TC_PARTS;
                 const int s0 = min(a.nseg, part * sh), s1 = min(a.nseg, s0 + sh);
                 // the row's output element offsets: Y (DM-major) or Yt (bin-major)
@@ -367,7 +397,24 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                             yi[i] = tmem_ld1(tmem + lane_addr + ccol + a.nseg + sb + i);
                         }
                     }
+                    float zr[4], zi[4];
+                    if constexpr (FUSED) {
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            if (i < cnt) {
+                                zr[i] = tmem_ld1(tmem + lane_addr + ccol + half + sb + i);
+                                zi[i] = tmem_ld1(tmem + lane_addr + ccol + half + a.nseg + sb + i);
+                            }
+                        }
+                    }
                     tmem_wait_ld();
+                    if constexpr (FUSED) {
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            yr[i] += zr[i];
+                            yi[i] += zi[i];
+                        }
+                    }
                     if (mine) {
 #pragma unroll
                         for (int i = 0; i < 4; ++i)
@@ -385,10 +432,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
             bool aborted = false;
             // k == k_end: only the read-out of the item's last bin (one call
             // site of the epilogue keeps it inlined once)
+            // Per bin: (delay-table mode) the table, then every DM tile of the
+            // item, each one (bin, tile) pair with its own accumulator: the
+            // table is built once per bin for all tiles.
             for (size_t k = w.k_begin; k <= w.k_end; ++k) {
                 const bool tail = k == w.k_end;
                 if (tail) {
-                    if (ok && bin_iter > first_iter) ok = epilogue(bin_iter - 1, k - 1);
+                    if (ok && bin_iter > first_iter) ok = epilogue(bin_iter - 1, k - 1, prev_m);
                     if (!ok) *abort_flag = 1u;
                     break;
                 }
@@ -413,20 +463,49 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                 } else if (!ok) {
                     break;
                 }
+                for (int t = w.tile; t < w.tile + w.ntile; ++t) {
                 if (ok) {
+                    const int m = t * TC_M + row;
+                    const float dm = a.dms[min(m, a.ndm - 1)];
                     for (int ch = 0; ch < nchunks; ++ch, ++g) {
-                        const uint32_t buf = g & 1u;
+                        const uint32_t buf = g % F::NBUF, use = g / F::NBUF;
                         // the phasors first: their gathers overlap the MMAs still
                         // reading this A buffer
+                        constexpr int TC_PART_CH = F::PART_CH;
                         uint32_t hi[TC_PART_CH], lo[TC_PART_CH];
-                        const int c0 = ch * TC_CHUNK + part * TC_PART_CH;
+                        const int c0 = ch * F::CH + part * TC_PART_CH;
                         if (ptab) {
+                            // delays of the 16 channels (4 vector loads); the table
+                            // covers 0..dmax, the largest delay over the plan's DMs and
+                            // channels computed on the host with the same float
+                            // operations, so the unsigned clamp is only a guard
+                            float dl[TC_PART_CH];
+                            const float4* sd4 = reinterpret_cast<const float4*>(s_delay + c0);
 #pragma unroll
-                            for (int i = 0; i < TC_PART_CH; ++i) {
-                                const int d = min(max(tc_delay_small(dm, s_delay[c0 + i], a.round_delays), 0), a.dmax);
-                                const uint2 v = s_table[d];
-                                hi[i] = v.x;
-                                lo[i] = v.y;
+                            for (int q = 0; q < TC_PART_CH / 4; ++q) {
+                                const float4 v4 = sd4[q];
+                                dl[4 * q] = v4.x;
+                                dl[4 * q + 1] = v4.y;
+                                dl[4 * q + 2] = v4.z;
+                                dl[4 * q + 3] = v4.w;
+                            }
+                            const uint32_t dmax = (uint32_t)a.dmax;
+                            if (a.round_delays) {
+#pragma unroll
+                                for (int i = 0; i < TC_PART_CH; ++i) {
+                                    const float y = __fadd_rn(__fmul_rn(dm, dl[i]), 8388608.0f);
+                                    const uint2 v = s_table[min(__float_as_uint(y) - 0x4B000000u, dmax)];
+                                    hi[i] = v.x;
+                                    lo[i] = v.y;
+                                }
+                            } else {
+#pragma unroll
+                                for (int i = 0; i < TC_PART_CH; ++i) {
+                                    const float y = __fadd_rz(__fmul_rn(dm, dl[i]), 8388608.0f);
+                                    const uint2 v = s_table[min(__float_as_uint(y) - 0x4B000000u, dmax)];
+                                    hi[i] = v.x;
+                                    lo[i] = v.y;
+                                }
                             }
                         } else if (direct) {
 #pragma unroll
@@ -464,20 +543,28 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                                 lo[i] = __byte_perm(t.y, 0u, sy.x) ^ sy.y;
                             }
                         }
-                        if (!mbar_wait_warp(&bars->a_empty[buf], ((g >> 1) & 1u) ^ 1u, L.wait_ns)) { ok = false; break; }
+                        if (!mbar_wait_warp(&bars->a_empty[buf], (use & 1u) ^ 1u, L.wait_ns)) { ok = false; break; }
                         tc_fence_after();
-                        const uint32_t acol = buf ? TM_A1 : TM_A0;
-                        tmem_st16(tmem + lane_addr + acol + part * TC_PART_CH, hi);
-                        tmem_st16(tmem + lane_addr + acol + 64 + part * TC_PART_CH, lo);
+                        const uint32_t acol = F::A_BASE + buf * F::A_COLS;
+                        if constexpr (FUSED) {
+                            tmem_st8(tmem + lane_addr + acol + part * TC_PART_CH, hi);
+                            tmem_st8(tmem + lane_addr + acol + F::CH + part * TC_PART_CH, lo);
+                        } else {
+                            tmem_st16(tmem + lane_addr + acol + part * TC_PART_CH, hi);
+                            tmem_st16(tmem + lane_addr + acol + F::CH + part * TC_PART_CH, lo);
+                        }
                         tmem_wait_st();
                         tc_fence_before();
                         __syncwarp();
                         if (lane == 0) mbar_arrive(&bars->a_full[buf]);
                     }
                 }
-                if (ok && bin_iter > first_iter) ok = epilogue(bin_iter - 1, k - 1);
+                // the previous pair's read-out overlaps this pair's MMAs
+                if (ok && bin_iter > first_iter) ok = epilogue(bin_iter - 1, t > w.tile ? k : k - 1, prev_m);
                 if (!ok) *abort_flag = 1u;  // the others stop at the next barrier
+                prev_m = t * TC_M + row;
                 ++bin_iter;
+                }
             }
             if (aborted) ok = false;
             if (!ok) *abort_flag = 1u;
@@ -490,17 +577,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                 const TcWork w = items[it];
                 const CUtensorMap* bmap = maps + w.desc;
                 const uint32_t atom_bytes = (uint32_t)descs[w.desc].npad * 128u;  // one 64-kk atom of one split
-                for (size_t k = w.k_begin; k < w.k_end && ok; ++k) {
+                for (size_t kt = (size_t)w.k_begin * w.ntile; kt < (size_t)w.k_end * w.ntile && ok; ++kt) {
+                    const size_t k = kt / (size_t)w.ntile;  // every tile of bin k reads bin k's B
                     for (int ch = 0; ch < nchunks; ++ch, ++g) {
                         const uint32_t st = g % (uint32_t)nst;
                         if (!mbar_wait(&bars->b_empty[st], ((g / nst) & 1u) ^ 1u, L.wait_ns)) { ok = false; break; }
-                        mbar_expect_tx(&bars->b_full[st], 4u * atom_bytes);
+                        mbar_expect_tx(&bars->b_full[st], 2u * F::ATOMS * atom_bytes);
                         uint8_t* dst = s_b + st * L.stage_bytes;
-                        // coordinates: (kk, n, split, bin)
-                        for (int sp = 0; sp < 2; ++sp)
-                            for (int at = 0; at < 2; ++at)
-                                tma_load_4d(dst + (sp * 2 + at) * atom_bytes, bmap, &bars->b_full[st],
-                                            ch * 128 + at * 64, 0, sp, (int)k);
+                        // coordinates: (kk, n, split, bin); atoms in the order
+                        // (atom, split), so each atom's hi and lo rows are adjacent
+                        for (int at = 0; at < F::ATOMS; ++at)
+                            for (int sp = 0; sp < 2; ++sp)
+                                tma_load_4d(dst + (at * 2 + sp) * atom_bytes, bmap, &bars->b_full[st],
+                                            ch * (2 * F::CH) + at * 64, 0, sp, (int)k);
                     }
                 }
             }
@@ -520,30 +609,38 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                 const uint32_t atom_bytes = npad * 128u;
                 const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((npad >> 3) << 17) |
                                        ((uint32_t)(TC_M >> 4) << 24);
-                for (size_t k = w.k_begin; k < w.k_end && ok; ++k, ++bin_iter) {
+                const uint32_t idesc2 = (1u << 4) | (1u << 7) | (1u << 10) | (((2u * npad) >> 3) << 17) |
+                                        ((uint32_t)(TC_M >> 4) << 24);
+                for (size_t kt = (size_t)w.k_begin * w.ntile; kt < (size_t)w.k_end * w.ntile && ok; ++kt, ++bin_iter) {
                     const uint32_t cb = (uint32_t)bin_iter & 1u;
                     if (!mbar_wait(&bars->c_empty[cb], (((uint32_t)bin_iter >> 1) & 1u) ^ 1u, L.wait_ns)) { ok = false; break; }
                     tc_fence_after();
-                    const uint32_t dcol = tmem + (cb ? TM_C1 : TM_C0);
+                    const uint32_t dcol = tmem + (cb ? F::C1 : F::C0);
                     for (int ch = 0; ch < nchunks; ++ch, ++g) {
-                        const uint32_t buf = g & 1u, st = g % (uint32_t)nst;
-                        if (!mbar_wait(&bars->a_full[buf], (g >> 1) & 1u, L.wait_ns)) { ok = false; break; }
+                        const uint32_t buf = g % F::NBUF, st = g % (uint32_t)nst;
+                        if (!mbar_wait(&bars->a_full[buf], (g / F::NBUF) & 1u, L.wait_ns)) { ok = false; break; }
                         if (!mbar_wait(&bars->b_full[st], (g / nst) & 1u, L.wait_ns)) { ok = false; break; }
                         // expiry test: one more wait, on a barrier nothing arrives on
                         if (L.wait_test && g == 0 && !mbar_wait(&bars->never, 0u, L.wait_ns)) { ok = false; break; }
                         tc_fence_after();
-                        const uint32_t acol = tmem + (buf ? TM_A1 : TM_A0);
+                        const uint32_t acol = tmem + F::A_BASE + buf * F::A_COLS;
                         const uint32_t bbase = smem_u32(s_b + st * L.stage_bytes);
 #pragma unroll
-                        for (int s = 0; s < 8; ++s) {
+                        for (int s = 0; s < F::KSTEPS; ++s) {
                             const uint32_t at = (uint32_t)s >> 2, sub = (uint32_t)s & 3u;
-                            const uint64_t bh = sw128_desc(bbase + (0 * 2 + at) * atom_bytes + sub * 32);
-                            const uint64_t bl = sw128_desc(bbase + (1 * 2 + at) * atom_bytes + sub * 32);
-                            const uint32_t ah = acol + s * 8, al = acol + 64 + s * 8;
+                            const uint64_t bh = sw128_desc(bbase + (at * 2 + 0) * atom_bytes + sub * 32);
+                            const uint32_t ah = acol + s * 8, al = acol + F::CH + s * 8;
                             const uint32_t first = (ch == 0 && s == 0) ? 0u : 1u;
-                            mma_ts(dcol, ah, bh, idesc, first);
-                            mma_ts(dcol, ah, bl, idesc, 1u);
-                            mma_ts(dcol, al, bh, idesc, 1u);
+                            if constexpr (FUSED) {
+                                // [Bh | Bl]: the lo atom follows the hi atom (2 npad rows)
+                                mma_ts(dcol, ah, bh, idesc2, first);
+                                mma_ts(dcol, al, bh, idesc, 1u);
+                            } else {
+                                const uint64_t bl = sw128_desc(bbase + (at * 2 + 1) * atom_bytes + sub * 32);
+                                mma_ts(dcol, ah, bh, idesc, first);
+                                mma_ts(dcol, ah, bl, idesc, 1u);
+                                mma_ts(dcol, al, bh, idesc, 1u);
+                            }
                         }
                         mma_commit(&bars->a_empty[buf]);
                         mma_commit(&bars->b_empty[st]);
@@ -714,7 +811,7 @@ size_t tc_smem_bytes(unsigned nfft, int nact_pad, int npad, int dmax, int stages
     // the layout of fdd_mac_tc_kernel (tc_layout) for one descriptor:
     // table mode: dmax + 1 phasors and the twiddle tables; direct mode: the
     // twiddle tables; quarter-wave mode: nfft/4 + 1 phasors
-    const size_t stage = 4ull * (size_t)npad * 128ull;
+    const size_t stage = 4ull * (size_t)npad * 128ull;  // the larger (three-MMA) stage
     const size_t table = dmax >= 0 ? (size_t)dmax + 1 : direct ? 0 : (size_t)nfft / 4 + 1;
     const size_t hi = (dmax >= 0 || direct) ? (size_t)nfft / 256 : 0;
     const size_t need = 1024 /* base alignment */ + (size_t)stages * stage + 256 +
@@ -786,7 +883,12 @@ TcLayout tc_layout(const std::vector<TcMacArgs>& descs, unsigned* err)
         if (a.nact_pad != descs[0].nact_pad)
             DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "tensor-core MAC: descriptors differ in channels");
     }
-    L.stage_bytes = 4u * (uint32_t)npad * 128u;
+    // MMA form: the three-MMA form unless DEDISP_TC_FORM=1 asks for the fused
+    // form (which needs npad <= 80); measured slower on config 2 (49.5 vs
+    // 45.6 ms per MAC), kept selectable for other shapes
+    const char* form = std::getenv("DEDISP_TC_FORM");
+    L.fused = (form && std::atoi(form) == 1 && npad <= TC_FUSED_MAX_NPAD) ? 1 : 0;
+    L.stage_bytes = (L.fused ? 2u : 4u) * (uint32_t)npad * 128u;
     L.table_entries = (uint32_t)((table + 1) & ~(size_t)1);  // keep the float2 tables 16-byte aligned
     L.tw_hi_entries = (uint32_t)((hi + 1) & ~(size_t)1);
     L.nact_pad = descs[0].nact_pad;
@@ -809,24 +911,58 @@ TcLayout tc_layout(const std::vector<TcMacArgs>& descs, unsigned* err)
 
 std::vector<TcWork> tc_work_items(const std::vector<TcMacArgs>& descs, int ctas)
 {
-    // Every (descriptor, DM tile) pair split into bin ranges so that the work
-    // list holds about `ctas` equal parts per wave of CTAs: the cost of a bin
-    // is taken as its chunks (phasor generation and MMAs scale with them).
-    double total = 0;
-    for (const TcMacArgs& a : descs) total += (double)((a.ndm + TC_M - 1) / TC_M) * (double)a.nbins;
-    const double per = std::max(1.0, total / (double)std::max(ctas, 1));
+    // An item is a bin range of one descriptor over all its DM tiles (the
+    // per-bin phasor table is built once for every tile).
+    ctas = std::max(ctas, 1);
     std::vector<TcWork> items;
-    for (size_t d = 0; d < descs.size(); ++d) {
-        const TcMacArgs& a = descs[d];
+    if (descs.size() == 1) {
+        // one descriptor: at most `ctas` equal items, CTA b takes item b
+        const TcMacArgs& a = descs[0];
         const int ntiles = (a.ndm + TC_M - 1) / TC_M;
-        // floor: one descriptor gives at most `ctas` items (one wave)
-        const size_t parts = std::max<size_t>(1, (size_t)std::floor((double)a.nbins / per + 1e-9));
+        const size_t parts = std::max<size_t>(1, std::min<size_t>(a.nbins, (size_t)ctas));
         for (size_t p = 0; p < parts; ++p) {
             const size_t k0 = a.nbins * p / parts, k1 = a.nbins * (p + 1) / parts;
-            if (k0 == k1) continue;
-            for (int t = 0; t < ntiles; ++t) items.push_back(TcWork{(int)d, t, (unsigned)k0, (unsigned)k1});
+            if (k0 < k1) items.push_back(TcWork{0, 0, ntiles, (unsigned)k0, (unsigned)k1});
+        }
+        return items;
+    }
+    // Several descriptors (a batch of beams): about 4 items per CTA, sized by
+    // an estimated cost per bin (tiles x chunks x (phasor source + columns)),
+    // assigned longest first to the least loaded CTA; CTA b runs the items at
+    // positions b, b + ctas, b + 2 ctas, ... (empty items fill the gaps).
+    auto cost_per_bin = [](const TcMacArgs& a) {
+        const double ntiles = (double)((a.ndm + TC_M - 1) / TC_M);
+        const double phasor = a.dmax >= 0 ? 1.0 : a.direct ? 2.5 : 1.3;
+        return ntiles * (double)(a.nact_pad / TC_CHUNK) * (phasor + (double)a.npad / 48.0);
+    };
+    double total = 0;
+    for (const TcMacArgs& a : descs) total += cost_per_bin(a) * (double)a.nbins;
+    const double per = std::max(1e-9, total / (4.0 * ctas));
+    std::vector<std::pair<double, TcWork>> parts;
+    for (size_t d = 0; d < descs.size(); ++d) {
+        const TcMacArgs& a = descs[d];
+        const double cb = cost_per_bin(a);
+        const int ntiles = (a.ndm + TC_M - 1) / TC_M;
+        const size_t n = std::max<size_t>(1, std::min<size_t>(a.nbins, (size_t)std::ceil(cb * (double)a.nbins / per)));
+        for (size_t p = 0; p < n; ++p) {
+            const size_t k0 = a.nbins * p / n, k1 = a.nbins * (p + 1) / n;
+            if (k0 < k1) parts.push_back({cb * (double)(k1 - k0), TcWork{(int)d, 0, ntiles, (unsigned)k0, (unsigned)k1}});
         }
     }
+    std::sort(parts.begin(), parts.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+    std::vector<double> load((size_t)ctas, 0.0);
+    std::vector<std::vector<TcWork>> per_cta((size_t)ctas);
+    for (const auto& pw : parts) {
+        const size_t b = (size_t)(std::min_element(load.begin(), load.end()) - load.begin());
+        load[b] += pw.first;
+        per_cta[b].push_back(pw.second);
+    }
+    size_t depth = 0;
+    for (const auto& l : per_cta) depth = std::max(depth, l.size());
+    const TcWork empty{0, 0, 1, 0u, 0u};
+    items.assign(depth * (size_t)ctas, empty);
+    for (size_t b = 0; b < (size_t)ctas; ++b)
+        for (size_t j = 0; j < per_cta[b].size(); ++j) items[j * (size_t)ctas + b] = per_cta[b][j];
     return items;
 }
 
@@ -856,8 +992,8 @@ void tc_prepare_list(TcParams& P, const std::vector<TcMacArgs>& descs_in, const 
     if (tc_work_bytes(items.size()) > items_bytes)
         DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "tensor-core MAC: work buffer too small");
     for (const TcWork& w : items)
-        if (w.desc < 0 || w.desc >= P.ndesc || w.k_end > descs[w.desc].nbins || w.k_begin >= w.k_end ||
-            w.tile < 0 || w.tile * 128 >= descs[w.desc].ndm)
+        if (w.desc < 0 || w.desc >= P.ndesc || w.k_end > descs[w.desc].nbins || w.k_begin > w.k_end ||
+            w.tile < 0 || w.ntile < 1 || (w.tile + w.ntile - 1) * 128 >= descs[w.desc].ndm)
             DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "tensor-core MAC: bad work item");
     // pageable source: the call returns once the bytes are staged
     if (!items.empty())
@@ -870,9 +1006,10 @@ void tc_prepare_list(TcParams& P, const std::vector<TcMacArgs>& descs_in, const 
 void launch_fdd_mac_tc_list(const TcParams& P, cudaStream_t s)
 {
     if (P.nitems <= 0) return;
-    rt::raise_smem_limit(fdd_mac_tc_kernel, P.layout.smem_bytes);
+    auto kern = P.layout.fused ? fdd_mac_tc_kernel<true> : fdd_mac_tc_kernel<false>;
+    rt::raise_smem_limit(kern, P.layout.smem_bytes);
     const int grid = std::min(P.nitems, tc_sm_count());
-    fdd_mac_tc_kernel<<<grid, TC_THREADS, P.layout.smem_bytes, s>>>(P);
+    kern<<<grid, TC_THREADS, P.layout.smem_bytes, s>>>(P);
     RT_CHECK(cudaGetLastError());
 }
 

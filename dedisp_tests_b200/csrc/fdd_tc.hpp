@@ -40,11 +40,13 @@ struct TcMacArgs {
     unsigned long long nmagic = 0;  // set by the launcher
 };
 
-// One item of a MAC launch: bins [k_begin, k_end) of DM tile `tile` (128
-// DMs) of descriptor `desc`.
+// One item of a MAC launch: bins [k_begin, k_end) of DM tiles
+// tile .. tile + ntile - 1 (128 DMs each) of descriptor `desc`; per bin the
+// tiles run one after another.
 struct TcWork {
     int desc;
     int tile;
+    int ntile;
     unsigned k_begin;
     unsigned k_end;
 };
@@ -53,6 +55,7 @@ struct TcWork {
 // descriptors, which share the channel set).
 struct TcLayout {
     int stages;                // B pipeline depth
+    int fused;                 // 1: fused MMA form (largest npad <= 80)
     uint32_t stage_bytes;      // per stage (largest npad)
     uint32_t table_entries;    // phasor table (largest)
     uint32_t tw_hi_entries;    // two-level twiddle table, hi part (largest nfft / 256)
@@ -111,7 +114,9 @@ void launch_fdd_prep_b(const float2* X, size_t bin_pitch, int nseg, size_t nbins
 void launch_fdd_mac_tc(const TcMacArgs& a, const void* B, void* d_items, size_t items_bytes, cudaStream_t s);
 
 // Up to kTcMaxDesc descriptors in one persistent launch: work items over all
-// of them (tc_work_items, about `ctas` equal parts), tensor maps encoded (B
+// of them (tc_work_items: one descriptor, at most `ctas` equal bin ranges;
+// several, about 4 per CTA assigned longest first, laid out for a grid of
+// exactly `ctas` CTAs, CTA b taking positions b, b + ctas, ...), tensor maps encoded (B
 // operand per descriptor) into P, items copied to d_items; then launched
 // (possibly later, or inside a graph: P is copied into the launch).
 size_t tc_work_bytes(size_t nitems);
