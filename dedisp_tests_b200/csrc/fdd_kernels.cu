@@ -669,11 +669,19 @@ __device__ __forceinline__ void stockham_pass(const float2* __restrict__ in, flo
                 dst[2 * Ns] = s02 - s13;
                 dst[3 * Ns] = d02 - rot;
             } else {
+                // W_r^{t u} = W_Q^{t u wr}: index stepped by u wr (mod Q)
                 for (int u = 0; u < r; ++u) {
                     float2 acc = v[0];
+                    const int su = u * wr;
+                    int x = 0;
 #pragma unroll
-                    for (int t = 1; t < 8; ++t)
-                        if (t < r) acc = acc + cmul(v[t], W(((t * u) % r) * wr));
+                    for (int t = 1; t < 8; ++t) {
+                        if (t < r) {
+                            x += su;
+                            if (x >= Q) x -= Q;
+                            acc = acc + cmul(v[t], W(x));
+                        }
+                    }
                     dst[u * Ns] = acc;
                 }
             }
@@ -686,8 +694,13 @@ __device__ __forceinline__ void stockham_pass(const float2* __restrict__ in, flo
             const int k = j % Ns;
             const float2* src = in + col * Q + j;
             float2 acc = src[0];
+            // input twiddle W_{Ns r}^{t k} times W_r^{t u}: W_Q^{t s}, s = k ws + u wr
+            // (wr r = Q), the index stepped by s (mod Q)
+            const int s = (k * ws + u * wr) % Q;
+            int x = 0;
             for (int t = 1; t < r; ++t) {
-                const int x = (t * k * ws + ((t * u) % r) * wr) % Q;
+                x += s;
+                if (x >= Q) x -= Q;
                 acc = acc + cmul(src[t * R], W(x));
             }
             out[col * Q + (j / Ns) * Ns * r + k + u * Ns] = acc;

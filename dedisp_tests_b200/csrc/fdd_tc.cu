@@ -64,18 +64,23 @@ constexpr size_t TC_MAX_SMEM = 227 * 1024;
 //     adjacent in shared memory), then Al Bh (N = npad) into its first npad
 //     columns; the epilogue adds the two halves. Accumulators of 160 columns at
 //     0 and 160, 32-channel A chunks in 3 buffers of 64 columns at 320, 384, 448.
-template <bool FUSED>
+//   deep (npad <= 64): the three-MMA form with 3 A buffers (0, 128, 256) and
+//     accumulators of 64 columns at 384 and 448: half again as many phasors
+//     in flight, which is what bounds the MAC when it waits on MMA
+//     completions rather than on the tensor pipe.
+template <bool FUSED, bool DEEP = false>
 struct TcForm {
     static constexpr int CH = FUSED ? 32 : 64;            // channels per A chunk
     static constexpr int PART_CH = CH / TC_PARTS;         // per producer thread
-    static constexpr int NBUF = FUSED ? 3 : 2;            // A buffers
+    static constexpr int NBUF = (FUSED || DEEP) ? 3 : 2;  // A buffers
     static constexpr uint32_t A_COLS = 2 * CH;            // hi CH + lo CH columns
     static constexpr uint32_t A_BASE = FUSED ? 320 : 0;
-    static constexpr uint32_t C0 = FUSED ? 0 : 256, C1 = FUSED ? 160 : 384;
+    static constexpr uint32_t C0 = FUSED ? 0 : DEEP ? 384 : 256, C1 = FUSED ? 160 : DEEP ? 448 : 384;
     static constexpr int KSTEPS = CH / 8;                 // K16 steps per chunk
     static constexpr int ATOMS = CH / 32;                 // 64-kk TMA atoms per split
 };
 constexpr int TC_FUSED_MAX_NPAD = 80;
+constexpr int TC_DEEP_MAX_NPAD = 64;
 constexpr int TC_MAX_ABUF = 3;
 
 struct alignas(8) SmemBarriers {
@@ -264,10 +269,10 @@ __device__ __forceinline__ uint2 split_bf16x2(float re, float im)
 // pipeline counters run on across items, so the hand-offs of consecutive
 // items overlap; each item's last accumulator is read out before the next
 // item starts. One plan's launch is the one-descriptor case.
-template <bool FUSED>
+template <bool FUSED, bool DEEP>
 __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_constant__ TcParams P)
 {
-    using F = TcForm<FUSED>;
+    using F = TcForm<FUSED, DEEP>;
     // descriptors and tensor maps live in the parameter bank (constant
     // operands, no registers); the items in global memory
     const TcMacArgs* descs = P.descs;
@@ -372,7 +377,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
             asm volatile("bar.sync 1, %0;" ::"n"(TC_PRODUCER_WARPS * 32) : "memory");
             const int row = quad * 32 + lane;  // this thread's DM row within a tile
             const int first_iter = bin_iter;
-            int prev_m = 0;                    // DM row of the previous (bin, tile) pair
+            const int last_tile = w.tile + w.ntile - 1;
 
             auto epilogue = [&](int itr, size_t kk, int m) -> bool {
                 const uint32_t cb = (uint32_t)itr & 1u;
@@ -438,7 +443,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
             for (size_t k = w.k_begin; k <= w.k_end; ++k) {
                 const bool tail = k == w.k_end;
                 if (tail) {
-                    if (ok && bin_iter > first_iter) ok = epilogue(bin_iter - 1, k - 1, prev_m);
+                    if (ok && bin_iter > first_iter) ok = epilogue(bin_iter - 1, k - 1, last_tile * TC_M + row);
                     if (!ok) *abort_flag = 1u;
                     break;
                 }
@@ -479,32 +484,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                             // covers 0..dmax, the largest delay over the plan's DMs and
                             // channels computed on the host with the same float
                             // operations, so the unsigned clamp is only a guard
-                            float dl[TC_PART_CH];
                             const float4* sd4 = reinterpret_cast<const float4*>(s_delay + c0);
+                            const uint32_t dmax = (uint32_t)a.dmax;
+                            const bool rn = a.round_delays != 0;
 #pragma unroll
                             for (int q = 0; q < TC_PART_CH / 4; ++q) {
                                 const float4 v4 = sd4[q];
-                                dl[4 * q] = v4.x;
-                                dl[4 * q + 1] = v4.y;
-                                dl[4 * q + 2] = v4.z;
-                                dl[4 * q + 3] = v4.w;
-                            }
-                            const uint32_t dmax = (uint32_t)a.dmax;
-                            if (a.round_delays) {
+                                const float dl[4] = {v4.x, v4.y, v4.z, v4.w};
 #pragma unroll
-                                for (int i = 0; i < TC_PART_CH; ++i) {
-                                    const float y = __fadd_rn(__fmul_rn(dm, dl[i]), 8388608.0f);
+                                for (int i = 0; i < 4; ++i) {
+                                    const float x = __fmul_rn(dm, dl[i]);
+                                    const float y = rn ? __fadd_rn(x, 8388608.0f) : __fadd_rz(x, 8388608.0f);
                                     const uint2 v = s_table[min(__float_as_uint(y) - 0x4B000000u, dmax)];
-                                    hi[i] = v.x;
-                                    lo[i] = v.y;
-                                }
-                            } else {
-#pragma unroll
-                                for (int i = 0; i < TC_PART_CH; ++i) {
-                                    const float y = __fadd_rz(__fmul_rn(dm, dl[i]), 8388608.0f);
-                                    const uint2 v = s_table[min(__float_as_uint(y) - 0x4B000000u, dmax)];
-                                    hi[i] = v.x;
-                                    lo[i] = v.y;
+                                    hi[4 * q + i] = v.x;
+                                    lo[4 * q + i] = v.y;
                                 }
                             }
                         } else if (direct) {
@@ -560,9 +553,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                     }
                 }
                 // the previous pair's read-out overlaps this pair's MMAs
-                if (ok && bin_iter > first_iter) ok = epilogue(bin_iter - 1, t > w.tile ? k : k - 1, prev_m);
+                if (ok && bin_iter > first_iter)
+                    ok = epilogue(bin_iter - 1, t > w.tile ? k : k - 1, (t > w.tile ? t - 1 : last_tile) * TC_M + row);
                 if (!ok) *abort_flag = 1u;  // the others stop at the next barrier
-                prev_m = t * TC_M + row;
                 ++bin_iter;
                 }
             }
@@ -888,6 +881,9 @@ TcLayout tc_layout(const std::vector<TcMacArgs>& descs, unsigned* err)
     // 45.6 ms per MAC), kept selectable for other shapes
     const char* form = std::getenv("DEDISP_TC_FORM");
     L.fused = (form && std::atoi(form) == 1 && npad <= TC_FUSED_MAX_NPAD) ? 1 : 0;
+    // three A buffers when the accumulators fit in 64 columns (DEDISP_TC_FORM=2
+    // keeps two, for comparison)
+    L.deep = (!L.fused && npad <= TC_DEEP_MAX_NPAD && !(form && std::atoi(form) == 2)) ? 1 : 0;
     L.stage_bytes = (L.fused ? 2u : 4u) * (uint32_t)npad * 128u;
     L.table_entries = (uint32_t)((table + 1) & ~(size_t)1);  // keep the float2 tables 16-byte aligned
     L.tw_hi_entries = (uint32_t)((hi + 1) & ~(size_t)1);
@@ -1006,7 +1002,9 @@ void tc_prepare_list(TcParams& P, const std::vector<TcMacArgs>& descs_in, const 
 void launch_fdd_mac_tc_list(const TcParams& P, cudaStream_t s)
 {
     if (P.nitems <= 0) return;
-    auto kern = P.layout.fused ? fdd_mac_tc_kernel<true> : fdd_mac_tc_kernel<false>;
+    auto kern = P.layout.fused  ? fdd_mac_tc_kernel<true, false>
+                : P.layout.deep ? fdd_mac_tc_kernel<false, true>
+                                : fdd_mac_tc_kernel<false, false>;
     rt::raise_smem_limit(kern, P.layout.smem_bytes);
     const int grid = std::min(P.nitems, tc_sm_count());
     kern<<<grid, TC_THREADS, P.layout.smem_bytes, s>>>(P);

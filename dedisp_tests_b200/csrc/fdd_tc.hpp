@@ -56,6 +56,7 @@ struct TcWork {
 struct TcLayout {
     int stages;                // B pipeline depth
     int fused;                 // 1: fused MMA form (largest npad <= 80)
+    int deep;                  // 1: three-MMA form with 3 A buffers (largest npad <= 64)
     uint32_t stage_bytes;      // per stage (largest npad)
     uint32_t table_entries;    // phasor table (largest)
     uint32_t tw_hi_entries;    // two-level twiddle table, hi part (largest nfft / 256)

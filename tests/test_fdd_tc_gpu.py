@@ -127,3 +127,22 @@ def test_tc_many_segments(nsamps):
     ref = po.fdd_timeseries(x, _delays(params), km, dms, nout, round_delays=True)
     rel, mx = _errs(out[:, :nout], ref)
     assert rel < TC_REL_L2 and mx < TC_MAX_ABS, (nseg, rel, mx)
+
+
+@pytest.mark.parametrize("form", ["1", "2"])
+def test_tc_selectable_mma_forms(form, monkeypatch):
+    """The MMA forms chosen by DEDISP_TC_FORM (read at each launch): 1 the
+    fused A_hi x [B_hi | B_lo] form, 2 the three-MMA form with two A buffers
+    (the default takes three when the accumulators fit 64 columns). Same
+    tolerance against FP64."""
+    monkeypatch.setenv("DEDISP_TC_FORM", form)
+    nchans, nsamps = 96, 90000
+    inp, params = _input(nchans, nsamps, 7)
+    dms = np.linspace(0, 120, 200, dtype=np.float32)
+    p = _plan(params, dms, segmented=1, precision=1)
+    nout = nsamps - p.get_max_delay()
+    out = _run(p, nsamps, inp, 8, len(dms))
+    x = _oracle_x(inp, nsamps, params, 8)
+    ref = po.fdd_timeseries(x, _delays(params), np.ones(nchans, np.int32), dms, nout)
+    rel, mx = _errs(out, ref)
+    assert rel < TC_REL_L2 and mx < TC_MAX_ABS, (form, rel, mx)
