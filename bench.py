@@ -622,7 +622,7 @@ def run_batched_fdd(args, local, world, stream, max_over_ranks, nbeams=12, nplai
             cur = trial
     waves.append(cur)
     pool = torch.empty(max(sum(out_bytes[j] for j in w) for w in waves), dtype=torch.uint8, device=dev)
-    batches = []
+    batches, bsources = [], {}
     for w in waves:
         b = dd.FddBatch(c0.nchans, c0.dt, c0.f_top, c0.df, in_nbits=8, device=local)
         sp, off = [], 0
@@ -630,6 +630,9 @@ def run_batched_fdd(args, local, world, stream, max_over_ranks, nbeams=12, nplai
             sp.append(spec(j, pool[off:off + out_bytes[j]]))
             off += out_bytes[j]
         b.set_beams(sp)
+        for j in range(len(w)):
+            src = b.phasor_source(j)
+            bsources[src] = bsources.get(src, 0) + 1
         batches.append(b)
     ws_bytes = max(b.workspace_size() for b in batches)
     ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
@@ -672,12 +675,24 @@ def run_batched_fdd(args, local, world, stream, max_over_ranks, nbeams=12, nplai
     res["batched_bf16x3_tc"]["rel_l2_vs_fp64"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
     res["batched_bf16x3_tc"]["max_abs_vs_fp64"] = float(np.abs(got - ref).max() / np.abs(ref).max())
     res["batched_bf16x3_tc"]["error_sample"] = f"beam {bi}, DMs {drows.tolist()} x first {nchk} samples"
+    # stage split of one more step (direct launches with events, untimed above)
+    split = {"prep_ms": 0.0, "mac_ms": 0.0, "post_ms": 0.0}
+    for b in batches:
+        b.set_timing(True)
+        b.execute(stream.cuda_stream, use_graph=False)
+        t = b.get_timing()
+        b.set_timing(False)
+        for k in split:
+            split[k] += t[k]
+    res["batched_bf16x3_tc"]["stage_ms"] = {k: round(v, 2) for k, v in split.items()}
+    res["batched_bf16x3_tc"]["phasor_sources"] = bsources
     for b in batches:
         b.close()
     del pool, ws, batches
     torch.cuda.empty_cache()
 
     # sequential single-beam plans (one execute per beam)
+    stage_sum, sources = {}, {}
     for name, prec, sub in (("tc_single_beam", 1, list(range(nbeams))),
                             ("plain_fp32_single_beam", 0, list(range(nplain)))):
         tms, su = 0.0, 0.0
@@ -696,12 +711,26 @@ def run_batched_fdd(args, local, world, stream, max_over_ranks, nbeams=12, nplai
             torch.cuda.synchronize()
             tms += max_over_ranks(e0.elapsed_time(e1))
             su += units[i]
+            # stage split and phasor source from one more (timed-stage) execute
+            p.set_timing(True)
+            p.execute(c.nsamps, d_in[i], 8, y, 32, dd.DEDISP_DEVICE_POINTERS)
+            st_ms = p.get_stage_times()
+            for k in ("prep", "mac", "post"):
+                stage_sum.setdefault(name, {}).setdefault(k + "_ms", 0.0)
+            stage_sum[name]["mac_ms"] += st_ms["mac"]
+            stage_sum[name]["prep_ms"] += st_ms["unpack"] + st_ms["fft_fwd"] + st_ms["layout"]
+            stage_sum[name]["post_ms"] += st_ms["transpose"] + st_ms["fft_inv"]
+            if prec == 1:
+                sources[p.get_phasor_source()] = sources.get(p.get_phasor_source(), 0) + 1
             p.close()
             del y
             torch.cuda.empty_cache()
         res[name] = {"value": su * world / (tms * 1e-3), "unit": UNIT, "ms": tms,
                      "sample": f"beams {sub[0]}-{sub[-1]} ({su:.3e} DM-trials x samples), one plan "
-                               f"execute per beam (each plan timed after its own warm-up)"}
+                               f"execute per beam (each plan timed after its own warm-up)",
+                     "stage_ms": {k: round(v, 2) for k, v in stage_sum[name].items()}}
+        if prec == 1:
+            res[name]["phasor_sources"] = dict(sources)
     res["batched_vs_plain_fp32"] = res["batched_bf16x3_tc"]["value"] / res["plain_fp32_single_beam"]["value"]
     res["batched_vs_tc_single_beam"] = res["batched_bf16x3_tc"]["value"] / res["tc_single_beam"]["value"]
     del d_in

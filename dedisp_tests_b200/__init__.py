@@ -119,6 +119,7 @@ def lib() -> C.CDLL:
         "dedisp_b200_set_fdd_options": (err, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _sz]),
         "dedisp_b200_output_row_length": (_sz, [_vp, _sz]),
         "dedisp_b200_get_stage_times": (err, [_vp, C.POINTER(C.c_float), C.c_int]),
+        "dedisp_b200_get_phasor_source": (err, [_vp, C.POINTER(C.c_int)]),
         "dedisp_b200_set_wait_limit_ns": (err, [C.c_ulonglong]),
         "dedisp_b200_get_wait_limit_ns": (C.c_ulonglong, []),
         "dedisp_b200_set_wait_expiry_test": (err, [C.c_int]),
@@ -274,6 +275,15 @@ class Plan:
         _check(lib().dedisp_b200_get_stage_times(self._h, v, 6))
         return dict(zip(self.STAGES, [float(x) for x in v]))
 
+    PHASOR_SOURCES = {-1: None, 0: "table", 1: "quarter", 2: "hybrid", 3: "direct"}
+
+    def get_phasor_source(self):
+        """FDD plans: phasor source of the last tensor-core MAC ("table",
+        "quarter", "hybrid", "direct"), None when none ran."""
+        v = C.c_int()
+        _check(lib().dedisp_b200_get_phasor_source(self._h, C.byref(v)))
+        return self.PHASOR_SOURCES[v.value]
+
 
 class DedispPlan(Plan):
     """Original dedisp interface (reference src/dedisp/DedispPlan.hpp)."""
@@ -369,6 +379,7 @@ _BATCH_SIGS = {
     "dedisp_b200_fdd_batch_get_timing": (C.c_int, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                                    C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "dedisp_b200_fdd_batch_max_delay": (_sz, [_vp, _sz]),
+    "dedisp_b200_fdd_batch_phasor_source": (C.c_int, [_vp, _sz]),
 }
 
 
@@ -544,6 +555,11 @@ class FddBatch:
 
     def max_delay(self, beam: int) -> int:
         return int(_batch_lib().dedisp_b200_fdd_batch_max_delay(self._h, beam))
+
+    def phasor_source(self, beam: int):
+        """Phasor source planned for a beam's tensor-core MAC ("table",
+        "quarter", "hybrid", "direct"), None without MAC work."""
+        return Plan.PHASOR_SOURCES[int(_batch_lib().dedisp_b200_fdd_batch_phasor_source(self._h, beam))]
 
 
 class _GulpRecord(C.Structure):

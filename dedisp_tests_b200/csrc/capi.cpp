@@ -343,6 +343,16 @@ dedisp_error dedisp_b200_get_stage_times(dedisp_plan plan, float* stage_ms, int 
     return DEDISP_NO_ERROR;
 }
 
+dedisp_error dedisp_b200_get_phasor_source(dedisp_plan plan, int* source)
+{
+    if (!plan) return DEDISP_INVALID_PLAN;
+    auto* g = dynamic_cast<dedisp::GPUPlan*>(plan->ptr.get());
+    if (!g) return DEDISP_INVALID_PLAN;
+    if (!source) return DEDISP_INVALID_POINTER;
+    *source = g->last_timing().phasor;
+    return DEDISP_NO_ERROR;
+}
+
 dedisp_error dedisp_b200_last_error(char* msg, dedisp_size len)
 {
     if (msg && len) {

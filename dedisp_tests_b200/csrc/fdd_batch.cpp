@@ -24,8 +24,7 @@ struct FddBatch::Beam {
     kern::BinMap bmap;
     size_t bin_pitch = 0, x_len = 0, seg_stride = 0;
     int dmax = -1;      // largest delay index (trunc), -1 if a DM is negative
-    int tc_dmax = -1;   // per-bin delay-table mode when >= 0
-    bool direct = false;
+    kern::TcSource src;  // phasor source of the tensor-core MAC
     int npad = 0, ngroups = 0;
     size_t b_bytes = 0;  // one segment group's B operand
     size_t off_b = 0, off_yt = 0;
@@ -98,6 +97,14 @@ size_t FddBatch::max_delay(size_t beam) const
     return m_beams[beam]->max_delay;
 }
 
+int FddBatch::phasor_source(size_t beam) const
+{
+    if (beam >= m_beams.size()) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "beam index out of range");
+    const Beam& b = *m_beams[beam];
+    if (b.nout == 0 || m_nact == 0) return -1;
+    return b.src.hybrid ? 2 : b.src.dmax >= 0 ? 0 : b.src.direct ? 3 : 1;
+}
+
 size_t FddBatch::nsamp_out(size_t beam) const
 {
     if (beam >= m_beams.size()) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "beam index out of range");
@@ -140,10 +147,10 @@ void FddBatch::plan()
         b.dmax = (ok && dmax < (1l << 30)) ? (int)dmax : -1;
         b.ngroups = (int)((nseg + kern::kTcMaxSeg - 1) / kern::kTcMaxSeg);
         b.npad = kern::tc_pad_n((int)std::min<size_t>(nseg, kern::kTcMaxSeg));
-        b.tc_dmax = kern::tc_table_mode_dmax(b.dmax, (unsigned)nfft, m_nact_pad, b.npad);
-        b.direct = b.tc_dmax < 0 && !kern::tc_quarter_mode_fits((unsigned)nfft, m_nact_pad, b.npad);
-        if (b.direct && !kern::tc_direct_mode_fits((unsigned)nfft, m_nact_pad, b.npad))
-            DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "tensor-core MAC: transform length too large");
+        const int cap = std::min(kern::tc_table_capacity(b.npad, nfft / 256, m_nact_pad), kern::tc_table_cap_limit());
+        b.src = kern::tc_choose_source(b.dmax, (unsigned)nfft, cap,
+                                       kern::tc_quarter_mode_fits((unsigned)nfft, m_nact_pad, b.npad));
+        if (b.src.dmax == -2) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "tensor-core MAC: transform length too large");
         b.b_bytes = round_up(kern::tc_b_bytes(nbins, m_nact_pad, (int)std::min<size_t>(nseg, kern::kTcMaxSeg)),
                              kAlign);
         const size_t yt = round_up(nbins * nseg * ndm * sizeof(float2), kAlign);
@@ -159,33 +166,42 @@ void FddBatch::plan()
         const size_t sc = b.qpath ? rows * (nfft / 2) : kern::fft_scratch_elems((int)nfft, rows);
         scratch = std::max(scratch, round_up(sc * sizeof(float2), kAlign));
     }
-    // The MAC's shared-memory layout is the union of the beams' tables:
-    // beams whose tables would not fit together fall back to direct phasors.
-    auto union_fits = [&]() {
+    // The MAC's shared-memory layout is the union of the beams' tables. When
+    // they do not fit together, every beam's source is chosen again for the
+    // room left beside all beams' twiddle tables (a shorter per-bin table with
+    // the larger delays computed, the quarter-wave table if it fits, or every
+    // phasor computed): then the union fits by construction.
+    int npad_u = 16;
+    size_t hi_all = 0;
+    for (auto& bp : m_beams) {
+        if (bp->nout == 0) continue;
+        npad_u = std::max(npad_u, bp->npad);
+        if (bp->g.nfft % 256 == 0) hi_all = std::max(hi_all, bp->g.nfft / 256);
+    }
+    auto union_bytes = [&]() {
         size_t table = 0, hi = 0;
-        int npad = 16;
         for (auto& bp : m_beams) {
             const Beam& b = *bp;
             if (b.nout == 0) continue;
-            npad = std::max(npad, b.npad);
-            const size_t t = b.tc_dmax >= 0 ? (size_t)b.tc_dmax + 1 : b.direct ? 0 : b.g.nfft / 4 + 1;
+            const size_t t = b.src.dmax >= 0 ? (size_t)b.src.dmax + 1 : b.src.direct ? 0 : b.g.nfft / 4 + 1;
             table = std::max(table, t);
-            if (b.tc_dmax >= 0 || b.direct) hi = std::max(hi, b.g.nfft / 256);
+            if (b.src.dmax >= 0 || b.src.direct) hi = std::max(hi, b.g.nfft / 256);
         }
-        const size_t bytes = 1024 + 2 * (size_t)(4 * npad * 128) + 256 + (table + 2 + 256 + hi + 2) * 8 +
-                             (size_t)m_nact_pad * 4 + 32;
-        return bytes <= 227 * 1024;
+        return kern::tc_layout_bytes(npad_u, table, hi, m_nact_pad, 2);
     };
-    if (!union_fits())
-        for (auto& bp : m_beams)
-            if (bp->tc_dmax < 0) bp->direct = true;
-    while (!union_fits()) {
-        Beam* worst = nullptr;
-        for (auto& bp : m_beams)
-            if (bp->nout && bp->tc_dmax >= 0 && (!worst || bp->tc_dmax > worst->tc_dmax)) worst = bp.get();
-        if (!worst) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "tensor-core MAC: the beams' tables do not fit");
-        worst->tc_dmax = -1;
-        worst->direct = true;
+    if (union_bytes() > kern::kTcMaxSmem) {
+        const int cap = std::min(kern::tc_table_capacity(npad_u, hi_all, m_nact_pad), kern::tc_table_cap_limit());
+        for (auto& bp : m_beams) {
+            Beam& b = *bp;
+            if (b.nout == 0) continue;
+            const unsigned n = (unsigned)b.g.nfft;
+            const bool quarter = cap >= 0 && (size_t)n / 4 <= (size_t)cap && kern::tc_quarter_mode_fits(n, m_nact_pad, b.npad);
+            b.src = kern::tc_choose_source(b.dmax, n, cap, quarter);
+            if (b.src.dmax == -2)
+                DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "tensor-core MAC: the beams' tables do not fit");
+        }
+        if (union_bytes() > kern::kTcMaxSmem)
+            DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "tensor-core MAC: the beams' tables do not fit");
     }
     m_shared_bytes = shared;
     m_scratch_off = shared;
@@ -260,7 +276,7 @@ void FddBatch::upload()
         b.tw_hi.reserve(hi.size() * sizeof(float2));
         RT_CHECK(cudaMemcpy(b.tw_lo.get(), lo.data(), lo.size() * sizeof(float2), cudaMemcpyHostToDevice));
         RT_CHECK(cudaMemcpy(b.tw_hi.get(), hi.data(), hi.size() * sizeof(float2), cudaMemcpyHostToDevice));
-        if (b.tc_dmax < 0 && !b.direct) {
+        if (b.src.dmax < 0 && !b.src.direct) {
             const std::vector<uint2> t = kern::tc_quarter_table((unsigned)b.g.nfft);
             b.qtable.reserve(t.size() * sizeof(uint2));
             RT_CHECK(cudaMemcpy(b.qtable.get(), t.data(), t.size() * sizeof(uint2), cudaMemcpyHostToDevice));
@@ -291,8 +307,9 @@ void FddBatch::upload()
             a.nbins = b.g.nbins;
             a.nfft = (unsigned)b.g.nfft;
             a.round_delays = 0;
-            a.dmax = b.tc_dmax;
-            a.direct = b.direct ? 1 : 0;
+            a.dmax = b.src.dmax;
+            a.direct = b.src.direct;
+            a.hybrid = b.src.hybrid;
             descs.push_back(a);
             Bs.push_back(ws + b.off_b + (size_t)gi * b.b_bytes);
         }
@@ -565,6 +582,14 @@ dedisp_error dedisp_b200_fdd_batch_get_timing(dedisp_b200_fdd_batch batch, float
         if (post_ms) *post_ms = b.last_post_ms;
         if (launches) *launches = b.last_launches;
     });
+}
+
+int dedisp_b200_fdd_batch_phasor_source(dedisp_b200_fdd_batch batch, dedisp_size beam)
+{
+    int v = -1;
+    if (fdd_batch_call(batch, [&](dedisp::detail::FddBatch& b) { v = b.phasor_source(beam); }) != DEDISP_NO_ERROR)
+        return -1;
+    return v;
 }
 
 dedisp_size dedisp_b200_fdd_batch_max_delay(dedisp_b200_fdd_batch batch, dedisp_size beam)

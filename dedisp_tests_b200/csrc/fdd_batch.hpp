@@ -49,6 +49,9 @@ public:
     void set_beams(std::vector<FddBeamSpec> beams);
     size_t beam_count() const { return m_beams.size(); }
     size_t max_delay(size_t beam) const;
+    // Phasor source of a beam's tensor-core MAC as planned by set_beams (the
+    // codes of dedisp_b200_get_phasor_source); -1 when it has no MAC work.
+    int phasor_source(size_t beam) const;
     size_t nsamp_out(size_t beam) const;
 
     // Device bytes of scratch and per-beam operands the batch needs.

@@ -155,7 +155,7 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
     m.x.reserve(nchans * x_len * sizeof(float));
     m.X.reserve(nchans * nseg * bin_pitch * sizeof(float2));
     int nact_pad = 0, npad = 0, tc_dmax = -1;
-    bool tc_direct = false;
+    bool tc_direct = false, tc_hybrid = false;
     const int seg_group = (int)std::min<size_t>(nseg, (size_t)kern::kTcMaxSeg);
     if (use_tc) {
         nact_pad = kern::tc_pad_channels(m.nact);
@@ -189,15 +189,20 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
             m.dmax_version = v.version;
             m.dmax_round = rnd;
         }
-        // Phasor source, in order of preference: the per-bin delay table,
-        // the quarter-wave table (power-of-two lengths), or each phasor from
-        // the two-level twiddle tables (any length whose tables fit).
-        tc_dmax = kern::tc_table_mode_dmax(m.dmax, (unsigned)g.nfft, nact_pad, npad);
-        tc_direct = tc_dmax < 0 && !kern::tc_quarter_mode_fits((unsigned)g.nfft, nact_pad, npad);
-        if (tc_direct && !kern::tc_direct_mode_fits((unsigned)g.nfft, nact_pad, npad))
+        // Phasor source: the per-bin delay table when it holds every delay,
+        // else the cheapest of the quarter-wave table (power-of-two lengths),
+        // the table over the small delays with the rest computed (hybrid),
+        // or each phasor from the two-level twiddle tables.
+        const int cap = std::min(kern::tc_table_capacity(npad, g.nfft / 256, nact_pad), kern::tc_table_cap_limit());
+        const kern::TcSource src = kern::tc_choose_source(
+            m.dmax, (unsigned)g.nfft, cap, kern::tc_quarter_mode_fits((unsigned)g.nfft, nact_pad, npad));
+        if (src.dmax == -2)
             DD_THROW_MSG(DEDISP_UNKNOWN_ERROR,
                          "tensor-core MAC: transform length too large for its twiddle tables in shared "
                          "memory; use precision 0");
+        tc_dmax = src.dmax;
+        tc_direct = src.direct != 0;
+        tc_hybrid = src.hybrid != 0;
         if (m.qtable_n != g.nfft) {
             const std::vector<uint2> t = kern::tc_quarter_table((unsigned)g.nfft);
             m.qtable.reserve(t.size() * sizeof(uint2));
@@ -281,6 +286,7 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
         ta.round_delays = opt.round_delays ? 1 : 0;
         ta.dmax = tc_dmax;
         ta.direct = tc_direct ? 1 : 0;
+        ta.hybrid = tc_hybrid ? 1 : 0;
         const size_t wb = kern::tc_work_bytes((size_t)kern::tc_sm_count() + 64);
         m.tcwork.reserve(wb);
         // Segment groups of at most kTcMaxSeg (the accumulator's 128
@@ -354,6 +360,7 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
         stats.kernel_ms = stats.stage_ms[3];
         stats.variant = use_tc ? 1 : 0;
     }
+    stats.phasor = !use_tc ? -1 : tc_hybrid ? 2 : tc_dmax >= 0 ? 0 : tc_direct ? 3 : 1;
 }
 
 }  // namespace detail

@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
@@ -54,7 +55,7 @@ constexpr uint32_t TC_WAIT_POLLS = 1u << 28;
 // Dynamic shared memory requested per CTA is at least this much so that only
 // one CTA fits on an SM (each CTA allocates all 512 tensor-memory columns).
 constexpr size_t TC_MIN_SMEM = 120 * 1024;
-constexpr size_t TC_MAX_SMEM = 227 * 1024;
+constexpr size_t TC_MAX_SMEM = kTcMaxSmem;
 
 // Two MMA forms. Per K step of 16 reals:
 //   plain (any npad <= 128): Ah Bh, Ah Bl, Al Bh as three N = npad MMAs into
@@ -255,6 +256,30 @@ __device__ __forceinline__ int tc_delay_small(float dm, float delay, int round_d
 
 // (re, im) -> packed bf16x2 hi parts (re low half) and lo parts
 // (bf16(x - hi)).
+__device__ __forceinline__ uint2 split_bf16x2(float re, float im);
+
+// The phasor exp(+2 pi i (k d mod N) / N), split into bf16 hi/lo pairs, from
+// the two-level twiddle tables in shared memory (the product the per-bin
+// delay table holds). pow2: N a power of two (index by mask), else by
+// Barrett reduction with nmagic = floor((2^64 - 1) / N).
+__device__ __forceinline__ uint2 phasor_direct(size_t k, int d, uint32_t nfft, bool pow2, uint64_t nmagic,
+                                               const float2* s_tw_lo, const float2* s_tw_hi)
+{
+    uint32_t idx;
+    if (pow2) {
+        idx = ((uint32_t)k * (uint32_t)d) & (nfft - 1u);
+    } else {
+        const uint32_t dn = d >= 0 ? (uint32_t)d % nfft : nfft - 1u - (uint32_t)(-(d + 1)) % nfft;
+        const uint64_t p = (uint64_t)k * dn;
+        uint64_t r = p - __umul64hi(p, nmagic) * (uint64_t)nfft;
+        while (r >= nfft) r -= nfft;
+        idx = (uint32_t)r;
+    }
+    const float2 h = s_tw_hi[idx >> 8], l = s_tw_lo[idx & 255u];
+    const float c = __fsub_rn(__fmul_rn(h.x, l.x), __fmul_rn(h.y, l.y));
+    const float sn = -__fadd_rn(__fmul_rn(h.x, l.y), __fmul_rn(h.y, l.x));
+    return split_bf16x2(c, sn);
+}
 __device__ __forceinline__ uint2 split_bf16x2(float re, float im)
 {
     const __nv_bfloat162 hi = __floats2bfloat162_rn(re, im);
@@ -487,40 +512,45 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                             const float4* sd4 = reinterpret_cast<const float4*>(s_delay + c0);
                             const uint32_t dmax = (uint32_t)a.dmax;
                             const bool rn = a.round_delays != 0;
+                            if (!a.hybrid) {
 #pragma unroll
-                            for (int q = 0; q < TC_PART_CH / 4; ++q) {
-                                const float4 v4 = sd4[q];
-                                const float dl[4] = {v4.x, v4.y, v4.z, v4.w};
+                                for (int q = 0; q < TC_PART_CH / 4; ++q) {
+                                    const float4 v4 = sd4[q];
+                                    const float dl[4] = {v4.x, v4.y, v4.z, v4.w};
 #pragma unroll
-                                for (int i = 0; i < 4; ++i) {
-                                    const float x = __fmul_rn(dm, dl[i]);
-                                    const float y = rn ? __fadd_rn(x, 8388608.0f) : __fadd_rz(x, 8388608.0f);
-                                    const uint2 v = s_table[min(__float_as_uint(y) - 0x4B000000u, dmax)];
-                                    hi[4 * q + i] = v.x;
-                                    lo[4 * q + i] = v.y;
+                                    for (int i = 0; i < 4; ++i) {
+                                        const float x = __fmul_rn(dm, dl[i]);
+                                        const float y = rn ? __fadd_rn(x, 8388608.0f) : __fadd_rz(x, 8388608.0f);
+                                        const uint2 v = s_table[min(__float_as_uint(y) - 0x4B000000u, dmax)];
+                                        hi[4 * q + i] = v.x;
+                                        lo[4 * q + i] = v.y;
+                                    }
+                                }
+                            } else {
+                                // the table covers delays 0..dmax; larger ones are
+                                // computed from the twiddle tables
+#pragma unroll
+                                for (int q = 0; q < TC_PART_CH / 4; ++q) {
+                                    const float4 v4 = sd4[q];
+                                    const float dl[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+                                    for (int i = 0; i < 4; ++i) {
+                                        const float x = __fmul_rn(dm, dl[i]);
+                                        const float y = rn ? __fadd_rn(x, 8388608.0f) : __fadd_rz(x, 8388608.0f);
+                                        const uint32_t d = __float_as_uint(y) - 0x4B000000u;
+                                        const uint2 v = d <= dmax ? s_table[d]
+                                                                  : phasor_direct(k, (int)d, nfft, pow2n, a.nmagic,
+                                                                                  s_tw_lo, s_tw_hi);
+                                        hi[4 * q + i] = v.x;
+                                        lo[4 * q + i] = v.y;
+                                    }
                                 }
                             }
                         } else if (direct) {
 #pragma unroll
                             for (int i = 0; i < TC_PART_CH; ++i) {
                                 const int d = tc_delay(dm, s_delay[c0 + i], a.round_delays);
-                                uint32_t idx;
-                                if (pow2n) {
-                                    idx = ((uint32_t)k * (uint32_t)d) & nmask;
-                                } else {
-                                    // (k d) mod N by Barrett reduction, d taken mod N first
-                                    const uint32_t dn = d >= 0 ? (uint32_t)d % nfft
-                                                               : nfft - 1u - (uint32_t)(-(d + 1)) % nfft;
-                                    const uint64_t p = (uint64_t)k * dn;
-                                    uint64_t r = p - __umul64hi(p, a.nmagic) * (uint64_t)nfft;
-                                    while (r >= nfft) r -= nfft;
-                                    idx = (uint32_t)r;
-                                }
-                                // exp(+2 pi i idx / N) = conj(tw_hi[idx >> 8] * tw_lo[idx & 255])
-                                const float2 h = s_tw_hi[idx >> 8], l = s_tw_lo[idx & 255u];
-                                const float c = __fsub_rn(__fmul_rn(h.x, l.x), __fmul_rn(h.y, l.y));
-                                const float sn = -__fadd_rn(__fmul_rn(h.x, l.y), __fmul_rn(h.y, l.x));
-                                const uint2 v = split_bf16x2(c, sn);
+                                const uint2 v = phasor_direct(k, d, nfft, pow2n, a.nmagic, s_tw_lo, s_tw_hi);
                                 hi[i] = v.x;
                                 lo[i] = v.y;
                             }
@@ -799,24 +829,86 @@ std::vector<uint2> tc_quarter_table(unsigned nfft)
     return t;
 }
 
-size_t tc_smem_bytes(unsigned nfft, int nact_pad, int npad, int dmax, int stages, bool direct)
+// Dynamic shared memory of fdd_mac_tc_kernel: base alignment, the B stages
+// (three-MMA form, the larger), barriers, the phasor table and the two
+// twiddle tables (float2 tables padded to even counts, 16-byte aligned), the
+// channel delays and the abort flag.
+size_t tc_layout_bytes(int npad, size_t table_entries, size_t hi_entries, int nact_pad, int stages)
 {
-    // the layout of fdd_mac_tc_kernel (tc_layout) for one descriptor:
-    // table mode: dmax + 1 phasors and the twiddle tables; direct mode: the
-    // twiddle tables; quarter-wave mode: nfft/4 + 1 phasors
-    const size_t stage = 4ull * (size_t)npad * 128ull;  // the larger (three-MMA) stage
-    const size_t table = dmax >= 0 ? (size_t)dmax + 1 : direct ? 0 : (size_t)nfft / 4 + 1;
-    const size_t hi = (dmax >= 0 || direct) ? (size_t)nfft / 256 : 0;
-    const size_t need = 1024 /* base alignment */ + (size_t)stages * stage + 256 +
-                        (((table + 1) & ~(size_t)1) + 256 + ((hi + 1) & ~(size_t)1)) * 8 +
+    const size_t stage = 4ull * (size_t)npad * 128ull;
+    const size_t need = 1024 + (size_t)stages * stage + 256 +
+                        (((table_entries + 1) & ~(size_t)1) + 256 + ((hi_entries + 1) & ~(size_t)1)) * 8 +
                         (size_t)nact_pad * 4 + 4 * 8;
     return std::max(need, TC_MIN_SMEM);
+}
+
+size_t tc_smem_bytes(unsigned nfft, int nact_pad, int npad, int dmax, int stages, bool direct)
+{
+    // one descriptor: table mode: dmax + 1 phasors and the twiddle tables;
+    // direct mode: the twiddle tables; quarter-wave mode: nfft/4 + 1 phasors
+    const size_t table = dmax >= 0 ? (size_t)dmax + 1 : direct ? 0 : (size_t)nfft / 4 + 1;
+    const size_t hi = (dmax >= 0 || direct) ? (size_t)nfft / 256 : 0;
+    return tc_layout_bytes(npad, table, hi, nact_pad, stages);
 }
 
 int tc_table_mode_dmax(int dmax, unsigned nfft, int nact_pad, int npad)
 {
     if (dmax < 0) return -1;
     return tc_smem_bytes(nfft, nact_pad, npad, dmax, 2, false) <= TC_MAX_SMEM ? dmax : -1;
+}
+
+int tc_table_capacity(int npad, size_t hi_entries, int nact_pad)
+{
+    // largest entry count t (= cap + 1) whose layout fits: bytes grow with t
+    size_t lo = 0, hi = TC_MAX_SMEM / 8;
+    if (tc_layout_bytes(npad, 1, hi_entries, nact_pad, 2) > TC_MAX_SMEM) return -1;
+    lo = 1;
+    while (lo < hi) {
+        const size_t mid = (lo + hi + 1) / 2;
+        if (tc_layout_bytes(npad, mid, hi_entries, nact_pad, 2) <= TC_MAX_SMEM) lo = mid;
+        else hi = mid - 1;
+    }
+    return (int)lo - 1;
+}
+
+int tc_table_cap_limit()
+{
+    const char* v = std::getenv("DEDISP_TC_TABLE_CAP");
+    if (!v || !*v) return INT_MAX;
+    const long x = std::strtol(v, nullptr, 10);
+    return x < 0 ? -1 : (int)std::min<long>(x, INT_MAX);
+}
+
+TcSource tc_choose_source(int dmax, unsigned nfft, int table_cap, bool quarter_fits)
+{
+    TcSource s;
+    if (dmax >= 0 && dmax <= table_cap) {
+        s.dmax = dmax;  // every delay from the per-bin table
+        return s;
+    }
+    const bool twiddles = nfft % 256 == 0 && table_cap >= 0;  // room for the twiddle tables
+    // relative cost per phasor: table gather 1, quarter-wave gather 1.3,
+    // direct 2.5 (a reduction, two twiddle loads, a complex product)
+    double best = 1e30;
+    if (quarter_fits) best = 1.3;
+    if (twiddles && dmax >= 0 && dmax < (1 << 22) && table_cap >= 1024) {
+        // share of (DM, channel) delays inside the table when both the DMs and
+        // the channel delays spread evenly from zero: c (1 - ln c)
+        const double c = (double)(table_cap + 1) / (double)(dmax + 1);
+        const double cov = c * (1.0 - std::log(c));
+        const double cost = cov + 2.5 * (1.0 - cov);
+        if (cost < best) {
+            best = cost;
+            s.dmax = table_cap;
+            s.hybrid = 1;
+        }
+    }
+    if (best > 2.5 && twiddles) {
+        s.direct = 1;
+        best = 2.5;
+    }
+    if (best > 2.5) s.dmax = -2;  // no source fits
+    return s;
 }
 
 int tc_stages(unsigned nfft, int nact_pad, int npad, int dmax, bool direct)
@@ -888,10 +980,9 @@ TcLayout tc_layout(const std::vector<TcMacArgs>& descs, unsigned* err)
     L.table_entries = (uint32_t)((table + 1) & ~(size_t)1);  // keep the float2 tables 16-byte aligned
     L.tw_hi_entries = (uint32_t)((hi + 1) & ~(size_t)1);
     L.nact_pad = descs[0].nact_pad;
+    // the fused form's stages are half as large: the same formula at npad / 2
     auto bytes = [&](int st) {
-        return std::max(TC_MIN_SMEM, (size_t)1024 + (size_t)st * L.stage_bytes + 256 +
-                                         ((size_t)L.table_entries + 256 + L.tw_hi_entries) * 8 +
-                                         (size_t)L.nact_pad * 4 + 4 * 8);
+        return tc_layout_bytes((int)(L.stage_bytes / 512u), L.table_entries, L.tw_hi_entries, L.nact_pad, st);
     };
     int st = TC_MAX_STAGES;
     while (st > 2 && bytes(st) > TC_MAX_SMEM) --st;
@@ -928,7 +1019,7 @@ std::vector<TcWork> tc_work_items(const std::vector<TcMacArgs>& descs, int ctas)
     // positions b, b + ctas, b + 2 ctas, ... (empty items fill the gaps).
     auto cost_per_bin = [](const TcMacArgs& a) {
         const double ntiles = (double)((a.ndm + TC_M - 1) / TC_M);
-        const double phasor = a.dmax >= 0 ? 1.0 : a.direct ? 2.5 : 1.3;
+        const double phasor = a.dmax >= 0 ? (a.hybrid ? 1.8 : 1.0) : a.direct ? 2.5 : 1.3;
         return ntiles * (double)(a.nact_pad / TC_CHUNK) * (phasor + (double)a.npad / 48.0);
     };
     double total = 0;

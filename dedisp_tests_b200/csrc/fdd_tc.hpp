@@ -37,6 +37,7 @@ struct TcMacArgs {
     int round_delays;
     int dmax;                  // >= 0: delay-table mode, every delay in 0..dmax; -1: quarter-wave mode
     int direct = 0;            // dmax < 0: 1 phasors from the two-level twiddles, 0 quarter-wave table
+    int hybrid = 0;            // dmax >= 0: 1 the table covers 0..dmax only, larger delays computed
     unsigned long long nmagic = 0;  // set by the launcher
 };
 
@@ -70,6 +71,8 @@ struct TcLayout {
 // Parameters of a MAC launch: descriptors and their tensor maps (kernel
 // parameter bank), work items (device memory).
 constexpr int kTcMaxDesc = 48;
+// Dynamic shared memory a MAC launch may use (the opt-in maximum per block).
+constexpr size_t kTcMaxSmem = 227 * 1024;
 struct alignas(64) TcParams {
     CUtensorMap maps[kTcMaxDesc];
     TcMacArgs descs[kTcMaxDesc];
@@ -100,6 +103,28 @@ bool tc_direct_mode_fits(unsigned nfft, int nact_pad, int npad);
 // dmax if the per-bin delay table (dmax + 1 phasors) fits shared memory,
 // else -1 (the kernel then indexes the quarter-wave table per phasor).
 int tc_table_mode_dmax(int dmax, unsigned nfft, int nact_pad, int npad);
+// Shared-memory bytes of a launch whose layout holds `table_entries` phasors
+// and `hi_entries` coarse twiddles (tc_layout's formula).
+size_t tc_layout_bytes(int npad, size_t table_entries, size_t hi_entries, int nact_pad, int stages);
+// Largest per-bin table extent (delays 0..cap) a layout with `hi_entries`
+// coarse twiddles leaves room for; -1 if none.
+int tc_table_capacity(int npad, size_t hi_entries, int nact_pad);
+
+// Phasor source of one descriptor: dmax >= 0 the per-bin table over 0..dmax
+// (hybrid: larger delays computed directly); dmax == -1 the quarter-wave
+// table (direct = 0) or the twiddle tables (direct = 1); dmax == -2 none fits.
+struct TcSource {
+    int dmax = -1;
+    int direct = 0;
+    int hybrid = 0;
+};
+// Upper limit on the table extent from the environment (DEDISP_TC_TABLE_CAP,
+// to compare the phasor sources on one shape); INT_MAX when unset.
+int tc_table_cap_limit();
+// Cheapest source for a largest delay `dmax` (-1: unknown or too large) when
+// the layout leaves room for a table over 0..table_cap (-1: none) and, with
+// quarter_fits, for the quarter-wave table.
+TcSource tc_choose_source(int dmax, unsigned nfft, int table_cap, bool quarter_fits);
 std::vector<uint2> tc_quarter_table(unsigned nfft);
 
 // X [nchans*nseg][bin_pitch] complex spectra -> B operand

@@ -27,6 +27,10 @@ struct ExecTiming {
      * forward FFT, operand layout (B split or bin-major), MAC, DM-major
      * transpose or spectrum output, inverse FFT (0 when a stage did not run) */
     float stage_ms[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    /* FDD plans, tensor-core MAC: phasor source of the last execute (0 the
+     * per-bin delay table, 1 the quarter-wave table, 2 the table for small
+     * delays with the rest computed, 3 computed from twiddle tables); -1 none */
+    int phasor = -1;
 };
 
 class GPUPlan : public Plan {

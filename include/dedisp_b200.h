@@ -53,6 +53,14 @@ dedisp_error dedisp_b200_get_timing(dedisp_plan plan, float* kernel_ms, float* p
  * Writes `count` values (at most 6 meaningful; the rest 0). */
 dedisp_error dedisp_b200_get_stage_times(dedisp_plan plan, float* stage_ms, int count);
 
+/* FDD plans: phasor source of the tensor-core MAC in the last execute: 0 the
+ * per-bin delay table (every delay), 1 the quarter-wave table, 2 the per-bin
+ * table for the small delays and the rest computed from the twiddle tables,
+ * 3 every phasor from the twiddle tables; -1 no tensor-core MAC ran. The
+ * environment variable DEDISP_TC_TABLE_CAP caps the per-bin table's extent
+ * (to compare the sources on one shape). */
+dedisp_error dedisp_b200_get_phasor_source(dedisp_plan plan, int* source);
+
 /* The C functions of dedisp.h report every failure inside the plan classes
  * as DEDISP_UNKNOWN_ERROR, like the reference (src/clib/dedisp.cpp:520-523).
  * This returns the specific code of the most recent such failure in the
@@ -220,6 +228,9 @@ dedisp_error dedisp_b200_fdd_batch_set_timing(dedisp_b200_fdd_batch batch, int e
 dedisp_error dedisp_b200_fdd_batch_get_timing(dedisp_b200_fdd_batch batch, float* prep_ms, float* mac_ms,
                                               float* post_ms, int* launches);
 dedisp_size dedisp_b200_fdd_batch_max_delay(dedisp_b200_fdd_batch batch, dedisp_size beam);
+/* Phasor source of a beam's tensor-core MAC as planned for the current beam
+ * set (codes of dedisp_b200_get_phasor_source); -1 on error or no MAC work. */
+int dedisp_b200_fdd_batch_phasor_source(dedisp_b200_fdd_batch batch, dedisp_size beam);
 
 /* ------------------------------------------------------------------------
  * Streaming server. No counterpart in the reference. Beams deliver host

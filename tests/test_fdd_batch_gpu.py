@@ -41,7 +41,7 @@ def _beam_inputs(nbits, seed, specs):
     return out
 
 
-def _run_batch(nbits, host, km=None, graph=True, reps=2):
+def _run_batch(nbits, host, km=None, graph=True, reps=2, sources=None):
     import torch
     b = dd.FddBatch(*PARAMS, in_nbits=nbits)
     if km is not None:
@@ -56,6 +56,8 @@ def _run_batch(nbits, host, km=None, graph=True, reps=2):
         beams.append((x, packed.shape[1], packed.shape[0], dms, y, y.shape[1] * 4))
         outs.append((y, nout))
     b.set_beams(beams)
+    if sources is not None:
+        sources.extend(b.phasor_source(i) for i in range(len(beams)))
     stream = torch.cuda.current_stream().cuda_stream
     for _ in range(reps):
         for y, _ in outs:
@@ -140,3 +142,25 @@ def test_fdd_batch_other_widths_and_killmask(nbits):
         ref = _oracle(packed, nbits, dms, km)
         rel, mx = _errs(g, ref)
         assert rel < TOL[0] and mx < TOL[1], (nbits, i, rel, mx)
+
+
+def test_fdd_batch_hybrid_phasors(monkeypatch):
+    """Every beam's per-bin table capped at delays 0..1024 (the larger delays
+    computed from the twiddle tables): the same outputs as the lone plans
+    and the FP64 oracle."""
+    monkeypatch.setenv("DEDISP_TC_TABLE_CAP", "1024")
+    specs = [(123457, np.linspace(0, 3000, 300)), (60000, np.linspace(0, 700, 140))]
+    host = _beam_inputs(8, 23, specs)
+    sources = []
+    got = _run_batch(8, host, sources=sources)
+    monkeypatch.delenv("DEDISP_TC_TABLE_CAP")
+    # 65536-point segments (max delay ~8400): the quarter-wave table costs
+    # less than 12 % table coverage; max delay ~1960: the hybrid source
+    assert sources == ["quarter", "hybrid"], sources
+    for i, ((packed, dms), g) in enumerate(zip(host, got)):
+        want = _plan_out(packed, 8, dms)
+        rel, mx = _errs(g, want)
+        assert rel < TOL[0] and mx < TOL[1], ("vs plan", i, rel, mx)
+        ref = _oracle(packed, 8, dms)
+        rel, mx = _errs(g, ref)
+        assert rel < TOL[0] and mx < TOL[1], ("vs FP64", i, rel, mx)

@@ -146,3 +146,45 @@ def test_tc_selectable_mma_forms(form, monkeypatch):
     ref = po.fdd_timeseries(x, _delays(params), np.ones(nchans, np.int32), dms, nout)
     rel, mx = _errs(out, ref)
     assert rel < TC_REL_L2 and mx < TC_MAX_ABS, (form, rel, mx)
+
+
+@pytest.mark.parametrize("cap,source", [(None, "table"), ("1024", "hybrid"), ("0", "direct")])
+def test_tc_phasor_sources(cap, source, monkeypatch):
+    """The three phasor sources of a non-power-of-two transform (whole series,
+    N = 16384 x 3), chosen through the table-extent cap DEDISP_TC_TABLE_CAP:
+    the per-bin table over every delay (max delay ~2700), the table over
+    delays 0..1024 with the larger ones computed from the twiddle tables, and
+    every phasor computed. Same tolerance against FP64."""
+    if cap is None:
+        monkeypatch.delenv("DEDISP_TC_TABLE_CAP", raising=False)
+    else:
+        monkeypatch.setenv("DEDISP_TC_TABLE_CAP", cap)
+    nchans, nsamps = 64, 40000
+    inp, params = _input(nchans, nsamps, 12)
+    dms = np.linspace(0, 3300, 40, dtype=np.float32)
+    p = _plan(params, dms, segmented=0, precision=1)
+    assert p.get_max_delay() > 2000
+    out = _run(p, nsamps, inp, 8, len(dms))
+    assert p.get_phasor_source() == source
+    x = _oracle_x(inp, nsamps, params, 8)
+    ref = po.fdd_spectrum(x, _delays(params), np.ones(nchans, np.int32), dms, out.shape[1])
+    rel, mx = _errs(out, ref)
+    print("tc phasor source", source, rel, mx)
+    assert rel < TC_REL_L2 and mx < TC_MAX_ABS, (source, rel, mx)
+
+
+def test_tc_quarter_wave_for_power_of_two_when_table_capped(monkeypatch):
+    """Power-of-two segments with the table capped at 0: the quarter-wave
+    table (cheaper than computing every phasor) serves the MAC."""
+    monkeypatch.setenv("DEDISP_TC_TABLE_CAP", "0")
+    nchans, nsamps = 96, 90000
+    inp, params = _input(nchans, nsamps, 3)
+    dms = np.linspace(0, 120, 200, dtype=np.float32)
+    p = _plan(params, dms, segmented=1, precision=1)
+    nout = nsamps - p.get_max_delay()
+    out = _run(p, nsamps, inp, 8, len(dms))
+    assert p.get_phasor_source() == "quarter"
+    x = _oracle_x(inp, nsamps, params, 8)
+    ref = po.fdd_timeseries(x, _delays(params), np.ones(nchans, np.int32), dms, nout)
+    rel, mx = _errs(out, ref)
+    assert rel < TC_REL_L2 and mx < TC_MAX_ABS, (rel, mx)
