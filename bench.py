@@ -677,14 +677,18 @@ def run_batched_fdd(args, local, world, stream, max_over_ranks, nbeams=12, nplai
     res["batched_bf16x3_tc"]["error_sample"] = f"beam {bi}, DMs {drows.tolist()} x first {nchk} samples"
     # stage split of one more step (direct launches with events, untimed above)
     split = {"prep_ms": 0.0, "mac_ms": 0.0, "post_ms": 0.0}
+    balance = []
     for b in batches:
         b.set_timing(True)
         b.execute(stream.cuda_stream, use_graph=False)
         t = b.get_timing()
+        bal = b.get_mac_balance()
         b.set_timing(False)
         for k in split:
             split[k] += t[k]
+        balance.append([round(bal["cta_max_ms"], 1), round(bal["cta_mean_ms"], 1)])
     res["batched_bf16x3_tc"]["stage_ms"] = {k: round(v, 2) for k, v in split.items()}
+    res["batched_bf16x3_tc"]["mac_cta_max_mean_ms"] = balance
     res["batched_bf16x3_tc"]["phasor_sources"] = bsources
     for b in batches:
         b.close()

@@ -380,6 +380,7 @@ _BATCH_SIGS = {
                                                    C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "dedisp_b200_fdd_batch_max_delay": (_sz, [_vp, _sz]),
     "dedisp_b200_fdd_batch_phasor_source": (C.c_int, [_vp, _sz]),
+    "dedisp_b200_fdd_batch_get_mac_balance": (C.c_int, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
 }
 
 
@@ -552,6 +553,13 @@ class FddBatch:
         _bcheck(_batch_lib().dedisp_b200_fdd_batch_get_timing(self._h, C.byref(p), C.byref(m),
                                                               C.byref(q), C.byref(n)))
         return {"prep_ms": p.value, "mac_ms": m.value, "post_ms": q.value, "launches": n.value}
+
+    def get_mac_balance(self) -> dict:
+        """After a direct execute with timing on: largest and mean per-CTA
+        busy time of the MAC launch (ms)."""
+        a, b = C.c_float(), C.c_float()
+        _bcheck(_batch_lib().dedisp_b200_fdd_batch_get_mac_balance(self._h, C.byref(a), C.byref(b)))
+        return {"cta_max_ms": a.value, "cta_mean_ms": b.value}
 
     def max_delay(self, beam: int) -> int:
         return int(_batch_lib().dedisp_b200_fdd_batch_max_delay(self._h, beam))

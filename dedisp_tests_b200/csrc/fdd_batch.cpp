@@ -362,7 +362,10 @@ void FddBatch::enqueue(cudaStream_t s, bool timing)
     }
     if (timing) m_ev[1]->record(s);
     if (m_nact > 0 && m_params && m_params->nitems > 0) {
+        if (timing) m_cta_ns.reserve((size_t)kern::tc_sm_count() * sizeof(unsigned long long));
+        m_params->cta_ns = timing ? m_cta_ns.get<unsigned long long>() : nullptr;
         kern::launch_fdd_mac_tc_list(*m_params, s);
+        m_params->cta_ns = nullptr;
         ++launches;
     }
     if (timing) m_ev[2]->record(s);
@@ -433,6 +436,19 @@ void FddBatch::execute(cudaStream_t stream, bool use_graph)
             RT_CHECK(cudaEventElapsedTime(&last_prep_ms, m_ev[0]->get(), m_ev[1]->get()));
             RT_CHECK(cudaEventElapsedTime(&last_mac_ms, m_ev[1]->get(), m_ev[2]->get()));
             RT_CHECK(cudaEventElapsedTime(&last_post_ms, m_ev[2]->get(), m_ev[3]->get()));
+            last_cta_max_ms = last_cta_mean_ms = 0.f;
+            if (m_nact > 0 && m_params && m_params->nitems > 0) {
+                const int n = std::min(m_params->nitems, kern::tc_sm_count());
+                std::vector<unsigned long long> ns((size_t)n);
+                RT_CHECK(cudaMemcpy(ns.data(), m_cta_ns.get(), ns.size() * sizeof(ns[0]), cudaMemcpyDeviceToHost));
+                double sum = 0, mx = 0;
+                for (unsigned long long v : ns) {
+                    sum += (double)v;
+                    mx = std::max(mx, (double)v);
+                }
+                last_cta_max_ms = (float)(mx * 1e-6);
+                last_cta_mean_ms = (float)(sum / n * 1e-6);
+            }
         }
     }
 }
@@ -581,6 +597,15 @@ dedisp_error dedisp_b200_fdd_batch_get_timing(dedisp_b200_fdd_batch batch, float
         if (mac_ms) *mac_ms = b.last_mac_ms;
         if (post_ms) *post_ms = b.last_post_ms;
         if (launches) *launches = b.last_launches;
+    });
+}
+
+dedisp_error dedisp_b200_fdd_batch_get_mac_balance(dedisp_b200_fdd_batch batch, float* cta_max_ms,
+                                                   float* cta_mean_ms)
+{
+    return fdd_batch_call(batch, [&](dedisp::detail::FddBatch& b) {
+        if (cta_max_ms) *cta_max_ms = b.last_cta_max_ms;
+        if (cta_mean_ms) *cta_mean_ms = b.last_cta_mean_ms;
     });
 }
 

@@ -71,6 +71,9 @@ public:
     bool record_timing = false;
     float last_prep_ms = 0.f, last_mac_ms = 0.f, last_post_ms = 0.f;
     int last_launches = 0;
+    // Direct (non-graph) executes with timing on: the MAC's CTAs' busy times,
+    // largest and mean (ms), to show how evenly the work list spreads.
+    float last_cta_max_ms = 0.f, last_cta_mean_ms = 0.f;
 
 private:
     struct Beam;
@@ -90,7 +93,7 @@ private:
     int m_nact = 0, m_nact_pad = 0;
     size_t m_ws_bytes = 0, m_shared_bytes = 0, m_scratch_off = 0, m_scratch_bytes = 0;
 
-    rt::DeviceBuffer m_chan, m_kmv, m_delay_pad, m_err, m_items, m_twp_lo, m_twp_hi;
+    rt::DeviceBuffer m_chan, m_kmv, m_delay_pad, m_err, m_items, m_twp_lo, m_twp_hi, m_cta_ns;
     rt::DeviceBuffer m_own_ws;
     void* m_ext_ws = nullptr;
     size_t m_ext_ws_bytes = 0;

@@ -93,6 +93,9 @@ struct alignas(8) SmemBarriers {
     uint64_t c_empty[2];
     uint64_t drain;
     uint64_t never;       // expiry test: nothing arrives on it
+    uint64_t item_full[2];   // item index published (TMA thread)
+    uint64_t item_empty[2];  // item index read (producer warps + MMA thread)
+    int item[2];             // two-slot ring of this CTA's next item indices (-1: none left)
     uint32_t tmem_base;
     uint32_t abort_flag;  // a producer gave up a bounded wait (delay-table mode)
 };
@@ -350,6 +353,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
         }
         mbar_init(&bars->drain, 1);
         mbar_init(&bars->never, 1);
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&bars->item_full[i], 1);
+            mbar_init(&bars->item_empty[i], TC_PRODUCER_WARPS + 1);
+        }
         bars->abort_flag = 0u;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -363,6 +370,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
     tc_fence_after();
     const uint32_t tmem = bars->tmem_base;
     bool ok = true;
+    const uint64_t t_start = (P.cta_ns && tid == 0) ? global_ns() : 0;
 
     if (warp < TC_PRODUCER_WARPS) {
         // --- phasor producers + epilogue ------------------------------------
@@ -379,9 +387,28 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
         uint32_t g = 0;    // chunk counter (A buffers)
         int bin_iter = 0;  // bin counter (accumulators)
         int cur_desc = -1; // descriptor whose tables are in shared memory
-        for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-            asm volatile("bar.sync 1, %0;" ::"n"(TC_PRODUCER_WARPS * 32) : "memory");
-            if (*abort_flag) { ok = false; break; }
+        for (uint32_t j = 0;; ++j) {
+            // item j of this CTA, as the TMA thread published it; one outcome
+            // for all producers (the named barrier's OR of "gave up the wait
+            // or an abort was raised"), which also orders the table reloads
+            // below after every producer's reads of the previous item
+            const uint32_t slot = j & 1u;
+            const bool got = mbar_wait(&bars->item_full[slot], (j >> 1) & 1u, L.wait_ns);
+            const int it = got ? *reinterpret_cast<volatile int*>(&bars->item[slot]) : -1;
+            const uint32_t bad = (!got || *abort_flag) ? 1u : 0u;
+            uint32_t fail;
+            asm volatile(
+                "{\n\t.reg .pred p, q;\n\t"
+                "setp.ne.u32 p, %1, 0;\n\t"
+                "bar.red.or.pred q, 1, %2, p;\n\t"
+                "selp.u32 %0, 1, 0, q;\n\t}"
+                : "=r"(fail)
+                : "r"(bad), "n"(TC_PRODUCER_WARPS * 32)
+                : "memory");
+            if (fail) { ok = false; break; }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bars->item_empty[slot]);
+            if (it < 0) break;
             const TcWork w = items[it];
             const TcMacArgs& a = descs[w.desc];  // read-only descriptor (L1)
             const uint32_t nfft = a.nfft, qn = nfft / 4;
@@ -596,7 +623,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
         // --- TMA producer ------------------------------------------------------
         if (lane == 0) {
             uint32_t g = 0;
-            for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+            // this CTA's items: blockIdx.x first, then the next unclaimed item
+            // of the list (longest first) each time one is done, published to
+            // the other roles through the two-slot ring
+            for (uint32_t j = 0; ok; ++j) {
+                const uint32_t slot = j & 1u;
+                int it = j == 0 ? (int)blockIdx.x : (int)gridDim.x + (int)atomicAdd(P.next_item, 1u);
+                if (it >= nitems) it = -1;
+                if (!mbar_wait(&bars->item_empty[slot], ((j >> 1) & 1u) ^ 1u, L.wait_ns)) { ok = false; break; }
+                bars->item[slot] = it;
+                mbar_arrive(&bars->item_full[slot]);
+                if (it < 0) break;
                 const TcWork w = items[it];
                 const CUtensorMap* bmap = maps + w.desc;
                 const uint32_t atom_bytes = (uint32_t)descs[w.desc].npad * 128u;  // one 64-kk atom of one split
@@ -626,7 +663,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
         if (lane == 0) {
             uint32_t g = 0;
             int bin_iter = 0;
-            for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+            for (uint32_t j = 0; ok; ++j) {
+                const uint32_t slot = j & 1u;
+                if (!mbar_wait(&bars->item_full[slot], (j >> 1) & 1u, L.wait_ns)) { ok = false; break; }
+                const int it = *reinterpret_cast<volatile int*>(&bars->item[slot]);
+                mbar_arrive(&bars->item_empty[slot]);
+                if (it < 0) break;
                 const TcWork w = items[it];
                 const uint32_t npad = (uint32_t)descs[w.desc].npad;
                 const uint32_t atom_bytes = npad * 128u;
@@ -682,6 +724,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
+    if (P.cta_ns && tid == 0) P.cta_ns[blockIdx.x] = global_ns() - t_start;
     if (warp == TC_PRODUCER_WARPS + 1) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
     }
@@ -1013,10 +1056,11 @@ std::vector<TcWork> tc_work_items(const std::vector<TcMacArgs>& descs, int ctas)
         }
         return items;
     }
-    // Several descriptors (a batch of beams): about 4 items per CTA, sized by
-    // an estimated cost per bin (tiles x chunks x (phasor source + columns)),
-    // assigned longest first to the least loaded CTA; CTA b runs the items at
-    // positions b, b + ctas, b + 2 ctas, ... (empty items fill the gaps).
+    // Several descriptors (a batch of beams): items of about 1/32 of a CTA's
+    // share of an estimated cost per bin (tiles x chunks x (phasor source +
+    // columns)), listed longest first. CTA b starts with item b and then
+    // claims the next unclaimed item whenever it finishes one, so the
+    // estimate only orders the list and the tail is at most one small item.
     auto cost_per_bin = [](const TcMacArgs& a) {
         const double ntiles = (double)((a.ndm + TC_M - 1) / TC_M);
         const double phasor = a.dmax >= 0 ? (a.hybrid ? 1.8 : 1.0) : a.direct ? 2.5 : 1.3;
@@ -1024,7 +1068,9 @@ std::vector<TcWork> tc_work_items(const std::vector<TcMacArgs>& descs, int ctas)
     };
     double total = 0;
     for (const TcMacArgs& a : descs) total += cost_per_bin(a) * (double)a.nbins;
-    const double per = std::max(1e-9, total / (4.0 * ctas));
+    // (8 items per CTA left 10 % of tail on the first 12 config-3 beams, 32 and
+    // 64 under 2 %)
+    const double per = std::max(1e-9, total / (32.0 * ctas));
     std::vector<std::pair<double, TcWork>> parts;
     for (size_t d = 0; d < descs.size(); ++d) {
         const TcMacArgs& a = descs[d];
@@ -1036,20 +1082,8 @@ std::vector<TcWork> tc_work_items(const std::vector<TcMacArgs>& descs, int ctas)
             if (k0 < k1) parts.push_back({cb * (double)(k1 - k0), TcWork{(int)d, 0, ntiles, (unsigned)k0, (unsigned)k1}});
         }
     }
-    std::sort(parts.begin(), parts.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
-    std::vector<double> load((size_t)ctas, 0.0);
-    std::vector<std::vector<TcWork>> per_cta((size_t)ctas);
-    for (const auto& pw : parts) {
-        const size_t b = (size_t)(std::min_element(load.begin(), load.end()) - load.begin());
-        load[b] += pw.first;
-        per_cta[b].push_back(pw.second);
-    }
-    size_t depth = 0;
-    for (const auto& l : per_cta) depth = std::max(depth, l.size());
-    const TcWork empty{0, 0, 1, 0u, 0u};
-    items.assign(depth * (size_t)ctas, empty);
-    for (size_t b = 0; b < (size_t)ctas; ++b)
-        for (size_t j = 0; j < per_cta[b].size(); ++j) items[j * (size_t)ctas + b] = per_cta[b][j];
+    std::stable_sort(parts.begin(), parts.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+    for (const auto& pw : parts) items.push_back(pw.second);
     return items;
 }
 
@@ -1087,6 +1121,8 @@ void tc_prepare_list(TcParams& P, const std::vector<TcMacArgs>& descs_in, const 
         RT_CHECK(cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(TcWork), cudaMemcpyHostToDevice, s));
     P.items = static_cast<const TcWork*>(d_items);
     P.nitems = (int)items.size();
+    P.next_item = reinterpret_cast<unsigned*>(static_cast<uint8_t*>(d_items) +
+                                              (items.size() * sizeof(TcWork) + 15) / 16 * 16);
     P.layout = tc_layout(descs, err);
 }
 
@@ -1098,6 +1134,7 @@ void launch_fdd_mac_tc_list(const TcParams& P, cudaStream_t s)
                                 : fdd_mac_tc_kernel<false, false>;
     rt::raise_smem_limit(kern, P.layout.smem_bytes);
     const int grid = std::min(P.nitems, tc_sm_count());
+    RT_CHECK(cudaMemsetAsync(P.next_item, 0, sizeof(unsigned), s));
     kern<<<grid, TC_THREADS, P.layout.smem_bytes, s>>>(P);
     RT_CHECK(cudaGetLastError());
 }

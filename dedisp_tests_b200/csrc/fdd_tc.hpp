@@ -80,6 +80,12 @@ struct alignas(64) TcParams {
     const TcWork* items;
     int nitems;
     TcLayout layout;
+    // optional: each CTA's busy time (ns, from after its set-up to its end),
+    // one entry per CTA of the launch
+    unsigned long long* cta_ns = nullptr;
+    // items claimed beyond the first one per CTA (device, zeroed before each
+    // launch; it follows the items in their buffer)
+    unsigned* next_item = nullptr;
 };
 
 // One launch covers at most kTcMaxSeg segments (2 x segments <= 128
@@ -141,10 +147,11 @@ void launch_fdd_mac_tc(const TcMacArgs& a, const void* B, void* d_items, size_t 
 
 // Up to kTcMaxDesc descriptors in one persistent launch: work items over all
 // of them (tc_work_items: one descriptor, at most `ctas` equal bin ranges;
-// several, about 4 per CTA assigned longest first, laid out for a grid of
-// exactly `ctas` CTAs, CTA b taking positions b, b + ctas, ...), tensor maps encoded (B
-// operand per descriptor) into P, items copied to d_items; then launched
-// (possibly later, or inside a graph: P is copied into the launch).
+// several, about 32 per CTA listed longest first; CTA b of the launch runs
+// item b, then claims the next unclaimed one each time it finishes one),
+// tensor maps encoded (B operand per descriptor) into P, items copied to
+// d_items; then launched (possibly later, or inside a graph: P is copied into
+// the launch, the claim counter is reset by a memset before it).
 size_t tc_work_bytes(size_t nitems);
 std::vector<TcWork> tc_work_items(const std::vector<TcMacArgs>& descs, int ctas);
 void tc_prepare_list(TcParams& P, const std::vector<TcMacArgs>& descs, const std::vector<const void*>& Bs,

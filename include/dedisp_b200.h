@@ -228,6 +228,11 @@ dedisp_error dedisp_b200_fdd_batch_set_timing(dedisp_b200_fdd_batch batch, int e
 dedisp_error dedisp_b200_fdd_batch_get_timing(dedisp_b200_fdd_batch batch, float* prep_ms, float* mac_ms,
                                               float* post_ms, int* launches);
 dedisp_size dedisp_b200_fdd_batch_max_delay(dedisp_b200_fdd_batch batch, dedisp_size beam);
+/* After a direct (use_graph = 0) execute with timing on: the MAC launch's
+ * largest and mean per-CTA busy time (ms); their ratio shows how evenly the
+ * work list spread over the SMs. 0 when not measured. */
+dedisp_error dedisp_b200_fdd_batch_get_mac_balance(dedisp_b200_fdd_batch batch, float* cta_max_ms,
+                                                   float* cta_mean_ms);
 /* Phasor source of a beam's tensor-core MAC as planned for the current beam
  * set (codes of dedisp_b200_get_phasor_source); -1 on error or no MAC work. */
 int dedisp_b200_fdd_batch_phasor_source(dedisp_b200_fdd_batch batch, dedisp_size beam);
