@@ -577,11 +577,13 @@ def run_batched(args, local, world, stream, max_over_ranks):
 def run_batched_fdd(args, local, world, stream, max_over_ranks, nbeams=12, nplain=4):
     """Config 3, Fourier domain: the first `nbeams` of the 96 seeded beams
     (1536 ch, 8-bit, nsamp U[2^17, 2^20], DM max U[500, 3000], 1024-4096
-    linear trials), segmented time series with the reference segment rule.
-    Batched: FddBatch objects in waves sized to the free memory, each one
-    replayed CUDA graph with ONE persistent tensor-core MAC launch over all
-    its beams. Compared with one FDD plan execute per beam on the same beams:
-    tensor-core plans, and plain FP32 plans on the first `nplain`."""
+    linear trials), segmented time series. Batched: FddBatch objects in waves
+    sized to the free memory, each one replayed CUDA graph with ONE persistent
+    tensor-core MAC launch over all its beams. Compared with one FDD plan
+    execute per beam on the same beams: tensor-core plans, and plain FP32
+    plans on the first `nplain`. Both tensor-core forms run with the reference
+    segment rule and with the automatic one (the segment length with the least
+    modelled device time; the same series, other rounding)."""
     import torch
     import dedisp_tests_b200 as dd
     from dedisp_tests_b200 import synthetic as sy
@@ -599,112 +601,112 @@ def run_batched_fdd(args, local, world, stream, max_over_ranks, nbeams=12, nplai
     out_bytes = [u * 4 for u in units]
     d_in = [sy.make_input_torch(c, device=dev) for c in beams]
     torch.cuda.synchronize()
-    free, _ = torch.cuda.mem_get_info(local)
-    budget = free - 8e9
+    total = float(sum(units))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
 
     def spec(i, y):
         c = beams[i]
         return (d_in[i], c.nchans, c.nsamps, c.dm_list, y, nouts[i] * 4)
 
-    # waves: add beams while workspace + outputs fit the budget
-    probe = torch.empty(16, dtype=torch.uint8, device=dev)  # stand-in output (sizing only)
-    waves, cur = [], []
-    for i in range(nbeams):
-        trial = cur + [i]
-        b = dd.FddBatch(c0.nchans, c0.dt, c0.f_top, c0.df, in_nbits=8, device=local)
-        b.set_beams([spec(j, probe) for j in trial])
-        need = b.workspace_size() + sum(out_bytes[j] for j in trial)
-        b.close()
-        if cur and need > budget / 1.05:
-            waves.append(cur)
-            cur = [i]
-        else:
-            cur = trial
-    waves.append(cur)
-    pool = torch.empty(max(sum(out_bytes[j] for j in w) for w in waves), dtype=torch.uint8, device=dev)
-    batches, bsources = [], {}
-    for w in waves:
-        b = dd.FddBatch(c0.nchans, c0.dt, c0.f_top, c0.df, in_nbits=8, device=local)
-        sp, off = [], 0
-        for j in w:
-            sp.append(spec(j, pool[off:off + out_bytes[j]]))
-            off += out_bytes[j]
-        b.set_beams(sp)
-        for j in range(len(w)):
-            src = b.phasor_source(j)
-            bsources[src] = bsources.get(src, 0) + 1
-        batches.append(b)
-    ws_bytes = max(b.workspace_size() for b in batches)
-    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
-    for b in batches:
-        b.set_workspace(ws, ws_bytes)
-
-    def batched_step():
+    def batched(seg):
+        free, _ = torch.cuda.mem_get_info(local)
+        budget = free - 8e9
+        # waves: add beams while workspace + outputs fit the budget
+        probe = torch.empty(16, dtype=torch.uint8, device=dev)  # stand-in output (sizing only)
+        waves, cur = [], []
+        for i in range(nbeams):
+            trial = cur + [i]
+            b = dd.FddBatch(c0.nchans, c0.dt, c0.f_top, c0.df, in_nbits=8, device=local)
+            b.set_segment_nfft(seg)
+            b.set_beams([spec(j, probe) for j in trial])
+            need = b.workspace_size() + sum(out_bytes[j] for j in trial)
+            b.close()
+            if cur and need > budget / 1.05:
+                waves.append(cur)
+                cur = [i]
+            else:
+                cur = trial
+        waves.append(cur)
+        pool = torch.empty(max(sum(out_bytes[j] for j in w) for w in waves), dtype=torch.uint8, device=dev)
+        batches, bsources = [], {}
+        for w in waves:
+            b = dd.FddBatch(c0.nchans, c0.dt, c0.f_top, c0.df, in_nbits=8, device=local)
+            b.set_segment_nfft(seg)
+            sp, off = [], 0
+            for j in w:
+                sp.append(spec(j, pool[off:off + out_bytes[j]]))
+                off += out_bytes[j]
+            b.set_beams(sp)
+            for j in range(len(w)):
+                src = b.phasor_source(j)
+                bsources[src] = bsources.get(src, 0) + 1
+            batches.append(b)
+        ws_bytes = max(b.workspace_size() for b in batches)
+        ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
         for b in batches:
-            b.execute(stream.cuda_stream, use_graph=True)
+            b.set_workspace(ws, ws_bytes)
 
-    batched_step()  # warm-up: captures each wave's graph
-    for b in batches:
-        b.sync(stream.cuda_stream)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    batched_step()
-    e1.record(stream)
-    for b in batches:
-        b.sync(stream.cuda_stream)
-    ms = max_over_ranks(e0.elapsed_time(e1))
-    total = float(sum(units))
-    res = {"workload": f"first {nbeams} of the 96 config-3 beams (1536 ch 8-bit, seeded), segmented "
-                       f"FDD, reference segment rule, f32 time-series out",
-           "units": total, "waves": len(waves), "beams_per_wave": [len(w) for w in waves],
-           "batched_bf16x3_tc": {"value": total * world / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
-                                 "mac_launches_per_step": len(waves)}}
-    # error of the last wave's first beam (the pool holds the last wave's
-    # rows) against float64 on two DMs x 2^16 samples
-    bi = waves[-1][0]
-    y0 = pool[:out_bytes[bi]].view(torch.float32).view(len(beams[bi].dm_list), -1)
-    c = beams[bi]
-    nchk = min(1 << 16, nouts[bi])
-    h = d_in[bi][:nchk + mds[bi]].cpu().numpy()
-    x = (h.astype(np.float32) - np.float32(127.5)) * np.float32(1.0 / c.nchans)
-    delays = delay_table_f32(c.nchans, c.dt, c.f_top, c.df)
-    drows = np.array([len(c.dm_list) // 3, len(c.dm_list) - 1])
-    ref = fdd_fp64_rows(x, delays, np.asarray(c.dm_list, np.float32)[drows], nchk)
-    got = y0[torch.as_tensor(drows, device=dev), :nchk].double().cpu().numpy()
-    res["batched_bf16x3_tc"]["rel_l2_vs_fp64"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
-    res["batched_bf16x3_tc"]["max_abs_vs_fp64"] = float(np.abs(got - ref).max() / np.abs(ref).max())
-    res["batched_bf16x3_tc"]["error_sample"] = f"beam {bi}, DMs {drows.tolist()} x first {nchk} samples"
-    # stage split of one more step (direct launches with events, untimed above)
-    split = {"prep_ms": 0.0, "mac_ms": 0.0, "post_ms": 0.0}
-    balance = []
-    for b in batches:
-        b.set_timing(True)
-        b.execute(stream.cuda_stream, use_graph=False)
-        t = b.get_timing()
-        bal = b.get_mac_balance()
-        b.set_timing(False)
-        for k in split:
-            split[k] += t[k]
-        balance.append([round(bal["cta_max_ms"], 1), round(bal["cta_mean_ms"], 1)])
-    res["batched_bf16x3_tc"]["stage_ms"] = {k: round(v, 2) for k, v in split.items()}
-    res["batched_bf16x3_tc"]["mac_cta_max_mean_ms"] = balance
-    res["batched_bf16x3_tc"]["phasor_sources"] = bsources
-    for b in batches:
-        b.close()
-    del pool, ws, batches
-    torch.cuda.empty_cache()
+        def batched_step():
+            for b in batches:
+                b.execute(stream.cuda_stream, use_graph=True)
 
-    # sequential single-beam plans (one execute per beam)
-    stage_sum, sources = {}, {}
-    for name, prec, sub in (("tc_single_beam", 1, list(range(nbeams))),
-                            ("plain_fp32_single_beam", 0, list(range(nplain)))):
-        tms, su = 0.0, 0.0
+        batched_step()  # warm-up: captures each wave's graph
+        for b in batches:
+            b.sync(stream.cuda_stream)
+        e0.record(stream)
+        batched_step()
+        e1.record(stream)
+        for b in batches:
+            b.sync(stream.cuda_stream)
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        r = {"value": total * world / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+             "mac_launches_per_step": len(waves), "waves": len(waves),
+             "beams_per_wave": [len(w) for w in waves]}
+        # error of the last wave's first beam (the pool holds the last wave's
+        # rows) against float64 on two DMs x 2^16 samples
+        bi = waves[-1][0]
+        y0 = pool[:out_bytes[bi]].view(torch.float32).view(len(beams[bi].dm_list), -1)
+        c = beams[bi]
+        nchk = min(1 << 16, nouts[bi])
+        h = d_in[bi][:nchk + mds[bi]].cpu().numpy()
+        x = (h.astype(np.float32) - np.float32(127.5)) * np.float32(1.0 / c.nchans)
+        delays = delay_table_f32(c.nchans, c.dt, c.f_top, c.df)
+        drows = np.array([len(c.dm_list) // 3, len(c.dm_list) - 1])
+        ref = fdd_fp64_rows(x, delays, np.asarray(c.dm_list, np.float32)[drows], nchk)
+        got = y0[torch.as_tensor(drows, device=dev), :nchk].double().cpu().numpy()
+        r["rel_l2_vs_fp64"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+        r["max_abs_vs_fp64"] = float(np.abs(got - ref).max() / np.abs(ref).max())
+        r["error_sample"] = f"beam {bi}, DMs {drows.tolist()} x first {nchk} samples"
+        # stage split of one more step (direct launches with events, untimed above)
+        split = {"prep_ms": 0.0, "mac_ms": 0.0, "post_ms": 0.0}
+        balance = []
+        for b in batches:
+            b.set_timing(True)
+            b.execute(stream.cuda_stream, use_graph=False)
+            t = b.get_timing()
+            bal = b.get_mac_balance()
+            b.set_timing(False)
+            for k in split:
+                split[k] += t[k]
+            balance.append([round(bal["cta_max_ms"], 1), round(bal["cta_mean_ms"], 1)])
+        r["stage_ms"] = {k: round(v, 2) for k, v in split.items()}
+        r["mac_cta_max_mean_ms"] = balance
+        r["phasor_sources"] = bsources
+        for b in batches:
+            b.close()
+        del pool, ws, batches
+        torch.cuda.empty_cache()
+        return r
+
+    def single(prec, sub, seg):
+        """One plan execute per beam (each timed after its own warm-up)."""
+        tms, su, stage_sum, sources = 0.0, 0.0, {"prep_ms": 0.0, "mac_ms": 0.0, "post_ms": 0.0}, {}
         for i in sub:
             c = beams[i]
             p = dd.FDDGPUPlan(c.nchans, c.dt, c.f_top, c.df, local)
             p.set_dm_list(c.dm_list)
-            p.set_options(segmented=1, precision=prec)
+            p.set_options(segmented=1, precision=prec, segment_nfft=seg)
             p.set_stream(stream.cuda_stream)
             y = torch.empty((len(c.dm_list), nouts[i]), dtype=torch.float32, device=dev)
             p.execute(c.nsamps, d_in[i], 8, y, 32, dd.DEDISP_DEVICE_POINTERS)  # warm-up (allocation)
@@ -719,24 +721,41 @@ def run_batched_fdd(args, local, world, stream, max_over_ranks, nbeams=12, nplai
             p.set_timing(True)
             p.execute(c.nsamps, d_in[i], 8, y, 32, dd.DEDISP_DEVICE_POINTERS)
             st_ms = p.get_stage_times()
-            for k in ("prep", "mac", "post"):
-                stage_sum.setdefault(name, {}).setdefault(k + "_ms", 0.0)
-            stage_sum[name]["mac_ms"] += st_ms["mac"]
-            stage_sum[name]["prep_ms"] += st_ms["unpack"] + st_ms["fft_fwd"] + st_ms["layout"]
-            stage_sum[name]["post_ms"] += st_ms["transpose"] + st_ms["fft_inv"]
+            stage_sum["mac_ms"] += st_ms["mac"]
+            stage_sum["prep_ms"] += st_ms["unpack"] + st_ms["fft_fwd"] + st_ms["layout"]
+            stage_sum["post_ms"] += st_ms["transpose"] + st_ms["fft_inv"]
             if prec == 1:
-                sources[p.get_phasor_source()] = sources.get(p.get_phasor_source(), 0) + 1
+                src = p.get_phasor_source()
+                sources[src] = sources.get(src, 0) + 1
             p.close()
             del y
             torch.cuda.empty_cache()
-        res[name] = {"value": su * world / (tms * 1e-3), "unit": UNIT, "ms": tms,
-                     "sample": f"beams {sub[0]}-{sub[-1]} ({su:.3e} DM-trials x samples), one plan "
-                               f"execute per beam (each plan timed after its own warm-up)",
-                     "stage_ms": {k: round(v, 2) for k, v in stage_sum[name].items()}}
+        r = {"value": su * world / (tms * 1e-3), "unit": UNIT, "ms": tms,
+             "sample": f"beams {sub[0]}-{sub[-1]} ({su:.3e} DM-trials x samples), one plan "
+                       f"execute per beam (each plan timed after its own warm-up)",
+             "stage_ms": {k: round(v, 2) for k, v in stage_sum.items()}}
         if prec == 1:
-            res[name]["phasor_sources"] = dict(sources)
+            r["phasor_sources"] = sources
+        return r
+
+    res = {"workload": f"first {nbeams} of the 96 config-3 beams (1536 ch 8-bit, seeded), segmented "
+                       f"FDD, f32 time-series out", "units": total}
+    res["batched_bf16x3_tc"] = batched(0)
+    res["batched_bf16x3_tc"]["segments"] = "reference rule"
+    _log("batched fdd (reference segments) done")
+    res["batched_bf16x3_tc_auto_segments"] = batched("auto")
+    res["batched_bf16x3_tc_auto_segments"]["segments"] = "automatic (least modelled time)"
+    _log("batched fdd (automatic segments) done")
+    res["tc_single_beam"] = single(1, list(range(nbeams)), 0)
+    res["tc_single_beam_auto_segments"] = single(1, list(range(nbeams)), "auto")
+    res["plain_fp32_single_beam"] = single(0, list(range(nplain)), 0)
+    _log("per-beam fdd plans done")
     res["batched_vs_plain_fp32"] = res["batched_bf16x3_tc"]["value"] / res["plain_fp32_single_beam"]["value"]
     res["batched_vs_tc_single_beam"] = res["batched_bf16x3_tc"]["value"] / res["tc_single_beam"]["value"]
+    res["batched_auto_vs_plain_fp32"] = (res["batched_bf16x3_tc_auto_segments"]["value"] /
+                                         res["plain_fp32_single_beam"]["value"])
+    res["batched_auto_vs_tc_single_beam_auto"] = (res["batched_bf16x3_tc_auto_segments"]["value"] /
+                                                  res["tc_single_beam_auto_segments"]["value"])
     del d_in
     torch.cuda.empty_cache()
     return res

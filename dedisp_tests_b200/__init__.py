@@ -120,6 +120,7 @@ def lib() -> C.CDLL:
         "dedisp_b200_output_row_length": (_sz, [_vp, _sz]),
         "dedisp_b200_get_stage_times": (err, [_vp, C.POINTER(C.c_float), C.c_int]),
         "dedisp_b200_get_phasor_source": (err, [_vp, C.POINTER(C.c_int)]),
+        "dedisp_b200_fdd_segment_length": (_sz, [_sz, _sz, _sz, _sz, C.c_int, _sz]),
         "dedisp_b200_set_wait_limit_ns": (err, [C.c_ulonglong]),
         "dedisp_b200_get_wait_limit_ns": (C.c_ulonglong, []),
         "dedisp_b200_set_wait_expiry_test": (err, [C.c_int]),
@@ -303,14 +304,32 @@ class TDDPlan(DedispPlan):
     IMPLEMENTATION = DEDISP_TDD
 
 
+FDD_SEGMENT_AUTO = 1
+
+
+def _segment_arg(segment_nfft) -> int:
+    return FDD_SEGMENT_AUTO if segment_nfft == "auto" else int(segment_nfft)
+
+
+def fdd_segment_length(nsamps: int, max_delay: int, dm_count: int, nchans: int, precision: int = 1,
+                       segment_nfft=0) -> int:
+    """Segment length (points) of segmented FDD for these sizes under the
+    rule `segment_nfft` (0 reference, "auto", or a length); 0 if none fits."""
+    return int(lib().dedisp_b200_fdd_segment_length(nsamps, max_delay, dm_count, nchans, precision,
+                                                    _segment_arg(segment_nfft)))
+
+
 class FDDGPUPlan(Plan):
     """Fourier-domain dedispersion (reference src/fdd/FDDGPUPlan.hpp)."""
     IMPLEMENTATION = DEDISP_FDD
 
     def set_options(self, segmented: int = -1, timeseries: bool = False, precision: int = 0,
-                    round_delays: bool = False, segment_nfft: int = 0) -> None:
+                    round_delays: bool = False, segment_nfft=0) -> None:
+        """segment_nfft: 0 the reference doubling rule, "auto" the power of two
+        with the least modelled device time, else a power of two."""
         _check(lib().dedisp_b200_set_fdd_options(self._h, segmented, int(timeseries),
-                                                 precision, int(round_delays), segment_nfft))
+                                                 precision, int(round_delays),
+                                                 _segment_arg(segment_nfft)))
 
 
 def set_wait_limit_ns(ns: int) -> None:
@@ -381,6 +400,7 @@ _BATCH_SIGS = {
     "dedisp_b200_fdd_batch_max_delay": (_sz, [_vp, _sz]),
     "dedisp_b200_fdd_batch_phasor_source": (C.c_int, [_vp, _sz]),
     "dedisp_b200_fdd_batch_get_mac_balance": (C.c_int, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "dedisp_b200_fdd_batch_set_segment_nfft": (C.c_int, [_vp, _sz]),
 }
 
 
@@ -514,6 +534,11 @@ class FddBatch:
             self.close()
         except Exception:
             pass
+
+    def set_segment_nfft(self, segment_nfft) -> None:
+        """0 the reference doubling rule (default), "auto" the least modelled
+        time per beam, else a power of two; takes effect at set_beams."""
+        _bcheck(_batch_lib().dedisp_b200_fdd_batch_set_segment_nfft(self._h, _segment_arg(segment_nfft)))
 
     def set_killmask(self, killmask=None) -> None:
         if killmask is None:

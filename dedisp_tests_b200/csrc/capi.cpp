@@ -380,6 +380,20 @@ dedisp_error dedisp_b200_set_fdd_options(dedisp_plan plan, int segmented, int ti
     });
 }
 
+dedisp_size dedisp_b200_fdd_segment_length(dedisp_size nsamps, dedisp_size max_delay, dedisp_size dm_count,
+                                           dedisp_size nchans, int precision, dedisp_size segment_nfft)
+{
+    dedisp_size n = 0;
+    guarded([&] {
+        dedisp::FddOptions o;
+        o.segmented = 1;
+        o.precision = precision ? dedisp::FddPrecision::BF16x3 : dedisp::FddPrecision::FP32;
+        o.segment_nfft = segment_nfft;
+        n = dedisp::detail::fdd_geometry(o, nsamps, max_delay, dm_count, nchans).nfft;
+    });
+    return n;
+}
+
 dedisp_error dedisp_b200_set_wait_limit_ns(unsigned long long ns)
 {
     dedisp::rt::set_wait_limit_ns(ns);

@@ -125,7 +125,8 @@ void FddBatch::plan()
         opt.segmented = 1;
         opt.output = FddOutput::TimeSeries;
         opt.precision = FddPrecision::BF16x3;
-        b.g = fdd_geometry(opt, b.spec.nsamps, b.max_delay);
+        opt.segment_nfft = m_segment_nfft;
+        b.g = fdd_geometry(opt, b.spec.nsamps, b.max_delay, b.spec.dms.size(), (size_t)std::max(m_nact, 1));
         const size_t nfft = b.g.nfft, nseg = b.g.nchunk, nbins = b.g.nbins;
         const bool pow2 = (nfft & (nfft - 1)) == 0;
         b.qpath = !(pow2 && nfft >= 512 && nfft <= (size_t)kern::kMaxFft);
@@ -135,7 +136,6 @@ void FddBatch::plan()
         b.seg_stride = b.g.nsamp_good;
         b.x_len = round_up((nseg - 1) * b.seg_stride + nfft, 32);
         const size_t ndm = b.spec.dms.size();
-        if (m_nchans * nseg > 65535 || ndm * nseg > 65535) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "too many FFT rows");
         // largest delay index over DMs and active channels (reference trunc rule)
         long dmax = 0;
         bool ok = true;
@@ -598,6 +598,11 @@ dedisp_error dedisp_b200_fdd_batch_get_timing(dedisp_b200_fdd_batch batch, float
         if (post_ms) *post_ms = b.last_post_ms;
         if (launches) *launches = b.last_launches;
     });
+}
+
+dedisp_error dedisp_b200_fdd_batch_set_segment_nfft(dedisp_b200_fdd_batch batch, dedisp_size segment_nfft)
+{
+    return fdd_batch_call(batch, [&](dedisp::detail::FddBatch& b) { b.set_segment_nfft(segment_nfft); });
 }
 
 dedisp_error dedisp_b200_fdd_batch_get_mac_balance(dedisp_b200_fdd_batch batch, float* cta_max_ms,

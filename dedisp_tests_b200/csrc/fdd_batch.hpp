@@ -46,6 +46,10 @@ public:
     ~FddBatch();
 
     void set_killmask(const int32_t* killmask);  // nullptr: all channels
+    // Segment length of every beam: 0 the reference doubling rule (default),
+    // FddOptions::kSegmentAuto the least modelled time per beam, else that
+    // power of two. Takes effect at the next set_beams.
+    void set_segment_nfft(size_t n) { m_segment_nfft = n; }
     void set_beams(std::vector<FddBeamSpec> beams);
     size_t beam_count() const { return m_beams.size(); }
     size_t max_delay(size_t beam) const;
@@ -90,6 +94,7 @@ private:
     std::vector<int32_t> m_km;
     std::vector<std::unique_ptr<Beam>> m_beams;
     bool m_dirty = true;
+    size_t m_segment_nfft = 0;
     int m_nact = 0, m_nact_pad = 0;
     size_t m_ws_bytes = 0, m_shared_bytes = 0, m_scratch_off = 0, m_scratch_bytes = 0;
 

@@ -54,7 +54,9 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
     Impl& m = *m_impl;
     stats = ExecTiming();
 
-    const FddGeometry g = fdd_geometry(opt, c.nsamps, v.max_delay);
+    size_t nlive = 0;  // channels the killmask keeps (automatic segment length)
+    for (size_t i = 0; i < v.nchans; ++i) nlive += (!v.killmask || v.killmask[i]) ? 1 : 0;
+    const FddGeometry g = fdd_geometry(opt, c.nsamps, v.max_delay, v.ndm, std::max<size_t>(1, nlive));
     // Power-of-two lengths up to 2^20: one-CTA or four-step transforms;
     // other multiples of 16384 (the whole-series rule) and longer lengths:
     // the 16384 Q-point transforms (spectra in the BinMap order).

@@ -41,7 +41,13 @@ struct FddGeometry {
     size_t nbins = 0;       // bins computed per segment (nfft/2 + 1)
     size_t row_len = 0;     // floats per output row
 };
-FddGeometry fdd_geometry(const FddOptions& opt, size_t nsamps, size_t max_delay);
+// ndm, nchans (active channels): used by the automatic segment length only.
+FddGeometry fdd_geometry(const FddOptions& opt, size_t nsamps, size_t max_delay, size_t ndm = 0,
+                         size_t nchans = 0);
+// Segmented FDD, tensor-core MAC: the power-of-two segment length (2^11..2^20,
+// above the max delay) with the least modelled device time for the DM count
+// and the active channels.
+size_t fdd_auto_segment(size_t nsamps, size_t max_delay, size_t ndm, size_t nchans);
 
 class FddEngine {
 public:

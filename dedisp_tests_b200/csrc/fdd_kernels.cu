@@ -1261,20 +1261,39 @@ void launch_fdd_unpack(const uint8_t* in, size_t in_stride, int in_nbits, size_t
     RT_CHECK(cudaGetLastError());
 }
 
+// The four-step and Q-point kernels carry the row (channel x segment or DM x
+// segment) in grid.y: launches of whole channels or DMs, at most 65535 rows
+// each, one after another (they share the scratch buffer).
+static size_t rows_per_launch(size_t nseg)
+{
+    if (nseg == 0 || nseg > 65535) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "too many segments");
+    return 65535 / nseg;
+}
+
 void launch_fft_r2c(const float* x, size_t x_pitch, size_t nchans, size_t nseg, size_t seg_stride,
                     int nfft, float2* X, size_t bin_pitch, const TwiddleTable& tw, float2* scratch,
                     cudaStream_t s)
 {
-    const size_t rows = nchans * nseg;
-    if (rows > 65535 && log2_exact(nfft) > 15) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "too many FFT rows");
-    switch (log2_exact(nfft)) {
+    const int lg = log2_exact(nfft);
+    if (lg >= 5 && lg <= 15) {
+        switch (lg) {
 #define R2C(L) case L + 1: launch_r2c_n<L>(x, x_pitch, nchans, nseg, seg_stride, X, bin_pitch, tw, s); break;
-        R2C(4) R2C(5) R2C(6) R2C(7) R2C(8) R2C(9) R2C(10) R2C(11) R2C(12) R2C(13) R2C(14)
+            R2C(4) R2C(5) R2C(6) R2C(7) R2C(8) R2C(9) R2C(10) R2C(11) R2C(12) R2C(13) R2C(14)
 #undef R2C
-#define R4(L1, L2) case L1 + L2 + 1: launch_r2c_4step<L1, L2>(x, x_pitch, rows, nseg, seg_stride, X, bin_pitch, scratch, tw, s); break;
-        R4(8, 7) R4(8, 8) R4(9, 8) R4(9, 9) R4(10, 9)
+        }
+        return;
+    }
+    const size_t per = rows_per_launch(nseg);
+    for (size_t c0 = 0; c0 < nchans; c0 += per) {
+        const size_t rows = std::min(per, nchans - c0) * nseg;
+        const float* xc = x + c0 * x_pitch;
+        float2* Xc = X + c0 * nseg * bin_pitch;
+        switch (lg) {
+#define R4(L1, L2) case L1 + L2 + 1: launch_r2c_4step<L1, L2>(xc, x_pitch, rows, nseg, seg_stride, Xc, bin_pitch, scratch, tw, s); break;
+            R4(8, 7) R4(8, 8) R4(9, 8) R4(9, 9) R4(10, 9)
 #undef R4
-    default: DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unsupported FFT length");
+        default: DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unsupported FFT length");
+        }
     }
 }
 
@@ -1282,16 +1301,26 @@ void launch_fft_c2r(float2* Y, size_t bin_pitch, size_t ndm, size_t nseg, int nf
                     float* out, size_t out_stride, size_t keep, size_t out_len,
                     const TwiddleTable& tw, float2* scratch, cudaStream_t s)
 {
-    const size_t rows = ndm * nseg;
-    if (rows > 65535 && log2_exact(nfft) > 15) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "too many FFT rows");
-    switch (log2_exact(nfft)) {
+    const int lg = log2_exact(nfft);
+    if (lg >= 5 && lg <= 15) {
+        switch (lg) {
 #define C2R(L) case L + 1: launch_c2r_n<L>(Y, bin_pitch, ndm, nseg, out, out_stride, keep, out_len, tw, s); break;
-        C2R(4) C2R(5) C2R(6) C2R(7) C2R(8) C2R(9) C2R(10) C2R(11) C2R(12) C2R(13) C2R(14)
+            C2R(4) C2R(5) C2R(6) C2R(7) C2R(8) C2R(9) C2R(10) C2R(11) C2R(12) C2R(13) C2R(14)
 #undef C2R
-#define C4(L1, L2) case L1 + L2 + 1: launch_c2r_4step<L1, L2>(Y, bin_pitch, rows, nseg, out, out_stride, keep, out_len, scratch, tw, s); break;
-        C4(8, 7) C4(8, 8) C4(9, 8) C4(9, 9) C4(10, 9)
+        }
+        return;
+    }
+    const size_t per = rows_per_launch(nseg);
+    for (size_t d0 = 0; d0 < ndm; d0 += per) {
+        const size_t rows = std::min(per, ndm - d0) * nseg;
+        float2* Yd = Y + d0 * nseg * bin_pitch;
+        float* od = out + d0 * out_stride;
+        switch (lg) {
+#define C4(L1, L2) case L1 + L2 + 1: launch_c2r_4step<L1, L2>(Yd, bin_pitch, rows, nseg, od, out_stride, keep, out_len, scratch, tw, s); break;
+            C4(8, 7) C4(8, 8) C4(9, 8) C4(9, 9) C4(10, 9)
 #undef C4
-    default: DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unsupported FFT length");
+        default: DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unsupported FFT length");
+        }
     }
 }
 
@@ -1359,26 +1388,31 @@ void launch_fft_r2c_q(const float* x, size_t x_pitch, size_t nchans, size_t nseg
 {
     if (!fftq_length(nfft)) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unsupported FFT length");
     const unsigned Q = (unsigned)(nfft / 16384);
-    const size_t rows = nchans * nseg;
-    if (rows == 0) return;
-    if (rows > 65535) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "too many FFT rows");
+    if (nchans * nseg == 0) return;
     const int T = fftq_tile(Q);
     const QRadices rad = fftq_radices(Q);
     const BinMap map = fdd_binmap(nfft);
     const size_t sq = (2 * (size_t)T * Q + Q) * sizeof(float2);
     rt::raise_smem_limit(fftq_cols_fwd_kernel, sq);
-    fftq_cols_fwd_kernel<<<dim3(FQ_P / T, (unsigned)rows), FQ_THREADS, sq, s>>>(x, x_pitch, nseg, seg_stride,
-                                                                              scratch, (int)Q, T, rad, wq, tw);
-    RT_CHECK(cudaGetLastError());
     auto kr = fft_c2c_rows_kernel<FQ_LOGP, false>;
     const size_t sr = (FQ_P + 256 + 2 * FQ_P / 256) * sizeof(float2);
     rt::raise_smem_limit(kr, sr);
-    const size_t nrows = rows * Q;
-    kr<<<persistent_grid(kr, FftPlan<FQ_LOGP>::threads(), sr, nrows), FftPlan<FQ_LOGP>::threads(), sr, s>>>(
-        scratch, map.M, X, bin_pitch, Q, twp, nrows);
-    RT_CHECK(cudaGetLastError());
-    r2c_post_q_kernel<<<dim3((unsigned)((map.M + 255) / 256), (unsigned)rows), 256, 0, s>>>(X, bin_pitch, map, tw);
-    RT_CHECK(cudaGetLastError());
+    const size_t per = rows_per_launch(nseg);
+    for (size_t c0 = 0; c0 < nchans; c0 += per) {
+        const size_t rows = std::min(per, nchans - c0) * nseg;
+        const float* xc = x + c0 * x_pitch;
+        float2* Xc = X + c0 * nseg * bin_pitch;
+        fftq_cols_fwd_kernel<<<dim3(FQ_P / T, (unsigned)rows), FQ_THREADS, sq, s>>>(xc, x_pitch, nseg, seg_stride,
+                                                                                  scratch, (int)Q, T, rad, wq, tw);
+        RT_CHECK(cudaGetLastError());
+        const size_t nrows = rows * Q;
+        kr<<<persistent_grid(kr, FftPlan<FQ_LOGP>::threads(), sr, nrows), FftPlan<FQ_LOGP>::threads(), sr, s>>>(
+            scratch, map.M, Xc, bin_pitch, Q, twp, nrows);
+        RT_CHECK(cudaGetLastError());
+        r2c_post_q_kernel<<<dim3((unsigned)((map.M + 255) / 256), (unsigned)rows), 256, 0, s>>>(Xc, bin_pitch, map,
+                                                                                                tw);
+        RT_CHECK(cudaGetLastError());
+    }
 }
 
 void launch_fft_c2r_q(float2* Y, size_t bin_pitch, size_t ndm, size_t nseg, size_t nfft, float* out,
@@ -1387,26 +1421,31 @@ void launch_fft_c2r_q(float2* Y, size_t bin_pitch, size_t ndm, size_t nseg, size
 {
     if (!fftq_length(nfft)) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "unsupported FFT length");
     const unsigned Q = (unsigned)(nfft / 16384);
-    const size_t rows = ndm * nseg;
-    if (rows == 0) return;
-    if (rows > 65535) DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "too many FFT rows");
+    if (ndm * nseg == 0) return;
     const int T = fftq_tile(Q);
     const QRadices rad = fftq_radices(Q);
     const BinMap map = fdd_binmap(nfft);
-    c2r_pre_q_kernel<<<dim3((unsigned)((map.M + 255) / 256), (unsigned)rows), 256, 0, s>>>(Y, bin_pitch, map, tw);
-    RT_CHECK(cudaGetLastError());
     auto kr = fft_c2c_rows_kernel<FQ_LOGP, true>;
     const size_t sr = (FQ_P + 256 + 2 * FQ_P / 256) * sizeof(float2);
     rt::raise_smem_limit(kr, sr);
-    const size_t nrows = rows * Q;
-    kr<<<persistent_grid(kr, FftPlan<FQ_LOGP>::threads(), sr, nrows), FftPlan<FQ_LOGP>::threads(), sr, s>>>(
-        Y, bin_pitch, scratch, map.M, Q, twp, nrows);
-    RT_CHECK(cudaGetLastError());
     const size_t sq = (2 * (size_t)T * Q + Q) * sizeof(float2);
     rt::raise_smem_limit(fftq_cols_inv_kernel, sq);
-    fftq_cols_inv_kernel<<<dim3(FQ_P / T, (unsigned)rows), FQ_THREADS, sq, s>>>(scratch, out, out_stride, nseg, keep,
-                                                                              out_len, (int)Q, T, rad, wq, tw);
-    RT_CHECK(cudaGetLastError());
+    const size_t per = rows_per_launch(nseg);
+    for (size_t d0 = 0; d0 < ndm; d0 += per) {
+        const size_t rows = std::min(per, ndm - d0) * nseg;
+        float2* Yd = Y + d0 * nseg * bin_pitch;
+        float* od = out + d0 * out_stride;
+        c2r_pre_q_kernel<<<dim3((unsigned)((map.M + 255) / 256), (unsigned)rows), 256, 0, s>>>(Yd, bin_pitch, map,
+                                                                                               tw);
+        RT_CHECK(cudaGetLastError());
+        const size_t nrows = rows * Q;
+        kr<<<persistent_grid(kr, FftPlan<FQ_LOGP>::threads(), sr, nrows), FftPlan<FQ_LOGP>::threads(), sr, s>>>(
+            Yd, bin_pitch, scratch, map.M, Q, twp, nrows);
+        RT_CHECK(cudaGetLastError());
+        fftq_cols_inv_kernel<<<dim3(FQ_P / T, (unsigned)rows), FQ_THREADS, sq, s>>>(
+            scratch, od, out_stride, nseg, keep, out_len, (int)Q, T, rad, wq, tw);
+        RT_CHECK(cudaGetLastError());
+    }
 }
 
 void launch_fdd_to_binmajor(const float2* X, size_t bin_pitch, size_t nseg, size_t nbins,

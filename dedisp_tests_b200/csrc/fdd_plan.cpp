@@ -10,7 +10,43 @@ namespace dedisp {
 
 namespace detail {
 
-FddGeometry fdd_geometry(const FddOptions& opt, size_t nsamps, size_t max_delay)
+size_t fdd_auto_segment(size_t nsamps, size_t max_delay, size_t ndm, size_t nchans)
+{
+    // Modelled device time (ps) of one execute with segments of n points,
+    // from stage times measured on B200 (1536- and 1024-channel beams):
+    // - tensor-core MAC: per (bin, DM row, channel) about 1.08 ps while the
+    //   phasor generation bounds it, growing as the MMA's columns (2 x
+    //   segments, padded to 16) pass about 70; segment groups of at most 64
+    //   build their phasors again;
+    // - transforms and layout changes: about 10 ps per channel point and 8
+    //   ps per DM point of the segmented series.
+    // The FP32 MAC's work is per (bin, segment), nearly the same for every
+    // length, and its 40-segment tiles favour many segments: it keeps the
+    // reference rule.
+    const double ndm_pad = (double)((ndm + 127) / 128 * 128);
+    double best = 0;
+    size_t best_n = 0;
+    for (size_t n = 2048; n <= (1u << 20); n *= 2) {
+        if (n <= max_delay) continue;
+        const double nbins = (double)(n / 2 + 1);
+        const size_t nseg = (nsamps + (n - max_delay) - 1) / (n - max_delay);
+        double mac = 0;
+        for (size_t s0 = 0; s0 < nseg; s0 += 64) {
+            const double npad = (double)((2 * std::min<size_t>(64, nseg - s0) + 15) / 16 * 16);
+            mac += nbins * ndm_pad * (double)nchans * 1.08 * std::max(1.0, npad / 70.0);
+        }
+        const double xf = (10.0 * (double)nchans + 8.0 * (double)ndm) * (double)nseg * (double)n;
+        const double t = mac + xf;
+        if (best_n == 0 || t < best) {
+            best = t;
+            best_n = n;
+        }
+    }
+    if (best_n == 0) DD_THROW_MSG(DEDISP_TOO_FEW_NSAMPS, "max delay above the longest segment");
+    return best_n;
+}
+
+FddGeometry fdd_geometry(const FddOptions& opt, size_t nsamps, size_t max_delay, size_t ndm, size_t nchans)
 {
     FddGeometry g;
     bool seg = opt.segmented > 0;
@@ -22,8 +58,11 @@ FddGeometry fdd_geometry(const FddOptions& opt, size_t nsamps, size_t max_delay)
     if (seg) {
         // nfft doubles from 16384 while nfft*(1 - 0.8f) < max_delay
         // (FDDGPUPlan.cpp:742,762-768); nsamp_good = nfft - max_delay.
-        size_t n = opt.segment_nfft ? opt.segment_nfft : 16384;
-        if (!opt.segment_nfft) {
+        const bool autoseg = opt.segment_nfft == FddOptions::kSegmentAuto;
+        size_t n = (opt.segment_nfft && !autoseg) ? opt.segment_nfft : 16384;
+        if (autoseg && ndm && nchans && opt.precision == FddPrecision::BF16x3) {
+            n = fdd_auto_segment(nsamps, max_delay, ndm, nchans);
+        } else if (!opt.segment_nfft || autoseg) {
             const float min_eff = 0.8f;
             while ((double)n * (1.0 - (double)min_eff) < (double)max_delay) n *= 2;
         }

@@ -72,7 +72,18 @@ dedisp_error dedisp_b200_last_error(char* msg, dedisp_size len);
  *   timeseries     whole-series output: 0 spectrum (default), 1 time series
  *   precision      0 FP32 CUDA cores, 1 3xBF16 tensor-core GEMM
  *   round_delays   0 truncate (reference FDD), 1 round half to even (TDD)
- *   segment_nfft   0 reference doubling rule, else a power of two */
+ *   segment_nfft   0 reference doubling rule, DEDISP_B200_FDD_SEGMENT_AUTO
+ *                  the power of two with the least modelled device time (the
+ *                  output is the same series; only rounding differs), else a
+ *                  power of two above the max delay */
+#define DEDISP_B200_FDD_SEGMENT_AUTO 1
+
+/* Segmented FDD: the segment length (points) a plan with these sizes uses
+ * under `segment_nfft` (0 reference rule, DEDISP_B200_FDD_SEGMENT_AUTO, or an
+ * explicit length); 0 if none fits (the max delay reaches the segment). Host
+ * only. */
+dedisp_size dedisp_b200_fdd_segment_length(dedisp_size nsamps, dedisp_size max_delay, dedisp_size dm_count,
+                                           dedisp_size nchans, int precision, dedisp_size segment_nfft);
 dedisp_error dedisp_b200_set_fdd_options(dedisp_plan plan, int segmented, int timeseries,
                                          int precision, int round_delays,
                                          dedisp_size segment_nfft);
@@ -228,6 +239,10 @@ dedisp_error dedisp_b200_fdd_batch_set_timing(dedisp_b200_fdd_batch batch, int e
 dedisp_error dedisp_b200_fdd_batch_get_timing(dedisp_b200_fdd_batch batch, float* prep_ms, float* mac_ms,
                                               float* post_ms, int* launches);
 dedisp_size dedisp_b200_fdd_batch_max_delay(dedisp_b200_fdd_batch batch, dedisp_size beam);
+/* Segment length of every beam, as segment_nfft of dedisp_b200_set_fdd_options
+ * (0 the reference rule, the default; DEDISP_B200_FDD_SEGMENT_AUTO the least
+ * modelled time per beam); takes effect at the next set_beams. */
+dedisp_error dedisp_b200_fdd_batch_set_segment_nfft(dedisp_b200_fdd_batch batch, dedisp_size segment_nfft);
 /* After a direct (use_graph = 0) execute with timing on: the MAC launch's
  * largest and mean per-CTA busy time (ms); their ratio shows how evenly the
  * work list spread over the SMs. 0 when not measured. */

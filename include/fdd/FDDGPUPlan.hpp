@@ -36,7 +36,12 @@ struct FddOptions {
     FddOutput output = FddOutput::Spectrum;   /* whole-series path only */
     FddPrecision precision = FddPrecision::FP32;
     bool round_delays = false;                /* false: (int) truncation */
-    size_t segment_nfft = 0;                  /* 0: reference doubling rule */
+    /* 0: reference doubling rule; 1 (kSegmentAuto): with the tensor-core MAC
+     * the power of two with the least modelled device time for the plan's
+     * DMs and channels (FP32: the reference rule); else the segment length
+     * (a power of two above the max delay) */
+    size_t segment_nfft = 0;
+    static constexpr size_t kSegmentAuto = 1;
 };
 
 class FDDGPUPlan : public GPUPlan {

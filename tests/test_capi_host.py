@@ -165,6 +165,26 @@ def test_fdd_output_row_length_follows_reference_geometry():
     assert p.output_row_length(n) == n - 5243
 
 
+def test_fdd_segment_length_rules():
+    """Reference rule: doubling from 16384 while nfft * 0.2 < max delay
+    (src/fdd/FDDGPUPlan.cpp:742,762-768). Automatic rule (tensor-core MAC):
+    shorter segments while the MAC stays bound by phasor generation; on B200
+    the config-3 beams below measured (MAC + transforms, ms) 488 / 296 / 182
+    for 131072 / 65536 / 32768 points (beam 0) and 140 / 77 / 133 for 65536 /
+    32768 / 16384 (beam 4), and the rule picks the fastest of each."""
+    f = dd.fdd_segment_length
+    assert f(1 << 20, 5243, 2048, 1024, 1, 0) == 32768
+    assert f(850907, 14271, 3642, 1536, 1, 0) == 131072
+    assert f(911111, 9918, 1481, 1536, 1, 0) == 65536
+    assert f(850907, 14271, 3642, 1536, 1, "auto") == 32768
+    assert f(911111, 9918, 1481, 1536, 1, "auto") == 32768
+    assert f(414083, 29372, 3225, 1536, 1, "auto") <= 65536
+    assert f(1000, 10, 16, 64, 1, 8192) == 8192
+    assert f(1000, 9000, 16, 64, 1, 8192) == 0            # segment shorter than the max delay
+    # FP32 MAC: the automatic rule is the reference rule
+    assert f(850907, 14271, 3642, 1536, 0, "auto") == 131072
+
+
 def test_batch_api_argument_checks():
     """Host-side checks of the batch interface; no GPU work is launched."""
     L = dd._batch_lib()

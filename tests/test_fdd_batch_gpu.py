@@ -164,3 +164,33 @@ def test_fdd_batch_hybrid_phasors(monkeypatch):
         ref = _oracle(packed, 8, dms)
         rel, mx = _errs(g, ref)
         assert rel < TOL[0] and mx < TOL[1], ("vs FP64", i, rel, mx)
+
+
+def test_fdd_batch_automatic_segment_lengths():
+    """set_segment_nfft("auto"): per beam the segment length with the least
+    modelled time (2048 to 32768 points for these beams, against 16384 and
+    65536 by the reference rule); same tolerance against the FP64 oracle."""
+    import torch
+    host = _beam_inputs(8, 29, _specs())
+    b = dd.FddBatch(*PARAMS, in_nbits=8)
+    b.set_segment_nfft("auto")
+    probe = dd.TDDPlan(*PARAMS)
+    beams, outs = [], []
+    for packed, dms in host:
+        probe.set_dm_list(dms)
+        nout = packed.shape[0] - probe.get_max_delay()
+        x = torch.from_numpy(packed).cuda()
+        y = torch.full((len(dms), nout), -7.0, dtype=torch.float32, device="cuda")
+        beams.append((x, packed.shape[1], packed.shape[0], dms, y, y.shape[1] * 4))
+        outs.append(y)
+    b.set_beams(beams)
+    stream = torch.cuda.current_stream().cuda_stream
+    b.execute(stream, use_graph=True)
+    b.sync(stream)
+    for i, ((packed, dms), y) in enumerate(zip(host, outs)):
+        if packed.shape[0] > 200000:
+            continue
+        ref = _oracle(packed, 8, dms)
+        rel, mx = _errs(y.cpu().numpy(), ref)
+        assert rel < TOL[0] and mx < TOL[1], ("auto segments vs FP64", i, rel, mx)
+    b.close()

@@ -9,6 +9,8 @@ rel-L2 <= 1e-5 against FP64 (max-abs, relative to max |ref|, <= 1e-4).
 import numpy as np
 import pytest
 
+import dedisp_tests_b200 as dd
+
 from tests.test_fdd_gpu import _delays, _errs, _input, _oracle_x, _plan
 from oracle import pyoracle as po
 
@@ -187,4 +189,54 @@ def test_tc_quarter_wave_for_power_of_two_when_table_capped(monkeypatch):
     x = _oracle_x(inp, nsamps, params, 8)
     ref = po.fdd_timeseries(x, _delays(params), np.ones(nchans, np.int32), dms, nout)
     rel, mx = _errs(out, ref)
+    assert rel < TC_REL_L2 and mx < TC_MAX_ABS, (rel, mx)
+
+
+def test_tc_automatic_segment_length():
+    """segment_nfft="auto": the segment length with the least modelled time
+    (16384 points here, against 65536 by the reference rule); the same series
+    within the same tolerance against FP64."""
+    params = (128, 128e-6, 1500.0, -1.0)
+    nchans, nsamps = params[0], 123457
+    inp, _ = _input(nchans, nsamps, 21, f0=params[2], df=params[3], dt=params[1])
+    dms = np.linspace(0, 3000, 300, dtype=np.float32)
+    p = _plan(params, dms, segmented=1, precision=1, segment_nfft="auto")
+    md = p.get_max_delay()
+    assert dd.fdd_segment_length(nsamps, md, len(dms), nchans, 1, "auto") == 16384
+    assert dd.fdd_segment_length(nsamps, md, len(dms), nchans, 1, 0) == 65536
+    nout = nsamps - md
+    out = _run(p, nsamps, inp, 8, len(dms))
+    x = _oracle_x(inp, nsamps, params, 8)
+    ref = po.fdd_timeseries(x, _delays(params), np.ones(nchans, np.int32), dms, nout)
+    rel, mx = _errs(out, ref)
+    print("tc auto segments", rel, mx)
+    assert rel < TC_REL_L2 and mx < TC_MAX_ABS, (rel, mx)
+
+
+def test_tc_fft_rows_beyond_one_launch():
+    """3900 DMs x 17 segments of 65536 points: more inverse-transform rows
+    than one launch's grid takes (65535), so the four-step transforms run in
+    launches of whole DMs. Rows at the start, middle and end of the DM list
+    against FP64 (device output; about 70 GB on the device)."""
+    import torch
+    nchans, nsamps = 64, 1_100_000
+    inp, params = _input(nchans, nsamps, 4)
+    dms = np.linspace(0, 10, 3900, dtype=np.float32)
+    p = _plan(params, dms, segmented=1, precision=1, segment_nfft=65536)
+    md = p.get_max_delay()
+    nout = nsamps - md
+    assert len(dms) * -(-nsamps // (65536 - md)) > 65535
+    d_in = torch.from_numpy(inp).cuda()
+    y = torch.empty((len(dms), nout), dtype=torch.float32, device="cuda")
+    p.set_timing(True)
+    p.execute(nsamps, d_in, 8, y, 32, dd.DEDISP_DEVICE_POINTERS)
+    torch.cuda.synchronize()
+    assert p.get_timing()["variant"] == 1
+    rows = np.array([0, 1950, 3899])
+    got = y[torch.as_tensor(rows, device="cuda")].double().cpu().numpy()
+    del y
+    torch.cuda.empty_cache()
+    x = _oracle_x(inp, nsamps, params, 8)
+    ref = po.fdd_timeseries(x, _delays(params), np.ones(nchans, np.int32), dms[rows], nout)
+    rel, mx = _errs(got, ref)
     assert rel < TC_REL_L2 and mx < TC_MAX_ABS, (rel, mx)
