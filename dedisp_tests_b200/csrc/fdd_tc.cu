@@ -623,6 +623,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
         // --- TMA producer ------------------------------------------------------
         if (lane == 0) {
             uint32_t g = 0;
+            uint32_t st = 0, st_phase = 0;  // B stage of chunk g (g % nst) and its use parity
             // this CTA's items: blockIdx.x first, then the next unclaimed item
             // of the list (longest first) each time one is done, published to
             // the other roles through the two-slot ring
@@ -640,8 +641,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                 for (size_t kt = (size_t)w.k_begin * w.ntile; kt < (size_t)w.k_end * w.ntile && ok; ++kt) {
                     const size_t k = kt / (size_t)w.ntile;  // every tile of bin k reads bin k's B
                     for (int ch = 0; ch < nchunks; ++ch, ++g) {
-                        const uint32_t st = g % (uint32_t)nst;
-                        if (!mbar_wait(&bars->b_empty[st], ((g / nst) & 1u) ^ 1u, L.wait_ns)) { ok = false; break; }
+                        if (!mbar_wait(&bars->b_empty[st], st_phase ^ 1u, L.wait_ns)) { ok = false; break; }
                         mbar_expect_tx(&bars->b_full[st], 2u * F::ATOMS * atom_bytes);
                         uint8_t* dst = s_b + st * L.stage_bytes;
                         // coordinates: (kk, n, split, bin); atoms in the order
@@ -650,6 +650,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                             for (int sp = 0; sp < 2; ++sp)
                                 tma_load_4d(dst + (at * 2 + sp) * atom_bytes, bmap, &bars->b_full[st],
                                             ch * (2 * F::CH) + at * 64, 0, sp, (int)k);
+                        if (++st == (uint32_t)nst) {
+                            st = 0;
+                            st_phase ^= 1u;
+                        }
                     }
                 }
             }
@@ -662,7 +666,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
         // --- MMA issuer ----------------------------------------------------------
         if (lane == 0) {
             uint32_t g = 0;
+            uint32_t st = 0, st_phase = 0;   // B stage of chunk g (g % nst) and its use parity
+            uint32_t buf = 0, a_phase = 0;   // A buffer of chunk g (g % NBUF) and its use parity
             int bin_iter = 0;
+            const uint64_t desc_s0 = sw128_desc(smem_u32(s_b));  // descriptor of stage 0's first atom
             for (uint32_t j = 0; ok; ++j) {
                 const uint32_t slot = j & 1u;
                 if (!mbar_wait(&bars->item_full[slot], (j >> 1) & 1u, L.wait_ns)) { ok = false; break; }
@@ -671,7 +678,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                 if (it < 0) break;
                 const TcWork w = items[it];
                 const uint32_t npad = (uint32_t)descs[w.desc].npad;
-                const uint32_t atom_bytes = npad * 128u;
+                const uint32_t atom16 = npad * 8u;  // one atom (npad rows x 128 bytes) in descriptor units
                 const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((npad >> 3) << 17) |
                                        ((uint32_t)(TC_M >> 4) << 24);
                 const uint32_t idesc2 = (1u << 4) | (1u << 7) | (1u << 10) | (((2u * npad) >> 3) << 17) |
@@ -682,26 +689,28 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                     tc_fence_after();
                     const uint32_t dcol = tmem + (cb ? F::C1 : F::C0);
                     for (int ch = 0; ch < nchunks; ++ch, ++g) {
-                        const uint32_t buf = g % F::NBUF, st = g % (uint32_t)nst;
-                        if (!mbar_wait(&bars->a_full[buf], (g / F::NBUF) & 1u, L.wait_ns)) { ok = false; break; }
-                        if (!mbar_wait(&bars->b_full[st], (g / nst) & 1u, L.wait_ns)) { ok = false; break; }
+                        if (!mbar_wait(&bars->a_full[buf], a_phase, L.wait_ns)) { ok = false; break; }
+                        if (!mbar_wait(&bars->b_full[st], st_phase, L.wait_ns)) { ok = false; break; }
                         // expiry test: one more wait, on a barrier nothing arrives on
                         if (L.wait_test && g == 0 && !mbar_wait(&bars->never, 0u, L.wait_ns)) { ok = false; break; }
                         tc_fence_after();
                         const uint32_t acol = tmem + F::A_BASE + buf * F::A_COLS;
-                        const uint32_t bbase = smem_u32(s_b + st * L.stage_bytes);
+                        // descriptors by adding offsets (16-byte units) to the low
+                        // word: shared addresses stay below 2^18, so the 14-bit
+                        // address field never carries
+                        const uint64_t d0 = desc_s0 + (uint64_t)((st * L.stage_bytes) >> 4);
 #pragma unroll
                         for (int s = 0; s < F::KSTEPS; ++s) {
                             const uint32_t at = (uint32_t)s >> 2, sub = (uint32_t)s & 3u;
-                            const uint64_t bh = sw128_desc(bbase + (at * 2 + 0) * atom_bytes + sub * 32);
+                            const uint64_t bh = d0 + (uint64_t)(at * 2u * atom16 + sub * 2u);
                             const uint32_t ah = acol + s * 8, al = acol + F::CH + s * 8;
-                            const uint32_t first = (ch == 0 && s == 0) ? 0u : 1u;
+                            const uint32_t first = (s == 0 && ch == 0) ? 0u : 1u;
                             if constexpr (FUSED) {
                                 // [Bh | Bl]: the lo atom follows the hi atom (2 npad rows)
                                 mma_ts(dcol, ah, bh, idesc2, first);
                                 mma_ts(dcol, al, bh, idesc, 1u);
                             } else {
-                                const uint64_t bl = sw128_desc(bbase + (at * 2 + 1) * atom_bytes + sub * 32);
+                                const uint64_t bl = bh + (uint64_t)atom16;
                                 mma_ts(dcol, ah, bh, idesc, first);
                                 mma_ts(dcol, ah, bl, idesc, 1u);
                                 mma_ts(dcol, al, bh, idesc, 1u);
@@ -709,6 +718,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                         }
                         mma_commit(&bars->a_empty[buf]);
                         mma_commit(&bars->b_empty[st]);
+                        if (++buf == (uint32_t)F::NBUF) {
+                            buf = 0;
+                            a_phase ^= 1u;
+                        }
+                        if (++st == (uint32_t)nst) {
+                            st = 0;
+                            st_phase ^= 1u;
+                        }
                     }
                     if (!ok) break;
                     mma_commit(&bars->c_full[cb]);
