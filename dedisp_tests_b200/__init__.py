@@ -120,6 +120,7 @@ def lib() -> C.CDLL:
         "dedisp_b200_output_row_length": (_sz, [_vp, _sz]),
         "dedisp_b200_get_stage_times": (err, [_vp, C.POINTER(C.c_float), C.c_int]),
         "dedisp_b200_get_phasor_source": (err, [_vp, C.POINTER(C.c_int)]),
+        "dedisp_b200_get_tc_form": (err, [_vp, C.POINTER(C.c_int)]),
         "dedisp_b200_fdd_segment_length": (_sz, [_sz, _sz, _sz, _sz, C.c_int, _sz]),
         "dedisp_b200_set_wait_limit_ns": (err, [C.c_ulonglong]),
         "dedisp_b200_get_wait_limit_ns": (C.c_ulonglong, []),
@@ -284,6 +285,14 @@ class Plan:
         v = C.c_int()
         _check(lib().dedisp_b200_get_phasor_source(self._h, C.byref(v)))
         return self.PHASOR_SOURCES[v.value]
+
+    TC_FORMS = {-1: None, 0: "three", 1: "fused", 2: "deep", 3: "pair", 4: "pair-deep"}
+
+    def get_tc_form(self):
+        """FDD plans: MMA form of the last tensor-core MAC launch."""
+        v = C.c_int()
+        _check(lib().dedisp_b200_get_tc_form(self._h, C.byref(v)))
+        return self.TC_FORMS[v.value]
 
 
 class DedispPlan(Plan):

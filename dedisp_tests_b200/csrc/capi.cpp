@@ -353,6 +353,16 @@ dedisp_error dedisp_b200_get_phasor_source(dedisp_plan plan, int* source)
     return DEDISP_NO_ERROR;
 }
 
+dedisp_error dedisp_b200_get_tc_form(dedisp_plan plan, int* form)
+{
+    if (!plan) return DEDISP_INVALID_PLAN;
+    auto* g = dynamic_cast<dedisp::GPUPlan*>(plan->ptr.get());
+    if (!g) return DEDISP_INVALID_PLAN;
+    if (!form) return DEDISP_INVALID_POINTER;
+    *form = g->last_timing().tc_form;
+    return DEDISP_NO_ERROR;
+}
+
 dedisp_error dedisp_b200_last_error(char* msg, dedisp_size len)
 {
     if (msg && len) {

@@ -158,6 +158,7 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
     m.X.reserve(nchans * nseg * bin_pitch * sizeof(float2));
     int nact_pad = 0, npad = 0, tc_dmax = -1;
     bool tc_direct = false, tc_hybrid = false;
+    int tc_form = -1;
     const int seg_group = (int)std::min<size_t>(nseg, (size_t)kern::kTcMaxSeg);
     if (use_tc) {
         nact_pad = kern::tc_pad_channels(m.nact);
@@ -302,7 +303,7 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
                                         (int)nseg, st);
             ta.nseg = ns;
             ta.seg0 = (int)s0;
-            kern::launch_fdd_mac_tc(ta, m.B.get(), m.tcwork.get(), wb, st);
+            tc_form = kern::launch_fdd_mac_tc(ta, m.B.get(), m.tcwork.get(), wb, st);
             ++stats.launches;
         }
     } else if (m.nact > 0) {
@@ -363,6 +364,7 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
         stats.variant = use_tc ? 1 : 0;
     }
     stats.phasor = !use_tc ? -1 : tc_hybrid ? 2 : tc_dmax >= 0 ? 0 : tc_direct ? 3 : 1;
+    stats.tc_form = use_tc ? tc_form : -1;
 }
 
 }  // namespace detail

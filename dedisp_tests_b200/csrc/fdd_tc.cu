@@ -131,19 +131,31 @@ __device__ __forceinline__ uint64_t global_ns()
 }
 
 // Bounded wait for phase `parity` of barrier b; false if the limit expired.
+// CLUSTER: acquire at cluster scope (arrivals and stores from the other CTA
+// of a pair).
+template <bool CLUSTER = false>
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, uint64_t limit_ns)
 {
     const uint32_t addr = smem_u32(b);
     uint64_t t0 = 0;
     for (uint32_t i = 0; i < TC_WAIT_POLLS; ++i) {
         uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(addr), "r"(parity)
-            : "memory");
+        if constexpr (CLUSTER)
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}"
+                : "=r"(done)
+                : "r"(addr), "r"(parity)
+                : "memory");
+        else
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}"
+                : "=r"(done)
+                : "r"(addr), "r"(parity)
+                : "memory");
         if (done) return true;
         if ((i & 15u) == 15u) {
             const uint64_t t = global_ns();
@@ -156,9 +168,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, uint64_t
 
 // The same wait for a whole warp, with one outcome for all its lanes (the
 // tensor-memory loads and stores that follow are warp-collective).
+template <bool CLUSTER = false>
 __device__ __forceinline__ bool mbar_wait_warp(uint64_t* b, uint32_t parity, uint64_t limit_ns)
 {
-    const bool done = mbar_wait(b, parity, limit_ns);
+    const bool done = mbar_wait<CLUSTER>(b, parity, limit_ns);
     return __all_sync(0xFFFFFFFFu, done);
 }
 
@@ -190,6 +203,74 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar)
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                      smem_u32(bar))
                  : "memory");
+}
+
+// --- CTA pairs (cluster of 2, tcgen05 cta_group::2) -------------------------
+__device__ __forceinline__ uint32_t cluster_rank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// Shared::cluster address of this CTA's variable p in CTA `rank` of the cluster.
+__device__ __forceinline__ uint32_t cluster_addr(const void* p, uint32_t rank)
+{
+    uint32_t a;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_u32(p)), "r"(rank));
+    return a;
+}
+
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t addr)
+{
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(addr) : "memory");
+}
+
+__device__ __forceinline__ void st_cluster_s32(uint32_t addr, int v)
+{
+    asm volatile("st.shared::cluster.s32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void cluster_sync_all()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// M = 256 MMA over the pair (issued by the leader CTA): A rows 0-127 from
+// the leader's tensor memory, 128-255 from the peer's (same address); B
+// columns 0..N/2-1 from the leader's shared memory, the rest from the peer's
+// (same offset); each CTA's accumulator holds its 128 rows x N.
+__device__ __forceinline__ void mma_ts_pair(uint32_t tmem_d, uint32_t tmem_a, uint64_t desc_b, uint32_t idesc,
+                                            uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(desc_b), "r"(idesc), "r"(accumulate));
+}
+
+// Completion of the pair's MMAs issued so far, signalled on barrier `bar` (same
+// offset) in the CTAs of `mask`.
+__device__ __forceinline__ void mma_commit_pair(uint64_t* bar, uint16_t mask)
+{
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            smem_u32(bar)),
+        "h"(mask)
+        : "memory");
+}
+
+// Tile load into this CTA's shared memory whose completion counts on the
+// barrier at shared::cluster address `bar` (the leader's).
+__device__ __forceinline__ void tma_load_4d_pair(void* smem, const CUtensorMap* map, uint32_t bar, int c0, int c1,
+                                                 int c2, int c3)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5, %6}], [%2];" ::"r"(smem_u32(smem)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+        : "memory");
 }
 
 // 32 consecutive 32-bit columns of this thread's lane.
@@ -297,7 +378,11 @@ __device__ __forceinline__ uint2 split_bf16x2(float re, float im)
 // pipeline counters run on across items, so the hand-offs of consecutive
 // items overlap; each item's last accumulator is read out before the next
 // item starts. One plan's launch is the one-descriptor case.
-template <bool FUSED, bool DEEP>
+// PAIR: clusters of two CTAs (cta_group::2): DM tiles of 256 rows, the
+// leader's MMA thread issues M = 256 MMAs over both CTAs' tensor memory, each
+// CTA loads half of every B chunk and produces the phasors of its 128 DMs;
+// the leader claims the pair's items and publishes them to both CTAs.
+template <bool FUSED, bool DEEP, bool PAIR>
 __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_constant__ TcParams P)
 {
     using F = TcForm<FUSED, DEEP>;
@@ -325,8 +410,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
     uint2* s_sym = reinterpret_cast<uint2*>(s_delay + L.nact_pad);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if ((int)blockIdx.x >= nitems) return;  // whole CTA leaves before touching barriers
+    const uint32_t crank = PAIR ? cluster_rank() : 0u;  // 0: the pair's leader
+    const bool leader = crank == 0u;
+    const int units = PAIR ? (int)(gridDim.x >> 1) : (int)gridDim.x;  // CTAs or pairs
+    const int unit = PAIR ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
+    if (unit >= nitems) return;  // whole CTA (pair) leaves before touching barriers
     const int nchunks = L.nact_pad / F::CH;
+    constexpr int TILE_M = PAIR ? 2 * TC_M : TC_M;  // DMs per tile
+    const int row_off = (int)crank * TC_M;         // this CTA's rows within a tile
+    // arrival on the leader's barrier (this CTA's own without pairs)
+    auto arrive_leader = [&](uint64_t* b) {
+        if constexpr (PAIR) mbar_arrive_cluster(cluster_addr(b, 0));
+        else mbar_arrive(b);
+    };
 
     // --- set-up -------------------------------------------------------------
     for (int i = tid; i < L.nact_pad; i += blockDim.x) s_delay[i] = descs[0].delay_act[i];
@@ -343,30 +439,43 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
             mbar_init(&bars->b_full[i], 1);
             mbar_init(&bars->b_empty[i], 1);
         }
+        // one arrive per producer warp (of both CTAs of a pair, on the leader's)
+        constexpr uint32_t nprod = TC_PRODUCER_WARPS * (PAIR ? 2 : 1);
         for (int i = 0; i < F::NBUF; ++i) {
-            mbar_init(&bars->a_full[i], TC_PRODUCER_WARPS);   // one arrive per producer warp
+            mbar_init(&bars->a_full[i], nprod);
             mbar_init(&bars->a_empty[i], 1);
         }
         for (int i = 0; i < 2; ++i) {
             mbar_init(&bars->c_full[i], 1);
-            mbar_init(&bars->c_empty[i], TC_PRODUCER_WARPS);
+            mbar_init(&bars->c_empty[i], nprod);
         }
         mbar_init(&bars->drain, 1);
         mbar_init(&bars->never, 1);
         for (int i = 0; i < 2; ++i) {
             mbar_init(&bars->item_full[i], 1);
-            mbar_init(&bars->item_empty[i], TC_PRODUCER_WARPS + 1);
+            // readers of an item index: the producer warps and the MMA thread
+            // (pairs: also the peer's producer warps and TMA thread)
+            mbar_init(&bars->item_empty[i], PAIR ? 2 * (TC_PRODUCER_WARPS + 1) : TC_PRODUCER_WARPS + 1);
         }
         bars->abort_flag = 0u;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == TC_PRODUCER_WARPS + 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
-                         smem_u32(&bars->tmem_base)));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+        if constexpr (PAIR) {
+            // the same warp of both CTAs, the same destination offset
+            asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
+                             smem_u32(&bars->tmem_base)));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::);
+        } else {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
+                             smem_u32(&bars->tmem_base)));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+        }
     }
     tc_fence_before();
     __syncthreads();
+    // pairs: both CTAs' barriers are initialised before any remote arrival
+    if constexpr (PAIR) cluster_sync_all();
     tc_fence_after();
     const uint32_t tmem = bars->tmem_base;
     bool ok = true;
@@ -393,7 +502,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
             // or an abort was raised"), which also orders the table reloads
             // below after every producer's reads of the previous item
             const uint32_t slot = j & 1u;
-            const bool got = mbar_wait(&bars->item_full[slot], (j >> 1) & 1u, L.wait_ns);
+            const bool got = mbar_wait<PAIR>(&bars->item_full[slot], (j >> 1) & 1u, L.wait_ns);
             const int it = got ? *reinterpret_cast<volatile int*>(&bars->item[slot]) : -1;
             const uint32_t bad = (!got || *abort_flag) ? 1u : 0u;
             uint32_t fail;
@@ -407,7 +516,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                 : "memory");
             if (fail) { ok = false; break; }
             __syncwarp();
-            if (lane == 0) mbar_arrive(&bars->item_empty[slot]);
+            if (lane == 0) arrive_leader(&bars->item_empty[slot]);
             if (it < 0) break;
             const TcWork w = items[it];
             const TcMacArgs& a = descs[w.desc];  // read-only descriptor (L1)
@@ -433,7 +542,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
 
             auto epilogue = [&](int itr, size_t kk, int m) -> bool {
                 const uint32_t cb = (uint32_t)itr & 1u;
-                if (!mbar_wait_warp(&bars->c_full[cb], ((uint32_t)itr >> 1) & 1u, L.wait_ns)) return false;
+                if (!mbar_wait_warp<PAIR>(&bars->c_full[cb], ((uint32_t)itr >> 1) & 1u, L.wait_ns)) return false;
                 tc_fence_after();
                 const uint32_t ccol = cb ? F::C1 : F::C0;
                 const uint32_t half = FUSED ? (uint32_t)a.npad : 0u;  // fused: Ah Bl columns
@@ -480,7 +589,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                 }
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&bars->c_empty[cb]);
+                if (lane == 0) arrive_leader(&bars->c_empty[cb]);
                 return true;
             };
 
@@ -495,7 +604,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
             for (size_t k = w.k_begin; k <= w.k_end; ++k) {
                 const bool tail = k == w.k_end;
                 if (tail) {
-                    if (ok && bin_iter > first_iter) ok = epilogue(bin_iter - 1, k - 1, last_tile * TC_M + row);
+                    if (ok && bin_iter > first_iter) ok = epilogue(bin_iter - 1, k - 1, last_tile * TILE_M + row_off + row);
                     if (!ok) *abort_flag = 1u;
                     break;
                 }
@@ -522,7 +631,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                 }
                 for (int t = w.tile; t < w.tile + w.ntile; ++t) {
                 if (ok) {
-                    const int m = t * TC_M + row;
+                    const int m = t * TILE_M + row_off + row;
                     const float dm = a.dms[min(m, a.ndm - 1)];
                     for (int ch = 0; ch < nchunks; ++ch, ++g) {
                         const uint32_t buf = g % F::NBUF, use = g / F::NBUF;
@@ -593,7 +702,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                                 lo[i] = __byte_perm(t.y, 0u, sy.x) ^ sy.y;
                             }
                         }
-                        if (!mbar_wait_warp(&bars->a_empty[buf], (use & 1u) ^ 1u, L.wait_ns)) { ok = false; break; }
+                        if (!mbar_wait_warp<PAIR>(&bars->a_empty[buf], (use & 1u) ^ 1u, L.wait_ns)) { ok = false; break; }
                         tc_fence_after();
                         const uint32_t acol = F::A_BASE + buf * F::A_COLS;
                         if constexpr (FUSED) {
@@ -606,12 +715,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                         tmem_wait_st();
                         tc_fence_before();
                         __syncwarp();
-                        if (lane == 0) mbar_arrive(&bars->a_full[buf]);
+                        if (lane == 0) arrive_leader(&bars->a_full[buf]);
                     }
                 }
                 // the previous pair's read-out overlaps this pair's MMAs
                 if (ok && bin_iter > first_iter)
-                    ok = epilogue(bin_iter - 1, t > w.tile ? k : k - 1, (t > w.tile ? t - 1 : last_tile) * TC_M + row);
+                    ok = epilogue(bin_iter - 1, t > w.tile ? k : k - 1,
+                                  (t > w.tile ? t - 1 : last_tile) * TILE_M + row_off + row);
                 if (!ok) *abort_flag = 1u;  // the others stop at the next barrier
                 ++bin_iter;
                 }
@@ -629,27 +739,53 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
             // the other roles through the two-slot ring
             for (uint32_t j = 0; ok; ++j) {
                 const uint32_t slot = j & 1u;
-                int it = j == 0 ? (int)blockIdx.x : (int)gridDim.x + (int)atomicAdd(P.next_item, 1u);
-                if (it >= nitems) it = -1;
-                if (!mbar_wait(&bars->item_empty[slot], ((j >> 1) & 1u) ^ 1u, L.wait_ns)) { ok = false; break; }
-                bars->item[slot] = it;
-                mbar_arrive(&bars->item_full[slot]);
+                int it;
+                if (!PAIR || leader) {
+                    it = j == 0 ? unit : units + (int)atomicAdd(P.next_item, 1u);
+                    if (it >= nitems) it = -1;
+                    if (!mbar_wait<PAIR>(&bars->item_empty[slot], ((j >> 1) & 1u) ^ 1u, L.wait_ns)) { ok = false; break; }
+                    bars->item[slot] = it;
+                    mbar_arrive(&bars->item_full[slot]);
+                    if constexpr (PAIR) {
+                        // the peer's copy of the slot; the release of the remote
+                        // arrival orders the store before it
+                        st_cluster_s32(cluster_addr(&bars->item[slot], 1), it);
+                        mbar_arrive_cluster(cluster_addr(&bars->item_full[slot], 1));
+                    }
+                } else {
+                    // the peer: the index its leader published
+                    if (!mbar_wait<PAIR>(&bars->item_full[slot], (j >> 1) & 1u, L.wait_ns)) { ok = false; break; }
+                    it = *reinterpret_cast<volatile int*>(&bars->item[slot]);
+                    mbar_arrive_cluster(cluster_addr(&bars->item_empty[slot], 0));
+                }
                 if (it < 0) break;
                 const TcWork w = items[it];
                 const CUtensorMap* bmap = maps + w.desc;
-                const uint32_t atom_bytes = (uint32_t)descs[w.desc].npad * 128u;  // one 64-kk atom of one split
+                // B rows this CTA loads (pairs: its half of the MMA's N) and
+                // one 64-kk atom of one split of them
+                const uint32_t rows = (uint32_t)descs[w.desc].npad / (PAIR ? 2u : 1u);
+                const uint32_t atom_bytes = rows * 128u;
+                const int n0 = (int)(crank * rows);
                 for (size_t kt = (size_t)w.k_begin * w.ntile; kt < (size_t)w.k_end * w.ntile && ok; ++kt) {
                     const size_t k = kt / (size_t)w.ntile;  // every tile of bin k reads bin k's B
                     for (int ch = 0; ch < nchunks; ++ch, ++g) {
-                        if (!mbar_wait(&bars->b_empty[st], st_phase ^ 1u, L.wait_ns)) { ok = false; break; }
-                        mbar_expect_tx(&bars->b_full[st], 2u * F::ATOMS * atom_bytes);
+                        if (!mbar_wait<PAIR>(&bars->b_empty[st], st_phase ^ 1u, L.wait_ns)) { ok = false; break; }
+                        // the leader's barrier counts both halves of a pair's chunk
+                        if (!PAIR || leader)
+                            mbar_expect_tx(&bars->b_full[st], (PAIR ? 2u : 1u) * 2u * F::ATOMS * atom_bytes);
                         uint8_t* dst = s_b + st * L.stage_bytes;
                         // coordinates: (kk, n, split, bin); atoms in the order
                         // (atom, split), so each atom's hi and lo rows are adjacent
                         for (int at = 0; at < F::ATOMS; ++at)
-                            for (int sp = 0; sp < 2; ++sp)
-                                tma_load_4d(dst + (at * 2 + sp) * atom_bytes, bmap, &bars->b_full[st],
-                                            ch * (2 * F::CH) + at * 64, 0, sp, (int)k);
+                            for (int sp = 0; sp < 2; ++sp) {
+                                if constexpr (PAIR)
+                                    tma_load_4d_pair(dst + (at * 2 + sp) * atom_bytes, bmap,
+                                                     cluster_addr(&bars->b_full[st], 0),
+                                                     ch * (2 * F::CH) + at * 64, n0, sp, (int)k);
+                                else
+                                    tma_load_4d(dst + (at * 2 + sp) * atom_bytes, bmap, &bars->b_full[st],
+                                                ch * (2 * F::CH) + at * 64, 0, sp, (int)k);
+                            }
                         if (++st == (uint32_t)nst) {
                             st = 0;
                             st_phase ^= 1u;
@@ -658,13 +794,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                 }
             }
             // do not leave while loads are in flight: wait for the last stages
-            const uint32_t issued = g;
-            for (uint32_t j = (issued > (uint32_t)nst ? issued - nst : 0); j < issued; ++j)
-                mbar_wait(&bars->b_full[j % nst], (j / nst) & 1u, L.wait_ns);
+            // (a pair's leader: both CTAs' loads count on its barriers; the
+            // peer stays resident until the pair's closing cluster barrier)
+            if (!PAIR || leader) {
+                const uint32_t issued = g;
+                for (uint32_t j = (issued > (uint32_t)nst ? issued - nst : 0); j < issued; ++j)
+                    mbar_wait<PAIR>(&bars->b_full[j % nst], (j / nst) & 1u, L.wait_ns);
+            }
         }
     } else {
-        // --- MMA issuer ----------------------------------------------------------
-        if (lane == 0) {
+        // --- MMA issuer (a pair's leader only) ----------------------------------
+        if (lane == 0 && (!PAIR || leader)) {
             uint32_t g = 0;
             uint32_t st = 0, st_phase = 0;   // B stage of chunk g (g % nst) and its use parity
             uint32_t buf = 0, a_phase = 0;   // A buffer of chunk g (g % NBUF) and its use parity
@@ -672,27 +812,28 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
             const uint64_t desc_s0 = sw128_desc(smem_u32(s_b));  // descriptor of stage 0's first atom
             for (uint32_t j = 0; ok; ++j) {
                 const uint32_t slot = j & 1u;
-                if (!mbar_wait(&bars->item_full[slot], (j >> 1) & 1u, L.wait_ns)) { ok = false; break; }
+                if (!mbar_wait<PAIR>(&bars->item_full[slot], (j >> 1) & 1u, L.wait_ns)) { ok = false; break; }
                 const int it = *reinterpret_cast<volatile int*>(&bars->item[slot]);
                 mbar_arrive(&bars->item_empty[slot]);
                 if (it < 0) break;
                 const TcWork w = items[it];
                 const uint32_t npad = (uint32_t)descs[w.desc].npad;
-                const uint32_t atom16 = npad * 8u;  // one atom (npad rows x 128 bytes) in descriptor units
+                // one atom (this CTA's B rows x 128 bytes) in descriptor units
+                const uint32_t atom16 = (npad / (PAIR ? 2u : 1u)) * 8u;
                 const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((npad >> 3) << 17) |
-                                       ((uint32_t)(TC_M >> 4) << 24);
+                                       ((uint32_t)(TILE_M >> 4) << 24);
                 const uint32_t idesc2 = (1u << 4) | (1u << 7) | (1u << 10) | (((2u * npad) >> 3) << 17) |
-                                        ((uint32_t)(TC_M >> 4) << 24);
+                                        ((uint32_t)(TILE_M >> 4) << 24);
                 for (size_t kt = (size_t)w.k_begin * w.ntile; kt < (size_t)w.k_end * w.ntile && ok; ++kt, ++bin_iter) {
                     const uint32_t cb = (uint32_t)bin_iter & 1u;
-                    if (!mbar_wait(&bars->c_empty[cb], (((uint32_t)bin_iter >> 1) & 1u) ^ 1u, L.wait_ns)) { ok = false; break; }
+                    if (!mbar_wait<PAIR>(&bars->c_empty[cb], (((uint32_t)bin_iter >> 1) & 1u) ^ 1u, L.wait_ns)) { ok = false; break; }
                     tc_fence_after();
                     const uint32_t dcol = tmem + (cb ? F::C1 : F::C0);
                     for (int ch = 0; ch < nchunks; ++ch, ++g) {
-                        if (!mbar_wait(&bars->a_full[buf], a_phase, L.wait_ns)) { ok = false; break; }
-                        if (!mbar_wait(&bars->b_full[st], st_phase, L.wait_ns)) { ok = false; break; }
+                        if (!mbar_wait<PAIR>(&bars->a_full[buf], a_phase, L.wait_ns)) { ok = false; break; }
+                        if (!mbar_wait<PAIR>(&bars->b_full[st], st_phase, L.wait_ns)) { ok = false; break; }
                         // expiry test: one more wait, on a barrier nothing arrives on
-                        if (L.wait_test && g == 0 && !mbar_wait(&bars->never, 0u, L.wait_ns)) { ok = false; break; }
+                        if (L.wait_test && g == 0 && !mbar_wait<PAIR>(&bars->never, 0u, L.wait_ns)) { ok = false; break; }
                         tc_fence_after();
                         const uint32_t acol = tmem + F::A_BASE + buf * F::A_COLS;
                         // descriptors by adding offsets (16-byte units) to the low
@@ -709,6 +850,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                                 // [Bh | Bl]: the lo atom follows the hi atom (2 npad rows)
                                 mma_ts(dcol, ah, bh, idesc2, first);
                                 mma_ts(dcol, al, bh, idesc, 1u);
+                            } else if constexpr (PAIR) {
+                                const uint64_t bl = bh + (uint64_t)atom16;
+                                mma_ts_pair(dcol, ah, bh, idesc, first);
+                                mma_ts_pair(dcol, ah, bl, idesc, 1u);
+                                mma_ts_pair(dcol, al, bh, idesc, 1u);
                             } else {
                                 const uint64_t bl = bh + (uint64_t)atom16;
                                 mma_ts(dcol, ah, bh, idesc, first);
@@ -716,8 +862,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                                 mma_ts(dcol, al, bh, idesc, 1u);
                             }
                         }
-                        mma_commit(&bars->a_empty[buf]);
-                        mma_commit(&bars->b_empty[st]);
+                        if constexpr (PAIR) {
+                            mma_commit_pair(&bars->a_empty[buf], 3);
+                            mma_commit_pair(&bars->b_empty[st], 3);
+                        } else {
+                            mma_commit(&bars->a_empty[buf]);
+                            mma_commit(&bars->b_empty[st]);
+                        }
                         if (++buf == (uint32_t)F::NBUF) {
                             buf = 0;
                             a_phase ^= 1u;
@@ -728,22 +879,28 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                         }
                     }
                     if (!ok) break;
-                    mma_commit(&bars->c_full[cb]);
+                    if constexpr (PAIR) mma_commit_pair(&bars->c_full[cb], 3);
+                    else mma_commit(&bars->c_full[cb]);
                 }
             }
             // all issued MMAs complete before the accumulator memory goes away
-            mma_commit(&bars->drain);
-            mbar_wait(&bars->drain, 0, L.wait_ns);
+            if constexpr (PAIR) mma_commit_pair(&bars->drain, 1);
+            else mma_commit(&bars->drain);
+            mbar_wait<PAIR>(&bars->drain, 0, L.wait_ns);
         }
     }
     if (!ok) atomicExch(L.err, 1u);
 
     tc_fence_before();
     __syncthreads();
+    // pairs: neither CTA leaves (nor frees tensor memory) while the other may
+    // still arrive on its barriers or the leader's MMAs read its memory
+    if constexpr (PAIR) cluster_sync_all();
     tc_fence_after();
     if (P.cta_ns && tid == 0) P.cta_ns[blockIdx.x] = global_ns() - t_start;
     if (warp == TC_PRODUCER_WARPS + 1) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
+        if constexpr (PAIR) asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, 512;" ::"r"(tmem));
+        else asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
     }
 }
 
@@ -983,7 +1140,7 @@ bool tc_direct_mode_fits(unsigned nfft, int nact_pad, int npad)
     return nfft % 256 == 0 && tc_smem_bytes(nfft, nact_pad, npad, -1, 2, true) <= TC_MAX_SMEM;
 }
 
-void tc_encode_map(void* map_out, const TcMacArgs& a, const void* B)
+void tc_encode_map(void* map_out, const TcMacArgs& a, const void* B, bool pair)
 {
     // Tensor map over Bsplit[bin][split][n][kk]: dims (kk, n, split, bin).
     CUtensorMap* map = static_cast<CUtensorMap*>(map_out);
@@ -993,7 +1150,8 @@ void tc_encode_map(void* map_out, const TcMacArgs& a, const void* B)
     const cuuint64_t dims[4] = {(cuuint64_t)(2 * a.nact_pad), nrow, 2, (cuuint64_t)a.nbins};
     const cuuint64_t strides[3] = {(cuuint64_t)(2 * a.nact_pad) * 2, (cuuint64_t)(2 * a.nact_pad) * 2 * nrow,
                                    (cuuint64_t)(2 * a.nact_pad) * 2 * nrow * 2};
-    const cuuint32_t box[4] = {64, (cuuint32_t)a.npad, 1, 1};
+    // pairs: each CTA loads half of the MMA's rows
+    const cuuint32_t box[4] = {64, (cuuint32_t)(pair ? a.npad / 2 : a.npad), 1, 1};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     const CUresult r = encode_fn()(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(B),
                                    dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -1002,10 +1160,28 @@ void tc_encode_map(void* map_out, const TcMacArgs& a, const void* B)
     if (r != CUDA_SUCCESS) DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "cuTensorMapEncodeTiled failed");
 }
 
-TcMacArgs tc_finish_args(const TcMacArgs& a)
+bool tc_pair_mode(const std::vector<TcMacArgs>& descs)
+{
+    // DEDISP_TC_PAIR=1 asks for pairs wherever they fit. Not the default:
+    // a pair issues one M = 256 MMA where two CTAs issue two M = 128 ones, at
+    // the same rate per SM, so only the halved B loads per CTA remain (config
+    // 2: 38.9 against 40.5 ms; one segment: 1129 against 1078 ms; per-beam
+    // config-3 plans 2.5 % slower)
+    const char* e = std::getenv("DEDISP_TC_PAIR");
+    if (!e || std::atoi(e) != 1) return false;
+    const char* form = std::getenv("DEDISP_TC_FORM");
+    if (form && std::atoi(form) == 1) return false;  // the fused form has no paired version
+    for (const TcMacArgs& a : descs)
+        if ((2 * a.nseg + 31) / 32 * 32 > 128) return false;
+    return tc_sm_count() >= 2;
+}
+
+TcMacArgs tc_finish_args(const TcMacArgs& a, bool pair)
 {
     TcMacArgs ka = a;
     if (ka.nseg_total <= 0) ka.nseg_total = ka.nseg;
+    // pairs: the M = 256 MMA takes N in multiples of 32 (16 rows per CTA)
+    if (pair) ka.npad = (std::max(ka.npad, 2 * ka.nseg) + 31) / 32 * 32;
     if (ka.nseg > kTcMaxSeg || ka.seg0 + ka.nseg > ka.nseg_total || ka.npad < 2 * ka.nseg ||
         ka.npad % 16 != 0 || ka.npad > 128 || ka.nact_pad % TC_CHUNK != 0 || ka.nfft % 256 != 0)
         DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "tensor-core MAC: bad shape");
@@ -1014,7 +1190,7 @@ TcMacArgs tc_finish_args(const TcMacArgs& a)
     return ka;
 }
 
-TcLayout tc_layout(const std::vector<TcMacArgs>& descs, unsigned* err)
+TcLayout tc_layout(const std::vector<TcMacArgs>& descs, unsigned* err, bool pair)
 {
     if (descs.empty()) DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "tensor-core MAC: no descriptors");
     TcLayout L{};
@@ -1032,11 +1208,13 @@ TcLayout tc_layout(const std::vector<TcMacArgs>& descs, unsigned* err)
     // form (which needs npad <= 80); measured slower on config 2 (49.5 vs
     // 45.6 ms per MAC), kept selectable for other shapes
     const char* form = std::getenv("DEDISP_TC_FORM");
-    L.fused = (form && std::atoi(form) == 1 && npad <= TC_FUSED_MAX_NPAD) ? 1 : 0;
+    L.pair = pair ? 1 : 0;
+    L.fused = (!pair && form && std::atoi(form) == 1 && npad <= TC_FUSED_MAX_NPAD) ? 1 : 0;
     // three A buffers when the accumulators fit in 64 columns (DEDISP_TC_FORM=2
     // keeps two, for comparison)
     L.deep = (!L.fused && npad <= TC_DEEP_MAX_NPAD && !(form && std::atoi(form) == 2)) ? 1 : 0;
-    L.stage_bytes = (L.fused ? 2u : 4u) * (uint32_t)npad * 128u;
+    // a stage: 2 splits x (CH / 64 atoms) x the CTA's B rows x 128 bytes
+    L.stage_bytes = (L.fused ? 2u : 4u) * (uint32_t)(pair ? npad / 2 : npad) * 128u;
     L.table_entries = (uint32_t)((table + 1) & ~(size_t)1);  // keep the float2 tables 16-byte aligned
     L.tw_hi_entries = (uint32_t)((hi + 1) & ~(size_t)1);
     L.nact_pad = descs[0].nact_pad;
@@ -1059,13 +1237,16 @@ TcLayout tc_layout(const std::vector<TcMacArgs>& descs, unsigned* err)
 std::vector<TcWork> tc_work_items(const std::vector<TcMacArgs>& descs, int ctas)
 {
     // An item is a bin range of one descriptor over all its DM tiles (the
-    // per-bin phasor table is built once for every tile).
-    ctas = std::max(ctas, 1);
+    // per-bin phasor table is built once for every tile). With CTA pairs the
+    // units are pairs and the tiles 256 DMs.
+    const bool pair = tc_pair_mode(descs);
+    const int tile_m = pair ? 2 * TC_M : TC_M;
+    ctas = std::max(pair ? ctas / 2 : ctas, 1);
     std::vector<TcWork> items;
     if (descs.size() == 1) {
         // one descriptor: at most `ctas` equal items, CTA b takes item b
         const TcMacArgs& a = descs[0];
-        const int ntiles = (a.ndm + TC_M - 1) / TC_M;
+        const int ntiles = (a.ndm + tile_m - 1) / tile_m;
         const size_t parts = std::max<size_t>(1, std::min<size_t>(a.nbins, (size_t)ctas));
         for (size_t p = 0; p < parts; ++p) {
             const size_t k0 = a.nbins * p / parts, k1 = a.nbins * (p + 1) / parts;
@@ -1078,8 +1259,8 @@ std::vector<TcWork> tc_work_items(const std::vector<TcMacArgs>& descs, int ctas)
     // columns)), listed longest first. CTA b starts with item b and then
     // claims the next unclaimed item whenever it finishes one, so the
     // estimate only orders the list and the tail is at most one small item.
-    auto cost_per_bin = [](const TcMacArgs& a) {
-        const double ntiles = (double)((a.ndm + TC_M - 1) / TC_M);
+    auto cost_per_bin = [&](const TcMacArgs& a) {
+        const double ntiles = (double)((a.ndm + tile_m - 1) / tile_m);
         const double phasor = a.dmax >= 0 ? (a.hybrid ? 1.8 : 1.0) : a.direct ? 2.5 : 1.3;
         return ntiles * (double)(a.nact_pad / TC_CHUNK) * (phasor + (double)a.npad / 48.0);
     };
@@ -1092,7 +1273,7 @@ std::vector<TcWork> tc_work_items(const std::vector<TcMacArgs>& descs, int ctas)
     for (size_t d = 0; d < descs.size(); ++d) {
         const TcMacArgs& a = descs[d];
         const double cb = cost_per_bin(a);
-        const int ntiles = (a.ndm + TC_M - 1) / TC_M;
+        const int ntiles = (a.ndm + tile_m - 1) / tile_m;
         const size_t n = std::max<size_t>(1, std::min<size_t>(a.nbins, (size_t)std::ceil(cb * (double)a.nbins / per)));
         for (size_t p = 0; p < n; ++p) {
             const size_t k0 = a.nbins * p / n, k1 = a.nbins * (p + 1) / n;
@@ -1120,18 +1301,20 @@ void tc_prepare_list(TcParams& P, const std::vector<TcMacArgs>& descs_in, const 
 {
     if (descs_in.empty() || descs_in.size() != Bs.size() || descs_in.size() > (size_t)kTcMaxDesc)
         DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "tensor-core MAC: 1 to 48 descriptors per launch");
+    const bool pair = tc_pair_mode(descs_in);
+    const int tile_m = pair ? 2 * TC_M : TC_M;
     std::vector<TcMacArgs> descs;
     for (size_t d = 0; d < descs_in.size(); ++d) {
-        descs.push_back(tc_finish_args(descs_in[d]));
+        descs.push_back(tc_finish_args(descs_in[d], pair));
         P.descs[d] = descs.back();
-        tc_encode_map(&P.maps[d], descs.back(), Bs[d]);
+        tc_encode_map(&P.maps[d], descs.back(), Bs[d], pair);
     }
     P.ndesc = (int)descs.size();
     if (tc_work_bytes(items.size()) > items_bytes)
         DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "tensor-core MAC: work buffer too small");
     for (const TcWork& w : items)
         if (w.desc < 0 || w.desc >= P.ndesc || w.k_end > descs[w.desc].nbins || w.k_begin > w.k_end ||
-            w.tile < 0 || w.ntile < 1 || (w.tile + w.ntile - 1) * 128 >= descs[w.desc].ndm)
+            w.tile < 0 || w.ntile < 1 || (w.tile + w.ntile - 1) * tile_m >= descs[w.desc].ndm)
             DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "tensor-core MAC: bad work item");
     // pageable source: the call returns once the bytes are staged
     if (!items.empty())
@@ -1140,29 +1323,60 @@ void tc_prepare_list(TcParams& P, const std::vector<TcMacArgs>& descs_in, const 
     P.nitems = (int)items.size();
     P.next_item = reinterpret_cast<unsigned*>(static_cast<uint8_t*>(d_items) +
                                               (items.size() * sizeof(TcWork) + 15) / 16 * 16);
-    P.layout = tc_layout(descs, err);
+    P.layout = tc_layout(descs, err, pair);
 }
 
 void launch_fdd_mac_tc_list(const TcParams& P, cudaStream_t s)
 {
     if (P.nitems <= 0) return;
-    auto kern = P.layout.fused  ? fdd_mac_tc_kernel<true, false>
-                : P.layout.deep ? fdd_mac_tc_kernel<false, true>
-                                : fdd_mac_tc_kernel<false, false>;
+    RT_CHECK(cudaMemsetAsync(P.next_item, 0, sizeof(unsigned), s));
+    if (P.layout.pair) {
+        auto kern = P.layout.deep ? fdd_mac_tc_kernel<false, true, true> : fdd_mac_tc_kernel<false, false, true>;
+        rt::raise_smem_limit(kern, P.layout.smem_bytes);
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.blockDim = dim3(TC_THREADS);
+        cfg.dynamicSmemBytes = P.layout.smem_bytes;
+        cfg.stream = s;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        // as many pairs as can be resident at once (one CTA per SM)
+        int pairs = tc_sm_count() / 2;
+        cfg.gridDim = dim3((unsigned)(2 * pairs));
+        int resident = 0;
+        if (cudaOccupancyMaxActiveClusters(&resident, kern, &cfg) == cudaSuccess && resident > 0)
+            pairs = std::min(pairs, resident);
+        else
+            (void)cudaGetLastError();
+        pairs = std::max(1, std::min(pairs, P.nitems));
+        cfg.gridDim = dim3((unsigned)(2 * pairs));
+        RT_CHECK(cudaLaunchKernelEx(&cfg, kern, P));
+        RT_CHECK(cudaGetLastError());
+        return;
+    }
+    auto kern = P.layout.fused  ? fdd_mac_tc_kernel<true, false, false>
+                : P.layout.deep ? fdd_mac_tc_kernel<false, true, false>
+                                : fdd_mac_tc_kernel<false, false, false>;
     rt::raise_smem_limit(kern, P.layout.smem_bytes);
     const int grid = std::min(P.nitems, tc_sm_count());
-    RT_CHECK(cudaMemsetAsync(P.next_item, 0, sizeof(unsigned), s));
     kern<<<grid, TC_THREADS, P.layout.smem_bytes, s>>>(P);
     RT_CHECK(cudaGetLastError());
 }
 
-void launch_fdd_mac_tc(const TcMacArgs& a, const void* B, void* d_items, size_t items_bytes, cudaStream_t s)
+int tc_form_code(const TcLayout& L) { return L.fused ? 1 : L.pair ? (L.deep ? 4 : 3) : L.deep ? 2 : 0; }
+
+int launch_fdd_mac_tc(const TcMacArgs& a, const void* B, void* d_items, size_t items_bytes, cudaStream_t s)
 {
-    const std::vector<TcMacArgs> descs{tc_finish_args(a)};
+    const std::vector<TcMacArgs> descs{tc_finish_args(a, false)};
     const std::vector<TcWork> items = tc_work_items(descs, tc_sm_count());
     std::unique_ptr<TcParams> P(new TcParams());
     tc_prepare_list(*P, descs, {B}, items, a.err, d_items, items_bytes, s);
     launch_fdd_mac_tc_list(*P, s);
+    return tc_form_code(P->layout);
 }
 
 }  // namespace kern

@@ -58,6 +58,7 @@ struct TcLayout {
     int stages;                // B pipeline depth
     int fused;                 // 1: fused MMA form (largest npad <= 80)
     int deep;                  // 1: three-MMA form with 3 A buffers (largest npad <= 64)
+    int pair;                  // 1: CTA pairs (cta_group::2, M = 256, npad a multiple of 32)
     uint32_t stage_bytes;      // per stage (largest npad)
     uint32_t table_entries;    // phasor table (largest)
     uint32_t tw_hi_entries;    // two-level twiddle table, hi part (largest nfft / 256)
@@ -143,7 +144,11 @@ void launch_fdd_prep_b(const float2* X, size_t bin_pitch, int nseg, size_t nbins
 
 // One plan's MAC (one descriptor). d_items: device scratch of at least
 // tc_work_bytes(SMs) bytes for its work items.
-void launch_fdd_mac_tc(const TcMacArgs& a, const void* B, void* d_items, size_t items_bytes, cudaStream_t s);
+// Returns the MMA form that ran (tc_form_code).
+int launch_fdd_mac_tc(const TcMacArgs& a, const void* B, void* d_items, size_t items_bytes, cudaStream_t s);
+// 0 three-MMA form, 1 fused, 2 three-MMA with 3 A buffers, 3 CTA pairs, 4 CTA
+// pairs with 3 A buffers.
+int tc_form_code(const TcLayout& L);
 
 // Up to kTcMaxDesc descriptors in one persistent launch: work items over all
 // of them (tc_work_items: one descriptor, at most `ctas` equal bin ranges;

@@ -31,6 +31,10 @@ struct ExecTiming {
      * per-bin delay table, 1 the quarter-wave table, 2 the table for small
      * delays with the rest computed, 3 computed from twiddle tables); -1 none */
     int phasor = -1;
+    /* FDD plans: MMA form of the last tensor-core MAC launch (0 three MMAs per
+     * K step, 1 fused, 2 three MMAs with 3 A buffers, 3 CTA pairs (M = 256),
+     * 4 CTA pairs with 3 A buffers); -1 none */
+    int tc_form = -1;
 };
 
 class GPUPlan : public Plan {

@@ -194,3 +194,17 @@ def test_fdd_batch_automatic_segment_lengths():
         rel, mx = _errs(y.cpu().numpy(), ref)
         assert rel < TOL[0] and mx < TOL[1], ("auto segments vs FP64", i, rel, mx)
     b.close()
+
+
+def test_fdd_batch_cta_pairs(monkeypatch):
+    """The batch's MAC on CTA pairs (DEDISP_TC_PAIR=1): every beam against
+    its FP64 oracle."""
+    monkeypatch.setenv("DEDISP_TC_PAIR", "1")
+    specs = [(40000, np.linspace(0, 60, 150)), (123457, np.linspace(0, 3000, 300)),
+             (30000, np.linspace(0, 10, 129))]
+    host = _beam_inputs(8, 31, specs)
+    got = _run_batch(8, host)
+    for i, ((packed, dms), g) in enumerate(zip(host, got)):
+        ref = _oracle(packed, 8, dms)
+        rel, mx = _errs(g, ref)
+        assert rel < TOL[0] and mx < TOL[1], ("pairs vs FP64", i, rel, mx)

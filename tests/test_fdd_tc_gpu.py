@@ -240,3 +240,47 @@ def test_tc_fft_rows_beyond_one_launch():
     ref = po.fdd_timeseries(x, _delays(params), np.ones(nchans, np.int32), dms[rows], nout)
     rel, mx = _errs(got, ref)
     assert rel < TC_REL_L2 and mx < TC_MAX_ABS, (rel, mx)
+
+
+@pytest.mark.parametrize("case", ["segmented", "many-segments", "whole-series", "table-capped"])
+def test_tc_cta_pairs(case, monkeypatch):
+    """DEDISP_TC_PAIR=1: the MAC on CTA pairs (tcgen05 cta_group::2, M = 256:
+    each CTA produces the phasors of its 128 DMs and loads half of every B
+    chunk; the leader issues the MMAs over both). Shapes: 200 DMs in one
+    256-DM tile (rows past the DM list masked), 36 segments (N = 72 -> 96),
+    one segment (N = 32, three A buffers), and the hybrid phasor source. Same
+    tolerance against FP64."""
+    monkeypatch.setenv("DEDISP_TC_PAIR", "1")
+    if case == "segmented":
+        nchans, nsamps = 96, 90000
+        inp, params = _input(nchans, nsamps, 3)
+        dms = np.linspace(0, 120, 200, dtype=np.float32)
+        p = _plan(params, dms, segmented=1, precision=1)
+    elif case == "many-segments":
+        nchans, nsamps = 64, 72000
+        inp, params = _input(nchans, nsamps, 11)
+        dms = np.linspace(0, 20, 300, dtype=np.float32)
+        p = _plan(params, dms, segmented=1, precision=1, segment_nfft=2048)
+    elif case == "whole-series":
+        nchans, nsamps = 64, 12000
+        inp, params = _input(nchans, nsamps, 5)
+        dms = np.linspace(0, 60, 18, dtype=np.float32)
+        p = _plan(params, dms, segmented=0, precision=1)
+    else:
+        monkeypatch.setenv("DEDISP_TC_TABLE_CAP", "1024")
+        nchans, nsamps = 64, 40000
+        inp, params = _input(nchans, nsamps, 12)
+        dms = np.linspace(0, 3300, 40, dtype=np.float32)
+        p = _plan(params, dms, segmented=0, precision=1)
+    out = _run(p, nsamps, inp, 8, len(dms))
+    assert p.get_tc_form() in ("pair", "pair-deep"), p.get_tc_form()
+    x = _oracle_x(inp, nsamps, params, 8)
+    if case in ("whole-series", "table-capped"):
+        ref = po.fdd_spectrum(x, _delays(params), np.ones(nchans, np.int32), dms, out.shape[1])
+        rel, mx = _errs(out, ref)
+    else:
+        nout = nsamps - p.get_max_delay()
+        ref = po.fdd_timeseries(x, _delays(params), np.ones(nchans, np.int32), dms, nout)
+        rel, mx = _errs(out[:, :nout], ref)
+    print("tc pairs", case, p.get_tc_form(), rel, mx)
+    assert rel < TC_REL_L2 and mx < TC_MAX_ABS, (case, rel, mx)
