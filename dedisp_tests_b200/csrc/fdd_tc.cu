@@ -178,13 +178,23 @@ __device__ __forceinline__ bool mbar_wait_warp(uint64_t* b, uint32_t parity, uin
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
+// L2 policy for the B chunks: kept in L2 in preference to streaming data (a
+// bin's chunks are read again by each of its DM tiles).
+__device__ __forceinline__ uint64_t l2_evict_last_policy()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
 __device__ __forceinline__ void tma_load_4d(void* smem, const CUtensorMap* map, uint64_t* bar,
-                                            int c0, int c1, int c2, int c3)
+                                            int c0, int c1, int c2, int c3, uint64_t policy)
 {
     asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%3, %4, %5, %6}], [%2];" ::"r"(smem_u32(smem)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+        " [%0], [%1, {%3, %4, %5, %6}], [%2], %7;" ::"r"(smem_u32(smem)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
+        "l"(policy)
         : "memory");
 }
 
@@ -264,12 +274,12 @@ __device__ __forceinline__ void mma_commit_pair(uint64_t* bar, uint16_t mask)
 // Tile load into this CTA's shared memory whose completion counts on the
 // barrier at shared::cluster address `bar` (the leader's).
 __device__ __forceinline__ void tma_load_4d_pair(void* smem, const CUtensorMap* map, uint32_t bar, int c0, int c1,
-                                                 int c2, int c3)
+                                                 int c2, int c3, uint64_t policy)
 {
     asm volatile(
-        "cp.async.bulk.tensor.4d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%3, %4, %5, %6}], [%2];" ::"r"(smem_u32(smem)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+        "cp.async.bulk.tensor.4d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+        " [%0], [%1, {%3, %4, %5, %6}], [%2], %7;" ::"r"(smem_u32(smem)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "l"(policy)
         : "memory");
 }
 
@@ -584,7 +594,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                     if (mine) {
 #pragma unroll
                         for (int i = 0; i < 4; ++i)
-                            if (i < cnt) yrow[(size_t)(sb + i) * ystep] = make_float2(yr[i], yi[i]);
+                            if (i < cnt) __stcs(yrow + (size_t)(sb + i) * ystep, make_float2(yr[i], yi[i]));
                     }
                 }
                 tc_fence_before();
@@ -734,6 +744,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
         if (lane == 0) {
             uint32_t g = 0;
             uint32_t st = 0, st_phase = 0;  // B stage of chunk g (g % nst) and its use parity
+            const uint64_t b_policy = l2_evict_last_policy();
             // this CTA's items: blockIdx.x first, then the next unclaimed item
             // of the list (longest first) each time one is done, published to
             // the other roles through the two-slot ring
@@ -781,10 +792,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                                 if constexpr (PAIR)
                                     tma_load_4d_pair(dst + (at * 2 + sp) * atom_bytes, bmap,
                                                      cluster_addr(&bars->b_full[st], 0),
-                                                     ch * (2 * F::CH) + at * 64, n0, sp, (int)k);
+                                                     ch * (2 * F::CH) + at * 64, n0, sp, (int)k, b_policy);
                                 else
                                     tma_load_4d(dst + (at * 2 + sp) * atom_bytes, bmap, &bars->b_full[st],
-                                                ch * (2 * F::CH) + at * 64, 0, sp, (int)k);
+                                                ch * (2 * F::CH) + at * 64, 0, sp, (int)k, b_policy);
                             }
                         if (++st == (uint32_t)nst) {
                             st = 0;
