@@ -71,7 +71,12 @@ __device__ __forceinline__ void dft_reg(float2 (&v)[R])
                 v[i] = a + b;
                 const float2 d = a - b;
                 const int t = (i & (span - 1)) * (16 / span);  // W_{2 span}^t' in units of W_32
-                v[j] = (t == 0) ? d : cmul(d, w32(t, INV));
+                // W_32^8 = -i (forward) or +i (inverse): a swap and a sign
+                // (a product with the constants would keep the multiplications
+                // by 0 and 1 under IEEE rules)
+                v[j] = (t == 0) ? d
+                     : (t == 8) ? (INV ? make_float2(-d.y, d.x) : make_float2(d.y, -d.x))
+                                : cmul(d, w32(t, INV));
             }
         }
     }
