@@ -1216,8 +1216,8 @@ TcLayout tc_layout(const std::vector<TcMacArgs>& descs, unsigned* err, bool pair
             DD_THROW_MSG(DEDISP_INTERNAL_GPU_ERROR, "tensor-core MAC: descriptors differ in channels");
     }
     // MMA form: the three-MMA form unless DEDISP_TC_FORM=1 asks for the fused
-    // form (which needs npad <= 80); measured slower on config 2 (49.5 vs
-    // 45.6 ms per MAC), kept selectable for other shapes
+    // form (which needs npad <= 80; its 32-channel chunks double the hand-offs
+    // per channel: config 2 41.6 against 40.5 ms), kept selectable
     const char* form = std::getenv("DEDISP_TC_FORM");
     L.pair = pair ? 1 : 0;
     L.fused = (!pair && form && std::atoi(form) == 1 && npad <= TC_FUSED_MAX_NPAD) ? 1 : 0;
