@@ -260,15 +260,20 @@ __device__ __forceinline__ void mma_ts_pair(uint32_t tmem_d, uint32_t tmem_a, ui
         "r"(tmem_a), "l"(desc_b), "r"(idesc), "r"(accumulate));
 }
 
-// Completion of the pair's MMAs issued so far, signalled on barrier `bar` (same
-// offset) in the CTAs of `mask`.
-__device__ __forceinline__ void mma_commit_pair(uint64_t* bar, uint16_t mask)
+// Completion of the pair's MMAs issued so far, signalled on the barrier at
+// shared::cluster address `bar` (this CTA's or the peer's).
+__device__ __forceinline__ void mma_commit_pair_to(uint32_t bar)
 {
-    asm volatile(
-        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
-            smem_u32(bar)),
-        "h"(mask)
-        : "memory");
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+// ... on barrier `b` of the leader (mask 1) or of both CTAs (mask 3), one
+// commit per CTA.
+__device__ __forceinline__ void mma_commit_pair(uint64_t* b, int mask)
+{
+    mma_commit_pair_to(cluster_addr(b, 0));
+    if (mask & 2) mma_commit_pair_to(cluster_addr(b, 1));
 }
 
 // Tile load into this CTA's shared memory whose completion counts on the

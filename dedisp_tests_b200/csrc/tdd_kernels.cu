@@ -209,7 +209,7 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 // Set by a kernel whose bounded wait expired (device-wide; read and cleared
 // by tdd_take_error).
 
-// mbarrier + bulk asynchronous copy (global -> shared, no multicast).
+// mbarrier + bulk asynchronous copy (global -> shared of this CTA only).
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count)
 {
