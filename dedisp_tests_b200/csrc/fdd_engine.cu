@@ -160,22 +160,11 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
     bool tc_direct = false, tc_hybrid = false;
     int tc_form = -1;
     const int seg_group = (int)std::min<size_t>(nseg, (size_t)kern::kTcMaxSeg);
-    if (use_tc) {
-        nact_pad = kern::tc_pad_channels(m.nact);
-        npad = kern::tc_pad_n(seg_group);
-        m.B.reserve(kern::tc_b_bytes(nbins, nact_pad, seg_group));
-        if (m.pad_version != v.version || m.delay_pad_n != nact_pad) {
-            std::vector<float> dp(m.delays_active);
-            dp.resize(nact_pad, 0.f);
-            m.delay_pad.reserve(dp.size() * 4);
-            RT_CHECK(cudaMemcpy(m.delay_pad.get(), dp.data(), dp.size() * 4, cudaMemcpyHostToDevice));
-            m.pad_version = v.version;
-            m.delay_pad_n = nact_pad;
-        }
+    if (use_tc || nseg == 1) {
         // Largest delay index over all DMs and active channels (same float
-        // operations as the kernel); the kernel builds a per-bin phasor table
-        // over 0..dmax when it fits shared memory, else it indexes the
-        // quarter-wave table (power-of-two lengths whose table fits).
+        // operations as the kernels): the tensor-core MAC and the one-segment
+        // FP32 MAC build a per-bin phasor table over 0..dmax when it fits
+        // shared memory.
         const int rnd = opt.round_delays ? 1 : 0;
         if (m.dmax_version != v.version || m.dmax_round != rnd) {
             long dmax = 0;
@@ -191,6 +180,19 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
             m.dmax = (ok && dmax < (1l << 30)) ? (int)dmax : -1;
             m.dmax_version = v.version;
             m.dmax_round = rnd;
+        }
+    }
+    if (use_tc) {
+        nact_pad = kern::tc_pad_channels(m.nact);
+        npad = kern::tc_pad_n(seg_group);
+        m.B.reserve(kern::tc_b_bytes(nbins, nact_pad, seg_group));
+        if (m.pad_version != v.version || m.delay_pad_n != nact_pad) {
+            std::vector<float> dp(m.delays_active);
+            dp.resize(nact_pad, 0.f);
+            m.delay_pad.reserve(dp.size() * 4);
+            RT_CHECK(cudaMemcpy(m.delay_pad.get(), dp.data(), dp.size() * 4, cudaMemcpyHostToDevice));
+            m.pad_version = v.version;
+            m.delay_pad_n = nact_pad;
         }
         // Phasor source: the per-bin delay table when it holds every delay,
         // else the cheapest of the quarter-wave table (power-of-two lengths),
@@ -319,7 +321,13 @@ void FddEngine::execute(const FddOptions& opt, const FddView& v, const FddCall& 
         a.nfft = (unsigned)g.nfft;
         a.round_delays = opt.round_delays ? 1 : 0;
         a.tw = tw;
-        kern::launch_fdd_mac_plain(a, st);
+        // one segment: the per-bin phasor table (each phasor feeds one
+        // product); several: the tiled kernel, which reuses each phasor
+        // across the segments
+        if (nseg == 1 && kern::fdd_mac_series_fits(m.dmax, (unsigned)g.nfft, m.nact))
+            kern::launch_fdd_mac_series(a, m.dmax, st);
+        else
+            kern::launch_fdd_mac_plain(a, st);
         stats.launches = 1;
     } else {
         RT_CHECK(cudaMemsetAsync(m.Yt.get(), 0, nbins * nseg * ndm * sizeof(float2), st));

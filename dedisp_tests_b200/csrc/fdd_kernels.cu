@@ -1184,6 +1184,88 @@ __global__ void __launch_bounds__(MAC_THREADS) mac_plain_kernel(MacArgs a, int b
     }
 }
 
+// FP32 MAC for one segment (the whole-series forms): each phasor feeds a
+// single product, so generating it is the work. Per bin the CTA builds the
+// phasors of every delay 0..dmax in shared memory (index k d mod N stepped
+// exactly by (k S) mod N, the same phasor() product as the tiled kernel), loads
+// the bin's spectra, and each thread accumulates SERIES_DPT DMs over all
+// channels, in the tiled kernel's channel order and FMA sequence (so the sums
+// are the same). Delays: dm * delay rounded by adding 2^23 (toward zero, or to
+// nearest even), exact for 0 <= dm * delay < 2^22 (dmax bounds it).
+constexpr int SERIES_THREADS = 256;
+constexpr int SERIES_DPT = 8;  // DMs per thread and pass
+
+__global__ void __launch_bounds__(SERIES_THREADS) mac_series_kernel(MacArgs a, int dmax, int bins_per_block)
+{
+    extern __shared__ __align__(16) float2 s_ser[];
+    const unsigned tab_n = ((unsigned)dmax + 2u) & ~1u;  // even counts keep the float2 arrays aligned
+    const unsigned nhi = a.nfft / 256;
+    float2* table = s_ser;
+    float2* lo = table + tab_n;
+    float2* hi = lo + 256;
+    float2* xs = hi + ((nhi + 1u) & ~1u);
+    float* dl = reinterpret_cast<float*>(xs + ((a.nact + 1) & ~1));
+    const int tid = threadIdx.x;
+    for (unsigned i = tid; i < 256; i += SERIES_THREADS) lo[i] = a.tw.lo[i];
+    for (unsigned i = tid; i < nhi; i += SERIES_THREADS) hi[i] = a.tw.hi[i];
+    for (int i = tid; i < a.nact; i += SERIES_THREADS) dl[i] = a.delay_act[i];
+    const bool rn = a.round_delays != 0;
+    const uint32_t dcap = (uint32_t)dmax;
+
+    const size_t kb0 = (size_t)blockIdx.x * bins_per_block;
+    const size_t kb1 = min(a.nbins, kb0 + bins_per_block);
+    for (size_t k = kb0; k < kb1; ++k) {
+        __syncthreads();  // the previous bin's table and spectra are no longer read
+        {
+            constexpr uint32_t S = SERIES_THREADS;
+            uint32_t idx = (uint32_t)(((uint64_t)k * (uint64_t)tid) % a.nfft);
+            const uint32_t step = (uint32_t)(((uint64_t)k * S) % a.nfft);
+            for (int d = tid; d <= dmax; d += S) {
+                table[d] = phasor(lo, hi, idx);
+                idx = (idx + step >= a.nfft) ? idx + step - a.nfft : idx + step;
+            }
+        }
+        for (int i = tid; i < a.nact; i += SERIES_THREADS) xs[i] = a.Xt[k * (size_t)a.nact + i];
+        __syncthreads();
+        for (int m0 = 0; m0 < a.ndm; m0 += SERIES_THREADS * SERIES_DPT) {
+            float dmv[SERIES_DPT];
+            float2 acc[SERIES_DPT];
+#pragma unroll
+            for (int q = 0; q < SERIES_DPT; ++q) {
+                dmv[q] = a.dms[min(m0 + tid + q * SERIES_THREADS, a.ndm - 1)];
+                acc[q] = make_float2(0.f, 0.f);
+            }
+#pragma unroll 2
+            for (int c = 0; c < a.nact; ++c) {
+                const float delay = dl[c];
+                const float2 bv = xs[c];
+#pragma unroll
+                for (int q = 0; q < SERIES_DPT; ++q) {
+                    const float x = __fmul_rn(dmv[q], delay);
+                    const float y = rn ? __fadd_rn(x, 8388608.0f) : __fadd_rz(x, 8388608.0f);
+                    const float2 av = table[min(__float_as_uint(y) - 0x4B000000u, dcap)];
+                    acc[q].x = fmaf(av.x, bv.x, acc[q].x);
+                    acc[q].x = fmaf(-av.y, bv.y, acc[q].x);
+                    acc[q].y = fmaf(av.x, bv.y, acc[q].y);
+                    acc[q].y = fmaf(av.y, bv.x, acc[q].y);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < SERIES_DPT; ++q) {
+                const int m = m0 + tid + q * SERIES_THREADS;
+                if (m < a.ndm) a.Yt[k * (size_t)a.ndm + m] = acc[q];
+            }
+        }
+    }
+}
+
+size_t series_smem_bytes(int dmax, unsigned nfft, int nact)
+{
+    return ((size_t)(((unsigned)dmax + 2u) & ~1u) + 256 + ((nfft / 256 + 1) & ~1u) + (size_t)((nact + 1) & ~1)) *
+               sizeof(float2) +
+           (size_t)nact * sizeof(float);
+}
+
 // CTAs of one wave of a persistent kernel: resident CTAs per SM x SMs,
 // at most `rows` (at least one).
 template <typename K>
@@ -1475,6 +1557,23 @@ void launch_fdd_spectrum_out(const float2* Yt, size_t ndm, size_t nspec, float* 
 {
     dim3 grid((unsigned)((nspec + 31) / 32), (unsigned)((ndm + 31) / 32));
     spectrum_out_kernel<<<grid, 256, 0, s>>>(Yt, ndm, nspec, out, out_stride);
+    RT_CHECK(cudaGetLastError());
+}
+
+bool fdd_mac_series_fits(int dmax, unsigned nfft, int nact)
+{
+    return dmax >= 0 && dmax < (1 << 22) && series_smem_bytes(dmax, nfft, nact) <= 200 * 1024;
+}
+
+void launch_fdd_mac_series(const MacArgs& a, int dmax, cudaStream_t s)
+{
+    if (a.nseg != 1 || !fdd_mac_series_fits(dmax, a.nfft, a.nact) || a.nfft % 256 != 0)
+        DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "one-segment MAC: shape out of range");
+    const size_t smem = series_smem_bytes(dmax, a.nfft, a.nact);
+    rt::raise_smem_limit(mac_series_kernel, smem);
+    const unsigned grid = persistent_grid(mac_series_kernel, SERIES_THREADS, smem, a.nbins);
+    const int per = (int)((a.nbins + grid - 1) / grid);
+    mac_series_kernel<<<(unsigned)((a.nbins + per - 1) / per), SERIES_THREADS, smem, s>>>(a, dmax, per);
     RT_CHECK(cudaGetLastError());
 }
 

@@ -122,6 +122,11 @@ struct MacArgs {
     TwiddleTable tw;
 };
 void launch_fdd_mac_plain(const MacArgs& a, cudaStream_t s);
+// One segment (whole series): per-bin phasor table over delays 0..dmax (the
+// largest delay index of the plan's DMs and channels), same sums as the
+// tiled kernel. fdd_mac_series_fits: dmax known and the tables fit.
+bool fdd_mac_series_fits(int dmax, unsigned nfft, int nact);
+void launch_fdd_mac_series(const MacArgs& a, int dmax, cudaStream_t s);
 
 }  // namespace kern
 }  // namespace dedisp
