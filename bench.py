@@ -373,31 +373,40 @@ def run_fdd(args, local, world, stream, max_over_ranks):
                 "contiguous rows; ours read overlapping segments (r2c) and write the stitched "
                 "series (c2r)"}
 
-    # (c) whole-series spectrum on tensor cores (N = 1064960)
-    p, d_out, ms, mac_ms, launches, stages = _fdd_run(
-        dd, cfg, d_in, 32, dm_list, local, stream, steps, 1, segmented=0, precision=1)
-    ms = max_over_ranks(ms)
-    md = p.get_max_delay()
-    nfft = p.output_row_length(cfg.nsamps)
-    units = 2048 * (cfg.nsamps - md)
+    # (c) whole-series spectrum (N = 1064960; the fork's default output): the
+    # default FP32 form (one-segment MAC) and the tensor-core form
     wrows = np.array([3, 1500])
     x_full = np.ascontiguousarray((h_in * scale).T)
-    spec_ref = po.fdd_spectrum(x_full, delays, np.ones(cfg.nchans, np.int32), dm_list[wrows], nfft)
+    spec_ref = None
+    for name, prec in (("fdd_fp32_whole_series_spectrum", 0), ("fdd_bf16x3_tc_whole_series_spectrum", 1)):
+        p, d_out, ms, mac_ms, launches, stages = _fdd_run(
+            dd, cfg, d_in, 32, dm_list, local, stream, steps, 1, segmented=0, precision=prec)
+        ms = max_over_ranks(ms)
+        md = p.get_max_delay()
+        nfft = p.output_row_length(cfg.nsamps)
+        units = 2048 * (cfg.nsamps - md)
+        if spec_ref is None:
+            spec_ref = po.fdd_spectrum(x_full, delays, np.ones(cfg.nchans, np.int32), dm_list[wrows], nfft)
+        got = d_out[torch.as_tensor(wrows, device=d_out.device)].double().cpu().numpy()
+        cmac = 2048.0 * cfg.nchans * (nfft // 2 + 1)
+        out[name] = {
+            "value": units * world / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "mac_ms": mac_ms,
+            "stage_ms": {k: round(v, 3) for k, v in stages.items()}, "nfft": nfft,
+            "rel_l2_vs_fp64": float(np.linalg.norm(got - spec_ref) / np.linalg.norm(spec_ref)),
+            "max_abs_vs_fp64": float(np.abs(got - spec_ref).max() / np.abs(spec_ref).max()),
+            "error_sample": f"DMs {wrows.tolist()}, all {nfft // 2} bins"}
+        if prec == 1:
+            out[name]["mac_TFLOPs"] = round(24 * cmac / (mac_ms * 1e-3) / 1e12, 2)
+            out[name]["note"] = ("one series: 2 of the MMA's 16 columns carry data, so the MAC is "
+                                 "bound by phasor generation, not the tensor pipe")
+            out[name]["cufft_r2c_ms"] = _time_cufft((cfg.nchans, nfft), False, nfft, dev, stream)
+        else:
+            out[name]["mac_TFLOPs"] = round(8 * cmac / (mac_ms * 1e-3) / 1e12, 2)
+            out[name]["note"] = ("one-segment FP32 MAC: per-bin phasor table, 8 real flops per "
+                                 "complex MAC on CUDA cores")
+        del d_out, p
+        torch.cuda.empty_cache()
     del x_full
-    got = d_out[torch.as_tensor(wrows, device=d_out.device)].double().cpu().numpy()
-    cmac = 2048.0 * cfg.nchans * (nfft // 2 + 1)
-    out["fdd_bf16x3_tc_whole_series_spectrum"] = {
-        "value": units * world / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "mac_ms": mac_ms,
-        "stage_ms": {k: round(v, 3) for k, v in stages.items()}, "nfft": nfft,
-        "rel_l2_vs_fp64": float(np.linalg.norm(got - spec_ref) / np.linalg.norm(spec_ref)),
-        "max_abs_vs_fp64": float(np.abs(got - spec_ref).max() / np.abs(spec_ref).max()),
-        "error_sample": f"DMs {wrows.tolist()}, all {nfft // 2} bins",
-        "mac_TFLOPs": round(24 * cmac / (mac_ms * 1e-3) / 1e12, 2),
-        "note": "one series: 2 of the MMA's 16 columns carry data, so the MAC is bound by "
-                "phasor generation, not the tensor pipe",
-        "cufft_r2c_ms": _time_cufft((cfg.nchans, nfft), False, nfft, dev, stream)}
-    del d_out, p
-    torch.cuda.empty_cache()
 
     # (b) against the TDD plan: config-2 geometry with 8-bit samples
     cfg8 = dataclasses.replace(cfg, nbits=8, mean=127.5, sigma=24.0, float_input=False,
