@@ -290,3 +290,24 @@ def test_single_cta_fft_lengths(segment_nfft, nchans, nsamps, dm_max):
     ref = po.fdd_timeseries(x, _delays(params), np.ones(nchans, np.int32), dms, nout)
     rel, mx = _errs(out, ref)
     assert rel < FP32_REL_L2 and mx < FP32_MAX_ABS, (rel, mx)
+
+
+@pytest.mark.parametrize("dm_max", [4000.0, 9000.0])
+def test_whole_series_large_delays(dm_max):
+    """The FP32 whole-series MAC with max delays of about 14000 samples (the
+    one-segment kernel's per-bin table) and about 31000 (its table would not
+    fit shared memory: the tiled kernel), spectrum output, round-half-even
+    delays; FP32 tolerance against FP64."""
+    nchans, nsamps = 64, 60000
+    inp, params = _input(nchans, nsamps, 13, dt=64e-6)
+    dms = np.linspace(0, dm_max, 24, dtype=np.float32)
+    p = _plan(params, dms, segmented=0, round_delays=True)
+    md = p.get_max_delay()
+    assert (md > 25000) == (dm_max > 5000), md
+    nfft = po.fdd_nfft_spectrum(nsamps, md)
+    out = np.zeros((len(dms), nfft), np.float32)
+    p.execute(nsamps, inp, 8, out, 32)
+    x = _oracle_x(inp, nsamps, params, 8)
+    ref = po.fdd_spectrum(x, _delays(params), np.ones(nchans, np.int32), dms, nfft, round_delays=True)
+    rel, mx = _errs(out, ref)
+    assert rel < FP32_REL_L2 and mx < FP32_MAX_ABS, (md, rel, mx)
