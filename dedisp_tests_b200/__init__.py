@@ -286,7 +286,7 @@ class Plan:
         _check(lib().dedisp_b200_get_phasor_source(self._h, C.byref(v)))
         return self.PHASOR_SOURCES[v.value]
 
-    TC_FORMS = {-1: None, 0: "three", 1: "fused", 2: "deep", 3: "pair", 4: "pair-deep"}
+    TC_FORMS = {-1: None, 0: "three", 1: "fused", 2: "deep", 3: "pair", 4: "pair-deep", 5: "fused-wide"}
 
     def get_tc_form(self):
         """FDD plans: MMA form of the last tensor-core MAC launch."""

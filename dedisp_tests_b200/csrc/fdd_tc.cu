@@ -69,14 +69,20 @@ constexpr size_t TC_MAX_SMEM = kTcMaxSmem;
 //     accumulators of 64 columns at 384 and 448: half again as many phasors
 //     in flight, which is what bounds the MAC when it waits on MMA
 //     completions rather than on the tensor pipe.
+//   fused wide (FUSED and DEEP, npad <= 32; the default there): the fused form at 64-channel
+//     chunks, 3 A buffers (0, 128, 256) and accumulators of 2 npad <= 64
+//     columns at 384 and 448: 16 MMAs per chunk instead of 24 (one thread
+//     issues an MMA about every 30 ns whatever its N, so narrow MMAs are
+//     bound by their count).
 template <bool FUSED, bool DEEP = false>
 struct TcForm {
-    static constexpr int CH = FUSED ? 32 : 64;            // channels per A chunk
+    static constexpr bool NARROW = FUSED && !DEEP;        // fused at 32-channel chunks
+    static constexpr int CH = NARROW ? 32 : 64;           // channels per A chunk
     static constexpr int PART_CH = CH / TC_PARTS;         // per producer thread
     static constexpr int NBUF = (FUSED || DEEP) ? 3 : 2;  // A buffers
     static constexpr uint32_t A_COLS = 2 * CH;            // hi CH + lo CH columns
-    static constexpr uint32_t A_BASE = FUSED ? 320 : 0;
-    static constexpr uint32_t C0 = FUSED ? 0 : DEEP ? 384 : 256, C1 = FUSED ? 160 : DEEP ? 448 : 384;
+    static constexpr uint32_t A_BASE = NARROW ? 320 : 0;
+    static constexpr uint32_t C0 = NARROW ? 0 : DEEP ? 384 : 256, C1 = NARROW ? 160 : DEEP ? 448 : 384;
     static constexpr int KSTEPS = CH / 8;                 // K16 steps per chunk
     static constexpr int ATOMS = CH / 32;                 // 64-kk TMA atoms per split
 };
@@ -720,7 +726,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fdd_mac_tc_kernel(const __grid_
                         if (!mbar_wait_warp<PAIR>(&bars->a_empty[buf], (use & 1u) ^ 1u, L.wait_ns)) { ok = false; break; }
                         tc_fence_after();
                         const uint32_t acol = F::A_BASE + buf * F::A_COLS;
-                        if constexpr (FUSED) {
+                        if constexpr (TC_PART_CH == 8) {
                             tmem_st8(tmem + lane_addr + acol + part * TC_PART_CH, hi);
                             tmem_st8(tmem + lane_addr + acol + F::CH + part * TC_PART_CH, lo);
                         } else {
@@ -1186,7 +1192,7 @@ bool tc_pair_mode(const std::vector<TcMacArgs>& descs)
     const char* e = std::getenv("DEDISP_TC_PAIR");
     if (!e || std::atoi(e) != 1) return false;
     const char* form = std::getenv("DEDISP_TC_FORM");
-    if (form && std::atoi(form) == 1) return false;  // the fused form has no paired version
+    if (form && (std::atoi(form) == 1 || std::atoi(form) == 3)) return false;  // no paired fused forms
     for (const TcMacArgs& a : descs)
         if ((2 * a.nseg + 31) / 32 * 32 > 128) return false;
     return tc_sm_count() >= 2;
@@ -1225,12 +1231,18 @@ TcLayout tc_layout(const std::vector<TcMacArgs>& descs, unsigned* err, bool pair
     // per channel: config 2 41.6 against 40.5 ms), kept selectable
     const char* form = std::getenv("DEDISP_TC_FORM");
     L.pair = pair ? 1 : 0;
-    L.fused = (!pair && form && std::atoi(form) == 1 && npad <= TC_FUSED_MAX_NPAD) ? 1 : 0;
+    const int fsel = form ? std::atoi(form) : 0;
+    // the fused form at 64-channel chunks wherever npad <= 32 (DEDISP_TC_FORM=1
+    // or 2 select the others): 16 MMAs per chunk instead of 24; measured
+    // 4491 -> 4101 ms of MAC over the first 12 config-3 beams (reference
+    // segments), 1077 -> 872 ms for the config-2 whole-series spectrum
+    const bool wide = !pair && (fsel == 0 || fsel == 3) && npad <= 32;
+    L.fused = (wide || (!pair && fsel == 1 && npad <= TC_FUSED_MAX_NPAD)) ? 1 : 0;
     // three A buffers when the accumulators fit in 64 columns (DEDISP_TC_FORM=2
-    // keeps two, for comparison)
-    L.deep = (!L.fused && npad <= TC_DEEP_MAX_NPAD && !(form && std::atoi(form) == 2)) ? 1 : 0;
+    // keeps two, for comparison); the wide fused form always has three
+    L.deep = (wide || (!L.fused && npad <= TC_DEEP_MAX_NPAD && fsel != 2)) ? 1 : 0;
     // a stage: 2 splits x (CH / 64 atoms) x the CTA's B rows x 128 bytes
-    L.stage_bytes = (L.fused ? 2u : 4u) * (uint32_t)(pair ? npad / 2 : npad) * 128u;
+    L.stage_bytes = ((L.fused && !L.deep) ? 2u : 4u) * (uint32_t)(pair ? npad / 2 : npad) * 128u;
     L.table_entries = (uint32_t)((table + 1) & ~(size_t)1);  // keep the float2 tables 16-byte aligned
     L.tw_hi_entries = (uint32_t)((hi + 1) & ~(size_t)1);
     L.nact_pad = descs[0].nact_pad;
@@ -1374,7 +1386,8 @@ void launch_fdd_mac_tc_list(const TcParams& P, cudaStream_t s)
         RT_CHECK(cudaGetLastError());
         return;
     }
-    auto kern = P.layout.fused  ? fdd_mac_tc_kernel<true, false, false>
+    auto kern = P.layout.fused  ? (P.layout.deep ? fdd_mac_tc_kernel<true, true, false>
+                                                 : fdd_mac_tc_kernel<true, false, false>)
                 : P.layout.deep ? fdd_mac_tc_kernel<false, true, false>
                                 : fdd_mac_tc_kernel<false, false, false>;
     rt::raise_smem_limit(kern, P.layout.smem_bytes);
@@ -1383,7 +1396,10 @@ void launch_fdd_mac_tc_list(const TcParams& P, cudaStream_t s)
     RT_CHECK(cudaGetLastError());
 }
 
-int tc_form_code(const TcLayout& L) { return L.fused ? 1 : L.pair ? (L.deep ? 4 : 3) : L.deep ? 2 : 0; }
+int tc_form_code(const TcLayout& L)
+{
+    return L.fused ? (L.deep ? 5 : 1) : L.pair ? (L.deep ? 4 : 3) : L.deep ? 2 : 0;
+}
 
 int launch_fdd_mac_tc(const TcMacArgs& a, const void* B, void* d_items, size_t items_bytes, cudaStream_t s)
 {

@@ -147,7 +147,7 @@ void launch_fdd_prep_b(const float2* X, size_t bin_pitch, int nseg, size_t nbins
 // Returns the MMA form that ran (tc_form_code).
 int launch_fdd_mac_tc(const TcMacArgs& a, const void* B, void* d_items, size_t items_bytes, cudaStream_t s);
 // 0 three-MMA form, 1 fused, 2 three-MMA with 3 A buffers, 3 CTA pairs, 4 CTA
-// pairs with 3 A buffers.
+// pairs with 3 A buffers, 5 fused at 64-channel chunks.
 int tc_form_code(const TcLayout& L);
 
 // Up to kTcMaxDesc descriptors in one persistent launch: work items over all

@@ -131,12 +131,13 @@ def test_tc_many_segments(nsamps):
     assert rel < TC_REL_L2 and mx < TC_MAX_ABS, (nseg, rel, mx)
 
 
-@pytest.mark.parametrize("form", ["1", "2"])
+@pytest.mark.parametrize("form", ["1", "2", "3"])
 def test_tc_selectable_mma_forms(form, monkeypatch):
     """The MMA forms chosen by DEDISP_TC_FORM (read at each launch): 1 the
     fused A_hi x [B_hi | B_lo] form, 2 the three-MMA form with two A buffers
-    (the default takes three when the accumulators fit 64 columns). Same
-    tolerance against FP64."""
+    (the default takes three when the accumulators fit 64 columns), 3 the
+    fused form at 64-channel chunks (npad <= 32; this shape has more segments,
+    so it takes the default form). Same tolerance against FP64."""
     monkeypatch.setenv("DEDISP_TC_FORM", form)
     nchans, nsamps = 96, 90000
     inp, params = _input(nchans, nsamps, 7)
@@ -283,4 +284,38 @@ def test_tc_cta_pairs(case, monkeypatch):
         ref = po.fdd_timeseries(x, _delays(params), np.ones(nchans, np.int32), dms, nout)
         rel, mx = _errs(out[:, :nout], ref)
     print("tc pairs", case, p.get_tc_form(), rel, mx)
+    assert rel < TC_REL_L2 and mx < TC_MAX_ABS, (case, rel, mx)
+
+
+@pytest.mark.parametrize("case", ["whole-series", "segmented"])
+def test_tc_fused_wide_form(case, monkeypatch):
+    """The fused MMAs (A_hi x [B_hi | B_lo], A_lo x B_hi) at 64-channel
+    chunks with three A buffers, the default for npad <= 32 (also selected by
+    DEDISP_TC_FORM=3): one segment
+    (whole series, spectrum) and 16 segments (time series, killmask). Same
+    tolerance against FP64."""
+    monkeypatch.setenv("DEDISP_TC_FORM", "3")
+    if case == "whole-series":
+        nchans, nsamps = 128, 30000
+        inp, params = _input(nchans, nsamps, 17)
+        dms = np.linspace(0, 80, 150, dtype=np.float32)
+        p = _plan(params, dms, segmented=0, precision=1)
+        km = np.ones(nchans, np.int32)
+    else:
+        nchans, nsamps = 96, 30000
+        inp, params = _input(nchans, nsamps, 19)
+        dms = np.linspace(0, 40, 140, dtype=np.float32)
+        km = np.ones(nchans, np.int32)
+        km[5::11] = 0
+        p = _plan(params, dms, km=km, segmented=1, precision=1, segment_nfft=2048)
+    out = _run(p, nsamps, inp, 8, len(dms))
+    assert p.get_tc_form() == "fused-wide", p.get_tc_form()
+    x = _oracle_x(inp, nsamps, params, 8)
+    if case == "whole-series":
+        ref = po.fdd_spectrum(x, _delays(params), km, dms, out.shape[1])
+        rel, mx = _errs(out, ref)
+    else:
+        nout = nsamps - p.get_max_delay()
+        ref = po.fdd_timeseries(x, _delays(params), km, dms, nout)
+        rel, mx = _errs(out[:, :nout], ref)
     assert rel < TC_REL_L2 and mx < TC_MAX_ABS, (case, rel, mx)
