@@ -587,8 +587,9 @@ def run_batched_fdd(args, local, world, stream, max_over_ranks, nbeams=12, nplai
     """Config 3, Fourier domain: the first `nbeams` of the 96 seeded beams
     (1536 ch, 8-bit, nsamp U[2^17, 2^20], DM max U[500, 3000], 1024-4096
     linear trials), segmented time series. Batched: FddBatch objects in waves
-    sized to the free memory, each one replayed CUDA graph with ONE persistent
-    tensor-core MAC launch over all its beams. Compared with one FDD plan
+    sized to the free memory, each one replayed CUDA graph with one persistent
+    tensor-core MAC launch over all its beams per MMA-form class (segment
+    groups of at most 32 MMA columns and wider ones). Compared with one FDD plan
     execute per beam on the same beams: tensor-core plans, and plain FP32
     plans on the first `nplain`. Both tensor-core forms run with the reference
     segment rule and with the automatic one (the segment length with the least
@@ -670,8 +671,7 @@ def run_batched_fdd(args, local, world, stream, max_over_ranks, nbeams=12, nplai
             b.sync(stream.cuda_stream)
         ms = max_over_ranks(e0.elapsed_time(e1))
         r = {"value": total * world / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
-             "mac_launches_per_step": len(waves), "waves": len(waves),
-             "beams_per_wave": [len(w) for w in waves]}
+             "waves": len(waves), "beams_per_wave": [len(w) for w in waves]}
         # error of the last wave's first beam (the pool holds the last wave's
         # rows) against float64 on two DMs x 2^16 samples
         bi = waves[-1][0]
@@ -690,6 +690,7 @@ def run_batched_fdd(args, local, world, stream, max_over_ranks, nbeams=12, nplai
         # stage split of one more step (direct launches with events, untimed above)
         split = {"prep_ms": 0.0, "mac_ms": 0.0, "post_ms": 0.0}
         balance = []
+        nlaunch = 0
         for b in batches:
             b.set_timing(True)
             b.execute(stream.cuda_stream, use_graph=False)
@@ -698,7 +699,9 @@ def run_batched_fdd(args, local, world, stream, max_over_ranks, nbeams=12, nplai
             b.set_timing(False)
             for k in split:
                 split[k] += t[k]
+            nlaunch += t["launches"]
             balance.append([round(bal["cta_max_ms"], 1), round(bal["cta_mean_ms"], 1)])
+        r["launches_per_step"] = nlaunch
         r["stage_ms"] = {k: round(v, 2) for k, v in split.items()}
         r["mac_cta_max_mean_ms"] = balance
         r["phasor_sources"] = bsources

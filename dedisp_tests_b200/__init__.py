@@ -518,8 +518,9 @@ class Batch:
 
 class FddBatch:
     """Many beams with one channel setup, dedispersed in the Fourier domain
-    (segmented time series, 3xBF16 tensor-core MAC) with ONE persistent MAC
-    launch over all of them, the whole sequence graph-captured. Beams are
+    (segmented time series, 3xBF16 tensor-core MAC) with one persistent MAC
+    launch over all of them per MMA-form class (at most two), the whole
+    sequence graph-captured. Beams are
     (device input, in_stride, nsamps, DM list, device output, out_stride);
     output rows hold nsamps - max_delay floats."""
 

@@ -316,14 +316,27 @@ void FddBatch::upload()
     }
     if (descs.size() > (size_t)kern::kTcMaxDesc)
         DD_THROW_MSG(DEDISP_UNKNOWN_ERROR, "a batch holds at most 48 beam segment groups");
-    m_params.reset(new kern::TcParams());
-    if (!descs.empty()) {
-        const std::vector<kern::TcWork> items = kern::tc_work_items(descs, kern::tc_sm_count());
-        const size_t ib = kern::tc_work_bytes(items.size());
-        m_items.reserve(ib);
-        kern::tc_prepare_list(*m_params, descs, Bs, items, m_err.get<unsigned>(), m_items.get(), ib, nullptr);
-        RT_CHECK(cudaDeviceSynchronize());
+    // Segment groups of at most 32 MMA columns take the wide fused form, the
+    // others the three-MMA form: a launch for each class present (a launch's
+    // form follows its widest descriptor).
+    std::vector<kern::TcMacArgs> cls_descs[2];
+    std::vector<const void*> cls_bs[2];
+    for (size_t d = 0; d < descs.size(); ++d) {
+        const int c = descs[d].npad <= 32 ? 0 : 1;
+        cls_descs[c].push_back(descs[d]);
+        cls_bs[c].push_back(Bs[d]);
     }
+    for (int c = 0; c < 2; ++c) {
+        m_params[c].reset();
+        if (cls_descs[c].empty()) continue;
+        m_params[c].reset(new kern::TcParams());
+        const std::vector<kern::TcWork> items = kern::tc_work_items(cls_descs[c], kern::tc_sm_count());
+        const size_t ib = kern::tc_work_bytes(items.size());
+        m_items[c].reserve(ib);
+        kern::tc_prepare_list(*m_params[c], cls_descs[c], cls_bs[c], items, m_err.get<unsigned>(), m_items[c].get(),
+                              ib, nullptr);
+    }
+    RT_CHECK(cudaDeviceSynchronize());
 }
 
 void FddBatch::enqueue(cudaStream_t s, bool timing)
@@ -361,11 +374,13 @@ void FddBatch::enqueue(cudaStream_t s, bool timing)
         }
     }
     if (timing) m_ev[1]->record(s);
-    if (m_nact > 0 && m_params && m_params->nitems > 0) {
-        if (timing) m_cta_ns.reserve((size_t)kern::tc_sm_count() * sizeof(unsigned long long));
-        m_params->cta_ns = timing ? m_cta_ns.get<unsigned long long>() : nullptr;
-        kern::launch_fdd_mac_tc_list(*m_params, s);
-        m_params->cta_ns = nullptr;
+    for (int c = 0; c < 2; ++c) {
+        kern::TcParams* P = m_params[c].get();
+        if (m_nact == 0 || !P || P->nitems <= 0) continue;
+        if (timing) m_cta_ns[c].reserve((size_t)kern::tc_sm_count() * sizeof(unsigned long long));
+        P->cta_ns = timing ? m_cta_ns[c].get<unsigned long long>() : nullptr;
+        kern::launch_fdd_mac_tc_list(*P, s);
+        P->cta_ns = nullptr;
         ++launches;
     }
     if (timing) m_ev[2]->record(s);
@@ -436,18 +451,22 @@ void FddBatch::execute(cudaStream_t stream, bool use_graph)
             RT_CHECK(cudaEventElapsedTime(&last_prep_ms, m_ev[0]->get(), m_ev[1]->get()));
             RT_CHECK(cudaEventElapsedTime(&last_mac_ms, m_ev[1]->get(), m_ev[2]->get()));
             RT_CHECK(cudaEventElapsedTime(&last_post_ms, m_ev[2]->get(), m_ev[3]->get()));
+            // the launches run one after the other: sums of their slowest
+            // and of their mean CTA times
             last_cta_max_ms = last_cta_mean_ms = 0.f;
-            if (m_nact > 0 && m_params && m_params->nitems > 0) {
-                const int n = std::min(m_params->nitems, kern::tc_sm_count());
+            for (int c = 0; c < 2; ++c) {
+                const kern::TcParams* P = m_params[c].get();
+                if (m_nact == 0 || !P || P->nitems <= 0) continue;
+                const int n = std::min(P->nitems, kern::tc_sm_count());
                 std::vector<unsigned long long> ns((size_t)n);
-                RT_CHECK(cudaMemcpy(ns.data(), m_cta_ns.get(), ns.size() * sizeof(ns[0]), cudaMemcpyDeviceToHost));
+                RT_CHECK(cudaMemcpy(ns.data(), m_cta_ns[c].get(), ns.size() * sizeof(ns[0]), cudaMemcpyDeviceToHost));
                 double sum = 0, mx = 0;
                 for (unsigned long long v : ns) {
                     sum += (double)v;
                     mx = std::max(mx, (double)v);
                 }
-                last_cta_max_ms = (float)(mx * 1e-6);
-                last_cta_mean_ms = (float)(sum / n * 1e-6);
+                last_cta_max_ms += (float)(mx * 1e-6);
+                last_cta_mean_ms += (float)(sum / n * 1e-6);
             }
         }
     }

@@ -7,9 +7,11 @@
 // (dm_count rows of nsamps - max_delay floats: the segmented overlap-save
 // time series, segment length from the reference doubling rule). One
 // execute() enqueues, per beam, the unpack, the forward real FFTs and the
-// split B operand of each segment group, then ONE persistent tensor-core
-// (3xBF16) MAC launch over a work list of (beam segment group, DM tile, bin
-// range) items of all beams, then per beam the DM-major transpose and the
+// split B operand of each segment group, then one persistent tensor-core
+// (3xBF16) MAC launch over a work list of (beam segment group, DM tiles, bin
+// range) items of all beams per MMA-form class (segment groups of at most 32
+// MMA columns take the wide fused form, wider ones the three-MMA form: at
+// most two launches), then per beam the DM-major transpose and the
 // inverse FFTs straight into the caller's rows. The sequence is captured once
 // into a CUDA graph and replayed. Results equal those of an FDDGPUPlan per
 // beam (segmented, tensor-core precision), which is what the tests check.
@@ -98,11 +100,14 @@ private:
     int m_nact = 0, m_nact_pad = 0;
     size_t m_ws_bytes = 0, m_shared_bytes = 0, m_scratch_off = 0, m_scratch_bytes = 0;
 
-    rt::DeviceBuffer m_chan, m_kmv, m_delay_pad, m_err, m_items, m_twp_lo, m_twp_hi, m_cta_ns;
+    rt::DeviceBuffer m_chan, m_kmv, m_delay_pad, m_err, m_twp_lo, m_twp_hi;
+    // MAC launches: one per MMA-form class of the beams' segment groups
+    // (at most 32 columns: the wide fused form; more: the three-MMA form)
+    rt::DeviceBuffer m_items[2], m_cta_ns[2];
     rt::DeviceBuffer m_own_ws;
     void* m_ext_ws = nullptr;
     size_t m_ext_ws_bytes = 0;
-    std::unique_ptr<kern::TcParams> m_params;
+    std::unique_ptr<kern::TcParams> m_params[2];
     cudaGraph_t m_graph = nullptr;
     cudaGraphExec_t m_exec = nullptr;
     int m_graph_launches = 0;
