@@ -33,7 +33,7 @@ struct ExecTiming {
     int phasor = -1;
     /* FDD plans: MMA form of the last tensor-core MAC launch (0 three MMAs per
      * K step, 1 fused, 2 three MMAs with 3 A buffers, 3 CTA pairs (M = 256),
-     * 4 CTA pairs with 3 A buffers); -1 none */
+     * 4 CTA pairs with 3 A buffers, 5 fused at 64-channel chunks); -1 none */
     int tc_form = -1;
 };
 

@@ -62,9 +62,10 @@ dedisp_error dedisp_b200_get_stage_times(dedisp_plan plan, float* stage_ms, int 
 dedisp_error dedisp_b200_get_phasor_source(dedisp_plan plan, int* source);
 
 /* FDD plans: MMA form of the last tensor-core MAC launch: 0 three MMAs per K
- * step, 1 fused (DEDISP_TC_FORM=1), 2 three MMAs with 3 A buffers, 3 CTA pairs
- * (cta_group::2, M = 256; DEDISP_TC_PAIR), 4 CTA pairs with 3 A buffers; -1
- * none ran. */
+ * step, 1 fused at 32-channel chunks (DEDISP_TC_FORM=1), 2 three MMAs with 3 A
+ * buffers, 3 CTA pairs (cta_group::2, M = 256; DEDISP_TC_PAIR), 4 CTA pairs
+ * with 3 A buffers, 5 fused at 64-channel chunks with 3 A buffers (the
+ * default for at most 32 MMA columns); -1 none ran. */
 dedisp_error dedisp_b200_get_tc_form(dedisp_plan plan, int* form);
 
 /* The C functions of dedisp.h report every failure inside the plan classes
