@@ -110,6 +110,14 @@ def profile_case(args):
         p.set_dm_list(cfg.dm_list)
         p.set_options(segmented=1, precision=1, segment_nfft=8192)
         nbits = 32
+    elif args.profile_case == "fdd-series":
+        # whole-series spectrum, FP32 one-segment MAC: config 2 at 2^18
+        # samples (N = 16384 x 17, 139264 bins)
+        cfg = sy.config2(nsamps=1 << 18)
+        p = dd.FDDGPUPlan(cfg.nchans, cfg.dt, cfg.f_top, cfg.df)
+        p.set_dm_list(cfg.dm_list)
+        p.set_options(segmented=0, precision=0)
+        nbits = 32
     else:
         cfg = sy.config2(nsamps=1 << 18)
         p = dd.FDDGPUPlan(cfg.nchans, cfg.dt, cfg.f_top, cfg.df)
