@@ -82,7 +82,8 @@ def parse():
                     help="run one small case for ncu and exit: tdd (the TDD workload with "
                          "2^17 samples), fdd / fdd-tc (config-2 geometry with 2^18 samples, FP32 "
                          "or tensor-core MAC), fdd-tc-n80 (the tensor-core MAC's config-2 shape "
-                         "per bin, 80 columns, on a few GB)")
+                         "per bin, 80 columns, on a few GB), fdd-series (config-2 geometry with "
+                         "2^18 samples, whole-series spectrum, one-segment FP32 MAC)")
     return ap.parse_args()
 
 
