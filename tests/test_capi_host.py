@@ -200,6 +200,29 @@ def test_batch_api_argument_checks():
     assert not h.value
 
 
+def test_fdd_extension_queries_reject_bad_handles():
+    """The FDD queries and batch settings added with the phasor sources, MMA
+    forms, segment lengths and MAC balance reject missing handles and
+    pointers without touching a GPU."""
+    L = dd.lib()
+    B = dd._batch_lib()
+    v = C.c_int(7)
+    assert L.dedisp_b200_get_phasor_source(None, C.byref(v)) == 4      # invalid plan
+    assert L.dedisp_b200_get_tc_form(None, C.byref(v)) == 4
+    assert L.dedisp_b200_get_stage_times(None, None, 0) == 4
+    assert B.dedisp_b200_fdd_batch_set_segment_nfft(None, 1) == 4
+    assert B.dedisp_b200_fdd_batch_phasor_source(None, 0) == -1
+    a, b = C.c_float(), C.c_float()
+    assert B.dedisp_b200_fdd_batch_get_mac_balance(None, C.byref(a), C.byref(b)) == 4
+    # a TDD plan has no FDD form; host-only plan objects need no GPU
+    p = dd.TDDPlan(64, 250e-6, 1581.8, -1.5625)
+    assert L.dedisp_b200_get_phasor_source(p._h, None) == 5            # invalid pointer
+    assert L.dedisp_b200_get_tc_form(p._h, None) == 5
+    assert L.dedisp_b200_get_phasor_source(p._h, C.byref(v)) == 0 and v.value == -1
+    assert L.dedisp_b200_get_tc_form(p._h, C.byref(v)) == 0 and v.value == -1
+    p.close()
+
+
 def test_tile_variant_counts():
     """8-bit input: five shapes on channel-major packed rows and four on
     quad-strided rows; 1/2/4-bit: the packed-row kernel and the four
