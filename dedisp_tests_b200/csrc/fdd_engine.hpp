@@ -46,7 +46,8 @@ FddGeometry fdd_geometry(const FddOptions& opt, size_t nsamps, size_t max_delay,
                          size_t nchans = 0);
 // Segmented FDD, tensor-core MAC: the power-of-two segment length (2^11..2^20,
 // above the max delay) with the least modelled device time for the DM count
-// and the active channels.
+// and the active channels; 0 if none exceeds the max delay (the reference
+// rule then applies).
 size_t fdd_auto_segment(size_t nsamps, size_t max_delay, size_t ndm, size_t nchans);
 
 class FddEngine {

@@ -42,8 +42,7 @@ size_t fdd_auto_segment(size_t nsamps, size_t max_delay, size_t ndm, size_t ncha
             best_n = n;
         }
     }
-    if (best_n == 0) DD_THROW_MSG(DEDISP_TOO_FEW_NSAMPS, "max delay above the longest segment");
-    return best_n;
+    return best_n;  // 0: no power of two up to 2^20 exceeds the max delay
 }
 
 FddGeometry fdd_geometry(const FddOptions& opt, size_t nsamps, size_t max_delay, size_t ndm, size_t nchans)
@@ -60,8 +59,11 @@ FddGeometry fdd_geometry(const FddOptions& opt, size_t nsamps, size_t max_delay,
         // (FDDGPUPlan.cpp:742,762-768); nsamp_good = nfft - max_delay.
         const bool autoseg = opt.segment_nfft == FddOptions::kSegmentAuto;
         size_t n = (opt.segment_nfft && !autoseg) ? opt.segment_nfft : 16384;
-        if (autoseg && ndm && nchans && opt.precision == FddPrecision::BF16x3) {
-            n = fdd_auto_segment(nsamps, max_delay, ndm, nchans);
+        const size_t na = (autoseg && ndm && nchans && opt.precision == FddPrecision::BF16x3)
+                              ? fdd_auto_segment(nsamps, max_delay, ndm, nchans)
+                              : 0;
+        if (na) {
+            n = na;
         } else if (!opt.segment_nfft || autoseg) {
             const float min_eff = 0.8f;
             while ((double)n * (1.0 - (double)min_eff) < (double)max_delay) n *= 2;

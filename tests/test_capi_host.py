@@ -183,6 +183,8 @@ def test_fdd_segment_length_rules():
     assert f(1000, 9000, 16, 64, 1, 8192) == 0            # segment shorter than the max delay
     # FP32 MAC: the automatic rule is the reference rule
     assert f(850907, 14271, 3642, 1536, 0, "auto") == 131072
+    # no power of two up to 2^20 exceeds the max delay: the reference rule
+    assert f(5_000_000, 2_000_000, 512, 256, 1, "auto") == f(5_000_000, 2_000_000, 512, 256, 1, 0) > 2_000_000
 
 
 def test_batch_api_argument_checks():
