@@ -887,6 +887,11 @@ def run_ours(args):
     reps = Replicas.from_env("nccl")
     world, rank, local = reps.world, reps.rank, reps.local
     barrier, max_over_ranks = reps.barrier, reps.max_over_ranks
+    if world > 1 and not (args.serve_only or args.batched_fdd_only or args.batched_only or args.fdd_only):
+        # several GPUs: the headline workload (replicas) only; the one-GPU
+        # sections (FDD forms, batches, serving, input widths) would hold
+        # every GPU for minutes without adding to the scaling figure
+        args.no_fdd = args.no_batched = args.no_serve = args.no_variants = True
 
     stream = torch.cuda.current_stream()
     if args.serve_only:
