@@ -47,7 +47,6 @@ constexpr int TC_CHUNK = 64;           // channel padding (a multiple of both fo
 constexpr int TC_MAX_STAGES = 6;       // B pipeline depth: as many as shared memory allows, 2..6
 constexpr int TC_PRODUCER_WARPS = 16;  // 4 per TMEM lane quadrant
 constexpr int TC_PARTS = TC_PRODUCER_WARPS / 4;  // producers sharing one DM row
-constexpr int TC_PART_CH = 64 / TC_PARTS;        // channels per producer per chunk
 constexpr int TC_THREADS = (TC_PRODUCER_WARPS + 2) * 32;
 // Bounded mbarrier waits: give up after a.wait_ns of global time (checked
 // every 16 polls) or TC_WAIT_POLLS polls, whichever comes first.
@@ -312,19 +311,6 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&v)[16
         "r"(v[15]));
 }
 
-__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32])
-{
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
-        "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
-        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
-        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
-        "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]),
-        "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]),
-        "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]),
-        "r"(v[29]), "r"(v[30]), "r"(v[31]));
-}
-
 __device__ __forceinline__ float tmem_ld1(uint32_t taddr)
 {
     uint32_t r;
@@ -347,16 +333,6 @@ __device__ __forceinline__ int tc_delay(float dm, float delay, int round_delays)
 {
     const float x = __fmul_rn(dm, delay);
     return round_delays ? (int)__float2uint_rn(x) : __float2int_rz(x);
-}
-
-// The same delay for 0 <= dm*delay < 2^22 without a conversion instruction:
-// adding 2^23 leaves the integer part (rounded toward zero, or to nearest
-// even) in the low mantissa bits.
-__device__ __forceinline__ int tc_delay_small(float dm, float delay, int round_delays)
-{
-    const float x = __fmul_rn(dm, delay);
-    const float y = round_delays ? __fadd_rn(x, 8388608.0f) : __fadd_rz(x, 8388608.0f);
-    return (int)(__float_as_uint(y) - 0x4B000000u);
 }
 
 // (re, im) -> packed bf16x2 hi parts (re low half) and lo parts
@@ -1088,12 +1064,6 @@ size_t tc_smem_bytes(unsigned nfft, int nact_pad, int npad, int dmax, int stages
     const size_t table = dmax >= 0 ? (size_t)dmax + 1 : direct ? 0 : (size_t)nfft / 4 + 1;
     const size_t hi = (dmax >= 0 || direct) ? (size_t)nfft / 256 : 0;
     return tc_layout_bytes(npad, table, hi, nact_pad, stages);
-}
-
-int tc_table_mode_dmax(int dmax, unsigned nfft, int nact_pad, int npad)
-{
-    if (dmax < 0) return -1;
-    return tc_smem_bytes(nfft, nact_pad, npad, dmax, 2, false) <= TC_MAX_SMEM ? dmax : -1;
 }
 
 int tc_table_capacity(int npad, size_t hi_entries, int nact_pad)

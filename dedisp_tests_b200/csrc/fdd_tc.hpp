@@ -93,8 +93,8 @@ struct alignas(64) TcParams {
 // accumulator columns); the engine runs segment groups.
 constexpr int kTcMaxSeg = 64;
 // Quarter-wave mode (the phasor table of exp(2 pi i r / N), r <= N/4) fits
-// shared memory and N is a power of two; otherwise the per-bin delay table
-// (tc_table_mode_dmax) must fit.
+// shared memory and N is a power of two (tc_choose_source weighs it against
+// the per-bin delay table and the computed phasors).
 bool tc_quarter_mode_fits(unsigned nfft, int nact_pad, int npad);
 int tc_pad_channels(int nact);
 int tc_pad_n(int nseg);
@@ -107,9 +107,6 @@ int tc_stages(unsigned nfft, int nact_pad, int npad, int dmax, bool direct);
 // Direct mode (every phasor from the two-level twiddle tables, any length
 // that is a multiple of 256) fits shared memory.
 bool tc_direct_mode_fits(unsigned nfft, int nact_pad, int npad);
-// dmax if the per-bin delay table (dmax + 1 phasors) fits shared memory,
-// else -1 (the kernel then indexes the quarter-wave table per phasor).
-int tc_table_mode_dmax(int dmax, unsigned nfft, int nact_pad, int npad);
 // Shared-memory bytes of a launch whose layout holds `table_entries` phasors
 // and `hi_entries` coarse twiddles (tc_layout's formula).
 size_t tc_layout_bytes(int npad, size_t table_entries, size_t hi_entries, int nact_pad, int stages);
